@@ -1,0 +1,101 @@
+"""ctypes binding of the C ABI in include/gc_lattice.h (libgc_b200.so).
+
+The library is built in-tree (general_code_b200/build.py). Loading it does not
+need a GPU; every entry point that touches the device returns
+GC_ERR_NODEVICE on a machine without an sm_100 GPU, which the Python layer
+raises as GCError. There is no CPU fallback.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+from pathlib import Path
+
+import numpy as np
+
+LIB_PATH = Path(__file__).resolve().parent / "libgc_b200.so"
+
+GC_OK = 0
+GC_ERR_ARG = 1
+GC_ERR_CUDA = 2
+GC_ERR_NOMEM = 3
+GC_ERR_NODEVICE = 4
+GC_ERR_IO = 5
+GC_ERR_STATE = 6
+GC_ERR_TIMEOUT = 7
+GC_ERR_BUSY = 8
+
+GC_PREC_FP64 = 0
+GC_PREC_MIXED = 1
+GC_LAYOUT_ROWMAJOR = 0
+GC_LAYOUT_EIGEN_COLMAJOR = 1
+
+ERROR_NAMES = {
+    GC_ERR_ARG: "GC_ERR_ARG", GC_ERR_CUDA: "GC_ERR_CUDA", GC_ERR_NOMEM: "GC_ERR_NOMEM",
+    GC_ERR_NODEVICE: "GC_ERR_NODEVICE", GC_ERR_IO: "GC_ERR_IO", GC_ERR_STATE: "GC_ERR_STATE",
+    GC_ERR_TIMEOUT: "GC_ERR_TIMEOUT", GC_ERR_BUSY: "GC_ERR_BUSY",
+}
+
+# Every symbol include/gc_lattice.h declares, with (restype, argtypes).
+_c_int, _c_dbl, _c_uint = ctypes.c_int, ctypes.c_double, ctypes.c_uint
+_p, _pint, _pdbl = ctypes.c_void_p, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_double)
+SIGNATURES = {
+    "gc_version": (_c_int, []),
+    "gc_last_error": (ctypes.c_char_p, [_p]),
+    "gc_lattice_create": (_c_int, [_pint, _c_int, _c_int, ctypes.POINTER(_p)]),
+    "gc_lattice_destroy": (_c_int, [_p]),
+    "gc_set_stream": (_c_int, [_p, _p]),
+    "gc_synchronize": (_c_int, [_p]),
+    "gc_upload": (_c_int, [_p, _pdbl, _c_int]),
+    "gc_download": (_c_int, [_p, _pdbl, _c_int]),
+    "gc_ape": (_c_int, [_p, _c_dbl, _c_int]),
+    "gc_hyp": (_c_int, [_p, _c_dbl, _c_dbl, _c_dbl, _c_int]),
+    "gc_wilson_onaxis": (_c_int, [_p, _c_int, _c_int, _c_int, _c_int, _pdbl]),
+    "gc_plaquette": (_c_int, [_p, _pdbl]),
+    "gc_generate": (_c_int, [_p, _c_dbl, _c_uint, _c_uint, _c_int]),
+    "gc_generate_host": (_c_int, [_pint, _c_int, _c_dbl, _c_uint, _c_uint, _c_int, _pdbl]),
+    "gc_job_device_bytes": (ctypes.c_longlong, [_pint, _c_int, _c_int, _c_int, _c_int]),
+}
+
+_lib = None
+
+
+class GCError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"{ERROR_NAMES.get(code, code)}: {msg}")
+        self.code = code
+
+
+def lib() -> ctypes.CDLL:
+    """Loads libgc_b200.so (raises if it has not been built)."""
+    global _lib
+    if _lib is None:
+        if not LIB_PATH.exists():
+            raise ImportError(
+                f"{LIB_PATH} is missing: build it with `python -m general_code_b200.build`")
+        l = ctypes.CDLL(str(LIB_PATH))
+        for name, (res, args) in SIGNATURES.items():
+            fn = getattr(l, name)
+            fn.restype = res
+            fn.argtypes = args
+        _lib = l
+    return _lib
+
+
+def check(rc: int, handle=None) -> None:
+    if rc != GC_OK:
+        msg = lib().gc_last_error(handle)
+        raise GCError(rc, msg.decode() if msg else "")
+
+
+def dims_arg(dims) -> ctypes.Array:
+    d = [int(v) for v in dims]
+    if len(d) != 4:
+        raise ValueError("dims must have 4 entries (Lx, Ly, Lz, Lt)")
+    return (ctypes.c_int * 4)(*d)
+
+
+def dbl_ptr(a: np.ndarray):
+    if a.dtype != np.float64 or not a.flags["C_CONTIGUOUS"]:
+        raise ValueError("expected a C-contiguous float64 array")
+    return a.ctypes.data_as(_pdbl)

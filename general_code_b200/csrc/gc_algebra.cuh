@@ -1,0 +1,284 @@
+// Group algebra for SU(2) (quaternion a0 + i a.sigma) and SU(3) (3x3 complex),
+// usable on host and device, templated on the arithmetic type (double/float).
+//
+// Semantics follow the reference's matrix types (lib/cpu/include/matrix.h):
+//   mul(A,B)      = A*B        su2 :93-98,  su3 :348-350
+//   mul_ad(A,B)   = A*B^dag    ("A ^ B")  su2 :99-104,  su3 :352-354
+//   mul_da(A,B)   = A^dag*B    ("A % B")  su2 :105-110, su3 :356-358
+//   conj_tr(A,B)  = Re Tr(A B^dag)/N  ("multiply_conj_tr") su2 :54-56, su3 :260-262
+//   proj(A)       su2 :74-77 (a/|a|); su3 :279-292 (6 x [Newton-Schulz step,
+//                 determinant phase fix])
+// The quaternion product formulas and the projection iteration are the
+// algebra itself and therefore have the same form as the reference's.
+#pragma once
+
+#include <cmath>
+
+#if defined(__CUDACC__)
+#define GC_HD __host__ __device__ __forceinline__
+#else
+#define GC_HD inline
+#endif
+
+namespace gc {
+
+template <class T> struct cx {
+  T re, im;
+};
+
+template <class T> GC_HD cx<T> cmul(cx<T> a, cx<T> b) {
+  return {a.re * b.re - a.im * b.im, a.re * b.im + a.im * b.re};
+}
+// conj(a) * b
+template <class T> GC_HD cx<T> cmulc(cx<T> a, cx<T> b) {
+  return {a.re * b.re + a.im * b.im, a.re * b.im - a.im * b.re};
+}
+// a * conj(b)
+template <class T> GC_HD cx<T> cmul_c(cx<T> a, cx<T> b) {
+  return {a.re * b.re + a.im * b.im, a.im * b.re - a.re * b.im};
+}
+template <class T> GC_HD cx<T> cadd(cx<T> a, cx<T> b) {
+  return {a.re + b.re, a.im + b.im};
+}
+template <class T> GC_HD cx<T> csub(cx<T> a, cx<T> b) {
+  return {a.re - b.re, a.im - b.im};
+}
+
+// ----------------------------------------------------------------- SU(2)
+template <class T> struct SU2 {
+  T a0, a1, a2, a3;
+  static constexpr int N = 2;
+};
+
+template <class T> GC_HD SU2<T> unit(SU2<T>) { return {T(1), T(0), T(0), T(0)}; }
+
+template <class T> GC_HD SU2<T> mul(const SU2<T> &A, const SU2<T> &B) {
+  return {A.a0 * B.a0 - A.a1 * B.a1 - A.a2 * B.a2 - A.a3 * B.a3,
+          A.a0 * B.a1 + B.a0 * A.a1 + A.a3 * B.a2 - A.a2 * B.a3,
+          A.a0 * B.a2 + B.a0 * A.a2 + A.a1 * B.a3 - A.a3 * B.a1,
+          A.a0 * B.a3 + B.a0 * A.a3 + A.a2 * B.a1 - A.a1 * B.a2};
+}
+template <class T> GC_HD SU2<T> mul_ad(const SU2<T> &A, const SU2<T> &B) {
+  return {A.a0 * B.a0 + A.a1 * B.a1 + A.a2 * B.a2 + A.a3 * B.a3,
+          -A.a0 * B.a1 + B.a0 * A.a1 - A.a3 * B.a2 + A.a2 * B.a3,
+          -A.a0 * B.a2 + B.a0 * A.a2 - A.a1 * B.a3 + A.a3 * B.a1,
+          -A.a0 * B.a3 + B.a0 * A.a3 - A.a2 * B.a1 + A.a1 * B.a2};
+}
+template <class T> GC_HD SU2<T> mul_da(const SU2<T> &A, const SU2<T> &B) {
+  return {A.a0 * B.a0 + A.a1 * B.a1 + A.a2 * B.a2 + A.a3 * B.a3,
+          A.a0 * B.a1 - B.a0 * A.a1 - A.a3 * B.a2 + A.a2 * B.a3,
+          A.a0 * B.a2 - B.a0 * A.a2 - A.a1 * B.a3 + A.a3 * B.a1,
+          A.a0 * B.a3 - B.a0 * A.a3 - A.a2 * B.a1 + A.a1 * B.a2};
+}
+template <class T> GC_HD SU2<T> scale(const SU2<T> &A, T s) {
+  return {A.a0 * s, A.a1 * s, A.a2 * s, A.a3 * s};
+}
+template <class T> GC_HD SU2<T> add(const SU2<T> &A, const SU2<T> &B) {
+  return {A.a0 + B.a0, A.a1 + B.a1, A.a2 + B.a2, A.a3 + B.a3};
+}
+template <class T> GC_HD T conj_tr(const SU2<T> &A, const SU2<T> &B) {
+  return A.a0 * B.a0 + A.a1 * B.a1 + A.a2 * B.a2 + A.a3 * B.a3;
+}
+template <class T> GC_HD T tr_real(const SU2<T> &A) { return A.a0; }
+template <class T> GC_HD SU2<T> adjoint(const SU2<T> &A) {
+  return {A.a0, -A.a1, -A.a2, -A.a3};
+}
+template <class T> GC_HD SU2<T> proj(const SU2<T> &A) {
+  T rho = sqrt(A.a0 * A.a0 + A.a1 * A.a1 + A.a2 * A.a2 + A.a3 * A.a3);
+  return {A.a0 / rho, A.a1 / rho, A.a2 / rho, A.a3 / rho};
+}
+
+// ----------------------------------------------------------------- SU(3)
+// Row-major: e[i][j] is the element in row i, column j.
+template <class T> struct SU3 {
+  cx<T> e[3][3];
+  static constexpr int N = 3;
+};
+
+template <class T> GC_HD SU3<T> unit(SU3<T>) {
+  SU3<T> U;
+#pragma unroll
+  for (int i = 0; i < 3; i++)
+#pragma unroll
+    for (int j = 0; j < 3; j++)
+      U.e[i][j] = {i == j ? T(1) : T(0), T(0)};
+  return U;
+}
+
+template <class T> GC_HD SU3<T> mul(const SU3<T> &A, const SU3<T> &B) {
+  SU3<T> C;
+#pragma unroll
+  for (int i = 0; i < 3; i++)
+#pragma unroll
+    for (int j = 0; j < 3; j++) {
+      cx<T> s = cmul(A.e[i][0], B.e[0][j]);
+      s = cadd(s, cmul(A.e[i][1], B.e[1][j]));
+      s = cadd(s, cmul(A.e[i][2], B.e[2][j]));
+      C.e[i][j] = s;
+    }
+  return C;
+}
+// A * B^dag : C_ij = sum_k A_ik conj(B_jk)
+template <class T> GC_HD SU3<T> mul_ad(const SU3<T> &A, const SU3<T> &B) {
+  SU3<T> C;
+#pragma unroll
+  for (int i = 0; i < 3; i++)
+#pragma unroll
+    for (int j = 0; j < 3; j++) {
+      cx<T> s = cmul_c(A.e[i][0], B.e[j][0]);
+      s = cadd(s, cmul_c(A.e[i][1], B.e[j][1]));
+      s = cadd(s, cmul_c(A.e[i][2], B.e[j][2]));
+      C.e[i][j] = s;
+    }
+  return C;
+}
+// A^dag * B : C_ij = sum_k conj(A_ki) B_kj
+template <class T> GC_HD SU3<T> mul_da(const SU3<T> &A, const SU3<T> &B) {
+  SU3<T> C;
+#pragma unroll
+  for (int i = 0; i < 3; i++)
+#pragma unroll
+    for (int j = 0; j < 3; j++) {
+      cx<T> s = cmulc(A.e[0][i], B.e[0][j]);
+      s = cadd(s, cmulc(A.e[1][i], B.e[1][j]));
+      s = cadd(s, cmulc(A.e[2][i], B.e[2][j]));
+      C.e[i][j] = s;
+    }
+  return C;
+}
+template <class T> GC_HD SU3<T> scale(const SU3<T> &A, T s) {
+  SU3<T> C;
+#pragma unroll
+  for (int i = 0; i < 3; i++)
+#pragma unroll
+    for (int j = 0; j < 3; j++)
+      C.e[i][j] = {A.e[i][j].re * s, A.e[i][j].im * s};
+  return C;
+}
+template <class T> GC_HD SU3<T> add(const SU3<T> &A, const SU3<T> &B) {
+  SU3<T> C;
+#pragma unroll
+  for (int i = 0; i < 3; i++)
+#pragma unroll
+    for (int j = 0; j < 3; j++)
+      C.e[i][j] = cadd(A.e[i][j], B.e[i][j]);
+  return C;
+}
+template <class T> GC_HD SU3<T> adjoint(const SU3<T> &A) {
+  SU3<T> C;
+#pragma unroll
+  for (int i = 0; i < 3; i++)
+#pragma unroll
+    for (int j = 0; j < 3; j++)
+      C.e[i][j] = {A.e[j][i].re, -A.e[j][i].im};
+  return C;
+}
+// Re Tr(A B^dag) / 3
+template <class T> GC_HD T conj_tr(const SU3<T> &A, const SU3<T> &B) {
+  T s = T(0);
+#pragma unroll
+  for (int i = 0; i < 3; i++)
+#pragma unroll
+    for (int j = 0; j < 3; j++)
+      s += A.e[i][j].re * B.e[i][j].re + A.e[i][j].im * B.e[i][j].im;
+  return s / T(3);
+}
+template <class T> GC_HD T tr_real(const SU3<T> &A) {
+  return (A.e[0][0].re + A.e[1][1].re + A.e[2][2].re) / T(3);
+}
+template <class T> GC_HD cx<T> det(const SU3<T> &m) {
+  // cofactor expansion along the first column
+  cx<T> c0 = csub(cmul(m.e[1][1], m.e[2][2]), cmul(m.e[2][1], m.e[1][2]));
+  cx<T> c1 = csub(cmul(m.e[0][1], m.e[2][2]), cmul(m.e[2][1], m.e[0][2]));
+  cx<T> c2 = csub(cmul(m.e[0][1], m.e[1][2]), cmul(m.e[1][1], m.e[0][2]));
+  cx<T> d = cmul(m.e[0][0], c0);
+  d = csub(d, cmul(m.e[1][0], c1));
+  d = cadd(d, cmul(m.e[2][0], c2));
+  return d;
+}
+
+// One Newton-Schulz step toward the unitary polar factor,
+// A <- 3/2 A - 1/2 (A A^dag) A, followed by the determinant phase fix
+// A <- (1 - (det A - 1)/3) A.  H = A A^dag is Hermitian: its upper triangle
+// is computed and mirrored (the mirrored entries equal the full product's).
+template <class T> GC_HD SU3<T> ns_step(const SU3<T> &A) {
+  cx<T> H[3][3];
+#pragma unroll
+  for (int i = 0; i < 3; i++) {
+    T d = A.e[i][0].re * A.e[i][0].re + A.e[i][0].im * A.e[i][0].im;
+    d += A.e[i][1].re * A.e[i][1].re + A.e[i][1].im * A.e[i][1].im;
+    d += A.e[i][2].re * A.e[i][2].re + A.e[i][2].im * A.e[i][2].im;
+    H[i][i] = {d, T(0)};
+#pragma unroll
+    for (int j = i + 1; j < 3; j++) {
+      cx<T> s = cmul_c(A.e[i][0], A.e[j][0]);
+      s = cadd(s, cmul_c(A.e[i][1], A.e[j][1]));
+      s = cadd(s, cmul_c(A.e[i][2], A.e[j][2]));
+      H[i][j] = s;
+      H[j][i] = {s.re, -s.im};
+    }
+  }
+  SU3<T> B;
+#pragma unroll
+  for (int i = 0; i < 3; i++)
+#pragma unroll
+    for (int j = 0; j < 3; j++) {
+      cx<T> s = cmul(H[i][0], A.e[0][j]);
+      s = cadd(s, cmul(H[i][1], A.e[1][j]));
+      s = cadd(s, cmul(H[i][2], A.e[2][j]));
+      B.e[i][j] = {T(1.5) * A.e[i][j].re - T(0.5) * s.re,
+                   T(1.5) * A.e[i][j].im - T(0.5) * s.im};
+    }
+  cx<T> dt = det(B);
+  const T third = T(1) / T(3);
+  cx<T> c = {T(1) - third * (dt.re - T(1)), -third * dt.im};
+#pragma unroll
+  for (int i = 0; i < 3; i++)
+#pragma unroll
+    for (int j = 0; j < 3; j++)
+      B.e[i][j] = cmul(c, B.e[i][j]);
+  return B;
+}
+
+template <class T> GC_HD SU3<T> proj(const SU3<T> &A) {
+  SU3<T> B = ns_step(A);
+#pragma unroll 1
+  for (int it = 0; it < 5; it++)
+    B = ns_step(B);
+  return B;
+}
+
+// Gram-Schmidt reunitarisation: rows 0 and 1 orthonormalised, row 2 =
+// conj(row0 x row1). Used by the configuration generator (not on the
+// reference path).
+template <class T> GC_HD SU3<T> reunitarize_gs(const SU3<T> &A) {
+  SU3<T> U;
+  T n0 = T(0);
+  for (int j = 0; j < 3; j++)
+    n0 += A.e[0][j].re * A.e[0][j].re + A.e[0][j].im * A.e[0][j].im;
+  n0 = T(1) / sqrt(n0);
+  for (int j = 0; j < 3; j++)
+    U.e[0][j] = {A.e[0][j].re * n0, A.e[0][j].im * n0};
+  // p = <u0, a1> = sum conj(u0_j) a1_j
+  cx<T> p = {T(0), T(0)};
+  for (int j = 0; j < 3; j++)
+    p = cadd(p, cmulc(U.e[0][j], A.e[1][j]));
+  cx<T> r[3];
+  T n1 = T(0);
+  for (int j = 0; j < 3; j++) {
+    r[j] = csub(A.e[1][j], cmul(p, U.e[0][j]));
+    n1 += r[j].re * r[j].re + r[j].im * r[j].im;
+  }
+  n1 = T(1) / sqrt(n1);
+  for (int j = 0; j < 3; j++)
+    U.e[1][j] = {r[j].re * n1, r[j].im * n1};
+  // row2 = conj(row0 x row1)
+  for (int j = 0; j < 3; j++) {
+    int a = (j + 1) % 3, b = (j + 2) % 3;
+    cx<T> c = csub(cmul(U.e[0][a], U.e[1][b]), cmul(U.e[0][b], U.e[1][a]));
+    U.e[2][j] = {c.re, -c.im};
+  }
+  return U;
+}
+
+} // namespace gc

@@ -1,0 +1,501 @@
+// C ABI (include/gc_lattice.h): device-resident lattice handles, uploads and
+// downloads in the reference's host layouts, and dispatch to the kernels by
+// group (SU(2)/SU(3)) and precision (FP64 / mixed).
+#include "../../include/gc_lattice.h"
+#include "gc_internal.cuh"
+#include "gc_kernels.h"
+
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+#include <string>
+
+namespace gc {
+int generate_host(const int dims[4], int nc, double eps, unsigned seed,
+                  unsigned cfg, int gauge, double *out);
+
+namespace {
+thread_local std::string g_launch_error;
+std::mutex g_global_err_mu;
+std::string g_global_err;
+} // namespace
+
+int launch_check(const char *what) {
+  cudaError_t e = cudaGetLastError();
+  if (e == cudaSuccess)
+    return GC_OK;
+  g_launch_error = std::string(what) + ": " + cudaGetErrorString(e);
+  return GC_ERR_CUDA;
+}
+
+} // namespace gc
+
+struct gc_lattice {
+  gc::Geom g{};
+  int nc = 0, prec = 0;
+  size_t field_bytes = 0;   // one direction's field
+  void *links = nullptr;    // 8 fields: two sets of 4 directions
+  gc::Fields4 cur{}, alt{}; // current / spare buffer of each direction
+  void *hyp = nullptr;      // 15 decorated-link fields (allocated on first HYP)
+  double *staging = nullptr; // host-layout staging buffer (device)
+  double *partials = nullptr;
+  size_t partials_cap = 0;  // doubles
+  double *dev_out = nullptr;
+  size_t dev_out_cap = 0;   // doubles
+  cudaStream_t own_stream = nullptr;
+  cudaStream_t stream = nullptr;
+  bool has_links = false;
+  std::string err;
+  std::mutex mu;
+};
+
+namespace {
+
+using namespace gc;
+
+int fail(gc_lattice *h, int code, const std::string &msg) {
+  if (h)
+    h->err = msg;
+  else {
+    std::lock_guard<std::mutex> lk(g_global_err_mu);
+    g_global_err = msg;
+  }
+  return code;
+}
+
+int cuda_fail(gc_lattice *h, const char *what, cudaError_t e) {
+  return fail(h, e == cudaErrorMemoryAllocation ? GC_ERR_NOMEM : GC_ERR_CUDA,
+              std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+int launch_fail(gc_lattice *h, int rc) {
+  if (rc == GC_OK)
+    return GC_OK;
+  return fail(h, rc, g_launch_error);
+}
+
+size_t bytes_per_link(int nc, int prec) {
+  if (nc == 3)
+    return prec == GC_PREC_FP64 ? 144 : 48;
+  return prec == GC_PREC_FP64 ? 32 : 16;
+}
+
+int check_device(gc_lattice *h) {
+  int n = 0;
+  cudaError_t e = cudaGetDeviceCount(&n);
+  if (e != cudaSuccess || n == 0)
+    return fail(h, GC_ERR_NODEVICE, "no CUDA device available");
+  int dev = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceProp p;
+  e = cudaGetDeviceProperties(&p, dev);
+  if (e != cudaSuccess)
+    return cuda_fail(h, "cudaGetDeviceProperties", e);
+  if (p.major != 10)
+    return fail(h, GC_ERR_NODEVICE,
+                "device " + std::string(p.name) +
+                    " is not sm_100 (this library is built for sm_100a only)");
+  return GC_OK;
+}
+
+int ensure_staging(gc_lattice *h) {
+  if (h->staging)
+    return GC_OK;
+  const size_t per = (h->nc == 3 ? 18 : 4) * sizeof(double);
+  cudaError_t e = cudaMalloc(&h->staging, per * 4 * (size_t)h->g.V);
+  if (e != cudaSuccess) {
+    h->staging = nullptr;
+    return cuda_fail(h, "cudaMalloc(staging)", e);
+  }
+  return GC_OK;
+}
+
+int ensure_partials(gc_lattice *h, size_t n) {
+  if (h->partials_cap >= n)
+    return GC_OK;
+  if (h->partials)
+    cudaFree(h->partials);
+  h->partials = nullptr;
+  h->partials_cap = 0;
+  cudaError_t e = cudaMalloc(&h->partials, n * sizeof(double));
+  if (e != cudaSuccess) {
+    h->partials = nullptr;
+    return cuda_fail(h, "cudaMalloc(partials)", e);
+  }
+  h->partials_cap = n;
+  return GC_OK;
+}
+
+int ensure_dev_out(gc_lattice *h, size_t n) {
+  if (h->dev_out_cap >= n)
+    return GC_OK;
+  if (h->dev_out)
+    cudaFree(h->dev_out);
+  h->dev_out = nullptr;
+  h->dev_out_cap = 0;
+  cudaError_t e = cudaMalloc(&h->dev_out, n * sizeof(double));
+  if (e != cudaSuccess) {
+    h->dev_out = nullptr;
+    return cuda_fail(h, "cudaMalloc(result)", e);
+  }
+  h->dev_out_cap = n;
+  return GC_OK;
+}
+
+int ensure_hyp(gc_lattice *h) {
+  if (h->hyp)
+    return GC_OK;
+  cudaError_t e = cudaMalloc(&h->hyp, 15 * h->field_bytes);
+  if (e != cudaSuccess) {
+    h->hyp = nullptr;
+    return cuda_fail(h, "cudaMalloc(HYP decorated links)", e);
+  }
+  return GC_OK;
+}
+
+#define GC_DISPATCH(h, FN, ...)                                                \
+  ((h)->nc == 3 ? ((h)->prec == GC_PREC_FP64                                   \
+                       ? FN<StoreF64SU3, double>(__VA_ARGS__)                  \
+                       : FN<StoreF32SU3, float>(__VA_ARGS__))                  \
+                : ((h)->prec == GC_PREC_FP64                                   \
+                       ? FN<StoreF64SU2, double>(__VA_ARGS__)                  \
+                       : FN<StoreF32SU2, float>(__VA_ARGS__)))
+
+int check_ready(gc_lattice *h) {
+  if (!h)
+    return fail(nullptr, GC_ERR_ARG, "null handle");
+  if (!h->has_links)
+    return fail(h, GC_ERR_STATE, "no links on the device yet (upload or generate first)");
+  return GC_OK;
+}
+
+} // namespace
+
+extern "C" {
+
+int gc_version(void) { return 100; }
+
+const char *gc_last_error(const gc_lattice *h) {
+  if (h)
+    return h->err.c_str();
+  std::lock_guard<std::mutex> lk(g_global_err_mu);
+  static thread_local std::string copy;
+  copy = g_global_err;
+  return copy.c_str();
+}
+
+int gc_lattice_create(const int dims[4], int nc, int precision,
+                      gc_lattice **out) {
+  if (!out || !dims)
+    return fail(nullptr, GC_ERR_ARG, "null argument");
+  *out = nullptr;
+  if (nc != 2 && nc != 3)
+    return fail(nullptr, GC_ERR_ARG, "nc must be 2 or 3");
+  if (precision != GC_PREC_FP64 && precision != GC_PREC_MIXED)
+    return fail(nullptr, GC_ERR_ARG, "precision must be GC_PREC_FP64 or GC_PREC_MIXED");
+  long long V = 1;
+  for (int d = 0; d < 4; d++) {
+    if (dims[d] < 2)
+      return fail(nullptr, GC_ERR_ARG, "every lattice extent must be >= 2");
+    V *= dims[d];
+  }
+  if (V * 4 * 18 >= (1LL << 31) * 8)
+    return fail(nullptr, GC_ERR_ARG, "lattice too large (4*V*18 must fit in 2^34)");
+  if (V >= (1LL << 30))
+    return fail(nullptr, GC_ERR_ARG, "lattice too large (V must be < 2^30)");
+  int rc = check_device(nullptr);
+  if (rc)
+    return rc;
+  gc_lattice *h = new gc_lattice();
+  h->nc = nc;
+  h->prec = precision;
+  for (int d = 0; d < 4; d++)
+    h->g.L[d] = dims[d];
+  h->g.stride[0] = 1;
+  h->g.stride[1] = dims[0];
+  h->g.stride[2] = dims[0] * dims[1];
+  h->g.stride[3] = dims[0] * dims[1] * dims[2];
+  h->g.V = (int)V;
+  h->g.Vs = dims[0] * dims[1] * dims[2];
+  // 256-byte aligned fields
+  h->field_bytes = ((bytes_per_link(nc, precision) * (size_t)V + 255) / 256) * 256;
+  cudaError_t e = cudaMalloc(&h->links, 8 * h->field_bytes);
+  if (e != cudaSuccess) {
+    delete h;
+    return cuda_fail(nullptr, "cudaMalloc(links)", e);
+  }
+  for (int d = 0; d < 4; d++) {
+    h->cur.f[d] = (char *)h->links + d * h->field_bytes;
+    h->alt.f[d] = (char *)h->links + (4 + d) * h->field_bytes;
+  }
+  e = cudaStreamCreateWithFlags(&h->own_stream, cudaStreamNonBlocking);
+  if (e != cudaSuccess) {
+    cudaFree(h->links);
+    delete h;
+    return cuda_fail(nullptr, "cudaStreamCreate", e);
+  }
+  h->stream = h->own_stream;
+  *out = h;
+  return GC_OK;
+}
+
+int gc_lattice_destroy(gc_lattice *h) {
+  if (!h)
+    return GC_OK;
+  {
+    std::lock_guard<std::mutex> lk(h->mu);
+    cudaStreamSynchronize(h->stream);
+    cudaFree(h->links);
+    if (h->hyp)
+      cudaFree(h->hyp);
+    if (h->staging)
+      cudaFree(h->staging);
+    if (h->partials)
+      cudaFree(h->partials);
+    if (h->dev_out)
+      cudaFree(h->dev_out);
+    if (h->own_stream)
+      cudaStreamDestroy(h->own_stream);
+  }
+  delete h;
+  return GC_OK;
+}
+
+int gc_set_stream(gc_lattice *h, void *stream) {
+  if (!h)
+    return fail(nullptr, GC_ERR_ARG, "null handle");
+  std::lock_guard<std::mutex> lk(h->mu);
+  h->stream = stream ? (cudaStream_t)stream : h->own_stream;
+  return GC_OK;
+}
+
+int gc_synchronize(gc_lattice *h) {
+  if (!h)
+    return fail(nullptr, GC_ERR_ARG, "null handle");
+  std::lock_guard<std::mutex> lk(h->mu);
+  cudaError_t e = cudaStreamSynchronize(h->stream);
+  if (e != cudaSuccess)
+    return cuda_fail(h, "cudaStreamSynchronize", e);
+  return GC_OK;
+}
+
+int gc_upload(gc_lattice *h, const double *host, int layout) {
+  if (!h || !host)
+    return fail(h, GC_ERR_ARG, "null argument");
+  if (layout != GC_LAYOUT_ROWMAJOR && layout != GC_LAYOUT_EIGEN_COLMAJOR)
+    return fail(h, GC_ERR_ARG, "unknown layout");
+  std::lock_guard<std::mutex> lk(h->mu);
+  int rc = ensure_staging(h);
+  if (rc)
+    return rc;
+  const size_t bytes = (h->nc == 3 ? 18 : 4) * sizeof(double) * 4 * (size_t)h->g.V;
+  cudaError_t e = cudaMemcpyAsync(h->staging, host, bytes, cudaMemcpyHostToDevice, h->stream);
+  if (e != cudaSuccess)
+    return cuda_fail(h, "cudaMemcpyAsync(upload)", e);
+  rc = launch_aos_to_soa(h->g, h->nc, h->prec, layout, h->staging, h->cur, h->stream);
+  if (rc)
+    return launch_fail(h, rc);
+  h->has_links = true;
+  return GC_OK;
+}
+
+int gc_download(gc_lattice *h, double *host, int layout) {
+  int rc = check_ready(h);
+  if (rc)
+    return rc;
+  if (!host)
+    return fail(h, GC_ERR_ARG, "null argument");
+  if (layout != GC_LAYOUT_ROWMAJOR && layout != GC_LAYOUT_EIGEN_COLMAJOR)
+    return fail(h, GC_ERR_ARG, "unknown layout");
+  std::lock_guard<std::mutex> lk(h->mu);
+  rc = ensure_staging(h);
+  if (rc)
+    return rc;
+  rc = launch_soa_to_aos(h->g, h->nc, h->prec, layout, h->cur, h->staging, h->stream);
+  if (rc)
+    return launch_fail(h, rc);
+  const size_t bytes = (h->nc == 3 ? 18 : 4) * sizeof(double) * 4 * (size_t)h->g.V;
+  cudaError_t e = cudaMemcpyAsync(host, h->staging, bytes, cudaMemcpyDeviceToHost, h->stream);
+  if (e != cudaSuccess)
+    return cuda_fail(h, "cudaMemcpyAsync(download)", e);
+  e = cudaStreamSynchronize(h->stream);
+  if (e != cudaSuccess)
+    return cuda_fail(h, "download synchronize", e);
+  return GC_OK;
+}
+
+int gc_ape(gc_lattice *h, double alpha, int steps) {
+  int rc = check_ready(h);
+  if (rc)
+    return rc;
+  if (steps < 0)
+    return fail(h, GC_ERR_ARG, "steps must be >= 0");
+  std::lock_guard<std::mutex> lk(h->mu);
+  for (int s = 0; s < steps; s++) {
+    Fields4 out = h->cur;
+    for (int d = 0; d < 3; d++)
+      out.f[d] = h->alt.f[d];
+    rc = GC_DISPATCH(h, launch_ape, h->g, h->cur, out, alpha, h->stream);
+    if (rc)
+      return launch_fail(h, rc);
+    for (int d = 0; d < 3; d++)
+      std::swap(h->cur.f[d], h->alt.f[d]);
+  }
+  return GC_OK;
+}
+
+int gc_hyp(gc_lattice *h, double a1, double a2, double a3, int steps) {
+  int rc = check_ready(h);
+  if (rc)
+    return rc;
+  if (steps < 0)
+    return fail(h, GC_ERR_ARG, "steps must be >= 0");
+  std::lock_guard<std::mutex> lk(h->mu);
+  if (steps == 0)
+    return GC_OK;
+  rc = ensure_hyp(h);
+  if (rc)
+    return rc;
+  HypL1 l1;
+  HypL2 l2;
+  for (int i = 0; i < 9; i++)
+    l1.f[i] = (char *)h->hyp + i * h->field_bytes;
+  for (int i = 0; i < 6; i++)
+    l2.f[i] = (char *)h->hyp + (9 + i) * h->field_bytes;
+  for (int s = 0; s < steps; s++) {
+    rc = GC_DISPATCH(h, launch_hyp, h->g, h->cur, l1, l2, h->alt.f[3], a1, a2, a3,
+                     h->stream);
+    if (rc)
+      return launch_fail(h, rc);
+    std::swap(h->cur.f[3], h->alt.f[3]);
+  }
+  return GC_OK;
+}
+
+int gc_wilson_onaxis(gc_lattice *h, int rmin, int rmax, int tmin, int tmax,
+                     double *out) {
+  int rc = check_ready(h);
+  if (rc)
+    return rc;
+  if (!out)
+    return fail(h, GC_ERR_ARG, "null output");
+  if (rmin < 1 || tmin < 1 || rmax < rmin || tmax < tmin)
+    return fail(h, GC_ERR_ARG, "need 1 <= r_min <= r_max and 1 <= time_min <= time_max");
+  std::lock_guard<std::mutex> lk(h->mu);
+  const int nr = rmax - rmin + 1, nt = tmax - tmin + 1;
+  // The per-warp accumulators live in shared memory; split R into chunks so
+  // that a block's accumulators stay small.
+  const int max_entries = 1024;
+  if (nt > max_entries)
+    return fail(h, GC_ERR_ARG, "time range too large (at most 1024 values of T)");
+  const int rchunk = std::max(1, max_entries / nt);
+  rc = ensure_dev_out(h, (size_t)nr * nt + (size_t)rchunk * nt);
+  if (rc)
+    return rc;
+  rc = ensure_partials(h, wilson_partials_count(h->g, std::min(rchunk, nr), nt, h->nc));
+  if (rc)
+    return rc;
+  double *chunk_out = h->dev_out + (size_t)nr * nt;
+  for (int r0 = rmin; r0 <= rmax; r0 += rchunk) {
+    const int r1 = std::min(rmax, r0 + rchunk - 1);
+    const int ncr = r1 - r0 + 1;
+    rc = GC_DISPATCH(h, launch_wilson, h->g, h->cur, r0, r1, tmin, tmax,
+                     h->partials, chunk_out, h->stream);
+    if (rc)
+      return launch_fail(h, rc);
+    // chunk_out[(T-tmin)*ncr + (R-r0)] -> dev_out[(T-tmin)*nr + (R-rmin)]
+    cudaError_t e = cudaMemcpy2DAsync(h->dev_out + (r0 - rmin), nr * sizeof(double),
+                                      chunk_out, ncr * sizeof(double),
+                                      ncr * sizeof(double), nt,
+                                      cudaMemcpyDeviceToDevice, h->stream);
+    if (e != cudaSuccess)
+      return cuda_fail(h, "cudaMemcpy2DAsync(wilson chunk)", e);
+  }
+  cudaError_t e = cudaMemcpyAsync(out, h->dev_out, (size_t)nr * nt * sizeof(double),
+                                  cudaMemcpyDeviceToHost, h->stream);
+  if (e != cudaSuccess)
+    return cuda_fail(h, "cudaMemcpyAsync(wilson result)", e);
+  e = cudaStreamSynchronize(h->stream);
+  if (e != cudaSuccess)
+    return cuda_fail(h, "wilson synchronize", e);
+  return GC_OK;
+}
+
+int gc_plaquette(gc_lattice *h, double *out) {
+  int rc = check_ready(h);
+  if (rc)
+    return rc;
+  if (!out)
+    return fail(h, GC_ERR_ARG, "null output");
+  std::lock_guard<std::mutex> lk(h->mu);
+  rc = ensure_dev_out(h, 1);
+  if (rc)
+    return rc;
+  rc = ensure_partials(h, plaquette_partials_count(h->g));
+  if (rc)
+    return rc;
+  rc = GC_DISPATCH(h, launch_plaquette, h->g, h->cur, h->partials, h->dev_out, h->stream);
+  if (rc)
+    return launch_fail(h, rc);
+  cudaError_t e = cudaMemcpyAsync(out, h->dev_out, sizeof(double),
+                                  cudaMemcpyDeviceToHost, h->stream);
+  if (e != cudaSuccess)
+    return cuda_fail(h, "cudaMemcpyAsync(plaquette)", e);
+  e = cudaStreamSynchronize(h->stream);
+  if (e != cudaSuccess)
+    return cuda_fail(h, "plaquette synchronize", e);
+  return GC_OK;
+}
+
+int gc_generate_host(const int dims[4], int nc, double eps, unsigned int seed,
+                     unsigned int config_index, int gauge, double *host) {
+  if (!dims || !host)
+    return fail(nullptr, GC_ERR_ARG, "null argument");
+  if (nc != 2 && nc != 3)
+    return fail(nullptr, GC_ERR_ARG, "nc must be 2 or 3");
+  for (int d = 0; d < 4; d++)
+    if (dims[d] < 2)
+      return fail(nullptr, GC_ERR_ARG, "every lattice extent must be >= 2");
+  return gc::generate_host(dims, nc, eps, seed, config_index, gauge, host);
+}
+
+int gc_generate(gc_lattice *h, double eps, unsigned int seed,
+                unsigned int config_index, int gauge) {
+  if (!h)
+    return fail(nullptr, GC_ERR_ARG, "null handle");
+  const size_t n = (size_t)(h->nc == 3 ? 18 : 4) * 4 * (size_t)h->g.V;
+  double *buf = nullptr;
+  cudaError_t e = cudaMallocHost(&buf, n * sizeof(double));
+  if (e != cudaSuccess)
+    return cuda_fail(h, "cudaMallocHost(generator)", e);
+  int rc = gc::generate_host(h->g.L, h->nc, eps, seed, config_index, gauge, buf);
+  if (rc == GC_OK) {
+    rc = gc_upload(h, buf, GC_LAYOUT_ROWMAJOR);
+    if (rc == GC_OK)
+      rc = gc_synchronize(h);
+  }
+  cudaFreeHost(buf);
+  return rc;
+}
+
+long long gc_job_device_bytes(const int dims[4], int nc, int precision,
+                              int rmax, int tmax) {
+  if (!dims || (nc != 2 && nc != 3))
+    return -1;
+  long long V = 1;
+  for (int d = 0; d < 4; d++)
+    V *= dims[d];
+  const long long field = ((long long)bytes_per_link(nc, precision) * V + 255) / 256 * 256;
+  const long long staging = (long long)(nc == 3 ? 18 : 4) * 8 * 4 * V;
+  Geom g{};
+  for (int d = 0; d < 4; d++)
+    g.L[d] = dims[d];
+  g.V = (int)V;
+  g.Vs = dims[0] * dims[1] * dims[2];
+  const int nr = std::max(1, rmax), nt = std::max(1, tmax);
+  const long long partials =
+      (long long)wilson_partials_count(g, std::min(nr, std::max(1, 1024 / nt)), nt, nc) * 8;
+  return 8 * field + 15 * field + staging + partials + 64LL * 1024;
+}
+
+} // extern "C"

@@ -1,0 +1,55 @@
+// Host-side declarations of the kernel launchers (implemented in the .cu files).
+#pragma once
+
+#include "gc_internal.cuh"
+
+namespace gc {
+
+struct HypL1 {
+  void *f[9];
+};
+struct HypL2 {
+  void *f[6];
+};
+
+template <class Store, class CT>
+int launch_ape(const Geom &g, const Fields4 &in, const Fields4 &out,
+               double alpha, cudaStream_t s);
+
+template <class Store, class CT>
+int launch_hyp(const Geom &g, const Fields4 &U, const HypL1 &l1,
+               const HypL2 &l2, void *out_t, double a1, double a2, double a3,
+               cudaStream_t s);
+
+// Wilson loops: per-block partial sums into `partials` (device, sized by
+// wilson_partials_count), then a fixed-order reduction into `out_dev`
+// ((tmax-tmin+1)*(rmax-rmin+1) doubles, index (T-tmin)*nR + (R-rmin)).
+struct WilsonPlan {
+  int cols_per_block; // spatial columns per block
+  int rows;           // threads per column (a divisor of Lt, <= 32)
+  int threads;        // cols_per_block * rows
+  int blocks;         // ceil(Vs / cols_per_block) * 3
+  size_t smem;        // dynamic shared memory bytes
+};
+
+WilsonPlan wilson_plan(const Geom &g, int nr, int nt, int nc, int ct_bytes);
+
+template <class Store, class CT>
+int launch_wilson(const Geom &g, const Fields4 &U, int rmin, int rmax,
+                  int tmin, int tmax, double *partials, double *out_dev,
+                  cudaStream_t s);
+
+template <class Store, class CT>
+int launch_plaquette(const Geom &g, const Fields4 &U, double *partials,
+                     double *out_dev, cudaStream_t s);
+
+int plaquette_partials_count(const Geom &g);
+size_t wilson_partials_count(const Geom &g, int nr, int nt, int nc);
+
+// Host AoS (uploaded raw to a device staging buffer) <-> device SoA fields.
+int launch_aos_to_soa(const Geom &g, int nc, int prec, int layout,
+                      const double *staging, const Fields4 &U, cudaStream_t s);
+int launch_soa_to_aos(const Geom &g, int nc, int prec, int layout,
+                      const Fields4 &U, double *staging, cudaStream_t s);
+
+} // namespace gc

@@ -1,0 +1,221 @@
+// APE and HYP smearing kernels (sm_100a).
+//
+// APE  (reference smearing.h:115-161): thread per (site, spatial mu); reads
+//      the current links, writes the smeared spatial links into a second
+//      buffer (Jacobi update, no copy: the host swaps the field pointers).
+// HYP  (reference smearing.h:305-516, smearing.cpp:333-350): three kernels,
+//      one per decoration level, with the reference's staple order:
+//        level 1: 9 fields   Vbar_{mu;nu rho}  (one staple direction each,
+//                 alpha3/2)  — thread per (site, field)
+//        level 2: 6 fields   Vtilde_{t;nu}, Vtilde_{nu;t}  (alpha2/4)
+//        level 3: U_t'       (alpha1/6), written to a second temporal buffer.
+// The staple sums use the compute type CT (FP64 for the plain form, FP32 for
+// the mixed form); the SU(N) projection always runs in FP64.
+#include "gc_internal.cuh"
+#include "gc_kernels.h"
+
+namespace gc {
+
+namespace {
+
+// S += ((c * (Fnu(x) Fmu(x+nu))) Fnu(x+mu)^dag)                  upper staple
+//    + ((c * (Fnu(x-nu)^dag Fmu(x-nu))) Fnu(x-nu+mu))             lower staple
+// exactly in the operation order of smearing.h:134-149 / :305-318 / :343-356.
+template <class Store, class CT, class M>
+__device__ __forceinline__ void add_staples(M &S, const void *fmu,
+                                            const void *fnu, size_t V, int x,
+                                            int x_pnu, int x_pmu, int x_mnu,
+                                            int x_mnu_pmu, CT c) {
+  M a = mul(Store::template load<CT>(fnu, V, x),
+            Store::template load<CT>(fmu, V, x_pnu));
+  S = add(S, mul_ad(scale(a, c), Store::template load<CT>(fnu, V, x_pmu)));
+  M b = mul_da(Store::template load<CT>(fnu, V, x_mnu),
+               Store::template load<CT>(fmu, V, x_mnu));
+  S = add(S, mul(scale(b, c), Store::template load<CT>(fnu, V, x_mnu_pmu)));
+}
+
+template <class Store, class CT, class M>
+__device__ __forceinline__ void proj_store(void *out, size_t V, int site,
+                                           const M &S) {
+  using MD = typename Store::template M<double>;
+  MD d = convert(S, (MD *)nullptr);
+  Store::template store<double>(out, V, site, proj(d));
+}
+
+struct Nbr {
+  int pnu, pmu, mnu, mnu_pmu;
+};
+
+__device__ __forceinline__ Nbr neighbours(const Geom &g, int site,
+                                          const int x[4], int mu, int nu) {
+  Nbr n;
+  const int dpn = step_off(g, x[nu], nu, +1);
+  const int dmn = step_off(g, x[nu], nu, -1);
+  const int dpm = step_off(g, x[mu], mu, +1);
+  n.pnu = site + dpn;
+  n.pmu = site + dpm;
+  n.mnu = site + dmn;
+  n.mnu_pmu = site + dmn + dpm;
+  return n;
+}
+
+template <class Store, class CT>
+__global__ void __launch_bounds__(128)
+    ape_kernel(Geom g, const __grid_constant__ Fields4 in,
+               const __grid_constant__ Fields4 out, double alpha) {
+  const int site = blockIdx.x * blockDim.x + threadIdx.x;
+  const int mu = blockIdx.y;
+  if (site >= g.V)
+    return;
+  using M = typename Store::template M<CT>;
+  int x[4];
+  site_coords(g, site, x);
+  const size_t V = g.V;
+  M S = scale(Store::template load<CT>(in.f[mu], V, site), CT(1 - alpha));
+  const CT c = CT(alpha / 4);
+#pragma unroll 1
+  for (int nu = 0; nu < 3; nu++) {
+    if (nu == mu)
+      continue;
+    Nbr n = neighbours(g, site, x, mu, nu);
+    add_staples<Store, CT>(S, in.f[mu], in.f[nu], V, site, n.pnu, n.pmu,
+                           n.mnu, n.mnu_pmu, c);
+  }
+  proj_store<Store, CT>(out.f[mu], V, site, S);
+}
+
+// Level-1 decorated links. Field index f:
+//   0..5 : spatial mu with excluded spatial nu, pairs (0,1),(0,2),(1,0),(1,2),
+//          (2,0),(2,1); staple direction eta = 3 - mu - nu
+//   6..8 : temporal, staple direction eta = f - 6
+__constant__ int kL1Mu[9] = {0, 0, 1, 1, 2, 2, 3, 3, 3};
+__constant__ int kL1Eta[9] = {2, 1, 2, 0, 1, 0, 0, 1, 2};
+
+template <class Store, class CT>
+__global__ void __launch_bounds__(128)
+    hyp_level1_kernel(Geom g, const __grid_constant__ Fields4 U,
+                      const __grid_constant__ HypL1 out, double alpha3) {
+  const int site = blockIdx.x * blockDim.x + threadIdx.x;
+  const int f = blockIdx.y;
+  if (site >= g.V)
+    return;
+  using M = typename Store::template M<CT>;
+  int x[4];
+  site_coords(g, site, x);
+  const size_t V = g.V;
+  const int mu = kL1Mu[f], eta = kL1Eta[f];
+  M S = scale(Store::template load<CT>(U.f[mu], V, site), CT(1 - alpha3));
+  Nbr n = neighbours(g, site, x, mu, eta);
+  add_staples<Store, CT>(S, U.f[mu], U.f[eta], V, site, n.pnu, n.pmu, n.mnu,
+                         n.mnu_pmu, CT(alpha3 / 2));
+  proj_store<Store, CT>(out.f[f], V, site, S);
+}
+
+// Level-1 field holding Vbar_{mu; nu, t} for spatial mu != nu.
+__device__ __forceinline__ int l1_spatial(int mu, int nu) {
+  return 2 * mu + (nu > mu ? nu - 1 : nu);
+}
+// Level-1 field holding Vbar_{t; a, b} (a, b spatial): staple dir 3 - a - b.
+__device__ __forceinline__ int l1_temporal(int a, int b) { return 6 + (3 - a - b); }
+
+// Level-2 decorated links. Field index f:
+//   0..2 : Vtilde_{t;nu}, nu = f       (smearing.h:433-450)
+//   3..5 : Vtilde_{nu;t}, nu = f - 3   (smearing.h:455-466)
+template <class Store, class CT>
+__global__ void __launch_bounds__(128)
+    hyp_level2_kernel(Geom g, const __grid_constant__ Fields4 U,
+                      const __grid_constant__ HypL1 l1,
+                      const __grid_constant__ HypL2 out, double alpha2) {
+  const int site = blockIdx.x * blockDim.x + threadIdx.x;
+  const int f = blockIdx.y;
+  if (site >= g.V)
+    return;
+  using M = typename Store::template M<CT>;
+  int x[4];
+  site_coords(g, site, x);
+  const size_t V = g.V;
+  const bool temporal = f < 3;
+  const int nu = temporal ? f : f - 3;
+  const int mu = temporal ? 3 : nu;
+  M S = scale(Store::template load<CT>(U.f[mu], V, site), CT(1 - alpha2));
+  const CT c = CT(alpha2 / 4);
+#pragma unroll 1
+  for (int rho = 0; rho < 3; rho++) {
+    if (rho == nu)
+      continue;
+    const void *fmu = temporal ? l1.f[l1_temporal(nu, rho)]
+                               : l1.f[l1_spatial(nu, rho)];
+    const void *fnu = l1.f[l1_spatial(rho, nu)];
+    Nbr n = neighbours(g, site, x, mu, rho);
+    add_staples<Store, CT>(S, fmu, fnu, V, site, n.pnu, n.pmu, n.mnu,
+                           n.mnu_pmu, c);
+  }
+  proj_store<Store, CT>(out.f[f], V, site, S);
+}
+
+// Level 3: the new temporal link (smearing.h:484-503).
+template <class Store, class CT>
+__global__ void __launch_bounds__(128)
+    hyp_level3_kernel(Geom g, const void *Ut, const __grid_constant__ HypL2 l2,
+                      void *out_t,
+                      double alpha1) {
+  const int site = blockIdx.x * blockDim.x + threadIdx.x;
+  if (site >= g.V)
+    return;
+  using M = typename Store::template M<CT>;
+  int x[4];
+  site_coords(g, site, x);
+  const size_t V = g.V;
+  M S = scale(Store::template load<CT>(Ut, V, site), CT(1 - alpha1));
+  const CT c = CT(alpha1 / 6);
+#pragma unroll 1
+  for (int nu = 0; nu < 3; nu++) {
+    Nbr n = neighbours(g, site, x, 3, nu);
+    add_staples<Store, CT>(S, l2.f[nu], l2.f[3 + nu], V, site, n.pnu, n.pmu,
+                           n.mnu, n.mnu_pmu, c);
+  }
+  proj_store<Store, CT>(out_t, V, site, S);
+}
+
+constexpr int kSmearBlock = 128;
+
+} // namespace
+
+template <class Store, class CT>
+int launch_ape(const Geom &g, const Fields4 &in, const Fields4 &out,
+               double alpha, cudaStream_t s) {
+  dim3 grid((g.V + kSmearBlock - 1) / kSmearBlock, 3);
+  ape_kernel<Store, CT><<<grid, kSmearBlock, 0, s>>>(g, in, out, alpha);
+  return launch_check("ape_kernel");
+}
+
+template <class Store, class CT>
+int launch_hyp(const Geom &g, const Fields4 &U, const HypL1 &l1,
+               const HypL2 &l2, void *out_t, double a1, double a2, double a3,
+               cudaStream_t s) {
+  const int nb = (g.V + kSmearBlock - 1) / kSmearBlock;
+  hyp_level1_kernel<Store, CT><<<dim3(nb, 9), kSmearBlock, 0, s>>>(g, U, l1, a3);
+  int rc = launch_check("hyp_level1_kernel");
+  if (rc)
+    return rc;
+  hyp_level2_kernel<Store, CT><<<dim3(nb, 6), kSmearBlock, 0, s>>>(g, U, l1, l2, a2);
+  rc = launch_check("hyp_level2_kernel");
+  if (rc)
+    return rc;
+  hyp_level3_kernel<Store, CT><<<nb, kSmearBlock, 0, s>>>(g, U.f[3], l2, out_t, a1);
+  return launch_check("hyp_level3_kernel");
+}
+
+#define GC_INSTANTIATE_SMEAR(STORE, CT)                                        \
+  template int launch_ape<STORE, CT>(const Geom &, const Fields4 &,           \
+                                     const Fields4 &, double, cudaStream_t);  \
+  template int launch_hyp<STORE, CT>(const Geom &, const Fields4 &,           \
+                                     const HypL1 &, const HypL2 &, void *,    \
+                                     double, double, double, cudaStream_t);
+
+GC_INSTANTIATE_SMEAR(StoreF64SU3, double)
+GC_INSTANTIATE_SMEAR(StoreF64SU2, double)
+GC_INSTANTIATE_SMEAR(StoreF32SU3, float)
+GC_INSTANTIATE_SMEAR(StoreF32SU2, float)
+
+} // namespace gc

@@ -1,0 +1,327 @@
+// On-axis Wilson loops W(R,T) and the average plaquette (sm_100a).
+//
+// Reference: wilson_loop (wilson_loops.h:1047-1074) builds time lines
+// L(x,T) and space lines S_nu(x,R) as full-lattice fields and, for every
+// (R,T), sums Re Tr[L(x,T) S_nu(x+T,R) L(x+R nu,T)^dag S_nu(x,R)^dag]/N over
+// x and nu < 3, divided by 3V (:719-791).
+//
+// Here one block owns `cols` spatial columns (s, nu) over all t. The space
+// lines S(s,t,R) of its columns live in shared memory and are extended by one
+// link per R. For every corner (s,t0) a thread walks T with the exact
+// recursion
+//     K_0 = S(x,R),   K_T = U_t(x+(T-1)t)^dag K_{T-1} U_t(x+R nu+(T-1)t),
+// so that K_T = L(x,T)^dag S(x,R) L(x+R nu,T), and the loop trace is
+//     Re Tr[S(x+T t, R) K_T^dag] / N.
+// This is the same product of links as the reference's, reassociated; it
+// does not assume unitarity. Per (x,nu,R,T): two matrix products and one
+// 9-element dot product. No line fields are written to HBM.
+//
+// Reductions are deterministic: warp shuffles into per-warp shared
+// accumulators, a fixed-order sum over warps into one partial per block and
+// (R,T), then a fixed-order tree over blocks.
+#include "gc_internal.cuh"
+#include "gc_kernels.h"
+
+namespace gc {
+
+namespace {
+
+template <class M> struct Comps;
+template <class T> struct Comps<SU3<T>> {
+  static constexpr int n = 18;
+};
+template <class T> struct Comps<SU2<T>> {
+  static constexpr int n = 4;
+};
+
+// Shared-memory matrices are stored component-major: comp k of matrix i at
+// sm[k*stride + i], so consecutive threads touch consecutive words.
+template <class T>
+__device__ __forceinline__ void sm_store(T *sm, int stride, int i,
+                                         const SU3<T> &m) {
+#pragma unroll
+  for (int k = 0; k < 9; k++) {
+    sm[(2 * k) * stride + i] = m.e[k / 3][k % 3].re;
+    sm[(2 * k + 1) * stride + i] = m.e[k / 3][k % 3].im;
+  }
+}
+template <class T>
+__device__ __forceinline__ SU3<T> sm_load(const T *sm, int stride, int i,
+                                          SU3<T> *) {
+  SU3<T> m;
+#pragma unroll
+  for (int k = 0; k < 9; k++)
+    m.e[k / 3][k % 3] = {sm[(2 * k) * stride + i], sm[(2 * k + 1) * stride + i]};
+  return m;
+}
+template <class T>
+__device__ __forceinline__ void sm_store(T *sm, int stride, int i,
+                                         const SU2<T> &m) {
+  sm[i] = m.a0;
+  sm[stride + i] = m.a1;
+  sm[2 * stride + i] = m.a2;
+  sm[3 * stride + i] = m.a3;
+}
+template <class T>
+__device__ __forceinline__ SU2<T> sm_load(const T *sm, int stride, int i,
+                                          SU2<T> *) {
+  return {sm[i], sm[stride + i], sm[2 * stride + i], sm[3 * stride + i]};
+}
+
+__device__ __forceinline__ double warp_sum(double v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1)
+    v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+
+// Re Tr(A B^dag)/N evaluated in FP64 whatever the compute type.
+template <class T> __device__ __forceinline__ double conj_tr_d(const SU3<T> &a, const SU3<T> &b) {
+  double s = 0;
+#pragma unroll
+  for (int i = 0; i < 3; i++)
+#pragma unroll
+    for (int j = 0; j < 3; j++)
+      s += double(a.e[i][j].re) * double(b.e[i][j].re) +
+           double(a.e[i][j].im) * double(b.e[i][j].im);
+  return s / 3.0;
+}
+template <class T> __device__ __forceinline__ double conj_tr_d(const SU2<T> &a, const SU2<T> &b) {
+  return double(a.a0) * double(b.a0) + double(a.a1) * double(b.a1) +
+         double(a.a2) * double(b.a2) + double(a.a3) * double(b.a3);
+}
+
+template <class Store, class CT>
+__global__ void __launch_bounds__(256)
+    wilson_kernel(Geom g, const __grid_constant__ Fields4 U, int rmin, int rmax, int tmin, int tmax,
+                  int cols, int rows, double *partials) {
+  using M = typename Store::template M<CT>;
+  constexpr int NCOMP = Comps<M>::n;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int Lt = g.L[3];
+  const int nr = rmax - rmin + 1, nt = tmax - tmin + 1;
+  const int nwarps = blockDim.x >> 5;
+  double *wacc = reinterpret_cast<double *>(smem_raw);         // [nwarps][nr*nt]
+  CT *scol = reinterpret_cast<CT *>(wacc + (size_t)nwarps * nr * nt);
+  const int sstride = Lt * cols;                                // matrices in scol
+
+  const int tid = threadIdx.x;
+  const int warp = tid >> 5, lane = tid & 31;
+  for (int i = tid; i < nwarps * nr * nt; i += blockDim.x)
+    wacc[i] = 0.0;
+
+  const int c = tid % cols;
+  const int row = tid / cols;
+  const int s = blockIdx.x * cols + c;
+  const int nu = blockIdx.y;
+  const bool active = (row < rows) && (s < g.Vs);
+  const int kt = Lt / rows;
+  int xs[4] = {0, 0, 0, 0};
+  if (active)
+    site_coords(g, s, xs);
+  const size_t V = g.V;
+  const void *Unu = U.f[nu];
+  const void *Ut = U.f[3];
+  __syncthreads();
+
+#pragma unroll 1
+  for (int R = 1; R <= rmax; R++) {
+    // Extend the space lines of this thread's corners by one link.
+    if (active) {
+      const int sl = s + fwd_off(g, xs[nu], nu, R - 1);
+#pragma unroll 1
+      for (int k = 0; k < kt; k++) {
+        const int t0 = row + k * rows;
+        M u = Store::template load<CT>(Unu, V, sl + t0 * g.Vs);
+        M sn = (R == 1) ? u : mul(sm_load(scol, sstride, t0 * cols + c, (M *)nullptr), u);
+        sm_store(scol, sstride, t0 * cols + c, sn);
+      }
+    }
+    __syncthreads();
+    if (R >= rmin) {
+      const int sR = s + (active ? fwd_off(g, xs[nu], nu, R) : 0);
+      double *wrow = wacc + (size_t)warp * nr * nt + (R - rmin) * nt;
+#pragma unroll 1
+      for (int k = 0; k < kt; k++) {
+        const int t0 = row + k * rows;
+        M K = active ? sm_load(scol, sstride, t0 * cols + c, (M *)nullptr)
+                     : unit(M());
+#pragma unroll 1
+        for (int T = 1; T <= tmax; T++) {
+          int tt = t0 + T - 1;
+          tt -= (tt / Lt) * Lt;
+          if (active) {
+            M a = Store::template load<CT>(Ut, V, s + tt * g.Vs);
+            M b = Store::template load<CT>(Ut, V, sR + tt * g.Vs);
+            K = mul(mul_da(a, K), b);
+          }
+          if (T >= tmin) {
+            int tu = tt + 1;
+            tu = (tu == Lt) ? 0 : tu;
+            double term = active
+                ? conj_tr_d(sm_load(scol, sstride, tu * cols + c, (M *)nullptr), K)
+                : 0.0;
+            term = warp_sum(term);
+            if (lane == 0)
+              wrow[T - tmin] += term;
+          }
+        }
+      }
+    }
+    __syncthreads();
+  }
+
+  // Fixed-order sum over warps -> one partial per (block, R, T).
+  const size_t blk = (size_t)blockIdx.y * gridDim.x + blockIdx.x;
+  for (int e = tid; e < nr * nt; e += blockDim.x) {
+    double sum = 0.0;
+    for (int w = 0; w < nwarps; w++)
+      sum += wacc[(size_t)w * nr * nt + e];
+    partials[blk * nr * nt + e] = sum;
+  }
+}
+
+// out[(T-tmin)*nr + (R-rmin)] = (sum over blocks of partial e=(R-rmin)*nt+(T-tmin)) * scale
+__global__ void __launch_bounds__(256)
+    reduce_partials_kernel(const double *partials, int nblocks, int nentries,
+                           int nr, int nt, double scale, double *out) {
+  __shared__ double sh[256];
+  const int e = blockIdx.x;
+  double s = 0.0;
+  for (int b = threadIdx.x; b < nblocks; b += blockDim.x)
+    s += partials[(size_t)b * nentries + e];
+  sh[threadIdx.x] = s;
+  __syncthreads();
+  for (int w = blockDim.x / 2; w > 0; w >>= 1) {
+    if (threadIdx.x < w)
+      sh[threadIdx.x] += sh[threadIdx.x + w];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    const int ir = e / nt, it = e % nt;
+    out[it * nr + ir] = sh[0] * scale;
+  }
+}
+
+// Average plaquette: thread per site, six planes (plaket.h:24-42), fixed-order
+// block sums.
+template <class Store, class CT>
+__global__ void __launch_bounds__(256)
+    plaquette_kernel(Geom g, const __grid_constant__ Fields4 U, double *partials) {
+  using M = typename Store::template M<CT>;
+  __shared__ double sh[256];
+  const int site = blockIdx.x * blockDim.x + threadIdx.x;
+  double p = 0.0;
+  if (site < g.V) {
+    int x[4];
+    site_coords(g, site, x);
+    const size_t V = g.V;
+    double acc = 0.0;
+#pragma unroll 1
+    for (int mu = 0; mu < 3; mu++) {
+#pragma unroll 1
+      for (int nu = mu + 1; nu < 4; nu++) {
+        const int pm = site + step_off(g, x[mu], mu, +1);
+        const int pn = site + step_off(g, x[nu], nu, +1);
+        M a = mul(Store::template load<CT>(U.f[mu], V, site),
+                  Store::template load<CT>(U.f[nu], V, pm));
+        a = mul_ad(a, Store::template load<CT>(U.f[mu], V, pn));
+        acc += conj_tr_d(a, Store::template load<CT>(U.f[nu], V, site));
+      }
+    }
+    p = acc / 6.0;
+  }
+  sh[threadIdx.x] = p;
+  __syncthreads();
+  for (int w = blockDim.x / 2; w > 0; w >>= 1) {
+    if (threadIdx.x < w)
+      sh[threadIdx.x] += sh[threadIdx.x + w];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0)
+    partials[blockIdx.x] = sh[0];
+}
+
+int largest_divisor_upto(int n, int cap) {
+  for (int d = cap < n ? cap : n; d > 1; d--)
+    if (n % d == 0)
+      return d;
+  return 1;
+}
+
+} // namespace
+
+WilsonPlan wilson_plan(const Geom &g, int nr, int nt, int nc, int ct_bytes) {
+  WilsonPlan p;
+  const int Lt = g.L[3];
+  p.rows = largest_divisor_upto(Lt, 32);
+  p.cols_per_block = 256 / p.rows;
+  if (p.cols_per_block < 1)
+    p.cols_per_block = 1;
+  const int active = p.cols_per_block * p.rows;
+  p.threads = ((active + 31) / 32) * 32;
+  const int colblocks = (g.Vs + p.cols_per_block - 1) / p.cols_per_block;
+  p.blocks = colblocks * 3;
+  const int nwarps = p.threads / 32;
+  const int ncomp = (nc == 3) ? 18 : 4;
+  p.smem = (size_t)nwarps * nr * nt * sizeof(double) +
+           (size_t)ncomp * Lt * p.cols_per_block * ct_bytes;
+  return p;
+}
+
+size_t wilson_partials_count(const Geom &g, int nr, int nt, int nc) {
+  return (size_t)wilson_plan(g, nr, nt, nc, 8).blocks * nr * nt;
+}
+
+int plaquette_partials_count(const Geom &g) { return (g.V + 255) / 256; }
+
+template <class Store, class CT>
+int launch_wilson(const Geom &g, const Fields4 &U, int rmin, int rmax,
+                  int tmin, int tmax, double *partials, double *out_dev,
+                  cudaStream_t s) {
+  const int nr = rmax - rmin + 1, nt = tmax - tmin + 1;
+  WilsonPlan p = wilson_plan(g, nr, nt, Store::NC, (int)sizeof(CT));
+  if (p.smem > 48 * 1024) {
+    cudaError_t e = cudaFuncSetAttribute(
+        wilson_kernel<Store, CT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+        (int)p.smem);
+    if (e != cudaSuccess)
+      return launch_check("wilson_kernel smem attribute");
+  }
+  dim3 grid(p.blocks / 3, 3);
+  wilson_kernel<Store, CT><<<grid, p.threads, p.smem, s>>>(
+      g, U, rmin, rmax, tmin, tmax, p.cols_per_block, p.rows, partials);
+  int rc = launch_check("wilson_kernel");
+  if (rc)
+    return rc;
+  reduce_partials_kernel<<<nr * nt, 256, 0, s>>>(
+      partials, p.blocks, nr * nt, nr, nt, 1.0 / (3.0 * (double)g.V), out_dev);
+  return launch_check("reduce_partials_kernel");
+}
+
+template <class Store, class CT>
+int launch_plaquette(const Geom &g, const Fields4 &U, double *partials,
+                     double *out_dev, cudaStream_t s) {
+  const int nb = plaquette_partials_count(g);
+  plaquette_kernel<Store, CT><<<nb, 256, 0, s>>>(g, U, partials);
+  int rc = launch_check("plaquette_kernel");
+  if (rc)
+    return rc;
+  reduce_partials_kernel<<<1, 256, 0, s>>>(partials, nb, 1, 1, 1,
+                                           1.0 / (double)g.V, out_dev);
+  return launch_check("reduce_partials_kernel");
+}
+
+#define GC_INSTANTIATE_W(STORE, CT)                                            \
+  template int launch_wilson<STORE, CT>(const Geom &, const Fields4 &, int,   \
+                                        int, int, int, double *, double *,    \
+                                        cudaStream_t);                        \
+  template int launch_plaquette<STORE, CT>(const Geom &, const Fields4 &,     \
+                                           double *, double *, cudaStream_t);
+
+GC_INSTANTIATE_W(StoreF64SU3, double)
+GC_INSTANTIATE_W(StoreF64SU2, double)
+GC_INSTANTIATE_W(StoreF32SU3, float)
+GC_INSTANTIATE_W(StoreF32SU2, float)
+
+} // namespace gc

@@ -1,0 +1,213 @@
+"""Python host API over the C ABI, mirroring the reference's C++ interface.
+
+Reference interface (general_code, lib/cpu/include):
+  Data::LatticeData<DataPattern, MatrixType>   data.h:78-237   -> LatticeData
+  smearing_APE(conf, alpha)                    smearing.h:115  -> smearing_APE
+  smearing_HYP(conf, alpha1, alpha2, alpha3)   smearing.h:480  -> smearing_HYP
+  wilson_loop(conf, r_min, r_max, t_min, t_max) wilson_loops.h:1047 -> wilson_loop
+  plaket(conf)                                 plaket.h:83     -> plaket
+
+Like the reference, the LatticeData functions update the host links in place
+(smearing) or return a dict keyed (T, R) (Wilson loops). Each call uploads the
+links, runs the sm_100a kernels and downloads the result. `Lattice` is the
+device-resident form: links stay in HBM between calls.
+"""
+from __future__ import annotations
+
+import ctypes
+from typing import Dict, Sequence, Tuple
+
+import numpy as np
+
+from . import _lib
+from ._lib import (GC_LAYOUT_EIGEN_COLMAJOR, GC_LAYOUT_ROWMAJOR, GC_PREC_FP64,
+                   GC_PREC_MIXED, GCError, check, dbl_ptr, dims_arg, lib)
+
+_PREC = {"fp64": GC_PREC_FP64, "mixed": GC_PREC_MIXED}
+_LAYOUT = {"rowmajor": GC_LAYOUT_ROWMAJOR, "eigen": GC_LAYOUT_EIGEN_COLMAJOR}
+
+
+def link_size(nc: int) -> int:
+    """Doubles per link in the host layout: 4 (SU(2)) or 18 (SU(3))."""
+    if nc == 2:
+        return 4
+    if nc == 3:
+        return 18
+    raise ValueError("nc must be 2 or 3")
+
+
+def volume(dims: Sequence[int]) -> int:
+    v = 1
+    for d in dims:
+        v *= int(d)
+    return v
+
+
+def generate_config(dims: Sequence[int], nc: int, eps: float, seed: int,
+                    index: int = 0, gauge: bool = True, out: np.ndarray | None = None
+                    ) -> np.ndarray:
+    """Seeded synthetic configuration (host array, shape (4V, 4|18), row-major)."""
+    n = 4 * volume(dims)
+    if out is None:
+        out = np.empty((n, link_size(nc)), dtype=np.float64)
+    check(lib().gc_generate_host(dims_arg(dims), nc, float(eps), int(seed) & 0xffffffff,
+                                 int(index) & 0xffffffff, int(bool(gauge)), dbl_ptr(out)))
+    return out
+
+
+def unit_config(dims: Sequence[int], nc: int) -> np.ndarray:
+    n = 4 * volume(dims)
+    a = np.zeros((n, link_size(nc)), dtype=np.float64)
+    if nc == 2:
+        a[:, 0] = 1.0
+    else:
+        a[:, 0] = a[:, 8] = a[:, 16] = 1.0
+    return a
+
+
+class Lattice:
+    """A device-resident gauge configuration (one gc_lattice handle)."""
+
+    def __init__(self, dims: Sequence[int], nc: int, precision: str = "fp64"):
+        self.dims = tuple(int(d) for d in dims)
+        self.nc = int(nc)
+        self.precision = precision
+        self._h = ctypes.c_void_p()
+        check(lib().gc_lattice_create(dims_arg(self.dims), self.nc, _PREC[precision],
+                                      ctypes.byref(self._h)))
+
+    @property
+    def handle(self):
+        return self._h
+
+    @property
+    def V(self) -> int:
+        return volume(self.dims)
+
+    def _check(self, rc: int) -> None:
+        check(rc, self._h)
+
+    def close(self) -> None:
+        if self._h:
+            lib().gc_lattice_destroy(self._h)
+            self._h = ctypes.c_void_p()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_stream(self, stream_ptr: int | None) -> None:
+        self._check(lib().gc_set_stream(self._h, ctypes.c_void_p(stream_ptr or 0)))
+
+    def synchronize(self) -> None:
+        self._check(lib().gc_synchronize(self._h))
+
+    def upload(self, links: np.ndarray, layout: str = "rowmajor") -> None:
+        a = np.ascontiguousarray(links, dtype=np.float64)
+        if a.size != 4 * self.V * link_size(self.nc):
+            raise ValueError("link array has the wrong size for this lattice")
+        self._check(lib().gc_upload(self._h, dbl_ptr(a), _LAYOUT[layout]))
+        if a is not links:  # keep the temporary alive until the copy is done
+            self.synchronize()
+
+    def download(self, out: np.ndarray | None = None, layout: str = "rowmajor") -> np.ndarray:
+        if out is None:
+            out = np.empty((4 * self.V, link_size(self.nc)), dtype=np.float64)
+        self._check(lib().gc_download(self._h, dbl_ptr(out), _LAYOUT[layout]))
+        return out
+
+    def generate(self, eps: float, seed: int, index: int = 0, gauge: bool = True) -> None:
+        self._check(lib().gc_generate(self._h, float(eps), int(seed) & 0xffffffff,
+                                      int(index) & 0xffffffff, int(bool(gauge))))
+
+    def ape(self, alpha: float, steps: int = 1) -> None:
+        self._check(lib().gc_ape(self._h, float(alpha), int(steps)))
+
+    def hyp(self, alpha1: float, alpha2: float, alpha3: float, steps: int = 1) -> None:
+        self._check(lib().gc_hyp(self._h, float(alpha1), float(alpha2), float(alpha3),
+                                 int(steps)))
+
+    def wilson_loop(self, r_min: int, r_max: int, time_min: int, time_max: int) -> np.ndarray:
+        """W table, shape (time_max-time_min+1, r_max-r_min+1): [T-t_min, R-r_min]."""
+        out = np.empty((time_max - time_min + 1, r_max - r_min + 1), dtype=np.float64)
+        self._check(lib().gc_wilson_onaxis(self._h, int(r_min), int(r_max), int(time_min),
+                                           int(time_max), dbl_ptr(out)))
+        return out
+
+    def plaquette(self) -> float:
+        out = ctypes.c_double()
+        self._check(lib().gc_plaquette(self._h, ctypes.byref(out)))
+        return out.value
+
+
+class LatticeData:
+    """Host-side configuration, like Data::LatticeData<DataPatternLexicographical, MT>.
+
+    `array` has shape (4*V, 4) for SU(2) or (4*V, 18) for SU(3), link index
+    4*site + mu, in the row-major layout of the reference's get_data().
+    """
+
+    def __init__(self, lat_dim: Sequence[int], nc: int, array: np.ndarray | None = None):
+        self.lat_dim = tuple(int(d) for d in lat_dim)
+        self.nc = int(nc)
+        if array is None:
+            array = unit_config(self.lat_dim, self.nc)
+        self.array = np.ascontiguousarray(array, dtype=np.float64).reshape(
+            4 * volume(self.lat_dim), link_size(self.nc))
+
+    def _run(self, fn, precision: str = "fp64"):
+        with Lattice(self.lat_dim, self.nc, precision) as lat:
+            lat.upload(self.array)
+            r = fn(lat)
+            return lat, r
+
+
+def smearing_APE(conf: LatticeData, alpha: float) -> None:
+    """One APE step in place (smearing.h:115-161)."""
+    with Lattice(conf.lat_dim, conf.nc) as lat:
+        lat.upload(conf.array)
+        lat.ape(alpha, 1)
+        lat.download(conf.array)
+
+
+def smearing_HYP(conf: LatticeData, alpha1: float, alpha2: float, alpha3: float) -> None:
+    """One HYP step in place (smearing.h:480-516)."""
+    with Lattice(conf.lat_dim, conf.nc) as lat:
+        lat.upload(conf.array)
+        lat.hyp(alpha1, alpha2, alpha3, 1)
+        lat.download(conf.array)
+
+
+def wilson_loop(conf: LatticeData, r_min: int, r_max: int, time_min: int,
+                time_max: int) -> Dict[Tuple[int, int], float]:
+    """On-axis W(R,T) as a dict keyed (T, R) (wilson_loops.h:1047-1074)."""
+    with Lattice(conf.lat_dim, conf.nc) as lat:
+        lat.upload(conf.array)
+        w = lat.wilson_loop(r_min, r_max, time_min, time_max)
+    return {(t, r): float(w[t - time_min, r - r_min])
+            for t in range(time_min, time_max + 1) for r in range(r_min, r_max + 1)}
+
+
+def plaket(conf: LatticeData) -> float:
+    """Average plaquette (plaket.h:83-101)."""
+    with Lattice(conf.lat_dim, conf.nc) as lat:
+        lat.upload(conf.array)
+        return lat.plaquette()
+
+
+def job_device_bytes(dims: Sequence[int], nc: int, precision: str, r_max: int,
+                     time_max: int) -> int:
+    return int(lib().gc_job_device_bytes(dims_arg(dims), nc, _PREC[precision], r_max, time_max))
+
+
+__all__ = ["Lattice", "LatticeData", "smearing_APE", "smearing_HYP", "wilson_loop", "plaket",
+           "generate_config", "unit_config", "link_size", "volume", "job_device_bytes",
+           "GCError"]

@@ -1,0 +1,139 @@
+/*
+ * general_code_b200 — C ABI for APE/HYP link smearing and on-axis Wilson loops
+ * W(R,T) on SU(2)/SU(3) gauge configurations, computed by sm_100a kernels.
+ *
+ * The reference ("general_code", lib/cpu) exposes this path as C++ templates
+ * on Data::LatticeData<DataPatternLexicographical, MatrixType>; it has no FFI.
+ * Each entry point below names the reference interface it replaces. The C++
+ * drop-in overloads with the reference's own signatures live in gc_dropin.hpp
+ * and are thin wrappers over these functions.
+ *
+ * Conventions
+ *  - Plain pointers and sizes only. Every function returns GC_OK (0) or a
+ *    GC_ERR_* code; the message of the last failure on a handle is returned by
+ *    gc_last_error(handle) (gc_last_error(NULL) gives the last failure of a
+ *    call that had no handle). Nothing throws across the ABI.
+ *  - Lattice geometry: dims = {Lx, Ly, Lz, Lt}; site = x + Lx*(y + Ly*(z +
+ *    Lz*t)); directions mu = 0,1,2 (space), 3 (time); link index 4*site+mu
+ *    (reference indexing.h:71-126, DataPatternLexicographical).
+ *  - Host link arrays hold 4*V links in that order. Per link:
+ *      SU(2): 4 doubles (a0,a1,a2,a3), U = a0 + i a.sigma   (matrix.h:8-13)
+ *      SU(3): 18 doubles; GC_LAYOUT_ROWMAJOR stores element (i,j) at
+ *             (3i+j)*2 (re), +1 (im) — the reference's file / get_data order
+ *             (matrix.h:228-243); GC_LAYOUT_EIGEN_COLMAJOR stores it at
+ *             (i+3j)*2 — the in-memory image of std::vector<su3> (an
+ *             Eigen::Matrix3cd per link).
+ *  - Links stay resident on the device between calls. Calls on one handle are
+ *    serialised on the handle's CUDA stream; functions that return results to
+ *    host memory synchronise that stream. A handle may be used from one host
+ *    thread at a time per call (calls are internally locked).
+ */
+#ifndef GC_LATTICE_H
+#define GC_LATTICE_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define GC_OK 0
+#define GC_ERR_ARG 1       /* invalid argument (sizes, ranges, null pointers) */
+#define GC_ERR_CUDA 2      /* a CUDA runtime call or kernel launch failed     */
+#define GC_ERR_NOMEM 3     /* device or pinned-host allocation failed         */
+#define GC_ERR_NODEVICE 4  /* no CUDA device, or not an sm_100 device         */
+#define GC_ERR_IO 5        /* configuration file could not be read/written    */
+#define GC_ERR_STATE 6     /* handle not initialised with links yet           */
+#define GC_ERR_TIMEOUT 7   /* a bounded device-side wait expired              */
+#define GC_ERR_BUSY 8      /* admission refused (no free slot or memory)      */
+
+#define GC_PREC_FP64 0     /* links stored and computed in FP64               */
+#define GC_PREC_MIXED 1    /* FP32 links (SU(3): 12 reals, third row rebuilt),
+                              FP64 projection and FP64 trace accumulation     */
+
+#define GC_LAYOUT_ROWMAJOR 0
+#define GC_LAYOUT_EIGEN_COLMAJOR 1
+
+typedef struct gc_lattice gc_lattice;
+
+/* Library version as MAJOR*10000 + MINOR*100 + PATCH. */
+int gc_version(void);
+
+/* Text for the last failure on h (or of a handle-less call when h == NULL).
+ * The pointer stays valid until the next failing call on the same handle. */
+const char *gc_last_error(const gc_lattice *h);
+
+/* Creates a device-resident lattice (no links yet; upload or generate next).
+ * Replaces: Data::LatticeData<DP,MT>::LatticeData(lat_dim) (data.h:84-87).
+ * nc is 2 or 3; precision is GC_PREC_FP64 or GC_PREC_MIXED. */
+int gc_lattice_create(const int dims[4], int nc, int precision,
+                      gc_lattice **out);
+
+/* Frees all device memory of h. NULL is accepted. */
+int gc_lattice_destroy(gc_lattice *h);
+
+/* Runs h's work on an existing CUDA stream (a cudaStream_t passed as void*).
+ * NULL selects the handle's own stream. */
+int gc_set_stream(gc_lattice *h, void *cuda_stream);
+
+/* Blocks until all work queued on h has finished. */
+int gc_synchronize(gc_lattice *h);
+
+/* Copies 4*V host links (layout GC_LAYOUT_*) to the device.
+ * Replaces: filling LatticeData::array (data.h:95-112) before a call. */
+int gc_upload(gc_lattice *h, const double *host_links, int layout);
+
+/* Copies the device links back into 4*V host links (layout GC_LAYOUT_*). */
+int gc_download(gc_lattice *h, double *host_links, int layout);
+
+/* One or more APE steps on the spatial links (temporal links unchanged):
+ * U'_i = Proj[(1-alpha) U_i + alpha/4 sum_{j != i, j < 3} staples].
+ * Replaces: smearing_APE(conf, alpha) (smearing.h:115-161), called steps
+ * times. */
+int gc_ape(gc_lattice *h, double alpha, int steps);
+
+/* One or more HYP steps; only temporal links change (three decoration levels
+ * with alpha1/alpha2/alpha3, divisors 6/4/2).
+ * Replaces: smearing_HYP(conf, alpha1, alpha2, alpha3) (smearing.h:480-516),
+ * called steps times. */
+int gc_hyp(gc_lattice *h, double alpha1, double alpha2, double alpha3,
+           int steps);
+
+/* On-axis Wilson loops averaged over sites and the three spatial directions,
+ * for R in [r_min, r_max] (space) and T in [time_min, time_max] (time).
+ * out (host) receives (time_max-time_min+1)*(r_max-r_min+1) doubles:
+ * out[(T-time_min)*(r_max-r_min+1) + (R-r_min)] = W(R,T), i.e. the entries of
+ * the reference's std::map keyed (T,R), in the map's iteration order.
+ * Replaces: wilson_loop(conf, r_min, r_max, time_min, time_max)
+ * (wilson_loops.h:1047-1074) and the legacy vector overload
+ * (basic_observables.h:108-111). */
+int gc_wilson_onaxis(gc_lattice *h, int r_min, int r_max, int time_min,
+                     int time_max, double *out);
+
+/* Average plaquette over the 6 planes (1 for unit links).
+ * Replaces: plaket(conf) (plaket.h:83-101). */
+int gc_plaquette(gc_lattice *h, double *out);
+
+/* Fills h with the seeded synthetic configuration used by the benchmarks:
+ *   SU(2): U = (cos th, sin th a/|a|), th = eps*|a|, a_k ~ N(0,1);
+ *   SU(3): U = exp(i eps sum_a c_a lambda_a), c_a ~ N(0,1), reunitarised;
+ * then, if gauge != 0, a Haar-random gauge transformation
+ * U_mu(x) <- g(x) U_mu(x) g(x+mu)^dag. Randomness: Philox-4x32-10 with key
+ * (seed, config_index); identical on every host and thread count. The links
+ * are generated on the host and uploaded. */
+int gc_generate(gc_lattice *h, double eps, unsigned int seed,
+                unsigned int config_index, int gauge);
+
+/* Host-only generator (no device needed): writes 4*V links in layout
+ * GC_LAYOUT_ROWMAJOR to host_links. Same stream of numbers as gc_generate. */
+int gc_generate_host(const int dims[4], int nc, double eps, unsigned int seed,
+                     unsigned int config_index, int gauge, double *host_links);
+
+/* Bytes of device memory a handle of this shape uses for links plus working
+ * buffers of a full HYP + APE + W job (for admission control). */
+long long gc_job_device_bytes(const int dims[4], int nc, int precision,
+                              int r_max, int time_max);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* GC_LATTICE_H */

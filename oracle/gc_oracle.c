@@ -1,0 +1,513 @@
+/*
+ * CPU restatement of the reference's smear-and-measure path (FP64, plain C).
+ *
+ * TEST INFRASTRUCTURE ONLY — the checker for tests/, smoke() and the CPU
+ * baseline leg of bench.py. The product never calls it.
+ *
+ * Followed reference code (general_code, lib/cpu):
+ *   su2 algebra            include/matrix.h:54-110
+ *   su3 algebra, proj      include/matrix.h:256-292, :348-358 (Eigen products)
+ *   periodic indexing      include/indexing.h:71-126
+ *   smearing_APE           include/smearing.h:115-161
+ *   smearing_plane_HYP     include/smearing.h:283-378 (both overloads)
+ *   HYP_initialize_vector  include/smearing.h:380-399
+ *   make_step1/make_step2  include/smearing.h:401-467
+ *   smearing_HYP           include/smearing.h:480-516, make_indices3 src/smearing.cpp:333-350
+ *   wilson lines           include/wilson_loops.h:665-717
+ *   W(R,T) plane sums      include/wilson_loops.h:719-791
+ *   wilson_loop driver     include/wilson_loops.h:1047-1074
+ *   plaquette              include/plaket.h:24-42, :83-101 (accumulator zeroed)
+ * The operation order of every staple and product is the reference's.
+ */
+#include "gc_oracle.h"
+
+#include <math.h>
+#include <omp.h>
+#include <stdlib.h>
+#include <string.h>
+
+typedef struct {
+  int L[4];
+  long long V;
+} geom_t;
+
+static void geom_init(geom_t *g, const int dims[4]) {
+  g->V = 1;
+  for (int d = 0; d < 4; d++) {
+    g->L[d] = dims[d];
+    g->V *= dims[d];
+  }
+}
+
+static void coords(const geom_t *g, long long s, int x[4]) {
+  for (int d = 0; d < 4; d++) {
+    x[d] = (int)(s % g->L[d]);
+    s /= g->L[d];
+  }
+}
+
+static long long index_of(const geom_t *g, const int x[4]) {
+  return x[0] + (long long)g->L[0] * (x[1] + (long long)g->L[1] * (x[2] + (long long)g->L[2] * x[3]));
+}
+
+/* Site reached from s by n steps (any sign, any length) in direction mu. */
+static long long shift(const geom_t *g, long long s, int mu, int n) {
+  int x[4];
+  coords(g, s, x);
+  int m = (x[mu] + n) % g->L[mu];
+  if (m < 0)
+    m += g->L[mu];
+  x[mu] = m;
+  return index_of(g, x);
+}
+
+/* ------------------------------------------------------------ su2 */
+static void su2_mul(double *c, const double *a, const double *b) {
+  double r0 = a[0] * b[0] - a[1] * b[1] - a[2] * b[2] - a[3] * b[3];
+  double r1 = a[0] * b[1] + b[0] * a[1] + a[3] * b[2] - a[2] * b[3];
+  double r2 = a[0] * b[2] + b[0] * a[2] + a[1] * b[3] - a[3] * b[1];
+  double r3 = a[0] * b[3] + b[0] * a[3] + a[2] * b[1] - a[1] * b[2];
+  c[0] = r0; c[1] = r1; c[2] = r2; c[3] = r3;
+}
+static void su2_mul_ad(double *c, const double *a, const double *b) {
+  double r0 = a[0] * b[0] + a[1] * b[1] + a[2] * b[2] + a[3] * b[3];
+  double r1 = -a[0] * b[1] + b[0] * a[1] - a[3] * b[2] + a[2] * b[3];
+  double r2 = -a[0] * b[2] + b[0] * a[2] - a[1] * b[3] + a[3] * b[1];
+  double r3 = -a[0] * b[3] + b[0] * a[3] - a[2] * b[1] + a[1] * b[2];
+  c[0] = r0; c[1] = r1; c[2] = r2; c[3] = r3;
+}
+static void su2_mul_da(double *c, const double *a, const double *b) {
+  double r0 = a[0] * b[0] + a[1] * b[1] + a[2] * b[2] + a[3] * b[3];
+  double r1 = a[0] * b[1] - b[0] * a[1] - a[3] * b[2] + a[2] * b[3];
+  double r2 = a[0] * b[2] - b[0] * a[2] - a[1] * b[3] + a[3] * b[1];
+  double r3 = a[0] * b[3] - b[0] * a[3] - a[2] * b[1] + a[1] * b[2];
+  c[0] = r0; c[1] = r1; c[2] = r2; c[3] = r3;
+}
+static void su2_proj(double *a) {
+  double rho = sqrt(a[0] * a[0] + a[1] * a[1] + a[2] * a[2] + a[3] * a[3]);
+  for (int k = 0; k < 4; k++)
+    a[k] = a[k] / rho;
+}
+static double su2_conj_tr(const double *a, const double *b) {
+  return a[0] * b[0] + a[1] * b[1] + a[2] * b[2] + a[3] * b[3];
+}
+
+/* ------------------------------------------------------------ su3 */
+#define RE(m, i, j) (m)[(3 * (i) + (j)) * 2]
+#define IM(m, i, j) (m)[(3 * (i) + (j)) * 2 + 1]
+
+static void su3_mul(double *c, const double *a, const double *b) {
+  double r[18];
+  for (int i = 0; i < 3; i++)
+    for (int j = 0; j < 3; j++) {
+      double sr = 0, si = 0;
+      for (int k = 0; k < 3; k++) {
+        double ar = RE(a, i, k), ai = IM(a, i, k), br = RE(b, k, j), bi = IM(b, k, j);
+        sr += ar * br - ai * bi;
+        si += ar * bi + ai * br;
+      }
+      RE(r, i, j) = sr;
+      IM(r, i, j) = si;
+    }
+  memcpy(c, r, sizeof(r));
+}
+static void su3_adjoint(double *c, const double *a) {
+  double r[18];
+  for (int i = 0; i < 3; i++)
+    for (int j = 0; j < 3; j++) {
+      RE(r, i, j) = RE(a, j, i);
+      IM(r, i, j) = -IM(a, j, i);
+    }
+  memcpy(c, r, sizeof(r));
+}
+/* A * B^dag, as Eigen evaluates A * B.adjoint().eval() */
+static void su3_mul_ad(double *c, const double *a, const double *b) {
+  double bd[18];
+  su3_adjoint(bd, b);
+  su3_mul(c, a, bd);
+}
+/* A^dag * B */
+static void su3_mul_da(double *c, const double *a, const double *b) {
+  double ad[18];
+  su3_adjoint(ad, a);
+  su3_mul(c, ad, b);
+}
+static void su3_det(const double *m, double *dr, double *di) {
+  /* cofactor expansion along the first column */
+#define CM(ar, ai, br, bi, rr, ri) do { rr = (ar) * (br) - (ai) * (bi); ri = (ar) * (bi) + (ai) * (br); } while (0)
+  double p1r, p1i, p2r, p2i, c0r, c0i, c1r, c1i, c2r, c2i, tr, ti;
+  CM(RE(m, 1, 1), IM(m, 1, 1), RE(m, 2, 2), IM(m, 2, 2), p1r, p1i);
+  CM(RE(m, 2, 1), IM(m, 2, 1), RE(m, 1, 2), IM(m, 1, 2), p2r, p2i);
+  c0r = p1r - p2r; c0i = p1i - p2i;
+  CM(RE(m, 0, 1), IM(m, 0, 1), RE(m, 2, 2), IM(m, 2, 2), p1r, p1i);
+  CM(RE(m, 2, 1), IM(m, 2, 1), RE(m, 0, 2), IM(m, 0, 2), p2r, p2i);
+  c1r = p1r - p2r; c1i = p1i - p2i;
+  CM(RE(m, 0, 1), IM(m, 0, 1), RE(m, 1, 2), IM(m, 1, 2), p1r, p1i);
+  CM(RE(m, 1, 1), IM(m, 1, 1), RE(m, 0, 2), IM(m, 0, 2), p2r, p2i);
+  c2r = p1r - p2r; c2i = p1i - p2i;
+  CM(RE(m, 0, 0), IM(m, 0, 0), c0r, c0i, *dr, *di);
+  CM(RE(m, 1, 0), IM(m, 1, 0), c1r, c1i, tr, ti);
+  *dr -= tr; *di -= ti;
+  CM(RE(m, 2, 0), IM(m, 2, 0), c2r, c2i, tr, ti);
+  *dr += tr; *di += ti;
+#undef CM
+}
+/* matrix.h:279-292: 6 x [A = 3/2 M - 1/2 M M^dag M; A = (1 - (det A - 1)/3) A] */
+static void su3_proj(double *m) {
+  double a[18], h[18], md[18], t[18];
+  memcpy(a, m, sizeof(a));
+  for (int it = 0; it < 6; it++) {
+    su3_adjoint(md, a);
+    for (int k = 0; k < 18; k++)
+      t[k] = 0.5 * a[k];
+    su3_mul(h, t, md);  /* (0.5 M) M^dag */
+    su3_mul(h, h, a);   /* ... M */
+    for (int k = 0; k < 18; k++)
+      a[k] = 1.5 * a[k] - h[k];
+    double dr, di;
+    su3_det(a, &dr, &di);
+    const double third = 1. / 3;
+    double cr = 1.0 - third * (dr - 1.0), ci = -third * di;
+    for (int i = 0; i < 3; i++)
+      for (int j = 0; j < 3; j++) {
+        double xr = RE(a, i, j), xi = IM(a, i, j);
+        RE(a, i, j) = cr * xr - ci * xi;
+        IM(a, i, j) = cr * xi + ci * xr;
+      }
+  }
+  memcpy(m, a, sizeof(a));
+}
+static double su3_conj_tr(const double *a, const double *b) {
+  double c[18];
+  su3_mul_ad(c, a, b);
+  return (RE(c, 0, 0) + RE(c, 1, 1) + RE(c, 2, 2)) / 3;
+}
+static double su3_tr_real(const double *a) {
+  return (RE(a, 0, 0) + RE(a, 1, 1) + RE(a, 2, 2)) / 3.;
+}
+
+/* ------------------------------------------------------------ group table */
+typedef struct {
+  int ds;
+  void (*mul)(double *, const double *, const double *);
+  void (*mul_ad)(double *, const double *, const double *);
+  void (*mul_da)(double *, const double *, const double *);
+  void (*proj)(double *);
+} group_t;
+
+static const group_t SU2G = {4, su2_mul, su2_mul_ad, su2_mul_da, su2_proj};
+static const group_t SU3G = {18, su3_mul, su3_mul_ad, su3_mul_da, su3_proj};
+
+static const group_t *group_of(int nc) {
+  return nc == 2 ? &SU2G : (nc == 3 ? &SU3G : NULL);
+}
+
+static void axpy(int ds, double *s, double c, const double *a) {
+  for (int k = 0; k < ds; k++)
+    s[k] += c * a[k];
+}
+
+/* staple of smearing_plane_HYP / smearing_APE, added to sum:
+ *  sum += ((alpha/div * (Fnu(x) Fmu(x+nu))) ^ Fnu(x+mu))
+ *  sum += ((alpha/div * (Fnu(x-nu) % Fmu(x-nu))) * Fnu(x-nu+mu))
+ * F*(site) returns the link of a field at a site. */
+typedef const double *(*field_fn)(const void *ctx, long long site);
+
+static void add_staples(const group_t *G, const geom_t *g, double *sum,
+                        long long x, int mu, int nu, field_fn fmu,
+                        const void *cmu, field_fn fnu, const void *cnu,
+                        double coef) {
+  double st[18], t2[18];
+  const int ds = G->ds;
+  long long x_pnu = shift(g, x, nu, 1), x_pmu = shift(g, x, mu, 1);
+  long long x_mnu = shift(g, x, nu, -1), x_mnu_pmu = shift(g, x_mnu, mu, 1);
+  G->mul(st, fnu(cnu, x), fmu(cmu, x_pnu));
+  for (int k = 0; k < ds; k++)
+    st[k] = coef * st[k];
+  G->mul_ad(t2, st, fnu(cnu, x_pmu));
+  for (int k = 0; k < ds; k++)
+    sum[k] = sum[k] + t2[k];
+  G->mul_da(st, fnu(cnu, x_mnu), fmu(cmu, x_mnu));
+  for (int k = 0; k < ds; k++)
+    st[k] = coef * st[k];
+  G->mul(t2, st, fnu(cnu, x_mnu_pmu));
+  for (int k = 0; k < ds; k++)
+    sum[k] = sum[k] + t2[k];
+}
+
+typedef struct {
+  const double *links;
+  int mu;
+  int ds;
+} conf_ctx;
+static const double *conf_link(const void *c, long long site) {
+  const conf_ctx *cc = (const conf_ctx *)c;
+  return cc->links + (4 * site + cc->mu) * cc->ds;
+}
+typedef struct {
+  const double *f;
+  int ds;
+} vec_ctx;
+static const double *vec_link(const void *c, long long site) {
+  const vec_ctx *vc = (const vec_ctx *)c;
+  return vc->f + site * vc->ds;
+}
+
+void or_set_threads(int n) {
+  if (n > 0)
+    omp_set_num_threads(n);
+}
+
+int or_proj_all(int nc, long long n, double *links) {
+  const group_t *G = group_of(nc);
+  if (!G)
+    return -1;
+#pragma omp parallel for
+  for (long long i = 0; i < n; i++)
+    G->proj(links + i * G->ds);
+  return 0;
+}
+
+/* ------------------------------------------------------------ APE */
+int or_ape(int nc, const int dims[4], double *links, double alpha, int steps) {
+  const group_t *G = group_of(nc);
+  if (!G)
+    return -1;
+  geom_t g;
+  geom_init(&g, dims);
+  const int ds = G->ds;
+  const size_t n = (size_t)(4 * g.V * ds);
+  double *sm = (double *)malloc(n * sizeof(double));
+  for (int st = 0; st < steps; st++) {
+    memcpy(sm, links, n * sizeof(double));
+#pragma omp parallel for
+    for (long long x = 0; x < g.V; x++) {
+      for (int mu = 0; mu < 3; mu++) {
+        double S[18];
+        const double *u = links + (4 * x + mu) * ds;
+        for (int k = 0; k < ds; k++)
+          S[k] = (1 - alpha) * u[k];
+        for (int nu = 0; nu < 3; nu++) {
+          if (nu == mu)
+            continue;
+          conf_ctx cmu = {links, mu, ds}, cnu = {links, nu, ds};
+          add_staples(G, &g, S, x, mu, nu, conf_link, &cmu, conf_link, &cnu,
+                      alpha / 4);
+        }
+        G->proj(S);
+        memcpy(sm + (4 * x + mu) * ds, S, ds * sizeof(double));
+      }
+    }
+    memcpy(links, sm, n * sizeof(double));
+  }
+  free(sm);
+  return 0;
+}
+
+/* ------------------------------------------------------------ HYP */
+/* (1-alpha) * U_mu as a per-site vector (HYP_initialize_vector). */
+static double *init_vector(const group_t *G, const geom_t *g, const double *links,
+                           int mu, double alpha) {
+  const int ds = G->ds;
+  double *v = (double *)malloc((size_t)g->V * ds * sizeof(double));
+#pragma omp parallel for
+  for (long long x = 0; x < g->V; x++)
+    for (int k = 0; k < ds; k++)
+      v[x * ds + k] = (1 - alpha) * links[(4 * x + mu) * ds + k];
+  return v;
+}
+
+static void proj_vector(const group_t *G, const geom_t *g, double *v) {
+#pragma omp parallel for
+  for (long long x = 0; x < g->V; x++)
+    G->proj(v + x * G->ds);
+}
+
+/* smearing_plane_HYP on two per-site vectors (smearing.h:343-378). */
+static void plane_vec(const group_t *G, const geom_t *g, double *sm,
+                      const double *fmu, const double *fnu, int mu, int nu,
+                      double alpha, double divisor) {
+  vec_ctx cmu = {fmu, G->ds}, cnu = {fnu, G->ds};
+#pragma omp parallel for
+  for (long long x = 0; x < g->V; x++)
+    add_staples(G, g, sm + x * G->ds, x, mu, nu, vec_link, &cmu, vec_link, &cnu,
+                alpha / divisor);
+}
+
+/* Level-1 field Vbar for tuple (mu, a, b): the one staple direction eta < 3
+ * not in {mu, a, b} (make_step1, smearing.h:401-425). */
+static double *level1(const group_t *G, const geom_t *g, const double *links,
+                      int mu, int a, int b, double alpha3) {
+  double *v = init_vector(G, g, links, mu, alpha3);
+  for (int eta = 0; eta < 3; eta++) {
+    if (eta == mu || eta == a || eta == b)
+      continue;
+    conf_ctx cmu = {links, mu, G->ds}, cnu = {links, eta, G->ds};
+#pragma omp parallel for
+    for (long long x = 0; x < g->V; x++)
+      add_staples(G, g, v + x * G->ds, x, mu, eta, conf_link, &cmu, conf_link,
+                  &cnu, alpha3 / 2);
+  }
+  proj_vector(G, g, v);
+  return v;
+}
+
+int or_hyp(int nc, const int dims[4], double *links, double a1, double a2,
+           double a3, int steps) {
+  const group_t *G = group_of(nc);
+  if (!G)
+    return -1;
+  geom_t g;
+  geom_init(&g, dims);
+  const int ds = G->ds;
+  for (int st = 0; st < steps; st++) {
+    /* level-1 fields: s1[mu][nu] = (mu; nu, t) for spatial mu != nu,
+     * t1[eta] = (t; the two spatial directions other than eta) */
+    double *s1[3][3] = {{0}};
+    double *t1[3] = {0};
+    for (int mu = 0; mu < 3; mu++)
+      for (int nu = 0; nu < 3; nu++)
+        if (mu != nu)
+          s1[mu][nu] = level1(G, &g, links, mu, nu, 3, a3);
+    for (int eta = 0; eta < 3; eta++) {
+      int a = (eta == 0) ? 1 : 0, b = (eta == 2) ? 1 : 2;
+      t1[eta] = level1(G, &g, links, 3, a, b, a3);
+    }
+    double *sm = init_vector(G, &g, links, 3, a1);
+    for (int nu = 0; nu < 3; nu++) {
+      double *l20 = init_vector(G, &g, links, 3, a2);
+      for (int rho = 0; rho < 3; rho++) {
+        if (rho == nu)
+          continue;
+        plane_vec(G, &g, l20, t1[3 - nu - rho], s1[rho][nu], 3, rho, a2, 4);
+      }
+      proj_vector(G, &g, l20);
+      double *l21 = init_vector(G, &g, links, nu, a2);
+      for (int rho = 0; rho < 3; rho++) {
+        if (rho == nu)
+          continue;
+        plane_vec(G, &g, l21, s1[nu][rho], s1[rho][nu], nu, rho, a2, 4);
+      }
+      proj_vector(G, &g, l21);
+      plane_vec(G, &g, sm, l20, l21, 3, nu, a1, 6);
+      free(l20);
+      free(l21);
+    }
+    proj_vector(G, &g, sm);
+#pragma omp parallel for
+    for (long long x = 0; x < g.V; x++)
+      memcpy(links + (4 * x + 3) * ds, sm + x * ds, ds * sizeof(double));
+    free(sm);
+    for (int mu = 0; mu < 3; mu++)
+      for (int nu = 0; nu < 3; nu++)
+        free(s1[mu][nu]);
+    for (int eta = 0; eta < 3; eta++)
+      free(t1[eta]);
+  }
+  return 0;
+}
+
+/* ------------------------------------------------------------ Wilson loops */
+/* lines[x] <- lines[x] * U_mu(x + length mu)  (wilson_lines_prolong) */
+static void prolong(const group_t *G, const geom_t *g, const double *links,
+                    double *lines, int length, int mu) {
+  const int ds = G->ds;
+#pragma omp parallel for
+  for (long long x = 0; x < g->V; x++) {
+    long long y = shift(g, x, mu, length);
+    G->mul(lines + x * ds, lines + x * ds, links + (4 * y + mu) * ds);
+  }
+}
+
+static double *lines_indexed(const group_t *G, const geom_t *g,
+                             const double *links, int length, int mu) {
+  const int ds = G->ds;
+  double *l = (double *)malloc((size_t)g->V * ds * sizeof(double));
+#pragma omp parallel for
+  for (long long x = 0; x < g->V; x++)
+    memcpy(l + x * ds, links + (4 * x + mu) * ds, ds * sizeof(double));
+  for (int i = 1; i < length; i++)
+    prolong(G, g, links, l, i, mu);
+  return l;
+}
+
+int or_wilson(int nc, const int dims[4], const double *links, int rmin,
+              int rmax, int tmin, int tmax, double *out) {
+  const group_t *G = group_of(nc);
+  if (!G || rmin < 1 || tmin < 1 || rmax < rmin || tmax < tmin)
+    return -1;
+  geom_t g;
+  geom_init(&g, dims);
+  const int ds = G->ds;
+  const int nt = tmax - tmin + 1, nr = rmax - rmin + 1;
+  double **tl = (double **)malloc(nt * sizeof(double *));
+  tl[0] = lines_indexed(G, &g, links, tmin, 3);
+  for (int t = tmin + 1; t <= tmax; t++) {
+    tl[t - tmin] = (double *)malloc((size_t)g.V * ds * sizeof(double));
+    memcpy(tl[t - tmin], tl[t - tmin - 1], (size_t)g.V * ds * sizeof(double));
+    prolong(G, &g, links, tl[t - tmin], t - 1, 3);
+  }
+  double *sl[3];
+  for (int mu = 0; mu < 3; mu++)
+    sl[mu] = lines_indexed(G, &g, links, rmin, mu);
+  for (int r = rmin; r <= rmax; r++) {
+    for (int t = tmin; t <= tmax; t++) {
+      const double *L = tl[t - tmin];
+      double result = 0;
+#pragma omp parallel for reduction(+ : result)
+      for (long long x = 0; x < g.V; x++) {
+        long long x2 = shift(&g, x, 3, t);
+        for (int nu = 0; nu < 3; nu++) {
+          long long x3 = shift(&g, x, nu, r);
+          double w[18];
+          if (nc == 3) {
+            /* (L(x) * S(x+T) * L(x+R)^dag * S(x)^dag).tr_real()  (:781-784) */
+            su3_mul(w, L + x * ds, sl[nu] + x2 * ds);
+            su3_mul_ad(w, w, L + x3 * ds);
+            su3_mul_ad(w, w, sl[nu] + x * ds);
+            result += su3_tr_real(w);
+          } else {
+            /* generic form (:735-748) */
+            su2_mul(w, L + x * ds, sl[nu] + x2 * ds);
+            su2_mul_ad(w, w, L + x3 * ds);
+            result += su2_conj_tr(w, sl[nu] + x * ds);
+          }
+        }
+      }
+      out[(t - tmin) * nr + (r - rmin)] = result / (g.V * 3);
+    }
+    for (int mu = 0; mu < 3; mu++)
+      prolong(G, &g, links, sl[mu], r, mu);
+  }
+  for (int i = 0; i < nt; i++)
+    free(tl[i]);
+  free(tl);
+  for (int mu = 0; mu < 3; mu++)
+    free(sl[mu]);
+  return 0;
+}
+
+/* ------------------------------------------------------------ plaquette */
+double or_plaquette(int nc, const int dims[4], const double *links) {
+  const group_t *G = group_of(nc);
+  if (!G)
+    return 0;
+  geom_t g;
+  geom_init(&g, dims);
+  const int ds = G->ds;
+  double sum = 0;
+#pragma omp parallel for reduction(+ : sum)
+  for (long long x = 0; x < g.V; x++) {
+    double p = 0, a[18];
+    for (int mu = 0; mu < 3; mu++)
+      for (int nu = mu + 1; nu < 4; nu++) {
+        long long xm = shift(&g, x, mu, 1), xn = shift(&g, x, nu, 1);
+        G->mul(a, links + (4 * x + mu) * ds, links + (4 * xm + nu) * ds);
+        G->mul_ad(a, a, links + (4 * xn + mu) * ds);
+        p += (nc == 3) ? su3_conj_tr(a, links + (4 * x + nu) * ds)
+                       : su2_conj_tr(a, links + (4 * x + nu) * ds);
+      }
+    sum += p / 6;
+  }
+  return sum / g.V;
+}

@@ -1,0 +1,34 @@
+/*
+ * CPU restatement of the reference's APE/HYP smearing, on-axis Wilson loops
+ * and plaquette, in plain C (FP64).
+ *
+ * TEST INFRASTRUCTURE ONLY: used by tests/, __graft_entry__.smoke() and the
+ * CPU-baseline leg of bench.py as the checker. The product never links it.
+ * Parity pinned against golden fixtures produced by the reference's own code
+ * (oracle/_ref, tests/golden/make_golden.py).
+ *
+ * Links: host array of 4*V links, link index 4*site+mu, site = x + Lx*(y +
+ * Ly*(z + Lz*t)); SU(2) 4 doubles (a0..a3), SU(3) 18 doubles row-major
+ * (element (i,j) at (3i+j)*2 re, +1 im).
+ */
+#ifndef GC_ORACLE_H
+#define GC_ORACLE_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+int or_ape(int nc, const int dims[4], double *links, double alpha, int steps);
+int or_hyp(int nc, const int dims[4], double *links, double alpha1,
+           double alpha2, double alpha3, int steps);
+int or_wilson(int nc, const int dims[4], const double *links, int r_min,
+              int r_max, int time_min, int time_max, double *out);
+double or_plaquette(int nc, const int dims[4], const double *links);
+/* Applies proj() to every link (test helper for the projection alone). */
+int or_proj_all(int nc, long long nlinks, double *links);
+void or_set_threads(int n);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,160 @@
+"""ctypes access to the checkers. TEST INFRASTRUCTURE ONLY.
+
+  port()            -> oracle/liboracle.so  (plain-C restatement, gc_oracle.c)
+  ref("parity")     -> oracle/_ref/libref_parity.so (the reference's own code,
+                       -O2, no fast-math), if it was built here
+  ref("timed")      -> oracle/_ref/libref_timed.so (reference flags -Ofast)
+
+All take/return host link arrays of shape (4V, 4|18) in the row-major layout.
+Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg use this.
+"""
+from __future__ import annotations
+
+import ctypes
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+PORT_LIB = HERE / "liboracle.so"
+REF_LIBS = {"parity": HERE / "_ref" / "libref_parity.so",
+            "timed": HERE / "_ref" / "libref_timed.so"}
+
+_pint = ctypes.POINTER(ctypes.c_int)
+_pdbl = ctypes.POINTER(ctypes.c_double)
+_c_int, _c_dbl = ctypes.c_int, ctypes.c_double
+
+
+def _dims(d):
+    return (ctypes.c_int * 4)(*[int(x) for x in d])
+
+
+def _ptr(a: np.ndarray):
+    assert a.dtype == np.float64 and a.flags["C_CONTIGUOUS"]
+    return a.ctypes.data_as(_pdbl)
+
+
+class _Checker:
+    prefix = ""
+
+    def __init__(self, path: Path):
+        self.path = path
+        self.lib = ctypes.CDLL(str(path))
+        p = self.prefix
+        sig = {
+            f"{p}ape": (_c_int, [_c_int, _pint, _pdbl, _c_dbl, _c_int]),
+            f"{p}hyp": (_c_int, [_c_int, _pint, _pdbl, _c_dbl, _c_dbl, _c_dbl, _c_int]),
+            f"{p}wilson": (_c_int, [_c_int, _pint, _pdbl, _c_int, _c_int, _c_int, _c_int, _pdbl]),
+            f"{p}plaquette": (_c_dbl, [_c_int, _pint, _pdbl]),
+        }
+        for name, (res, args) in sig.items():
+            fn = getattr(self.lib, name)
+            fn.restype, fn.argtypes = res, args
+
+    def _fn(self, name):
+        return getattr(self.lib, self.prefix + name)
+
+    def ape(self, nc, dims, links, alpha, steps=1):
+        assert self._fn("ape")(nc, _dims(dims), _ptr(links), alpha, steps) == 0
+
+    def hyp(self, nc, dims, links, a1, a2, a3, steps=1):
+        assert self._fn("hyp")(nc, _dims(dims), _ptr(links), a1, a2, a3, steps) == 0
+
+    def wilson(self, nc, dims, links, rmin, rmax, tmin, tmax):
+        out = np.empty((tmax - tmin + 1, rmax - rmin + 1), dtype=np.float64)
+        assert self._fn("wilson")(nc, _dims(dims), _ptr(links), rmin, rmax, tmin, tmax,
+                                  _ptr(out)) == 0
+        return out
+
+    def plaquette(self, nc, dims, links):
+        return float(self._fn("plaquette")(nc, _dims(dims), _ptr(links)))
+
+
+class Port(_Checker):
+    prefix = "or_"
+
+    def __init__(self, path=PORT_LIB):
+        super().__init__(path)
+        self.lib.or_set_threads.argtypes = [_c_int]
+        self.lib.or_proj_all.argtypes = [_c_int, ctypes.c_longlong, _pdbl]
+        self.lib.or_proj_all.restype = _c_int
+
+    def set_threads(self, n):
+        self.lib.or_set_threads(int(n))
+
+    def proj_all(self, nc, links):
+        assert self.lib.or_proj_all(nc, links.shape[0], _ptr(links)) == 0
+
+
+class Ref(_Checker):
+    prefix = "ref_"
+
+    def __init__(self, path):
+        super().__init__(path)
+        self.lib.ref_job.restype = _c_int
+        self.lib.ref_job.argtypes = [_c_int, _pint, _pdbl, _c_int, _c_dbl, _c_dbl, _c_dbl,
+                                     _c_int, _c_dbl, _c_int, _c_int, _c_int, _c_int, _pdbl,
+                                     _pdbl]
+        self.lib.ref_num_threads.restype = _c_int
+        self.lib.ref_set_threads.argtypes = [_c_int]
+        self.lib.ref_read.restype = _c_int
+        self.lib.ref_read.argtypes = [_c_int, _pint, ctypes.c_char_p, ctypes.c_char_p, _c_int,
+                                      ctypes.c_char_p, _c_int, _pdbl]
+        self.lib.ref_write_lexicographical.restype = _c_int
+        self.lib.ref_write_lexicographical.argtypes = [_c_int, _pint, _pdbl, ctypes.c_char_p]
+
+    def num_threads(self):
+        return int(self.lib.ref_num_threads())
+
+    def set_threads(self, n):
+        self.lib.ref_set_threads(int(n))
+
+    def job(self, nc, dims, links, hyp_steps, a1, a2, a3, ape_steps, alpha, rmin, rmax,
+            tmin, tmax):
+        """Runs HYP x hyp_steps, APE x ape_steps, W table; returns (W, times[3])."""
+        out = np.zeros((max(tmax - tmin + 1, 1), max(rmax - rmin + 1, 1)), dtype=np.float64)
+        times = np.zeros(3, dtype=np.float64)
+        assert self.lib.ref_job(nc, _dims(dims), _ptr(links), hyp_steps, a1, a2, a3,
+                                ape_steps, alpha, rmin, rmax, tmin, tmax, _ptr(out),
+                                _ptr(times)) == 0
+        return out, times
+
+    def read(self, nc, dims, path, fmt, bytes_skip, precision, convert):
+        n = 4
+        for d in dims:
+            n *= int(d)
+        out = np.empty((n, 4 if nc == 2 else 18), dtype=np.float64)
+        assert self.lib.ref_read(nc, _dims(dims), str(path).encode(), fmt.encode(),
+                                 int(bytes_skip), precision.encode(), int(convert),
+                                 _ptr(out)) == 0
+        return out
+
+    def write_lexicographical(self, nc, dims, links, path):
+        assert self.lib.ref_write_lexicographical(nc, _dims(dims), _ptr(links),
+                                                  str(path).encode()) == 0
+
+
+_port = None
+_refs = {}
+
+
+def port() -> Port:
+    global _port
+    if _port is None:
+        if not PORT_LIB.exists():
+            raise ImportError(f"{PORT_LIB} missing: run `make -C oracle oracle`")
+        _port = Port()
+    return _port
+
+
+def ref_available(kind: str = "parity") -> bool:
+    return REF_LIBS[kind].exists()
+
+
+def ref(kind: str = "parity") -> Ref:
+    if kind not in _refs:
+        if not REF_LIBS[kind].exists():
+            raise ImportError(f"{REF_LIBS[kind]} missing (built only where the reference "
+                              "sources are present)")
+        _refs[kind] = Ref(REF_LIBS[kind])
+    return _refs[kind]

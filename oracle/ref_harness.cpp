@@ -1,0 +1,265 @@
+// C-ABI harness around the reference's OWN templated CPU path, compiled from
+// the reference sources by oracle/Makefile into oracle/_ref/.
+//
+// TEST INFRASTRUCTURE ONLY (the checker and the timed CPU baseline): the
+// product never links this. Every entry point calls the reference functions
+// unchanged:
+//   smearing_APE          lib/cpu/include/smearing.h:115-161
+//   smearing_HYP          lib/cpu/include/smearing.h:480-516
+//   wilson_loop           lib/cpu/include/wilson_loops.h:1047-1074
+//   plaket_site           lib/cpu/include/plaket.h:24-42
+//   Data::read_data_convert / write_data   lib/cpu/include/data.h:193-205,265-338
+//
+// Link exchange layout ("row-major"): link index 4*site+mu with
+// site = x + Lx*(y + Ly*(z + Lz*t)) (indexing.h:111-123); per link the
+// matrix's get_data() order: su2 = (a0,a1,a2,a3), su3 = 18 doubles,
+// element (i,j) at (3*i+j)*2 (re) and +1 (im) (matrix.h:236-243).
+#include "data.h"
+#include "indexing.h"
+#include "matrix.h"
+#include "plaket.h"
+#include "smearing.h"
+#include "wilson_loops.h"
+
+#include <chrono>
+#include <cstring>
+#include <omp.h>
+#include <string>
+
+// The legacy headers declare these as extern (indexing.h:8-13); each reference
+// app defines them in its main translation unit.
+int x_size;
+int y_size;
+int z_size;
+int t_size;
+int size1;
+int size2;
+
+namespace {
+
+typedef DataPatternLexicographical DP;
+
+void set_globals(const int *dims) {
+  x_size = dims[0];
+  y_size = dims[1];
+  z_size = dims[2];
+  t_size = dims[3];
+  size1 = x_size * y_size;
+  size2 = x_size * y_size * z_size;
+}
+
+template <class MT>
+Data::LatticeData<DP, MT> make_conf(const int *dims, const double *links) {
+  Data::LatticeData<DP, MT> conf({dims[0], dims[1], dims[2], dims[3]});
+  const int ds = MT::data_size;
+  std::vector<double> buf(ds);
+  for (size_t i = 0; i < conf.array.size(); i++) {
+    for (int k = 0; k < ds; k++)
+      buf[k] = links[i * ds + k];
+    conf.array[i] = MT(buf);
+  }
+  return conf;
+}
+
+template <class MT>
+void export_conf(Data::LatticeData<DP, MT> &conf, double *links) {
+  const int ds = MT::data_size;
+  for (size_t i = 0; i < conf.array.size(); i++) {
+    std::vector<double> buf = conf.array[i].get_data();
+    for (int k = 0; k < ds; k++)
+      links[i * ds + k] = buf[k];
+  }
+}
+
+template <class MT>
+void wilson_to_table(const std::map<std::tuple<int, int>, double> &w, int rmin,
+                     int rmax, int tmin, int tmax, double *out) {
+  const int nr = rmax - rmin + 1;
+  for (int t = tmin; t <= tmax; t++)
+    for (int r = rmin; r <= rmax; r++)
+      out[(t - tmin) * nr + (r - rmin)] = w.at(std::tuple<int, int>(t, r));
+}
+
+// The reference's plaket() leaves its OpenMP reduction variable uninitialised
+// (plaket.h:85), so its result depends on stack contents. The harness sums the
+// reference's own per-site function plaket_site (plaket.h:24-42) into a zeroed
+// accumulator instead, in the same site order.
+template <class MT> double plaquette(const Data::LatticeData<DP, MT> &conf) {
+  DP dp(conf.lat_dim);
+  double sum = 0;
+#pragma omp parallel for collapse(4) firstprivate(dp) reduction(+ : sum)
+  for (int t = 0; t < dp.lat_dim[3]; t++)
+    for (int z = 0; z < dp.lat_dim[2]; z++)
+      for (int y = 0; y < dp.lat_dim[1]; y++)
+        for (int x = 0; x < dp.lat_dim[0]; x++) {
+          dp.lat_coord = {x, y, z, t};
+          sum += plaket_site(conf, dp);
+        }
+  return sum / dp.get_lattice_size();
+}
+
+double now() {
+  return std::chrono::duration<double>(
+             std::chrono::steady_clock::now().time_since_epoch())
+      .count();
+}
+
+template <class MT>
+int job(const int *dims, double *links, int hyp_steps, double a1, double a2,
+        double a3, int ape_steps, double alpha, int rmin, int rmax, int tmin,
+        int tmax, double *out, double *times) {
+  set_globals(dims);
+  Data::LatticeData<DP, MT> conf = make_conf<MT>(dims, links);
+  double t0 = now();
+  for (int i = 0; i < hyp_steps; i++)
+    smearing_HYP(conf, a1, a2, a3);
+  double t1 = now();
+  for (int i = 0; i < ape_steps; i++)
+    smearing_APE(conf, alpha);
+  double t2 = now();
+  if (rmax >= rmin && tmax >= tmin) {
+    std::map<std::tuple<int, int>, double> w =
+        wilson_loop(conf, rmin, rmax, tmin, tmax);
+    wilson_to_table<MT>(w, rmin, rmax, tmin, tmax, out);
+  }
+  double t3 = now();
+  if (times) {
+    times[0] = t1 - t0;
+    times[1] = t2 - t1;
+    times[2] = t3 - t2;
+  }
+  export_conf(conf, links);
+  return 0;
+}
+
+template <class MT>
+int read_conf(const int *dims, const char *path, const char *format,
+              int bytes_skip, const char *precision, int convert,
+              double *links) {
+  set_globals(dims);
+  Data::LatticeData<DP, MT> conf({dims[0], dims[1], dims[2], dims[3]});
+  Data::read_data_convert(conf, std::string(path), std::string(format),
+                          bytes_skip, std::string(precision), convert != 0);
+  export_conf(conf, links);
+  return 0;
+}
+
+} // namespace
+
+extern "C" {
+
+int ref_num_threads() { return omp_get_max_threads(); }
+
+void ref_set_threads(int n) {
+  if (n > 0)
+    omp_set_num_threads(n);
+}
+
+int ref_ape(int nc, const int *dims, double *links, double alpha, int steps) {
+  double dummy = 0;
+  if (nc == 2)
+    return job<su2>(dims, links, 0, 0, 0, 0, steps, alpha, 1, 0, 1, 0, &dummy,
+                    nullptr);
+  if (nc == 3)
+    return job<su3>(dims, links, 0, 0, 0, 0, steps, alpha, 1, 0, 1, 0, &dummy,
+                    nullptr);
+  return -1;
+}
+
+int ref_hyp(int nc, const int *dims, double *links, double a1, double a2,
+            double a3, int steps) {
+  double dummy = 0;
+  if (nc == 2)
+    return job<su2>(dims, links, steps, a1, a2, a3, 0, 0, 1, 0, 1, 0, &dummy,
+                    nullptr);
+  if (nc == 3)
+    return job<su3>(dims, links, steps, a1, a2, a3, 0, 0, 1, 0, 1, 0, &dummy,
+                    nullptr);
+  return -1;
+}
+
+int ref_wilson(int nc, const int *dims, const double *links, int rmin,
+               int rmax, int tmin, int tmax, double *out) {
+  set_globals(dims);
+  if (nc == 2) {
+    Data::LatticeData<DP, su2> conf = make_conf<su2>(dims, links);
+    wilson_to_table<su2>(wilson_loop(conf, rmin, rmax, tmin, tmax), rmin, rmax,
+                         tmin, tmax, out);
+    return 0;
+  }
+  if (nc == 3) {
+    Data::LatticeData<DP, su3> conf = make_conf<su3>(dims, links);
+    wilson_to_table<su3>(wilson_loop(conf, rmin, rmax, tmin, tmax), rmin, rmax,
+                         tmin, tmax, out);
+    return 0;
+  }
+  return -1;
+}
+
+double ref_plaquette(int nc, const int *dims, const double *links) {
+  set_globals(dims);
+  if (nc == 2)
+    return plaquette(make_conf<su2>(dims, links));
+  if (nc == 3)
+    return plaquette(make_conf<su3>(dims, links));
+  return 0.0;
+}
+
+// Full smear-and-measure job as apps/smearing/smearing.cpp:228-301 runs it
+// (HYP steps, then APE steps, then one W table), without the app's extra W at
+// smearing step 0. times[0..2] = seconds in HYP, APE, W.
+int ref_job(int nc, const int *dims, double *links, int hyp_steps, double a1,
+            double a2, double a3, int ape_steps, double alpha, int rmin,
+            int rmax, int tmin, int tmax, double *out, double *times) {
+  if (nc == 2)
+    return job<su2>(dims, links, hyp_steps, a1, a2, a3, ape_steps, alpha, rmin,
+                    rmax, tmin, tmax, out, times);
+  if (nc == 3)
+    return job<su3>(dims, links, hyp_steps, a1, a2, a3, ape_steps, alpha, rmin,
+                    rmax, tmin, tmax, out, times);
+  return -1;
+}
+
+int ref_read(int nc, const int *dims, const char *path, const char *format,
+             int bytes_skip, const char *precision, int convert,
+             double *links) {
+  if (nc == 2)
+    return read_conf<su2>(dims, path, format, bytes_skip, precision, convert,
+                          links);
+  if (nc == 3)
+    return read_conf<su3>(dims, path, format, bytes_skip, precision, convert,
+                          links);
+  return -1;
+}
+
+// write_data with the lexicographical file pattern, as apps/smearing writes a
+// smeared configuration (smearing.cpp:336-339).
+int ref_write_lexicographical(int nc, const int *dims, const double *links,
+                              const char *path) {
+  set_globals(dims);
+  if (nc == 2) {
+    Data::LatticeData<DP, su2> conf = make_conf<su2>(dims, links);
+    FilePatternLexicographical<4, su2> fp;
+    conf.write_data(std::string(path), fp);
+    return 0;
+  }
+  if (nc == 3) {
+    Data::LatticeData<DP, su3> conf = make_conf<su3>(dims, links);
+    FilePatternLexicographical<4, su3> fp;
+    conf.write_data(std::string(path), fp);
+    return 0;
+  }
+  return -1;
+}
+
+} // extern "C"
+
+// Replacement for the reference's indices_to_delete (smearing.cpp:361-379),
+// whose symbol oracle/Makefile makes weak. The reference function only ever
+// returns an empty list (it never appends), but on the way it reads
+// indices[3] of a 3-element vector, which crashes. Same result, no read.
+std::vector<std::tuple<int, int, int>>
+indices_to_delete(std::vector<std::vector<std::tuple<int, int, int>>> &,
+                  std::vector<std::tuple<int, int, int>> &, int) {
+  return {};
+}
