@@ -1,0 +1,383 @@
+#!/usr/bin/env python
+"""Smear-and-measure throughput on B200.
+
+One step = one smear-and-measure job on one synthetic configuration:
+HYP x1 (alpha 1, 0.75, 0.6) + APE x n (alpha 0.5) + the on-axis W(R,T) table.
+Default workload: SU(3) 24^4, 1 HYP + 20 APE, R,T = 1..12 (the configuration
+the headline metric is quoted on). Metric: smeared+measured sites/s.
+
+  value  : device-resident throughput. Each step restores the unsmeared links
+           from a resident copy (device-to-device) and runs the job; inputs are
+           in HBM when the timed region starts.
+  e2e    : the same job through the public C ABI with HOST buffers: pinned
+           host links -> gc_upload, gc_hyp, gc_ape, gc_wilson_onaxis -> host.
+Between timed steps the L2 cache is flushed by writing a 256 MiB buffer.
+Timing: CUDA events on the stream the kernels run on, max over ranks.
+
+--gpus N (under torchrun): every rank runs the job on its own configuration
+(config index = rank); no data-path collective; weak scaling.
+--impl reference: the reference's own CPU implementation (oracle/_ref, compiled
+from the reference sources) on the host cores, rank 0 only.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+WORKLOADS = {
+    # SU(3) 24^4, 1 HYP + 20 APE, W R,T=1..12 (headline configuration)
+    "su3_24": dict(nc=3, dims=(24, 24, 24, 24), eps=0.25, hyp=(1.0, 0.75, 0.6), ape=20,
+                   alpha=0.5, r=(1, 12), t=(1, 12)),
+    # SU(2) 16^4, 1 HYP + 10 APE, W R,T=1..8 (the reference's CPU-sized case)
+    "su2_16": dict(nc=2, dims=(16, 16, 16, 16), eps=0.3, hyp=(1.0, 0.75, 0.6), ape=10,
+                   alpha=0.5, r=(1, 8), t=(1, 8)),
+    # SU(3) 32^4, 1 HYP + 40 APE, W R,T=1..16 (HBM scaling case)
+    "su3_32": dict(nc=3, dims=(32, 32, 32, 32), eps=0.25, hyp=(1.0, 0.75, 0.6), ape=40,
+                   alpha=0.5, r=(1, 16), t=(1, 16)),
+}
+SEED = 20261203
+L2_FLUSH_BYTES = 256 << 20
+
+
+def link_bytes(nc, form):
+    if nc == 3:
+        return 144 if form == "fp64" else 48
+    return 32 if form == "fp64" else 16
+
+
+def algorithmic(wl, form):
+    """Algorithmic bytes and FP flops per site for each kernel family."""
+    nc = wl["nc"]
+    b = link_bytes(nc, form)
+    mm = 198 if nc == 3 else 28          # one matrix product
+    proj = 3000 if nc == 3 else 11       # one projection
+    nr = wl["r"][1] - wl["r"][0] + 1
+    nt = wl["t"][1] - wl["t"][0] + 1
+    return {
+        "ape": {"bytes": 6 * b, "flops": 3 * (8 * mm + proj)},
+        "hyp": {"bytes": 5 * b, "flops": 96 * mm + 16 * proj},
+        # the fused W kernel reads the 4 link fields once per R (lines stay on
+        # chip); two products + a dot per (x, nu, R, T)
+        "wilson": {"bytes": 4 * b * nr, "flops": 3 * nr * nt * (2 * mm + (36 if nc == 3 else 8))},
+    }
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons, sampled during the timed region."""
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index: int):
+        self.dev = device_index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.dev}", f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            threading.Thread(target=self._read, daemon=True).start()
+        except (OSError, FileNotFoundError):
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx.append(float(parts[2]))
+            except ValueError:
+                continue
+            for n, v in zip(names, parts[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(mx),
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def load_peaks():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def load_traffic():
+    p = ROOT / "profiles" / "roofline_traffic.json"
+    if p.exists():
+        return json.loads(p.read_text())
+    return {}
+
+
+def cpu_baseline(wl, workload, host_links, steps=1, warmup=0):
+    """The reference's own CPU path (oracle/_ref, -Ofast -fopenmp, all host
+    threads) on the same configuration; the C restatement when the reference
+    was not compiled. Returns (sites/s, detail)."""
+    from oracle import py_oracle
+    if py_oracle.ref_available("timed"):
+        chk, kind = py_oracle.ref("timed"), "reference"
+        threads = os.cpu_count() or 1
+        chk.set_threads(threads)
+        cores = chk.num_threads()
+    else:
+        chk, kind = py_oracle.port(), "port"
+        cores = os.cpu_count() or 1
+        chk.set_threads(cores)
+    nc, dims = wl["nc"], wl["dims"]
+    V = int(np.prod(dims))
+    times = []
+    for i in range(warmup + steps):
+        links = host_links.copy()
+        t0 = time.perf_counter()
+        if kind == "reference":
+            chk.job(nc, dims, links, 1, *wl["hyp"], wl["ape"], wl["alpha"],
+                    wl["r"][0], wl["r"][1], wl["t"][0], wl["t"][1])
+        else:
+            chk.hyp(nc, dims, links, *wl["hyp"], 1)
+            chk.ape(nc, dims, links, wl["alpha"], wl["ape"])
+            chk.wilson(nc, dims, links, wl["r"][0], wl["r"][1], wl["t"][0], wl["t"][1])
+        dt = time.perf_counter() - t0
+        if i >= warmup:
+            times.append(dt)
+    total = sum(times)
+    sample = (f"{steps} full job(s) on {workload}: HYP x1 + APE x{wl['ape']} + W "
+              f"R={wl['r'][0]}..{wl['r'][1]} T={wl['t'][0]}..{wl['t'][1]}, FP64, "
+              f"{total:.1f} s of CPU time")
+    return V * steps / total, {"cores": cores, "kind": kind, "sample": sample,
+                               "seconds": total}
+
+
+def run_reference(args, wl, rank):
+    if rank != 0:
+        return 0
+    from general_code_b200 import generate_config
+    host = generate_config(wl["dims"], wl["nc"], wl["eps"], SEED, 0)
+    value, info = cpu_baseline(wl, args.workload, host, steps=args.steps, warmup=args.warmup)
+    V = int(np.prod(wl["dims"]))
+    line = {
+        "impl": "reference", "metric": "smeared+measured sites/s", "value": value,
+        "unit": "sites/s", "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": 1000.0 * info["seconds"] / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": args.workload, "lattice": list(wl["dims"]),
+                   "group": f"SU({wl['nc']})", "hyp_steps": 1, "ape_steps": wl["ape"],
+                   "r_range": list(wl["r"]), "t_range": list(wl["t"]), "sites": V},
+        "cpu_baseline": {"value": value, "unit": "sites/s", "cores": info["cores"],
+                         "kind": info["kind"], "sample": info["sample"]},
+        "e2e": {"value": value, "unit": "sites/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--form", choices=["fp64", "mixed"], default="fp64")
+    ap.add_argument("--workload", choices=sorted(WORKLOADS), default="su3_24")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        ap.error("--warmup must be >= 3")
+    wl = WORKLOADS[args.workload]
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+
+    if args.impl == "reference":
+        return run_reference(args, wl, rank)
+
+    import torch
+    torch.cuda.set_device(local_rank)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                device_id=torch.device("cuda", local_rank))
+
+    from general_code_b200 import Lattice, generate_config, link_size
+
+    nc, dims, form = wl["nc"], wl["dims"], args.form
+    V = int(np.prod(dims))
+    r0, r1 = wl["r"]
+    t0, t1 = wl["t"]
+    stream = torch.cuda.Stream()
+    # pinned host input (the job's input for the end-to-end measurement)
+    host_t = torch.empty((4 * V, link_size(nc)), dtype=torch.float64, pin_memory=True)
+    host = host_t.numpy()
+    generate_config(dims, nc, wl["eps"], SEED, rank, out=host)
+    pristine = Lattice(dims, nc, form)
+    work = Lattice(dims, nc, form)
+    for lat in (pristine, work):
+        lat.set_stream(stream.cuda_stream)
+    pristine.upload(host)
+    pristine.synchronize()
+    flush_buf = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device="cuda")
+
+    def flush():
+        with torch.cuda.stream(stream):
+            flush_buf.fill_(1.0)
+
+    def ev():
+        e = torch.cuda.Event(enable_timing=True)
+        e.record(stream)
+        return e
+
+    def device_step(record):
+        flush()
+        e0 = ev()
+        work.copy_from(pristine)
+        work.hyp(*wl["hyp"], 1)
+        e1 = ev()
+        work.ape(wl["alpha"], wl["ape"])
+        e2 = ev()
+        w = work.wilson_loop(r0, r1, t0, t1)
+        e3 = ev()
+        stream.synchronize()
+        if record is not None:
+            record.append((e0.elapsed_time(e3), e0.elapsed_time(e1), e1.elapsed_time(e2),
+                           e2.elapsed_time(e3)))
+        return w
+
+    def e2e_step(record):
+        flush()
+        e0 = ev()
+        work.upload(host)
+        work.hyp(*wl["hyp"], 1)
+        work.ape(wl["alpha"], wl["ape"])
+        w = work.wilson_loop(r0, r1, t0, t1)
+        e1 = ev()
+        stream.synchronize()
+        if record is not None:
+            record.append(e0.elapsed_time(e1))
+        return w
+
+    def barrier():
+        torch.cuda.synchronize()
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    def max_over_ranks(x):
+        if dist is None:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    for _ in range(args.warmup):
+        device_step(None)
+    sampler = ClockSampler(local_rank)
+    sampler.start()
+    barrier()
+    rec = []
+    for _ in range(args.steps):
+        w = device_step(rec)
+    barrier()
+    for _ in range(args.warmup):
+        e2e_step(None)
+    barrier()
+    rec_e2e = []
+    for _ in range(args.steps):
+        w_e2e = e2e_step(rec_e2e)
+    barrier()
+    clocks = sampler.stop()
+
+    total_ms = max_over_ranks(sum(r[0] for r in rec))
+    total_e2e_ms = max_over_ranks(sum(rec_e2e))
+    hyp_ms = sum(r[1] for r in rec) / args.steps
+    ape_ms = sum(r[2] for r in rec) / args.steps
+    w_ms = sum(r[3] for r in rec) / args.steps
+    assert np.array_equal(w, w_e2e), "device and end-to-end runs disagree"
+
+    if rank != 0:
+        if dist is not None:
+            dist.destroy_process_group()
+        return 0
+
+    alg = algorithmic(wl, form)
+    phases = {"hyp": hyp_ms, "ape": ape_ms / wl["ape"], "wilson": w_ms}
+    phase_total = {"hyp": hyp_ms, "ape": ape_ms, "wilson": w_ms}
+    dom = max(phase_total, key=phase_total.get)
+    per_launch_ms = phases[dom]
+    peak, peak_kind = load_peaks()
+    achieved = alg[dom]["bytes"] * V / (per_launch_ms * 1e-3) / 1e9
+    traffic_tbl = load_traffic().get(f"{dom}:{args.workload}:{form}")
+    value = world * V * args.steps / (total_ms * 1e-3)
+    e2e_value = world * V * args.steps / (total_e2e_ms * 1e-3)
+    line = {
+        "metric": "smeared+measured sites/s", "value": value, "unit": "sites/s",
+        "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": total_ms / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64" if form == "fp64" else "f32/f64",
+        "data": "synthetic",
+        "config": {"workload": args.workload, "form": form, "lattice": list(dims),
+                   "group": f"SU({nc})", "hyp_steps": 1, "hyp_alpha": list(wl["hyp"]),
+                   "ape_steps": wl["ape"], "ape_alpha": wl["alpha"], "r_range": [r0, r1],
+                   "t_range": [t0, t1], "sites": V, "l2": "flushed (256 MiB write) between steps",
+                   "parallelism": f"replicas x{world}"},
+        "phases_ms": {"hyp": hyp_ms, "ape_total": ape_ms, "ape_per_step": ape_ms / wl["ape"],
+                      "wilson": w_ms},
+        "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak,
+                     "peak_kind": peak_kind, "unit": "GB/s", "frac": achieved / peak,
+                     "traffic": (traffic_tbl * V if traffic_tbl else None),
+                     "alg_bytes_per_site": alg[dom]["bytes"],
+                     "fp_flops_per_site": alg[dom]["flops"],
+                     "fp_tflops": alg[dom]["flops"] * V / (per_launch_ms * 1e-3) / 1e12},
+        "e2e": {"value": e2e_value, "unit": "sites/s",
+                "h2d_bytes_per_step": int(host.nbytes),
+                "d2h_bytes_per_step": int(w.nbytes)},
+        "gpu_launches": args.steps * (3 + wl["ape"] + 2) + args.steps * (1 + 3 + wl["ape"] + 2),
+        "clocks": clocks,
+    }
+    if world == 1 and not args.no_cpu_baseline:
+        v, info = cpu_baseline(wl, args.workload, host)
+        line["cpu_baseline"] = {"value": v, "unit": "sites/s", "cores": info["cores"],
+                                "kind": info["kind"], "sample": info["sample"]}
+    print(json.dumps(line), flush=True)
+    pristine.close()
+    work.close()
+    if dist is not None:
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -48,6 +48,7 @@ SIGNATURES = {
     "gc_synchronize": (_c_int, [_p]),
     "gc_upload": (_c_int, [_p, _pdbl, _c_int]),
     "gc_download": (_c_int, [_p, _pdbl, _c_int]),
+    "gc_copy_links": (_c_int, [_p, _p]),
     "gc_ape": (_c_int, [_p, _c_dbl, _c_int]),
     "gc_hyp": (_c_int, [_p, _c_dbl, _c_dbl, _c_dbl, _c_int]),
     "gc_wilson_onaxis": (_c_int, [_p, _c_int, _c_int, _c_int, _c_int, _pdbl]),

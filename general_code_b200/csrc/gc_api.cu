@@ -324,6 +324,40 @@ int gc_download(gc_lattice *h, double *host, int layout) {
   return GC_OK;
 }
 
+int gc_copy_links(gc_lattice *dst, gc_lattice *src) {
+  if (!dst || !src)
+    return fail(dst, GC_ERR_ARG, "null handle");
+  if (dst == src)
+    return GC_OK;
+  int rc = check_ready(src);
+  if (rc)
+    return fail(dst, rc, std::string("source: ") + src->err);
+  bool same = dst->nc == src->nc && dst->prec == src->prec;
+  for (int d = 0; d < 4; d++)
+    same = same && dst->g.L[d] == src->g.L[d];
+  if (!same)
+    return fail(dst, GC_ERR_ARG, "gc_copy_links: handles differ in shape, group or precision");
+  std::scoped_lock lk(dst->mu, src->mu);
+  if (src->stream != dst->stream) {
+    cudaEvent_t ev;
+    cudaError_t e = cudaEventCreateWithFlags(&ev, cudaEventDisableTiming);
+    if (e != cudaSuccess)
+      return cuda_fail(dst, "cudaEventCreate", e);
+    cudaEventRecord(ev, src->stream);
+    cudaStreamWaitEvent(dst->stream, ev, 0);
+    cudaEventDestroy(ev);
+  }
+  const size_t bytes = bytes_per_link(dst->nc, dst->prec) * (size_t)dst->g.V;
+  for (int d = 0; d < 4; d++) {
+    cudaError_t e = cudaMemcpyAsync(dst->cur.f[d], src->cur.f[d], bytes,
+                                    cudaMemcpyDeviceToDevice, dst->stream);
+    if (e != cudaSuccess)
+      return cuda_fail(dst, "cudaMemcpyAsync(copy links)", e);
+  }
+  dst->has_links = true;
+  return GC_OK;
+}
+
 int gc_ape(gc_lattice *h, double alpha, int steps) {
   int rc = check_ready(h);
   if (rc)

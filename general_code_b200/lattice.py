@@ -124,6 +124,10 @@ class Lattice:
         self._check(lib().gc_download(self._h, dbl_ptr(out), _LAYOUT[layout]))
         return out
 
+    def copy_from(self, other: "Lattice") -> None:
+        """Device-to-device copy of other's links (same shape and precision)."""
+        self._check(lib().gc_copy_links(self._h, other.handle))
+
     def generate(self, eps: float, seed: int, index: int = 0, gauge: bool = True) -> None:
         self._check(lib().gc_generate(self._h, float(eps), int(seed) & 0xffffffff,
                                       int(index) & 0xffffffff, int(bool(gauge))))

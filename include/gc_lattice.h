@@ -84,6 +84,11 @@ int gc_upload(gc_lattice *h, const double *host_links, int layout);
 /* Copies the device links back into 4*V host links (layout GC_LAYOUT_*). */
 int gc_download(gc_lattice *h, double *host_links, int layout);
 
+/* Device-to-device copy of all links of src into dst (same dims, nc and
+ * precision), queued on dst's stream after src's queued work. Replaces:
+ * copy-assignment of LatticeData (data.h:78-93), e.g. `smeared = conf`. */
+int gc_copy_links(gc_lattice *dst, gc_lattice *src);
+
 /* One or more APE steps on the spatial links (temporal links unchanged):
  * U'_i = Proj[(1-alpha) U_i + alpha/4 sum_{j != i, j < 3} staples].
  * Replaces: smearing_APE(conf, alpha) (smearing.h:115-161), called steps

@@ -1,0 +1,161 @@
+"""GPU parity: the sm_100a kernels, called through the C ABI, against the
+golden fixtures (made by the reference's own code) and against the C oracle on
+seeded configurations.
+
+FP64 tolerances: links 1e-12 absolute (entries are O(1)); W(R,T) and the
+plaquette 1e-12 relative with a 1e-14 absolute floor (the GPU sums in a
+different, fixed order than the reference's OpenMP reduction).
+"""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+from conftest import golden_cases, load_golden, max_abs, unitarity_error
+from general_code_b200 import GCError, Lattice, generate_config, unit_config
+from general_code_b200 import _lib
+
+pytestmark = pytest.mark.gpu
+CASES = golden_cases()
+W_RTOL, W_ATOL = 1e-12, 1e-14
+LINK_ATOL = 1e-12
+
+
+def assert_w_close(w, ref):
+    np.testing.assert_allclose(w, ref, rtol=W_RTOL, atol=W_ATOL)
+
+
+@pytest.mark.parametrize("name,meta", CASES, ids=[c[0] for c in CASES])
+def test_fp64_matches_reference_fixture(name, meta):
+    g = load_golden(name)
+    nc, dims = meta["nc"], meta["dims"]
+    with Lattice(dims, nc, "fp64") as lat:
+        lat.upload(g["links0"])
+        assert lat.plaquette() == pytest.approx(g["plaquettes"][0], rel=1e-12)
+        lat.hyp(*meta["hyp_alpha"], 1)
+        assert max_abs(lat.download(), g["links_hyp"]) <= LINK_ATOL
+        lat.ape(meta["ape_alpha"], meta["ape_steps"])
+        assert max_abs(lat.download(), g["links_ape"]) <= LINK_ATOL
+        w = lat.wilson_loop(meta["r_min"], meta["r_max"], meta["time_min"], meta["time_max"])
+        assert_w_close(w, g["wilson"])
+        assert lat.plaquette() == pytest.approx(g["plaquettes"][1], rel=1e-12)
+
+
+@pytest.mark.parametrize("nc,dims,eps,hyp,n_ape,rng", [
+    (2, (8, 8, 8, 8), 0.3, (1.0, 0.75, 0.6), 10, (1, 4, 1, 4)),
+    (3, (8, 8, 8, 12), 0.25, (1.0, 0.75, 0.6), 5, (1, 4, 1, 6)),
+    (3, (6, 10, 4, 12), 0.25, (1.0, 1.0, 0.5), 3, (2, 3, 3, 6)),
+    (2, (5, 7, 3, 9), 0.3, (0.8, 0.6, 0.4), 4, (1, 3, 1, 5)),
+])
+def test_fp64_matches_oracle_seeded(port, nc, dims, eps, hyp, n_ape, rng):
+    links = generate_config(dims, nc, eps, 20261203, 7)
+    ref = links.copy()
+    port.hyp(nc, dims, ref, *hyp, 1)
+    port.ape(nc, dims, ref, 0.5, n_ape)
+    w_ref = port.wilson(nc, dims, ref, *rng)
+    with Lattice(dims, nc, "fp64") as lat:
+        lat.upload(links)
+        lat.hyp(*hyp, 1)
+        lat.ape(0.5, n_ape)
+        assert max_abs(lat.download(), ref) <= LINK_ATOL
+        assert_w_close(lat.wilson_loop(*rng), w_ref)
+        assert lat.plaquette() == pytest.approx(port.plaquette(nc, dims, ref), rel=1e-12)
+
+
+@pytest.mark.parametrize("nc", [2, 3])
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_unit_configuration(nc, precision):
+    dims = (4, 6, 4, 8)
+    with Lattice(dims, nc, precision) as lat:
+        lat.upload(unit_config(dims, nc))
+        lat.hyp(1.0, 0.75, 0.6, 1)
+        lat.ape(0.5, 3)
+        np.testing.assert_allclose(lat.wilson_loop(1, 2, 1, 4), 1.0, atol=1e-14)
+        assert lat.plaquette() == pytest.approx(1.0, abs=1e-14)
+        assert max_abs(lat.download(), unit_config(dims, nc)) <= 1e-15
+
+
+@pytest.mark.parametrize("nc", [2, 3])
+def test_long_time_range_uses_r_chunks(port, nc):
+    """nT*nR above the per-block accumulator budget splits R into chunks; T
+    beyond the extent wraps around the periodic lattice."""
+    dims = (4, 4, 4, 4)
+    links = generate_config(dims, nc, 0.2, 5, 0)
+    w_ref = port.wilson(nc, dims, links, 1, 4, 1, 300)
+    with Lattice(dims, nc, "fp64") as lat:
+        lat.upload(links)
+        assert_w_close(lat.wilson_loop(1, 4, 1, 300), w_ref)
+
+
+@pytest.mark.parametrize("nc", [2, 3])
+def test_eigen_layout_round_trip(nc):
+    dims = (4, 4, 4, 6)
+    links = generate_config(dims, nc, 0.3, 1, 0)
+    with Lattice(dims, nc, "fp64") as lat:
+        lat.upload(links)
+        eig = lat.download(layout="eigen")
+        back = lat.download()
+        assert max_abs(back, links) == 0.0
+        if nc == 3:
+            m = links.reshape(-1, 3, 3, 2)
+            assert max_abs(eig.reshape(-1, 3, 3, 2), np.transpose(m, (0, 2, 1, 3))) == 0.0
+        lat.upload(eig, layout="eigen")
+        assert max_abs(lat.download(), links) == 0.0
+
+
+def test_state_and_argument_errors():
+    with Lattice((4, 4, 4, 4), 3) as lat:
+        with pytest.raises(GCError) as e:
+            lat.wilson_loop(1, 2, 1, 2)
+        assert e.value.code == _lib.GC_ERR_STATE
+        lat.upload(unit_config((4, 4, 4, 4), 3))
+        with pytest.raises(GCError) as e:
+            lat.wilson_loop(2, 1, 1, 2)
+        assert e.value.code == _lib.GC_ERR_ARG
+        with pytest.raises(GCError) as e:
+            lat.ape(0.5, -1)
+        assert e.value.code == _lib.GC_ERR_ARG
+
+
+@pytest.mark.parametrize("nc,eps", [(2, 0.3), (3, 0.25)])
+def test_device_generator_matches_host(nc, eps):
+    dims = (6, 4, 4, 8)
+    host = generate_config(dims, nc, eps, 42, 3)
+    with Lattice(dims, nc) as lat:
+        lat.generate(eps, 42, 3)
+        assert max_abs(lat.download(), host) == 0.0
+
+
+@pytest.mark.parametrize("nc,eps", [(2, 0.3), (3, 0.25)])
+def test_mixed_precision_error_budget(port, nc, eps):
+    """Mixed form (FP32 links, FP64 projection and sums) against the FP64
+    oracle: links within 1e-5 and W within 1e-5 relative after HYP + 5 APE."""
+    dims = (8, 8, 8, 8)
+    links = generate_config(dims, nc, eps, 11, 0)
+    ref = links.copy()
+    port.hyp(nc, dims, ref, 1.0, 0.75, 0.6, 1)
+    port.ape(nc, dims, ref, 0.5, 5)
+    w_ref = port.wilson(nc, dims, ref, 1, 4, 1, 4)
+    with Lattice(dims, nc, "mixed") as lat:
+        lat.upload(links)
+        lat.hyp(1.0, 0.75, 0.6, 1)
+        lat.ape(0.5, 5)
+        got = lat.download()
+        assert max_abs(got, ref) < 1e-5
+        assert unitarity_error(nc, got) < 1e-6
+        w = lat.wilson_loop(1, 4, 1, 4)
+    np.testing.assert_allclose(w, w_ref, rtol=1e-5)
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_results_are_deterministic(precision):
+    dims = (8, 8, 8, 8)
+    out = []
+    for _ in range(2):
+        with Lattice(dims, 3, precision) as lat:
+            lat.generate(0.25, 1, 0)
+            lat.hyp(1.0, 0.75, 0.6, 1)
+            lat.ape(0.5, 3)
+            out.append((lat.wilson_loop(1, 4, 1, 4), lat.plaquette()))
+    assert np.array_equal(out[0][0], out[1][0])
+    assert out[0][1] == out[1][1]
