@@ -1,0 +1,176 @@
+// general_code_b200 — C++ drop-in for the reference's smearing / Wilson-loop
+// path. Include this header AFTER the reference's own headers
+// (lib/cpu/include/smearing.h, wilson_loops.h, plaket.h, data.h): it adds
+// non-template overloads with the reference's exact signatures for
+// Data::LatticeData<DataPatternLexicographical, su2|su3>. Overload resolution
+// prefers a non-template function over a template of equal match, so the
+// existing call sites in apps/smearing/smearing.cpp and
+// apps/observables/wilson_loops/wilson_loops.cpp bind to these without
+// further edits.
+//
+// Each call uploads conf.array to the GPU, runs the sm_100a kernels and copies
+// the result back, keeping the reference's semantics (in-place smearing; W
+// returned as std::map keyed (T, R)). There is no CPU fallback: a failure
+// (no sm_100 device, out of memory, ...) throws std::runtime_error with the
+// library's message. Link with libgc_b200.so.
+//
+//   reference signature                                   file:line
+//   smearing_APE(LatticeData&, double)                    smearing.h:115-117
+//   smearing_HYP(LatticeData&, double, double, double)    smearing.h:480-482
+//   wilson_loop(const LatticeData&, int, int, int, int)   wilson_loops.h:1047-1050
+//   wilson_loop(const std::vector<T>&, int, int, int, int)
+//                                              basic_observables.h:108-111
+//   plaket(const LatticeData&)                            plaket.h:83-84
+#pragma once
+
+#include "gc_lattice.h"
+
+#include <array>
+#include <map>
+#include <stdexcept>
+#include <string>
+#include <tuple>
+#include <type_traits>
+#include <vector>
+
+namespace gc_dropin {
+
+template <class MT> struct traits;
+template <> struct traits<su2> {
+  static constexpr int nc = 2;
+  static constexpr int layout = GC_LAYOUT_ROWMAJOR; // a0, a1, a2, a3
+};
+template <> struct traits<su3> {
+  static constexpr int nc = 3;
+  // std::vector<su3> holds one Eigen::Matrix3cd (column-major) per link
+  static constexpr int layout = GC_LAYOUT_EIGEN_COLMAJOR;
+};
+
+inline void check(int rc, gc_lattice *h, const char *what) {
+  if (rc != GC_OK)
+    throw std::runtime_error(std::string("general_code_b200 ") + what + ": " +
+                             gc_last_error(h));
+}
+
+// One device-resident copy of a configuration for the duration of a call.
+template <class MT> class Session {
+public:
+  static_assert(sizeof(MT) == (traits<MT>::nc == 3 ? 18 : 4) * sizeof(double),
+                "link type must be a plain array of doubles");
+  Session(const std::array<int, 4> &dims, const MT *links) {
+    check(gc_lattice_create(dims.data(), traits<MT>::nc, GC_PREC_FP64, &h_),
+          nullptr, "create");
+    int rc = gc_upload(h_, reinterpret_cast<const double *>(links),
+                       traits<MT>::layout);
+    if (rc != GC_OK) {
+      std::string msg = gc_last_error(h_);
+      gc_lattice_destroy(h_);
+      throw std::runtime_error("general_code_b200 upload: " + msg);
+    }
+  }
+  ~Session() { gc_lattice_destroy(h_); }
+  Session(const Session &) = delete;
+  Session &operator=(const Session &) = delete;
+  gc_lattice *get() const { return h_; }
+  void download(MT *links) {
+    check(gc_download(h_, reinterpret_cast<double *>(links), traits<MT>::layout),
+          h_, "download");
+  }
+
+private:
+  gc_lattice *h_ = nullptr;
+};
+
+template <class MT>
+void ape(Data::LatticeData<DataPatternLexicographical, MT> &conf, double alpha) {
+  Session<MT> s(conf.lat_dim, conf.array.data());
+  check(gc_ape(s.get(), alpha, 1), s.get(), "APE");
+  s.download(conf.array.data());
+}
+
+template <class MT>
+void hyp(Data::LatticeData<DataPatternLexicographical, MT> &conf, double a1,
+         double a2, double a3) {
+  Session<MT> s(conf.lat_dim, conf.array.data());
+  check(gc_hyp(s.get(), a1, a2, a3, 1), s.get(), "HYP");
+  s.download(conf.array.data());
+}
+
+template <class MT>
+std::map<std::tuple<int, int>, double>
+wilson(const std::array<int, 4> &dims, const MT *links, int r_min, int r_max,
+       int time_min, int time_max) {
+  std::map<std::tuple<int, int>, double> result;
+  if (r_max < r_min || time_max < time_min)
+    return result;
+  Session<MT> s(dims, links);
+  const int nr = r_max - r_min + 1, nt = time_max - time_min + 1;
+  std::vector<double> w((size_t)nr * nt);
+  check(gc_wilson_onaxis(s.get(), r_min, r_max, time_min, time_max, w.data()),
+        s.get(), "wilson_loop");
+  for (int t = time_min; t <= time_max; t++)
+    for (int r = r_min; r <= r_max; r++)
+      result[std::tuple<int, int>(t, r)] = w[(t - time_min) * nr + (r - r_min)];
+  return result;
+}
+
+template <class MT>
+double plaquette(const Data::LatticeData<DataPatternLexicographical, MT> &conf) {
+  Session<MT> s(conf.lat_dim, conf.array.data());
+  double p = 0;
+  check(gc_plaquette(s.get(), &p), s.get(), "plaket");
+  return p;
+}
+
+} // namespace gc_dropin
+
+// ---------------------------------------------------------------- overloads
+inline void smearing_APE(Data::LatticeData<DataPatternLexicographical, su2> &conf,
+                         double alpha) {
+  gc_dropin::ape(conf, alpha);
+}
+inline void smearing_APE(Data::LatticeData<DataPatternLexicographical, su3> &conf,
+                         double alpha) {
+  gc_dropin::ape(conf, alpha);
+}
+inline void smearing_HYP(Data::LatticeData<DataPatternLexicographical, su2> &conf,
+                         double alpha1, double alpha2, double alpha3) {
+  gc_dropin::hyp(conf, alpha1, alpha2, alpha3);
+}
+inline void smearing_HYP(Data::LatticeData<DataPatternLexicographical, su3> &conf,
+                         double alpha1, double alpha2, double alpha3) {
+  gc_dropin::hyp(conf, alpha1, alpha2, alpha3);
+}
+inline std::map<std::tuple<int, int>, double>
+wilson_loop(const Data::LatticeData<DataPatternLexicographical, su2> &conf,
+            int r_min, int r_max, int time_min, int time_max) {
+  return gc_dropin::wilson(conf.lat_dim, conf.array.data(), r_min, r_max,
+                           time_min, time_max);
+}
+inline std::map<std::tuple<int, int>, double>
+wilson_loop(const Data::LatticeData<DataPatternLexicographical, su3> &conf,
+            int r_min, int r_max, int time_min, int time_max) {
+  return gc_dropin::wilson(conf.lat_dim, conf.array.data(), r_min, r_max,
+                           time_min, time_max);
+}
+// Legacy vector form (basic_observables.h:108-111). The reference reads the
+// lattice size from the globals x_size, y_size, z_size, t_size
+// (indexing.h:8-11), which the calling program must set; so does this one.
+inline std::map<std::tuple<int, int>, double>
+wilson_loop(const std::vector<su2> &conf, int r_min, int r_max, int time_min,
+            int time_max) {
+  return gc_dropin::wilson(std::array<int, 4>{x_size, y_size, z_size, t_size},
+                           conf.data(), r_min, r_max, time_min, time_max);
+}
+inline std::map<std::tuple<int, int>, double>
+wilson_loop(const std::vector<su3> &conf, int r_min, int r_max, int time_min,
+            int time_max) {
+  return gc_dropin::wilson(std::array<int, 4>{x_size, y_size, z_size, t_size},
+                           conf.data(), r_min, r_max, time_min, time_max);
+}
+inline double plaket(const Data::LatticeData<DataPatternLexicographical, su2> &conf) {
+  return gc_dropin::plaquette(conf);
+}
+inline double plaket(const Data::LatticeData<DataPatternLexicographical, su3> &conf) {
+  return gc_dropin::plaquette(conf);
+}
