@@ -53,6 +53,8 @@ SIGNATURES = {
     "gc_hyp": (_c_int, [_p, _c_dbl, _c_dbl, _c_dbl, _c_int]),
     "gc_wilson_onaxis": (_c_int, [_p, _c_int, _c_int, _c_int, _c_int, _pdbl]),
     "gc_plaquette": (_c_int, [_p, _pdbl]),
+    "gc_wilson_onaxis_noalloc": (_c_int, [_pint, _c_int, _c_int, ctypes.POINTER(_p), _c_int,
+                                          _c_int, _c_int, _c_int, _p, _p]),
     "gc_generate": (_c_int, [_p, _c_dbl, _c_uint, _c_uint, _c_int]),
     "gc_generate_host": (_c_int, [_pint, _c_int, _c_dbl, _c_uint, _c_uint, _c_int, _pdbl]),
     "gc_job_device_bytes": (ctypes.c_longlong, [_pint, _c_int, _c_int, _c_int, _c_int]),

@@ -28,6 +28,16 @@ int launch_check(const char *what) {
   return GC_ERR_CUDA;
 }
 
+// For entry points without a handle defined in other files: records the
+// message returned by gc_last_error(NULL); returns code.
+int record_error(int code, const std::string &msg) {
+  std::lock_guard<std::mutex> lk(g_global_err_mu);
+  g_global_err = msg;
+  return code;
+}
+
+const std::string &last_launch_error() { return g_launch_error; }
+
 } // namespace gc
 
 struct gc_lattice {

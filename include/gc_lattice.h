@@ -113,6 +113,30 @@ int gc_hyp(gc_lattice *h, double alpha1, double alpha2, double alpha3,
 int gc_wilson_onaxis(gc_lattice *h, int r_min, int r_max, int time_min,
                      int time_max, double *out);
 
+/* The W(R,T) table of gc_wilson_onaxis for callers that cannot allocate
+ * device memory (an application whose allocator owns the whole device budget,
+ * or a timing-critical loop where cudaMalloc/cudaFree would synchronise the
+ * device). It has no counterpart in the reference. Nothing is allocated: the
+ * caller passes the links as four device buffers it owns (fields[mu], mu =
+ * 0..3, in this library's device layout: FP64 SU(3) = 9 planes of V double2,
+ * plane k = element (k/3, k%3) as (re, im); FP64 SU(2) = 2 planes of V double2,
+ * (a0,a1) then (a2,a3); mixed SU(3) = 3 planes of V float4, (u00,u01),
+ * (u02,u10), (u11,u12); mixed SU(2) = 1 plane of V float4) and a device
+ * buffer out_dev of (time_max-time_min+1)*(r_max-r_min+1) doubles, filled as
+ * gc_wilson_onaxis fills `out`. The work is queued on cuda_stream (a
+ * cudaStream_t as void*, NULL = default stream) and the call returns without
+ * waiting. Working memory is a fixed 16 MiB array in the library's static
+ * device memory, held by every GPU that loads the library until exit; a
+ * lattice for which one value of R does not fit in it is rejected with
+ * GC_ERR_ARG. The first call on a device looks up that array's device address
+ * and must come before any stream capture. All calls share the array: calls
+ * whose work overlaps on the GPU race and must be serialised by the caller.
+ * Errors: gc_last_error(NULL). */
+int gc_wilson_onaxis_noalloc(const int dims[4], int nc, int precision,
+                             const void *const fields[4], int r_min, int r_max,
+                             int time_min, int time_max, double *out_dev,
+                             void *cuda_stream);
+
 /* Average plaquette over the 6 planes (1 for unit links).
  * Replaces: plaket(conf) (plaket.h:83-101). */
 int gc_plaquette(gc_lattice *h, double *out);
