@@ -13,7 +13,8 @@ from pathlib import Path
 
 import numpy as np
 
-LIB_PATH = Path(__file__).resolve().parent / "libgc_b200.so"
+LIB_PATH = Path(os.environ.get("GC_B200_LIB") or
+                Path(__file__).resolve().parent / "libgc_b200.so")
 
 GC_OK = 0
 GC_ERR_ARG = 1

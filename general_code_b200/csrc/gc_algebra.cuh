@@ -20,6 +20,14 @@
 #define GC_HD inline
 #endif
 
+// Fused multiply-add on the device; a*b+c on the host (the host generator is
+// built without FMA instructions, where fma() would be a slow library call).
+#if defined(__CUDA_ARCH__)
+#define GC_FMA(a, b, c) fma((a), (b), (c))
+#else
+#define GC_FMA(a, b, c) ((a) * (b) + (c))
+#endif
+
 namespace gc {
 
 template <class T> struct cx {
@@ -105,16 +113,28 @@ template <class T> GC_HD SU3<T> unit(SU3<T>) {
   return U;
 }
 
+// The complex multiply-accumulates below are written as explicit fused
+// multiply-add chains (one rounding per term instead of a product and an add).
+// This is a different but equally accurate rounding order from the
+// reference's separate product and sum.
 template <class T> GC_HD SU3<T> mul(const SU3<T> &A, const SU3<T> &B) {
   SU3<T> C;
 #pragma unroll
   for (int i = 0; i < 3; i++)
 #pragma unroll
     for (int j = 0; j < 3; j++) {
-      cx<T> s = cmul(A.e[i][0], B.e[0][j]);
-      s = cadd(s, cmul(A.e[i][1], B.e[1][j]));
-      s = cadd(s, cmul(A.e[i][2], B.e[2][j]));
-      C.e[i][j] = s;
+      T re = A.e[i][0].re * B.e[0][j].re;
+      T im = A.e[i][0].re * B.e[0][j].im;
+      re = GC_FMA(-A.e[i][0].im, B.e[0][j].im, re);
+      im = GC_FMA(A.e[i][0].im, B.e[0][j].re, im);
+#pragma unroll
+      for (int k = 1; k < 3; k++) {
+        re = GC_FMA(A.e[i][k].re, B.e[k][j].re, re);
+        re = GC_FMA(-A.e[i][k].im, B.e[k][j].im, re);
+        im = GC_FMA(A.e[i][k].re, B.e[k][j].im, im);
+        im = GC_FMA(A.e[i][k].im, B.e[k][j].re, im);
+      }
+      C.e[i][j] = {re, im};
     }
   return C;
 }
@@ -125,10 +145,18 @@ template <class T> GC_HD SU3<T> mul_ad(const SU3<T> &A, const SU3<T> &B) {
   for (int i = 0; i < 3; i++)
 #pragma unroll
     for (int j = 0; j < 3; j++) {
-      cx<T> s = cmul_c(A.e[i][0], B.e[j][0]);
-      s = cadd(s, cmul_c(A.e[i][1], B.e[j][1]));
-      s = cadd(s, cmul_c(A.e[i][2], B.e[j][2]));
-      C.e[i][j] = s;
+      T re = A.e[i][0].re * B.e[j][0].re;
+      T im = A.e[i][0].im * B.e[j][0].re;
+      re = GC_FMA(A.e[i][0].im, B.e[j][0].im, re);
+      im = GC_FMA(-A.e[i][0].re, B.e[j][0].im, im);
+#pragma unroll
+      for (int k = 1; k < 3; k++) {
+        re = GC_FMA(A.e[i][k].re, B.e[j][k].re, re);
+        re = GC_FMA(A.e[i][k].im, B.e[j][k].im, re);
+        im = GC_FMA(A.e[i][k].im, B.e[j][k].re, im);
+        im = GC_FMA(-A.e[i][k].re, B.e[j][k].im, im);
+      }
+      C.e[i][j] = {re, im};
     }
   return C;
 }
@@ -139,10 +167,18 @@ template <class T> GC_HD SU3<T> mul_da(const SU3<T> &A, const SU3<T> &B) {
   for (int i = 0; i < 3; i++)
 #pragma unroll
     for (int j = 0; j < 3; j++) {
-      cx<T> s = cmulc(A.e[0][i], B.e[0][j]);
-      s = cadd(s, cmulc(A.e[1][i], B.e[1][j]));
-      s = cadd(s, cmulc(A.e[2][i], B.e[2][j]));
-      C.e[i][j] = s;
+      T re = A.e[0][i].re * B.e[0][j].re;
+      T im = A.e[0][i].re * B.e[0][j].im;
+      re = GC_FMA(A.e[0][i].im, B.e[0][j].im, re);
+      im = GC_FMA(-A.e[0][i].im, B.e[0][j].re, im);
+#pragma unroll
+      for (int k = 1; k < 3; k++) {
+        re = GC_FMA(A.e[k][i].re, B.e[k][j].re, re);
+        re = GC_FMA(A.e[k][i].im, B.e[k][j].im, re);
+        im = GC_FMA(A.e[k][i].re, B.e[k][j].im, im);
+        im = GC_FMA(-A.e[k][i].im, B.e[k][j].re, im);
+      }
+      C.e[i][j] = {re, im};
     }
   return C;
 }
@@ -186,36 +222,68 @@ template <class T> GC_HD T conj_tr(const SU3<T> &A, const SU3<T> &B) {
 template <class T> GC_HD T tr_real(const SU3<T> &A) {
   return (A.e[0][0].re + A.e[1][1].re + A.e[2][2].re) / T(3);
 }
+// a*b - c*d for complex numbers, as fused chains
+template <class T> GC_HD cx<T> cmul_sub(cx<T> a, cx<T> b, cx<T> c, cx<T> d) {
+  T re = a.re * b.re;
+  T im = a.re * b.im;
+  re = GC_FMA(-a.im, b.im, re);
+  im = GC_FMA(a.im, b.re, im);
+  re = GC_FMA(-c.re, d.re, re);
+  re = GC_FMA(c.im, d.im, re);
+  im = GC_FMA(-c.re, d.im, im);
+  im = GC_FMA(-c.im, d.re, im);
+  return {re, im};
+}
+// acc + a*b (complex)
+template <class T> GC_HD cx<T> cmadd(cx<T> acc, cx<T> a, cx<T> b) {
+  T re = GC_FMA(a.re, b.re, acc.re);
+  T im = GC_FMA(a.re, b.im, acc.im);
+  re = GC_FMA(-a.im, b.im, re);
+  im = GC_FMA(a.im, b.re, im);
+  return {re, im};
+}
 template <class T> GC_HD cx<T> det(const SU3<T> &m) {
   // cofactor expansion along the first column
-  cx<T> c0 = csub(cmul(m.e[1][1], m.e[2][2]), cmul(m.e[2][1], m.e[1][2]));
-  cx<T> c1 = csub(cmul(m.e[0][1], m.e[2][2]), cmul(m.e[2][1], m.e[0][2]));
-  cx<T> c2 = csub(cmul(m.e[0][1], m.e[1][2]), cmul(m.e[1][1], m.e[0][2]));
+  cx<T> c0 = cmul_sub(m.e[1][1], m.e[2][2], m.e[2][1], m.e[1][2]);
+  cx<T> c1 = cmul_sub(m.e[0][1], m.e[2][2], m.e[2][1], m.e[0][2]);
+  cx<T> c2 = cmul_sub(m.e[0][1], m.e[1][2], m.e[1][1], m.e[0][2]);
   cx<T> d = cmul(m.e[0][0], c0);
-  d = csub(d, cmul(m.e[1][0], c1));
-  d = cadd(d, cmul(m.e[2][0], c2));
+  d = cmadd(d, {-m.e[1][0].re, -m.e[1][0].im}, c1);
+  d = cmadd(d, m.e[2][0], c2);
   return d;
 }
 
 // One Newton-Schulz step toward the unitary polar factor,
 // A <- 3/2 A - 1/2 (A A^dag) A, followed by the determinant phase fix
 // A <- (1 - (det A - 1)/3) A.  H = A A^dag is Hermitian: its upper triangle
-// is computed and mirrored (the mirrored entries equal the full product's).
+// is computed and mirrored. The factor -1/2 is folded into H (exact: a power
+// of two), so B = 3/2 A + (-H/2) A is one fused chain per element.
 template <class T> GC_HD SU3<T> ns_step(const SU3<T> &A) {
   cx<T> H[3][3];
 #pragma unroll
   for (int i = 0; i < 3; i++) {
-    T d = A.e[i][0].re * A.e[i][0].re + A.e[i][0].im * A.e[i][0].im;
-    d += A.e[i][1].re * A.e[i][1].re + A.e[i][1].im * A.e[i][1].im;
-    d += A.e[i][2].re * A.e[i][2].re + A.e[i][2].im * A.e[i][2].im;
-    H[i][i] = {d, T(0)};
+    T d = A.e[i][0].re * A.e[i][0].re;
+    d = GC_FMA(A.e[i][0].im, A.e[i][0].im, d);
+    d = GC_FMA(A.e[i][1].re, A.e[i][1].re, d);
+    d = GC_FMA(A.e[i][1].im, A.e[i][1].im, d);
+    d = GC_FMA(A.e[i][2].re, A.e[i][2].re, d);
+    d = GC_FMA(A.e[i][2].im, A.e[i][2].im, d);
+    H[i][i] = {T(-0.5) * d, T(0)};
 #pragma unroll
     for (int j = i + 1; j < 3; j++) {
-      cx<T> s = cmul_c(A.e[i][0], A.e[j][0]);
-      s = cadd(s, cmul_c(A.e[i][1], A.e[j][1]));
-      s = cadd(s, cmul_c(A.e[i][2], A.e[j][2]));
-      H[i][j] = s;
-      H[j][i] = {s.re, -s.im};
+      T re = A.e[i][0].re * A.e[j][0].re;
+      T im = A.e[i][0].im * A.e[j][0].re;
+      re = GC_FMA(A.e[i][0].im, A.e[j][0].im, re);
+      im = GC_FMA(-A.e[i][0].re, A.e[j][0].im, im);
+#pragma unroll
+      for (int k = 1; k < 3; k++) {
+        re = GC_FMA(A.e[i][k].re, A.e[j][k].re, re);
+        re = GC_FMA(A.e[i][k].im, A.e[j][k].im, re);
+        im = GC_FMA(A.e[i][k].im, A.e[j][k].re, im);
+        im = GC_FMA(-A.e[i][k].re, A.e[j][k].im, im);
+      }
+      H[i][j] = {T(-0.5) * re, T(-0.5) * im};
+      H[j][i] = {T(-0.5) * re, T(0.5) * im};
     }
   }
   SU3<T> B;
@@ -223,11 +291,17 @@ template <class T> GC_HD SU3<T> ns_step(const SU3<T> &A) {
   for (int i = 0; i < 3; i++)
 #pragma unroll
     for (int j = 0; j < 3; j++) {
-      cx<T> s = cmul(H[i][0], A.e[0][j]);
-      s = cadd(s, cmul(H[i][1], A.e[1][j]));
-      s = cadd(s, cmul(H[i][2], A.e[2][j]));
-      B.e[i][j] = {T(1.5) * A.e[i][j].re - T(0.5) * s.re,
-                   T(1.5) * A.e[i][j].im - T(0.5) * s.im};
+      cx<T> s = {T(1.5) * A.e[i][j].re, T(1.5) * A.e[i][j].im};
+#pragma unroll
+      for (int k = 0; k < 3; k++) {
+        if (i == k) { // H_ii is real
+          s.re = GC_FMA(H[i][i].re, A.e[k][j].re, s.re);
+          s.im = GC_FMA(H[i][i].re, A.e[k][j].im, s.im);
+        } else {
+          s = cmadd(s, H[i][k], A.e[k][j]);
+        }
+      }
+      B.e[i][j] = s;
     }
   cx<T> dt = det(B);
   const T third = T(1) / T(3);

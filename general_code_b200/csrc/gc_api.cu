@@ -28,6 +28,11 @@ int launch_check(const char *what) {
   return GC_ERR_CUDA;
 }
 
+int plan_error(const char *what) {
+  g_launch_error = what;
+  return GC_ERR_ARG;
+}
+
 // For entry points without a handle defined in other files: records the
 // message returned by gc_last_error(NULL); returns code.
 int record_error(int code, const std::string &msg) {

@@ -175,5 +175,7 @@ struct Fields4 {
 
 // Launch-status helper used by all host launchers.
 int launch_check(const char *what);
+// Records a launch-planning error (returned by the launcher as GC_ERR_ARG).
+int plan_error(const char *what);
 
 } // namespace gc

@@ -30,7 +30,12 @@ struct WilsonPlan {
   int threads;        // cols_per_block * rows
   int blocks;         // ceil(Vs / cols_per_block) * 3
   size_t smem;        // dynamic shared memory bytes
+  bool fits;          // false when even one column exceeds the budget
 };
+// At most this many (R,T) entries per launch (callers split R into chunks).
+constexpr int kWilsonMaxEntries = 1024;
+// Shared-memory budget for the column storage of one block (bytes).
+constexpr size_t kWilsonColumnBudget = 156 * 1024;
 
 WilsonPlan wilson_plan(const Geom &g, int nr, int nt, int nc, int ct_bytes);
 

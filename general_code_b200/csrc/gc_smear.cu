@@ -60,11 +60,13 @@ __device__ __forceinline__ Nbr neighbours(const Geom &g, int site,
 }
 
 template <class Store, class CT>
-__global__ void __launch_bounds__(128)
+__global__ void __launch_bounds__(128, 4)
     ape_kernel(Geom g, const __grid_constant__ Fields4 in,
                const __grid_constant__ Fields4 out, double alpha) {
-  const int site = blockIdx.x * blockDim.x + threadIdx.x;
-  const int mu = blockIdx.y;
+  // mu varies fastest over blocks, so the three directions of a block of
+  // sites are smeared back to back while their links are in L2.
+  const int mu = blockIdx.x % 3;
+  const int site = (blockIdx.x / 3) * blockDim.x + threadIdx.x;
   if (site >= g.V)
     return;
   using M = typename Store::template M<CT>;
@@ -92,11 +94,11 @@ __constant__ int kL1Mu[9] = {0, 0, 1, 1, 2, 2, 3, 3, 3};
 __constant__ int kL1Eta[9] = {2, 1, 2, 0, 1, 0, 0, 1, 2};
 
 template <class Store, class CT>
-__global__ void __launch_bounds__(128)
+__global__ void __launch_bounds__(128, 4)
     hyp_level1_kernel(Geom g, const __grid_constant__ Fields4 U,
                       const __grid_constant__ HypL1 out, double alpha3) {
-  const int site = blockIdx.x * blockDim.x + threadIdx.x;
-  const int f = blockIdx.y;
+  const int f = blockIdx.x % 9;
+  const int site = (blockIdx.x / 9) * blockDim.x + threadIdx.x;
   if (site >= g.V)
     return;
   using M = typename Store::template M<CT>;
@@ -122,12 +124,12 @@ __device__ __forceinline__ int l1_temporal(int a, int b) { return 6 + (3 - a - b
 //   0..2 : Vtilde_{t;nu}, nu = f       (smearing.h:433-450)
 //   3..5 : Vtilde_{nu;t}, nu = f - 3   (smearing.h:455-466)
 template <class Store, class CT>
-__global__ void __launch_bounds__(128)
+__global__ void __launch_bounds__(128, 4)
     hyp_level2_kernel(Geom g, const __grid_constant__ Fields4 U,
                       const __grid_constant__ HypL1 l1,
                       const __grid_constant__ HypL2 out, double alpha2) {
-  const int site = blockIdx.x * blockDim.x + threadIdx.x;
-  const int f = blockIdx.y;
+  const int f = blockIdx.x % 6;
+  const int site = (blockIdx.x / 6) * blockDim.x + threadIdx.x;
   if (site >= g.V)
     return;
   using M = typename Store::template M<CT>;
@@ -184,8 +186,8 @@ constexpr int kSmearBlock = 128;
 template <class Store, class CT>
 int launch_ape(const Geom &g, const Fields4 &in, const Fields4 &out,
                double alpha, cudaStream_t s) {
-  dim3 grid((g.V + kSmearBlock - 1) / kSmearBlock, 3);
-  ape_kernel<Store, CT><<<grid, kSmearBlock, 0, s>>>(g, in, out, alpha);
+  const unsigned nb = (g.V + kSmearBlock - 1) / kSmearBlock;
+  ape_kernel<Store, CT><<<nb * 3, kSmearBlock, 0, s>>>(g, in, out, alpha);
   return launch_check("ape_kernel");
 }
 
@@ -194,11 +196,11 @@ int launch_hyp(const Geom &g, const Fields4 &U, const HypL1 &l1,
                const HypL2 &l2, void *out_t, double a1, double a2, double a3,
                cudaStream_t s) {
   const int nb = (g.V + kSmearBlock - 1) / kSmearBlock;
-  hyp_level1_kernel<Store, CT><<<dim3(nb, 9), kSmearBlock, 0, s>>>(g, U, l1, a3);
+  hyp_level1_kernel<Store, CT><<<nb * 9, kSmearBlock, 0, s>>>(g, U, l1, a3);
   int rc = launch_check("hyp_level1_kernel");
   if (rc)
     return rc;
-  hyp_level2_kernel<Store, CT><<<dim3(nb, 6), kSmearBlock, 0, s>>>(g, U, l1, l2, a2);
+  hyp_level2_kernel<Store, CT><<<nb * 6, kSmearBlock, 0, s>>>(g, U, l1, l2, a2);
   rc = launch_check("hyp_level2_kernel");
   if (rc)
     return rc;

@@ -7,7 +7,8 @@
 //
 // Here one block owns `cols` spatial columns (s, nu) over all t. The space
 // lines S(s,t,R) of its columns live in shared memory and are extended by one
-// link per R. For every corner (s,t0) a thread walks T with the exact
+// link per R; the columns' own time links U_t(s,t) are staged in shared
+// memory once. For every corner (s,t0) a thread walks T with the exact
 // recursion
 //     K_0 = S(x,R),   K_T = U_t(x+(T-1)t)^dag K_{T-1} U_t(x+R nu+(T-1)t),
 // so that K_T = L(x,T)^dag S(x,R) L(x+R nu,T), and the loop trace is
@@ -104,6 +105,8 @@ __global__ void __launch_bounds__(256)
   double *wacc = reinterpret_cast<double *>(smem_raw);         // [nwarps][nr*nt]
   CT *scol = reinterpret_cast<CT *>(wacc + (size_t)nwarps * nr * nt);
   const int sstride = Lt * cols;                                // matrices in scol
+  // the block's own time links U_t(s, t), reused for every R and T
+  CT *ucol = scol + (size_t)NCOMP * sstride;
 
   const int tid = threadIdx.x;
   const int warp = tid >> 5, lane = tid & 31;
@@ -122,6 +125,14 @@ __global__ void __launch_bounds__(256)
   const size_t V = g.V;
   const void *Unu = U.f[nu];
   const void *Ut = U.f[3];
+  if (active) {
+#pragma unroll 1
+    for (int k = 0; k < kt; k++) {
+      const int t0 = row + k * rows;
+      sm_store(ucol, sstride, t0 * cols + c,
+               Store::template load<CT>(Ut, V, s + t0 * g.Vs));
+    }
+  }
   __syncthreads();
 
 #pragma unroll 1
@@ -151,7 +162,7 @@ __global__ void __launch_bounds__(256)
           int tt = t0 + T - 1;
           tt -= (tt / Lt) * Lt;
           if (active) {
-            M a = Store::template load<CT>(Ut, V, s + tt * g.Vs);
+            M a = sm_load(ucol, sstride, tt * cols + c, (M *)nullptr);
             M b = Store::template load<CT>(Ut, V, sR + tt * g.Vs);
             K = mul(mul_da(a, K), b);
           }
@@ -251,21 +262,32 @@ int largest_divisor_upto(int n, int cap) {
 
 } // namespace
 
+// The block shape depends only on Lt and the group, never on the R/T ranges
+// or the compute type, so every caller that sizes the per-block partials
+// from a plan gets the same block count as the launch. Columns per block are
+// limited so that the shared column storage (FP64 worst case) plus the
+// largest per-warp accumulator set (8 warps x 1024 (R,T) entries) fits in a
+// block's shared memory.
 WilsonPlan wilson_plan(const Geom &g, int nr, int nt, int nc, int ct_bytes) {
   WilsonPlan p;
   const int Lt = g.L[3];
+  const int ncomp = (nc == 3) ? 18 : 4;
   p.rows = largest_divisor_upto(Lt, 32);
   p.cols_per_block = 256 / p.rows;
   if (p.cols_per_block < 1)
     p.cols_per_block = 1;
+  const size_t col_bytes = 2 * (size_t)ncomp * Lt * sizeof(double);
+  while (p.cols_per_block > 1 && p.cols_per_block * col_bytes > kWilsonColumnBudget)
+    p.cols_per_block--;
   const int active = p.cols_per_block * p.rows;
   p.threads = ((active + 31) / 32) * 32;
   const int colblocks = (g.Vs + p.cols_per_block - 1) / p.cols_per_block;
   p.blocks = colblocks * 3;
   const int nwarps = p.threads / 32;
-  const int ncomp = (nc == 3) ? 18 : 4;
+  // per-warp accumulators + space lines + own time links
   p.smem = (size_t)nwarps * nr * nt * sizeof(double) +
-           (size_t)ncomp * Lt * p.cols_per_block * ct_bytes;
+           2 * (size_t)ncomp * Lt * p.cols_per_block * ct_bytes;
+  p.fits = p.cols_per_block * col_bytes <= kWilsonColumnBudget;
   return p;
 }
 
@@ -281,6 +303,9 @@ int launch_wilson(const Geom &g, const Fields4 &U, int rmin, int rmax,
                   cudaStream_t s) {
   const int nr = rmax - rmin + 1, nt = tmax - tmin + 1;
   WilsonPlan p = wilson_plan(g, nr, nt, Store::NC, (int)sizeof(CT));
+  if (!p.fits || nr * nt > kWilsonMaxEntries)
+    return plan_error("wilson_kernel: time extent or (R,T) range too large for "
+                      "one block's shared memory");
   if (p.smem > 48 * 1024) {
     cudaError_t e = cudaFuncSetAttribute(
         wilson_kernel<Store, CT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
