@@ -34,8 +34,9 @@ struct WilsonPlan {
 };
 // At most this many (R,T) entries per launch (callers split R into chunks).
 constexpr int kWilsonMaxEntries = 1024;
-// Shared-memory budget for the column storage of one block (bytes).
-constexpr size_t kWilsonColumnBudget = 156 * 1024;
+// Shared-memory budget for the column storage of one block (bytes), sized
+// so that two blocks fit on an SM with their per-warp accumulators.
+constexpr size_t kWilsonColumnBudget = 96 * 1024;
 
 WilsonPlan wilson_plan(const Geom &g, int nr, int nt, int nc, int ct_bytes);
 

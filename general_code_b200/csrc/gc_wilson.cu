@@ -8,7 +8,9 @@
 // Here one block owns `cols` spatial columns (s, nu) over all t. The space
 // lines S(s,t,R) of its columns live in shared memory and are extended by one
 // link per R; the columns' own time links U_t(s,t) are staged in shared
-// memory once. For every corner (s,t0) a thread walks T with the exact
+// memory once and the neighbour columns' time links U_t(s+R nu,t) once per R,
+// so the T walk reads only shared memory. For every corner (s,t0) a thread
+// walks T with the exact
 // recursion
 //     K_0 = S(x,R),   K_T = U_t(x+(T-1)t)^dag K_{T-1} U_t(x+R nu+(T-1)t),
 // so that K_T = L(x,T)^dag S(x,R) L(x+R nu,T), and the loop trace is
@@ -27,47 +29,55 @@ namespace gc {
 
 namespace {
 
-template <class M> struct Comps;
-template <class T> struct Comps<SU3<T>> {
-  static constexpr int n = 18;
+// Shared-memory matrices are stored element-major as 2-vectors: complex
+// element k (or quaternion pair k) of matrix i at sm[k*stride + i], one
+// 8-byte (FP32) or 16-byte (FP64) load per element, consecutive threads on
+// consecutive addresses.
+template <class T> struct V2;
+template <> struct V2<double> {
+  using type = double2;
 };
-template <class T> struct Comps<SU2<T>> {
-  static constexpr int n = 4;
+template <> struct V2<float> {
+  using type = float2;
 };
 
-// Shared-memory matrices are stored component-major: comp k of matrix i at
-// sm[k*stride + i], so consecutive threads touch consecutive words.
 template <class T>
-__device__ __forceinline__ void sm_store(T *sm, int stride, int i,
-                                         const SU3<T> &m) {
-#pragma unroll
-  for (int k = 0; k < 9; k++) {
-    sm[(2 * k) * stride + i] = m.e[k / 3][k % 3].re;
-    sm[(2 * k + 1) * stride + i] = m.e[k / 3][k % 3].im;
-  }
-}
-template <class T>
-__device__ __forceinline__ SU3<T> sm_load(const T *sm, int stride, int i,
-                                          SU3<T> *) {
-  SU3<T> m;
+__device__ __forceinline__ void sm_store(typename V2<T>::type *sm, int stride,
+                                         int i, const SU3<T> &m) {
 #pragma unroll
   for (int k = 0; k < 9; k++)
-    m.e[k / 3][k % 3] = {sm[(2 * k) * stride + i], sm[(2 * k + 1) * stride + i]};
+    sm[k * stride + i] = {m.e[k / 3][k % 3].re, m.e[k / 3][k % 3].im};
+}
+template <class T>
+__device__ __forceinline__ SU3<T> sm_load(const typename V2<T>::type *sm,
+                                          int stride, int i, SU3<T> *) {
+  SU3<T> m;
+#pragma unroll
+  for (int k = 0; k < 9; k++) {
+    const auto v = sm[k * stride + i];
+    m.e[k / 3][k % 3] = {v.x, v.y};
+  }
   return m;
 }
 template <class T>
-__device__ __forceinline__ void sm_store(T *sm, int stride, int i,
-                                         const SU2<T> &m) {
-  sm[i] = m.a0;
-  sm[stride + i] = m.a1;
-  sm[2 * stride + i] = m.a2;
-  sm[3 * stride + i] = m.a3;
+__device__ __forceinline__ void sm_store(typename V2<T>::type *sm, int stride,
+                                         int i, const SU2<T> &m) {
+  sm[i] = {m.a0, m.a1};
+  sm[stride + i] = {m.a2, m.a3};
 }
 template <class T>
-__device__ __forceinline__ SU2<T> sm_load(const T *sm, int stride, int i,
-                                          SU2<T> *) {
-  return {sm[i], sm[stride + i], sm[2 * stride + i], sm[3 * stride + i]};
+__device__ __forceinline__ SU2<T> sm_load(const typename V2<T>::type *sm,
+                                          int stride, int i, SU2<T> *) {
+  const auto a = sm[i], b = sm[stride + i];
+  return {a.x, a.y, b.x, b.y};
 }
+template <class M> struct Elems;
+template <class T> struct Elems<SU3<T>> {
+  static constexpr int n = 9;
+};
+template <class T> struct Elems<SU2<T>> {
+  static constexpr int n = 2;
+};
 
 __device__ __forceinline__ double warp_sum(double v) {
 #pragma unroll
@@ -76,20 +86,23 @@ __device__ __forceinline__ double warp_sum(double v) {
   return v;
 }
 
-// Re Tr(A B^dag)/N evaluated in FP64 whatever the compute type.
+// Re Tr(A B^dag)/N in the compute type, returned in FP64 for accumulation.
 template <class T> __device__ __forceinline__ double conj_tr_d(const SU3<T> &a, const SU3<T> &b) {
-  double s = 0;
+  T s = a.e[0][0].re * b.e[0][0].re;
+  s = GC_FMA(a.e[0][0].im, b.e[0][0].im, s);
 #pragma unroll
-  for (int i = 0; i < 3; i++)
-#pragma unroll
-    for (int j = 0; j < 3; j++)
-      s += double(a.e[i][j].re) * double(b.e[i][j].re) +
-           double(a.e[i][j].im) * double(b.e[i][j].im);
-  return s / 3.0;
+  for (int k = 1; k < 9; k++) {
+    s = GC_FMA(a.e[k / 3][k % 3].re, b.e[k / 3][k % 3].re, s);
+    s = GC_FMA(a.e[k / 3][k % 3].im, b.e[k / 3][k % 3].im, s);
+  }
+  return double(s) / 3.0;
 }
 template <class T> __device__ __forceinline__ double conj_tr_d(const SU2<T> &a, const SU2<T> &b) {
-  return double(a.a0) * double(b.a0) + double(a.a1) * double(b.a1) +
-         double(a.a2) * double(b.a2) + double(a.a3) * double(b.a3);
+  T s = a.a0 * b.a0;
+  s = GC_FMA(a.a1, b.a1, s);
+  s = GC_FMA(a.a2, b.a2, s);
+  s = GC_FMA(a.a3, b.a3, s);
+  return double(s);
 }
 
 template <class Store, class CT>
@@ -97,16 +110,20 @@ __global__ void __launch_bounds__(256)
     wilson_kernel(Geom g, const __grid_constant__ Fields4 U, int rmin, int rmax, int tmin, int tmax,
                   int cols, int rows, double *partials) {
   using M = typename Store::template M<CT>;
-  constexpr int NCOMP = Comps<M>::n;
+  using VT = typename V2<CT>::type;
+  constexpr int NE = Elems<M>::n;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const int Lt = g.L[3];
   const int nr = rmax - rmin + 1, nt = tmax - tmin + 1;
   const int nwarps = blockDim.x >> 5;
   double *wacc = reinterpret_cast<double *>(smem_raw);         // [nwarps][nr*nt]
-  CT *scol = reinterpret_cast<CT *>(wacc + (size_t)nwarps * nr * nt);
-  const int sstride = Lt * cols;                                // matrices in scol
+  const int sstride = Lt * cols;                                // matrices per set
+  // space lines S(s,t,R) of the block's columns
+  VT *scol = reinterpret_cast<VT *>(wacc + (size_t)nwarps * nr * nt);
   // the block's own time links U_t(s, t), reused for every R and T
-  CT *ucol = scol + (size_t)NCOMP * sstride;
+  VT *ucol = scol + (size_t)NE * sstride;
+  // the time links of the neighbour columns U_t(s + R nu, t), one R at a time
+  VT *ncol = ucol + (size_t)NE * sstride;
 
   const int tid = threadIdx.x;
   const int warp = tid >> 5, lane = tid & 31;
@@ -137,38 +154,41 @@ __global__ void __launch_bounds__(256)
 
 #pragma unroll 1
   for (int R = 1; R <= rmax; R++) {
-    // Extend the space lines of this thread's corners by one link.
+    // Extend the space lines of this thread's corners by one link, and stage
+    // the neighbour column's time links for this R.
     if (active) {
       const int sl = s + fwd_off(g, xs[nu], nu, R - 1);
+      const int sR = s + fwd_off(g, xs[nu], nu, R);
 #pragma unroll 1
       for (int k = 0; k < kt; k++) {
         const int t0 = row + k * rows;
         M u = Store::template load<CT>(Unu, V, sl + t0 * g.Vs);
         M sn = (R == 1) ? u : mul(sm_load(scol, sstride, t0 * cols + c, (M *)nullptr), u);
         sm_store(scol, sstride, t0 * cols + c, sn);
+        if (R >= rmin)
+          sm_store(ncol, sstride, t0 * cols + c,
+                   Store::template load<CT>(Ut, V, sR + t0 * g.Vs));
       }
     }
     __syncthreads();
     if (R >= rmin) {
-      const int sR = s + (active ? fwd_off(g, xs[nu], nu, R) : 0);
       double *wrow = wacc + (size_t)warp * nr * nt + (R - rmin) * nt;
 #pragma unroll 1
       for (int k = 0; k < kt; k++) {
         const int t0 = row + k * rows;
         M K = active ? sm_load(scol, sstride, t0 * cols + c, (M *)nullptr)
                      : unit(M());
+        int tt = t0; // (t0 + T - 1) mod Lt
 #pragma unroll 1
         for (int T = 1; T <= tmax; T++) {
-          int tt = t0 + T - 1;
-          tt -= (tt / Lt) * Lt;
+          int tu = tt + 1; // (t0 + T) mod Lt
+          tu = (tu == Lt) ? 0 : tu;
           if (active) {
             M a = sm_load(ucol, sstride, tt * cols + c, (M *)nullptr);
-            M b = Store::template load<CT>(Ut, V, sR + tt * g.Vs);
+            M b = sm_load(ncol, sstride, tt * cols + c, (M *)nullptr);
             K = mul(mul_da(a, K), b);
           }
           if (T >= tmin) {
-            int tu = tt + 1;
-            tu = (tu == Lt) ? 0 : tu;
             double term = active
                 ? conj_tr_d(sm_load(scol, sstride, tu * cols + c, (M *)nullptr), K)
                 : 0.0;
@@ -176,6 +196,7 @@ __global__ void __launch_bounds__(256)
             if (lane == 0)
               wrow[T - tmin] += term;
           }
+          tt = tu;
         }
       }
     }
@@ -276,7 +297,7 @@ WilsonPlan wilson_plan(const Geom &g, int nr, int nt, int nc, int ct_bytes) {
   p.cols_per_block = 256 / p.rows;
   if (p.cols_per_block < 1)
     p.cols_per_block = 1;
-  const size_t col_bytes = 2 * (size_t)ncomp * Lt * sizeof(double);
+  const size_t col_bytes = 3 * (size_t)ncomp * Lt * sizeof(double);
   while (p.cols_per_block > 1 && p.cols_per_block * col_bytes > kWilsonColumnBudget)
     p.cols_per_block--;
   const int active = p.cols_per_block * p.rows;
@@ -284,9 +305,9 @@ WilsonPlan wilson_plan(const Geom &g, int nr, int nt, int nc, int ct_bytes) {
   const int colblocks = (g.Vs + p.cols_per_block - 1) / p.cols_per_block;
   p.blocks = colblocks * 3;
   const int nwarps = p.threads / 32;
-  // per-warp accumulators + space lines + own time links
+  // per-warp accumulators + space lines + own and neighbour time links
   p.smem = (size_t)nwarps * nr * nt * sizeof(double) +
-           2 * (size_t)ncomp * Lt * p.cols_per_block * ct_bytes;
+           3 * (size_t)ncomp * Lt * p.cols_per_block * ct_bytes;
   p.fits = p.cols_per_block * col_bytes <= kWilsonColumnBudget;
   return p;
 }
