@@ -11,6 +11,10 @@ the headline metric is quoted on). Metric: smeared+measured sites/s.
            in HBM when the timed region starts.
   e2e    : the same job through the public C ABI with HOST buffers: pinned
            host links -> gc_upload, gc_hyp, gc_ape, gc_wilson_onaxis -> host.
+Both forms are timed on the same configuration (--form both, the default):
+the headline is the mixed form (FP32 links, FP64 projection and sums); the
+FP64 form is reported under "forms", with the largest relative difference of
+the two W(R,T) tables (the mixed form's error against FP64).
 Between timed steps the L2 cache is flushed by writing a 256 MiB buffer.
 Timing: CUDA events on the stream the kernels run on, max over ranks.
 
@@ -209,7 +213,7 @@ def main():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--form", choices=["fp64", "mixed"], default="fp64")
+    ap.add_argument("--form", choices=["both", "fp64", "mixed"], default="both")
     ap.add_argument("--workload", choices=sorted(WORKLOADS), default="su3_24")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()
@@ -234,7 +238,7 @@ def main():
 
     from general_code_b200 import Lattice, generate_config, link_size
 
-    nc, dims, form = wl["nc"], wl["dims"], args.form
+    nc, dims = wl["nc"], wl["dims"]
     V = int(np.prod(dims))
     r0, r1 = wl["r"]
     t0, t1 = wl["t"]
@@ -243,12 +247,6 @@ def main():
     host_t = torch.empty((4 * V, link_size(nc)), dtype=torch.float64, pin_memory=True)
     host = host_t.numpy()
     generate_config(dims, nc, wl["eps"], SEED, rank, out=host)
-    pristine = Lattice(dims, nc, form)
-    work = Lattice(dims, nc, form)
-    for lat in (pristine, work):
-        lat.set_stream(stream.cuda_stream)
-    pristine.upload(host)
-    pristine.synchronize()
     flush_buf = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device="cuda")
 
     def flush():
@@ -259,35 +257,6 @@ def main():
         e = torch.cuda.Event(enable_timing=True)
         e.record(stream)
         return e
-
-    def device_step(record):
-        flush()
-        e0 = ev()
-        work.copy_from(pristine)
-        work.hyp(*wl["hyp"], 1)
-        e1 = ev()
-        work.ape(wl["alpha"], wl["ape"])
-        e2 = ev()
-        w = work.wilson_loop(r0, r1, t0, t1)
-        e3 = ev()
-        stream.synchronize()
-        if record is not None:
-            record.append((e0.elapsed_time(e3), e0.elapsed_time(e1), e1.elapsed_time(e2),
-                           e2.elapsed_time(e3)))
-        return w
-
-    def e2e_step(record):
-        flush()
-        e0 = ev()
-        work.upload(host)
-        work.hyp(*wl["hyp"], 1)
-        work.ape(wl["alpha"], wl["ape"])
-        w = work.wilson_loop(r0, r1, t0, t1)
-        e1 = ev()
-        stream.synchronize()
-        if record is not None:
-            record.append(e0.elapsed_time(e1))
-        return w
 
     def barrier():
         torch.cuda.synchronize()
@@ -302,82 +271,147 @@ def main():
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         return float(t.item())
 
-    for _ in range(args.warmup):
-        device_step(None)
+    def measure(form):
+        """Times the job in one form: device-resident steps, then end-to-end steps."""
+        pristine = Lattice(dims, nc, form)
+        work = Lattice(dims, nc, form)
+        for lat in (pristine, work):
+            lat.set_stream(stream.cuda_stream)
+        pristine.upload(host)
+        pristine.synchronize()
+
+        def device_step(record):
+            flush()
+            e0 = ev()
+            work.copy_from(pristine)
+            work.hyp(*wl["hyp"], 1)
+            e1 = ev()
+            work.ape(wl["alpha"], wl["ape"])
+            e2 = ev()
+            w = work.wilson_loop(r0, r1, t0, t1)
+            e3 = ev()
+            stream.synchronize()
+            if record is not None:
+                record.append((e0.elapsed_time(e3), e0.elapsed_time(e1), e1.elapsed_time(e2),
+                               e2.elapsed_time(e3)))
+            return w
+
+        def e2e_step(record):
+            flush()
+            e0 = ev()
+            work.upload(host)
+            work.hyp(*wl["hyp"], 1)
+            work.ape(wl["alpha"], wl["ape"])
+            w = work.wilson_loop(r0, r1, t0, t1)
+            e1 = ev()
+            stream.synchronize()
+            if record is not None:
+                record.append(e0.elapsed_time(e1))
+            return w
+
+        for _ in range(args.warmup):
+            device_step(None)
+        barrier()
+        rec = []
+        for _ in range(args.steps):
+            w = device_step(rec)
+        barrier()
+        for _ in range(args.warmup):
+            e2e_step(None)
+        barrier()
+        rec_e2e = []
+        for _ in range(args.steps):
+            w_e2e = e2e_step(rec_e2e)
+        barrier()
+        assert np.array_equal(w, w_e2e), "device and end-to-end runs disagree"
+        pristine.close()
+        work.close()
+        total_ms = max_over_ranks(sum(r[0] for r in rec))
+        total_e2e_ms = max_over_ranks(sum(rec_e2e))
+        return {"w": w, "total_ms": total_ms, "total_e2e_ms": total_e2e_ms,
+                "hyp_ms": sum(r[1] for r in rec) / args.steps,
+                "ape_ms": sum(r[2] for r in rec) / args.steps,
+                "w_ms": sum(r[3] for r in rec) / args.steps,
+                # our kernels per timed step: HYP 3 + APE n + W 2; e2e adds the
+                # layout conversion
+                "launches": args.steps * (3 + wl["ape"] + 2) * 2 + args.steps}
+
+    forms = ["mixed", "fp64"] if args.form == "both" else [args.form]
     sampler = ClockSampler(local_rank)
     sampler.start()
-    barrier()
-    rec = []
-    for _ in range(args.steps):
-        w = device_step(rec)
-    barrier()
-    for _ in range(args.warmup):
-        e2e_step(None)
-    barrier()
-    rec_e2e = []
-    for _ in range(args.steps):
-        w_e2e = e2e_step(rec_e2e)
-    barrier()
+    results = {f: measure(f) for f in forms}
     clocks = sampler.stop()
-
-    total_ms = max_over_ranks(sum(r[0] for r in rec))
-    total_e2e_ms = max_over_ranks(sum(rec_e2e))
-    hyp_ms = sum(r[1] for r in rec) / args.steps
-    ape_ms = sum(r[2] for r in rec) / args.steps
-    w_ms = sum(r[3] for r in rec) / args.steps
-    assert np.array_equal(w, w_e2e), "device and end-to-end runs disagree"
 
     if rank != 0:
         if dist is not None:
             dist.destroy_process_group()
         return 0
 
-    alg = algorithmic(wl, form)
-    phases = {"hyp": hyp_ms, "ape": ape_ms / wl["ape"], "wilson": w_ms}
-    phase_total = {"hyp": hyp_ms, "ape": ape_ms, "wilson": w_ms}
-    dom = max(phase_total, key=phase_total.get)
-    per_launch_ms = phases[dom]
+    head = forms[0]
+    hr = results[head]
     peak, peak_kind = load_peaks()
-    achieved = alg[dom]["bytes"] * V / (per_launch_ms * 1e-3) / 1e9
-    traffic_tbl = load_traffic().get(f"{dom}:{args.workload}:{form}")
-    value = world * V * args.steps / (total_ms * 1e-3)
-    e2e_value = world * V * args.steps / (total_e2e_ms * 1e-3)
+    traffic = load_traffic()
+
+    def summary(form, r):
+        alg = algorithmic(wl, form)
+        per_launch = {"hyp": r["hyp_ms"], "ape": r["ape_ms"] / wl["ape"], "wilson": r["w_ms"]}
+        totals = {"hyp": r["hyp_ms"], "ape": r["ape_ms"], "wilson": r["w_ms"]}
+        dom = max(totals, key=totals.get)
+        ms = per_launch[dom]
+        achieved = alg[dom]["bytes"] * V / (ms * 1e-3) / 1e9
+        tr = traffic.get(f"{dom}:{args.workload}:{form}")
+        return {
+            "value": world * V * args.steps / (r["total_ms"] * 1e-3),
+            "e2e_value": world * V * args.steps / (r["total_e2e_ms"] * 1e-3),
+            "ms_per_step": r["total_ms"] / args.steps,
+            "phases_ms": {"hyp": r["hyp_ms"], "ape_total": r["ape_ms"],
+                          "ape_per_step": r["ape_ms"] / wl["ape"], "wilson": r["w_ms"]},
+            "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak,
+                         "peak_kind": peak_kind, "unit": "GB/s", "frac": achieved / peak,
+                         "traffic": (tr["dram_bytes_per_site"] * V if tr else None),
+                         "alg_bytes_per_launch": alg[dom]["bytes"] * V,
+                         "fp_flops_per_launch": alg[dom]["flops"] * V,
+                         "fp_tflops": alg[dom]["flops"] * V / (ms * 1e-3) / 1e12},
+        }
+
+    sums = {f: summary(f, results[f]) for f in forms}
+    hs = sums[head]
     line = {
-        "metric": "smeared+measured sites/s", "value": value, "unit": "sites/s",
+        "metric": "smeared+measured sites/s", "value": hs["value"], "unit": "sites/s",
         "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
-        "ms_per_step": total_ms / args.steps, "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "f64" if form == "fp64" else "f32/f64",
+        "ms_per_step": hs["ms_per_step"], "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64" if head == "fp64" else "f32/f64",
         "data": "synthetic",
-        "config": {"workload": args.workload, "form": form, "lattice": list(dims),
+        "config": {"workload": args.workload, "form": head, "lattice": list(dims),
                    "group": f"SU({nc})", "hyp_steps": 1, "hyp_alpha": list(wl["hyp"]),
                    "ape_steps": wl["ape"], "ape_alpha": wl["alpha"], "r_range": [r0, r1],
-                   "t_range": [t0, t1], "sites": V, "l2": "flushed (256 MiB write) between steps",
+                   "t_range": [t0, t1], "sites": V,
+                   "l2": "flushed (256 MiB write) before every timed step",
                    "parallelism": f"replicas x{world}"},
-        "phases_ms": {"hyp": hyp_ms, "ape_total": ape_ms, "ape_per_step": ape_ms / wl["ape"],
-                      "wilson": w_ms},
-        "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak,
-                     "peak_kind": peak_kind, "unit": "GB/s", "frac": achieved / peak,
-                     "traffic": (traffic_tbl * V if traffic_tbl else None),
-                     "alg_bytes_per_site": alg[dom]["bytes"],
-                     "fp_flops_per_site": alg[dom]["flops"],
-                     "fp_tflops": alg[dom]["flops"] * V / (per_launch_ms * 1e-3) / 1e12},
-        "e2e": {"value": e2e_value, "unit": "sites/s",
+        "phases_ms": hs["phases_ms"],
+        "roofline": hs["roofline"],
+        "e2e": {"value": hs["e2e_value"], "unit": "sites/s",
                 "h2d_bytes_per_step": int(host.nbytes),
-                "d2h_bytes_per_step": int(w.nbytes)},
-        "gpu_launches": args.steps * (3 + wl["ape"] + 2) + args.steps * (1 + 3 + wl["ape"] + 2),
+                "d2h_bytes_per_step": int(hr["w"].nbytes)},
+        "gpu_launches": sum(results[f]["launches"] for f in forms),
         "clocks": clocks,
     }
+    if len(forms) > 1:
+        wm, wd = results["mixed"]["w"], results["fp64"]["w"]
+        line["mixed_vs_fp64"] = {"max_rel_err_W": float(np.max(np.abs(wm - wd) / np.abs(wd))),
+                                 "tolerance": 1e-6}
+        line["forms"] = {f: {"value": sums[f]["value"], "e2e": sums[f]["e2e_value"],
+                             "ms_per_step": sums[f]["ms_per_step"],
+                             "phases_ms": sums[f]["phases_ms"],
+                             "roofline": sums[f]["roofline"]} for f in forms}
     if world == 1 and not args.no_cpu_baseline:
         v, info = cpu_baseline(wl, args.workload, host)
         line["cpu_baseline"] = {"value": v, "unit": "sites/s", "cores": info["cores"],
                                 "kind": info["kind"], "sample": info["sample"]}
     print(json.dumps(line), flush=True)
-    pristine.close()
-    work.close()
     if dist is not None:
         dist.destroy_process_group()
     return 0
-
 
 if __name__ == "__main__":
     sys.exit(main())
