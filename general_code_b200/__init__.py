@@ -5,9 +5,9 @@ The compute path is libgc_b200.so (hand-written CUDA kernels behind the C ABI
 in include/gc_lattice.h); this package is a thin ctypes host layer over it.
 """
 from .lattice import (GCError, Lattice, LatticeData, generate_config, job_device_bytes,
-                      link_size, plaket, smearing_APE, smearing_HYP, unit_config, volume,
-                      wilson_loop)
+                      link_size, plaket, probe_config, read_data_convert, smearing_APE,
+                      smearing_HYP, unit_config, volume, wilson_loop)
 
 __all__ = ["GCError", "Lattice", "LatticeData", "generate_config", "job_device_bytes",
-           "link_size", "plaket", "smearing_APE", "smearing_HYP", "unit_config", "volume",
-           "wilson_loop"]
+           "link_size", "plaket", "probe_config", "read_data_convert", "smearing_APE",
+           "smearing_HYP", "unit_config", "volume", "wilson_loop"]

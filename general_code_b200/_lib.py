@@ -56,6 +56,13 @@ SIGNATURES = {
     "gc_plaquette": (_c_int, [_p, _pdbl]),
     "gc_wilson_onaxis_noalloc": (_c_int, [_pint, _c_int, _c_int, ctypes.POINTER(_p), _c_int,
                                           _c_int, _c_int, _c_int, _p, _p]),
+    "gc_read_config": (_c_int, [_p, ctypes.c_char_p, ctypes.c_char_p, ctypes.c_longlong,
+                                ctypes.c_char_p, _c_int]),
+    "gc_write_config": (_c_int, [_p, ctypes.c_char_p]),
+    "gc_probe_config": (_c_int, [_pint, _c_int, ctypes.c_char_p, ctypes.c_char_p,
+                                 ctypes.c_longlong, ctypes.c_char_p,
+                                 ctypes.POINTER(ctypes.c_longlong),
+                                 ctypes.POINTER(ctypes.c_longlong)]),
     "gc_generate": (_c_int, [_p, _c_dbl, _c_uint, _c_uint, _c_int]),
     "gc_generate_host": (_c_int, [_pint, _c_int, _c_dbl, _c_uint, _c_uint, _c_int, _pdbl]),
     "gc_job_device_bytes": (ctypes.c_longlong, [_pint, _c_int, _c_int, _c_int, _c_int]),

@@ -322,6 +322,31 @@ template <class T> GC_HD SU3<T> proj(const SU3<T> &A) {
   return B;
 }
 
+// The same six-step iteration, leaving early once a step changes no element
+// by more than tol. The iteration converges quadratically (the error after a
+// step of size d is O(d^2)), so the remaining steps would change the result
+// by O(tol^2) plus rounding; an input that needs all six steps gets all six.
+template <class T> GC_HD SU3<T> proj(const SU3<T> &A, T tol) {
+  SU3<T> B = ns_step(A);
+#pragma unroll 1
+  for (int it = 0; it < 5; it++) {
+    SU3<T> N = ns_step(B);
+    T d = T(0);
+#pragma unroll
+    for (int i = 0; i < 3; i++)
+#pragma unroll
+      for (int j = 0; j < 3; j++) {
+        d = fmax(d, fabs(N.e[i][j].re - B.e[i][j].re));
+        d = fmax(d, fabs(N.e[i][j].im - B.e[i][j].im));
+      }
+    B = N;
+    if (d <= tol)
+      break;
+  }
+  return B;
+}
+template <class T> GC_HD SU2<T> proj(const SU2<T> &A, T) { return proj(A); }
+
 // Gram-Schmidt reunitarisation: rows 0 and 1 orthonormalised, row 2 =
 // conj(row0 x row1). Used by the configuration generator (not on the
 // reference path).

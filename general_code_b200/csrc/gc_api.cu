@@ -13,6 +13,12 @@
 namespace gc {
 int generate_host(const int dims[4], int nc, double eps, unsigned seed,
                   unsigned cfg, int gauge, double *out);
+int probe_config(const int dims[4], int nc, const char *path, const char *format,
+                 long long bytes_skip, const char *precision, long long *offset,
+                 long long *length, std::string &err);
+int launch_file_to_soa(const Geom &g, int nc, int prec, const char *format,
+                       const char *precision, int convert, const unsigned char *data,
+                       const Fields4 &U, cudaStream_t s);
 
 namespace {
 thread_local std::string g_launch_error;
@@ -494,6 +500,73 @@ int gc_plaquette(gc_lattice *h, double *out) {
   if (e != cudaSuccess)
     return cuda_fail(h, "plaquette synchronize", e);
   return GC_OK;
+}
+
+int gc_read_config(gc_lattice *h, const char *path, const char *format,
+                   long long bytes_skip, const char *precision, int convert) {
+  if (!h || !path || !format)
+    return fail(h, GC_ERR_ARG, "null argument");
+  long long offset = 0, length = 0;
+  std::string err;
+  int rc = gc::probe_config(h->g.L, h->nc, path, format, bytes_skip, precision, &offset,
+                            &length, err);
+  if (rc)
+    return fail(h, rc, err);
+  std::lock_guard<std::mutex> lk(h->mu);
+  rc = ensure_staging(h);
+  if (rc)
+    return rc;
+  unsigned char *buf = nullptr;
+  cudaError_t e = cudaMallocHost(&buf, (size_t)length);
+  if (e != cudaSuccess)
+    return cuda_fail(h, "cudaMallocHost(read buffer)", e);
+  FILE *f = std::fopen(path, "rb");
+  bool ok = f && std::fseek(f, (long)offset, SEEK_SET) == 0 &&
+            std::fread(buf, 1, (size_t)length, f) == (size_t)length;
+  if (f)
+    std::fclose(f);
+  if (!ok) {
+    cudaFreeHost(buf);
+    return fail(h, GC_ERR_IO, std::string("read failed: ") + path);
+  }
+  e = cudaMemcpyAsync(h->staging, buf, (size_t)length, cudaMemcpyHostToDevice, h->stream);
+  if (e == cudaSuccess) {
+    rc = gc::launch_file_to_soa(h->g, h->nc, h->prec, format, precision, convert != 0,
+                                reinterpret_cast<const unsigned char *>(h->staging), h->cur,
+                                h->stream);
+    e = cudaStreamSynchronize(h->stream);
+  }
+  cudaFreeHost(buf);
+  if (rc)
+    return launch_fail(h, rc);
+  if (e != cudaSuccess)
+    return cuda_fail(h, "read_config", e);
+  h->has_links = true;
+  return GC_OK;
+}
+
+int gc_write_config(gc_lattice *h, const char *path) {
+  int rc = check_ready(h);
+  if (rc)
+    return rc;
+  if (!path)
+    return fail(h, GC_ERR_ARG, "null path");
+  const size_t n = (size_t)(h->nc == 3 ? 18 : 4) * 4 * (size_t)h->g.V;
+  double *buf = nullptr;
+  cudaError_t e = cudaMallocHost(&buf, n * sizeof(double));
+  if (e != cudaSuccess)
+    return cuda_fail(h, "cudaMallocHost(write buffer)", e);
+  rc = gc_download(h, buf, GC_LAYOUT_ROWMAJOR);
+  if (rc == GC_OK) {
+    FILE *f = std::fopen(path, "wb");
+    bool ok = f && std::fwrite(buf, sizeof(double), n, f) == n;
+    if (f)
+      ok = (std::fclose(f) == 0) && ok;
+    if (!ok)
+      rc = fail(h, GC_ERR_IO, std::string("write failed: ") + path);
+  }
+  cudaFreeHost(buf);
+  return rc;
 }
 
 int gc_generate_host(const int dims[4], int nc, double eps, unsigned int seed,

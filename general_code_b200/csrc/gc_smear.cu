@@ -34,12 +34,20 @@ __device__ __forceinline__ void add_staples(M &S, const void *fmu,
   S = add(S, mul(scale(b, c), Store::template load<CT>(fnu, V, x_mnu_pmu)));
 }
 
+// Projection tolerance: an update below it ends the iteration early (see
+// proj in gc_algebra.cuh). FP64 links: 1e-14, so the result equals the full
+// six-step iteration to rounding. FP32-stored links: 1e-9, far below the
+// 6e-8 rounding of the stored result.
+template <class Store> struct ProjTol {
+  static constexpr double value = (Store::kBytes == 144 || Store::kBytes == 32) ? 1e-14 : 1e-9;
+};
+
 template <class Store, class CT, class M>
 __device__ __forceinline__ void proj_store(void *out, size_t V, int site,
                                            const M &S) {
   using MD = typename Store::template M<double>;
   MD d = convert(S, (MD *)nullptr);
-  Store::template store<double>(out, V, site, proj(d));
+  Store::template store<double>(out, V, site, proj(d, ProjTol<Store>::value));
 }
 
 struct Nbr {

@@ -124,6 +124,17 @@ class Lattice:
         self._check(lib().gc_download(self._h, dbl_ptr(out), _LAYOUT[layout]))
         return out
 
+    def read(self, path, conf_format: str = "lexicographical", bytes_skip: int = 0,
+             file_precision: str = "double", convert: bool = False) -> None:
+        """Reads a configuration file into the device links (gc_read_config)."""
+        self._check(lib().gc_read_config(self._h, str(path).encode(), conf_format.encode(),
+                                         int(bytes_skip), file_precision.encode(),
+                                         int(bool(convert))))
+
+    def write(self, path) -> None:
+        """Writes the links as lexicographical doubles (gc_write_config)."""
+        self._check(lib().gc_write_config(self._h, str(path).encode()))
+
     def copy_from(self, other: "Lattice") -> None:
         """Device-to-device copy of other's links (same shape and precision)."""
         self._check(lib().gc_copy_links(self._h, other.handle))
@@ -207,11 +218,30 @@ def plaket(conf: LatticeData) -> float:
         return lat.plaquette()
 
 
+def read_data_convert(conf: LatticeData, file_path, conf_format: str, bytes_skip: int,
+                      file_precision: str, convert: bool) -> None:
+    """Fills conf.array from a file (data.h:265-338), through the device reader."""
+    with Lattice(conf.lat_dim, conf.nc) as lat:
+        lat.read(file_path, conf_format, bytes_skip, file_precision, convert)
+        lat.download(conf.array)
+
+
+def probe_config(dims: Sequence[int], nc: int, path, conf_format: str, bytes_skip: int = 0,
+                 file_precision: str = "double") -> Tuple[int, int]:
+    """(offset, length) of a configuration file's link payload; raises GCError."""
+    off, ln = ctypes.c_longlong(), ctypes.c_longlong()
+    check(lib().gc_probe_config(dims_arg(dims), nc, str(path).encode(), conf_format.encode(),
+                                int(bytes_skip), file_precision.encode(), ctypes.byref(off),
+                                ctypes.byref(ln)))
+    return off.value, ln.value
+
+
 def job_device_bytes(dims: Sequence[int], nc: int, precision: str, r_max: int,
                      time_max: int) -> int:
     return int(lib().gc_job_device_bytes(dims_arg(dims), nc, _PREC[precision], r_max, time_max))
 
 
 __all__ = ["Lattice", "LatticeData", "smearing_APE", "smearing_HYP", "wilson_loop", "plaket",
+           "read_data_convert", "probe_config",
            "generate_config", "unit_config", "link_size", "volume", "job_device_bytes",
            "GCError"]

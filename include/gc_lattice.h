@@ -141,6 +141,32 @@ int gc_wilson_onaxis_noalloc(const int dims[4], int nc, int precision,
  * Replaces: plaket(conf) (plaket.h:83-101). */
 int gc_plaquette(gc_lattice *h, double *out);
 
+/* Reads a configuration file straight into h's device links.
+ * format: "lexicographical" (link index 4*site+mu, get_data element order),
+ * "qcdstag" (direction-major with t first; SU(2) elements a0,a3,a2,a1) or
+ * "ildg" (LIME container, record "ildg-binary-data", big-endian doubles);
+ * precision: "float" or "double" (ignored for ildg, which is read as
+ * doubles); bytes_skip: header bytes before the links (not for ildg);
+ * convert != 0 applies the reference's MatrixConverter<MT,MT> (diagonal phase
+ * removal). Files shorter than the lattice are an error (GC_ERR_IO).
+ * Replaces: Data::read_data_convert(conf, path, format, bytes_skip,
+ * precision, convert) (data.h:265-338; patterns indexing.h:190-351). */
+int gc_read_config(gc_lattice *h, const char *path, const char *format,
+                   long long bytes_skip, const char *precision, int convert);
+
+/* Writes h's links as doubles in the lexicographical pattern.
+ * Replaces: conf.write_data(path, FilePatternLexicographical) (data.h:193-205),
+ * the format apps/smearing saves smeared configurations in. */
+int gc_write_config(gc_lattice *h, const char *path);
+
+/* Host-only check of a configuration file (no device needed): the byte
+ * offset and length of the link payload, or GC_ERR_IO with the reason
+ * (missing file, too short, not a LIME file, no ildg-binary-data record). */
+int gc_probe_config(const int dims[4], int nc, const char *path,
+                    const char *format, long long bytes_skip,
+                    const char *precision, long long *offset,
+                    long long *length);
+
 /* Fills h with the seeded synthetic configuration used by the benchmarks:
  *   SU(2): U = (cos th, sin th a/|a|), th = eps*|a|, a_k ~ N(0,1);
  *   SU(3): U = exp(i eps sum_a c_a lambda_a), c_a ~ N(0,1), reunitarised;
