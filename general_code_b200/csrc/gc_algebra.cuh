@@ -326,11 +326,17 @@ template <class T> GC_HD SU3<T> proj(const SU3<T> &A) {
 // by more than tol. The iteration converges quadratically (the error after a
 // step of size d is O(d^2)), so the remaining steps would change the result
 // by O(tol^2) plus rounding; an input that needs all six steps gets all six.
+// The first two steps are always taken (inputs of smearing steps are never
+// converged that early), so the check runs only after steps 3, 4 and 5.
 template <class T> GC_HD SU3<T> proj(const SU3<T> &A, T tol) {
-  SU3<T> B = ns_step(A);
+  SU3<T> B = ns_step(ns_step(A));
 #pragma unroll 1
-  for (int it = 0; it < 5; it++) {
+  for (int it = 0; it < 4; it++) {
     SU3<T> N = ns_step(B);
+    if (it == 3) { // the sixth and last step
+      B = N;
+      break;
+    }
     T d = T(0);
 #pragma unroll
     for (int i = 0; i < 3; i++)

@@ -1,6 +1,7 @@
 // Host-side declarations of the kernel launchers (implemented in the .cu files).
 #pragma once
 
+#include "../../include/gc_lattice.h"
 #include "gc_internal.cuh"
 
 namespace gc {
@@ -12,6 +13,18 @@ struct HypL2 {
   void *f[6];
 };
 
+// Per-lattice descriptors of the multi-lattice ("batch") launches. One launch
+// covers the blocks of every lattice in its table; block_start/start* is the
+// first block of the lattice in that launch (tables are sorted by it).
+struct ApeJob {
+  Geom g;
+  Fields4 in, out;
+  double alpha;
+  int block_start;
+};
+struct HypL1;
+struct HypL2;
+
 template <class Store, class CT>
 int launch_ape(const Geom &g, const Fields4 &in, const Fields4 &out,
                double alpha, cudaStream_t s);
@@ -20,6 +33,46 @@ template <class Store, class CT>
 int launch_hyp(const Geom &g, const Fields4 &U, const HypL1 &l1,
                const HypL2 &l2, void *out_t, double a1, double a2, double a3,
                cudaStream_t s);
+
+struct HypJob {
+  Geom g;
+  Fields4 U;
+  HypL1 l1;
+  HypL2 l2;
+  void *out_t;
+  double a1, a2, a3;
+  int start1, start2, start3; // first block in the level-1/2/3 launches
+};
+
+// jobs: device array (njobs entries, sorted by block_start); blocks: total.
+template <class Store, class CT>
+int launch_ape_batch(const ApeJob *jobs, int njobs, int blocks, cudaStream_t s);
+template <class Store, class CT>
+int launch_hyp_batch(const HypJob *jobs, int njobs, const int blocks[3],
+                     cudaStream_t s);
+
+struct WJob {
+  Geom g;
+  Fields4 U;
+  int rmin, rmax, tmin, tmax;
+  int cols, rows;       // block shape (columns x threads per column)
+  double *partials;     // this lattice's per-block partials
+  int block_start;      // first block (blocks = colblocks * 3, nu fastest)
+  int blocks;
+};
+struct RJob {           // fixed-order reduction of one lattice's partials
+  const double *partials;
+  int nblocks, nr, nt;
+  double scale;
+  double *out;          // (T-tmin)*nr + (R-rmin)
+  int entry_start;      // first block of the reduction launch
+};
+template <class Store, class CT>
+int launch_wilson_batch(const WJob *jobs, int njobs, int blocks, size_t smem,
+                        cudaStream_t s);
+int launch_reduce_batch(const RJob *jobs, int njobs, int entries, cudaStream_t s);
+// Shared memory one lattice's W blocks need.
+size_t wilson_job_smem(const WJob &j, int nc, int ct_bytes);
 
 // Wilson loops: per-block partial sums into `partials` (device, sized by
 // wilson_partials_count), then a fixed-order reduction into `out_dev`

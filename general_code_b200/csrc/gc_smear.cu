@@ -67,16 +67,13 @@ __device__ __forceinline__ Nbr neighbours(const Geom &g, int site,
   return n;
 }
 
+constexpr int kSmearBlock = 128;
+
+// One (site, mu) of an APE step (smearing.h:121-155).
 template <class Store, class CT>
-__global__ void __launch_bounds__(128, 4)
-    ape_kernel(Geom g, const __grid_constant__ Fields4 in,
-               const __grid_constant__ Fields4 out, double alpha) {
-  // mu varies fastest over blocks, so the three directions of a block of
-  // sites are smeared back to back while their links are in L2.
-  const int mu = blockIdx.x % 3;
-  const int site = (blockIdx.x / 3) * blockDim.x + threadIdx.x;
-  if (site >= g.V)
-    return;
+__device__ __forceinline__ void ape_site(const Geom &g, const Fields4 &in,
+                                         const Fields4 &out, double alpha,
+                                         int site, int mu) {
   using M = typename Store::template M<CT>;
   int x[4];
   site_coords(g, site, x);
@@ -102,13 +99,9 @@ __constant__ int kL1Mu[9] = {0, 0, 1, 1, 2, 2, 3, 3, 3};
 __constant__ int kL1Eta[9] = {2, 1, 2, 0, 1, 0, 0, 1, 2};
 
 template <class Store, class CT>
-__global__ void __launch_bounds__(128, 4)
-    hyp_level1_kernel(Geom g, const __grid_constant__ Fields4 U,
-                      const __grid_constant__ HypL1 out, double alpha3) {
-  const int f = blockIdx.x % 9;
-  const int site = (blockIdx.x / 9) * blockDim.x + threadIdx.x;
-  if (site >= g.V)
-    return;
+__device__ __forceinline__ void hyp_l1_site(const Geom &g, const Fields4 &U,
+                                            const HypL1 &out, double alpha3,
+                                            int site, int f) {
   using M = typename Store::template M<CT>;
   int x[4];
   site_coords(g, site, x);
@@ -132,14 +125,9 @@ __device__ __forceinline__ int l1_temporal(int a, int b) { return 6 + (3 - a - b
 //   0..2 : Vtilde_{t;nu}, nu = f       (smearing.h:433-450)
 //   3..5 : Vtilde_{nu;t}, nu = f - 3   (smearing.h:455-466)
 template <class Store, class CT>
-__global__ void __launch_bounds__(128, 4)
-    hyp_level2_kernel(Geom g, const __grid_constant__ Fields4 U,
-                      const __grid_constant__ HypL1 l1,
-                      const __grid_constant__ HypL2 out, double alpha2) {
-  const int f = blockIdx.x % 6;
-  const int site = (blockIdx.x / 6) * blockDim.x + threadIdx.x;
-  if (site >= g.V)
-    return;
+__device__ __forceinline__ void hyp_l2_site(const Geom &g, const Fields4 &U,
+                                            const HypL1 &l1, const HypL2 &out,
+                                            double alpha2, int site, int f) {
   using M = typename Store::template M<CT>;
   int x[4];
   site_coords(g, site, x);
@@ -165,13 +153,9 @@ __global__ void __launch_bounds__(128, 4)
 
 // Level 3: the new temporal link (smearing.h:484-503).
 template <class Store, class CT>
-__global__ void __launch_bounds__(128)
-    hyp_level3_kernel(Geom g, const void *Ut, const __grid_constant__ HypL2 l2,
-                      void *out_t,
-                      double alpha1) {
-  const int site = blockIdx.x * blockDim.x + threadIdx.x;
-  if (site >= g.V)
-    return;
+__device__ __forceinline__ void hyp_l3_site(const Geom &g, const void *Ut,
+                                            const HypL2 &l2, void *out_t,
+                                            double alpha1, int site) {
   using M = typename Store::template M<CT>;
   int x[4];
   site_coords(g, site, x);
@@ -187,7 +171,112 @@ __global__ void __launch_bounds__(128)
   proj_store<Store, CT>(out_t, V, site, S);
 }
 
-constexpr int kSmearBlock = 128;
+// ---------------------------------------------------------- single lattice
+// The field / direction index varies fastest over blocks, so all fields of
+// a block of sites are computed back to back while their inputs are in L2.
+template <class Store, class CT>
+__global__ void __launch_bounds__(128, 4)
+    ape_kernel(Geom g, const __grid_constant__ Fields4 in,
+               const __grid_constant__ Fields4 out, double alpha) {
+  const int mu = blockIdx.x % 3;
+  const int site = (blockIdx.x / 3) * blockDim.x + threadIdx.x;
+  if (site < g.V)
+    ape_site<Store, CT>(g, in, out, alpha, site, mu);
+}
+
+template <class Store, class CT>
+__global__ void __launch_bounds__(128, 4)
+    hyp_level1_kernel(Geom g, const __grid_constant__ Fields4 U,
+                      const __grid_constant__ HypL1 out, double alpha3) {
+  const int f = blockIdx.x % 9;
+  const int site = (blockIdx.x / 9) * blockDim.x + threadIdx.x;
+  if (site < g.V)
+    hyp_l1_site<Store, CT>(g, U, out, alpha3, site, f);
+}
+
+template <class Store, class CT>
+__global__ void __launch_bounds__(128, 4)
+    hyp_level2_kernel(Geom g, const __grid_constant__ Fields4 U,
+                      const __grid_constant__ HypL1 l1,
+                      const __grid_constant__ HypL2 out, double alpha2) {
+  const int f = blockIdx.x % 6;
+  const int site = (blockIdx.x / 6) * blockDim.x + threadIdx.x;
+  if (site < g.V)
+    hyp_l2_site<Store, CT>(g, U, l1, out, alpha2, site, f);
+}
+
+template <class Store, class CT>
+__global__ void __launch_bounds__(128)
+    hyp_level3_kernel(Geom g, const void *Ut, const __grid_constant__ HypL2 l2,
+                      void *out_t, double alpha1) {
+  const int site = blockIdx.x * blockDim.x + threadIdx.x;
+  if (site < g.V)
+    hyp_l3_site<Store, CT>(g, Ut, l2, out_t, alpha1, site);
+}
+
+// ---------------------------------------------------------- many lattices
+// One launch covers the blocks of several lattices; a block finds its
+// lattice by binary search over the jobs' first block indices.
+template <class J, int (*Start)(const J &)>
+__device__ __forceinline__ int find_job(const J *jobs, int njobs, int b) {
+  int lo = 0, hi = njobs - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (Start(jobs[mid]) <= b)
+      lo = mid;
+    else
+      hi = mid - 1;
+  }
+  return lo;
+}
+__device__ __forceinline__ int ape_start(const ApeJob &j) { return j.block_start; }
+__device__ __forceinline__ int hyp_start1(const HypJob &j) { return j.start1; }
+__device__ __forceinline__ int hyp_start2(const HypJob &j) { return j.start2; }
+__device__ __forceinline__ int hyp_start3(const HypJob &j) { return j.start3; }
+
+template <class Store, class CT>
+__global__ void __launch_bounds__(128, 4)
+    ape_batch_kernel(const ApeJob *__restrict__ jobs, int njobs) {
+  const int j = find_job<ApeJob, ape_start>(jobs, njobs, blockIdx.x);
+  const ApeJob &jb = jobs[j];
+  const int local = blockIdx.x - jb.block_start;
+  const int mu = local % 3;
+  const int site = (local / 3) * blockDim.x + threadIdx.x;
+  if (site < jb.g.V)
+    ape_site<Store, CT>(jb.g, jb.in, jb.out, jb.alpha, site, mu);
+}
+
+template <class Store, class CT>
+__global__ void __launch_bounds__(128, 4)
+    hyp_level1_batch_kernel(const HypJob *__restrict__ jobs, int njobs) {
+  const int j = find_job<HypJob, hyp_start1>(jobs, njobs, blockIdx.x);
+  const HypJob &jb = jobs[j];
+  const int local = blockIdx.x - jb.start1;
+  const int site = (local / 9) * blockDim.x + threadIdx.x;
+  if (site < jb.g.V)
+    hyp_l1_site<Store, CT>(jb.g, jb.U, jb.l1, jb.a3, site, local % 9);
+}
+
+template <class Store, class CT>
+__global__ void __launch_bounds__(128, 4)
+    hyp_level2_batch_kernel(const HypJob *__restrict__ jobs, int njobs) {
+  const int j = find_job<HypJob, hyp_start2>(jobs, njobs, blockIdx.x);
+  const HypJob &jb = jobs[j];
+  const int local = blockIdx.x - jb.start2;
+  const int site = (local / 6) * blockDim.x + threadIdx.x;
+  if (site < jb.g.V)
+    hyp_l2_site<Store, CT>(jb.g, jb.U, jb.l1, jb.l2, jb.a2, site, local % 6);
+}
+
+template <class Store, class CT>
+__global__ void __launch_bounds__(128)
+    hyp_level3_batch_kernel(const HypJob *__restrict__ jobs, int njobs) {
+  const int j = find_job<HypJob, hyp_start3>(jobs, njobs, blockIdx.x);
+  const HypJob &jb = jobs[j];
+  const int site = (blockIdx.x - jb.start3) * blockDim.x + threadIdx.x;
+  if (site < jb.g.V)
+    hyp_l3_site<Store, CT>(jb.g, jb.U.f[3], jb.l2, jb.out_t, jb.a1, site);
+}
 
 } // namespace
 
@@ -216,12 +305,41 @@ int launch_hyp(const Geom &g, const Fields4 &U, const HypL1 &l1,
   return launch_check("hyp_level3_kernel");
 }
 
+template <class Store, class CT>
+int launch_ape_batch(const ApeJob *jobs, int njobs, int blocks, cudaStream_t s) {
+  if (njobs <= 0 || blocks <= 0)
+    return GC_OK;
+  ape_batch_kernel<Store, CT><<<blocks, kSmearBlock, 0, s>>>(jobs, njobs);
+  return launch_check("ape_batch_kernel");
+}
+
+template <class Store, class CT>
+int launch_hyp_batch(const HypJob *jobs, int njobs, const int blocks[3],
+                     cudaStream_t s) {
+  if (njobs <= 0)
+    return GC_OK;
+  hyp_level1_batch_kernel<Store, CT><<<blocks[0], kSmearBlock, 0, s>>>(jobs, njobs);
+  int rc = launch_check("hyp_level1_batch_kernel");
+  if (rc)
+    return rc;
+  hyp_level2_batch_kernel<Store, CT><<<blocks[1], kSmearBlock, 0, s>>>(jobs, njobs);
+  rc = launch_check("hyp_level2_batch_kernel");
+  if (rc)
+    return rc;
+  hyp_level3_batch_kernel<Store, CT><<<blocks[2], kSmearBlock, 0, s>>>(jobs, njobs);
+  return launch_check("hyp_level3_batch_kernel");
+}
+
 #define GC_INSTANTIATE_SMEAR(STORE, CT)                                        \
   template int launch_ape<STORE, CT>(const Geom &, const Fields4 &,           \
                                      const Fields4 &, double, cudaStream_t);  \
   template int launch_hyp<STORE, CT>(const Geom &, const Fields4 &,           \
                                      const HypL1 &, const HypL2 &, void *,    \
-                                     double, double, double, cudaStream_t);
+                                     double, double, double, cudaStream_t);   \
+  template int launch_ape_batch<STORE, CT>(const ApeJob *, int, int,          \
+                                           cudaStream_t);                     \
+  template int launch_hyp_batch<STORE, CT>(const HypJob *, int, const int *,  \
+                                           cudaStream_t);
 
 GC_INSTANTIATE_SMEAR(StoreF64SU3, double)
 GC_INSTANTIATE_SMEAR(StoreF64SU2, double)

@@ -105,14 +105,16 @@ template <class T> __device__ __forceinline__ double conj_tr_d(const SU2<T> &a, 
   return double(s);
 }
 
+// One block of the W computation: `cols` spatial columns starting at
+// colblock*cols, direction nu; writes its nr*nt partial sums to part.
 template <class Store, class CT>
-__global__ void __launch_bounds__(256)
-    wilson_kernel(Geom g, const __grid_constant__ Fields4 U, int rmin, int rmax, int tmin, int tmax,
-                  int cols, int rows, double *partials) {
+__device__ __forceinline__ void wilson_block(const Geom &g, const Fields4 &U, int rmin,
+                                             int rmax, int tmin, int tmax, int cols,
+                                             int rows, int colblock, int nu,
+                                             double *part, unsigned char *smem_raw) {
   using M = typename Store::template M<CT>;
   using VT = typename V2<CT>::type;
   constexpr int NE = Elems<M>::n;
-  extern __shared__ __align__(16) unsigned char smem_raw[];
   const int Lt = g.L[3];
   const int nr = rmax - rmin + 1, nt = tmax - tmin + 1;
   const int nwarps = blockDim.x >> 5;
@@ -132,8 +134,7 @@ __global__ void __launch_bounds__(256)
 
   const int c = tid % cols;
   const int row = tid / cols;
-  const int s = blockIdx.x * cols + c;
-  const int nu = blockIdx.y;
+  const int s = colblock * cols + c;
   const bool active = (row < rows) && (s < g.Vs);
   const int kt = Lt / rows;
   int xs[4] = {0, 0, 0, 0};
@@ -204,12 +205,82 @@ __global__ void __launch_bounds__(256)
   }
 
   // Fixed-order sum over warps -> one partial per (block, R, T).
-  const size_t blk = (size_t)blockIdx.y * gridDim.x + blockIdx.x;
   for (int e = tid; e < nr * nt; e += blockDim.x) {
     double sum = 0.0;
     for (int w = 0; w < nwarps; w++)
       sum += wacc[(size_t)w * nr * nt + e];
-    partials[blk * nr * nt + e] = sum;
+    part[e] = sum;
+  }
+}
+
+template <class Store, class CT>
+__global__ void __launch_bounds__(256)
+    wilson_kernel(Geom g, const __grid_constant__ Fields4 U, int rmin, int rmax, int tmin,
+                  int tmax, int cols, int rows, double *partials) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const size_t blk = (size_t)blockIdx.y * gridDim.x + blockIdx.x;
+  const int ne = (rmax - rmin + 1) * (tmax - tmin + 1);
+  wilson_block<Store, CT>(g, U, rmin, rmax, tmin, tmax, cols, rows, blockIdx.x, blockIdx.y,
+                          partials + blk * ne, smem_raw);
+}
+
+// Several lattices in one launch. A block finds its lattice by binary search
+// over block_start; nu varies fastest over a lattice's blocks, and each block
+// writes its partials at the index the single-lattice kernel uses
+// (nu * colblocks + colblock), so the fixed-order sums are the same.
+template <class Store, class CT>
+__global__ void __launch_bounds__(256)
+    wilson_batch_kernel(const WJob *__restrict__ jobs, int njobs) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  int lo = 0, hi = njobs - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (jobs[mid].block_start <= (int)blockIdx.x)
+      lo = mid;
+    else
+      hi = mid - 1;
+  }
+  const WJob &jb = jobs[lo];
+  const int local = blockIdx.x - jb.block_start;
+  const int nu = local % 3, colblock = local / 3;
+  const int colblocks = jb.blocks / 3;
+  const int ne = (jb.rmax - jb.rmin + 1) * (jb.tmax - jb.tmin + 1);
+  if (jb.cols * jb.rows > (int)blockDim.x)
+    return; // a lattice whose shape needs more threads than the launch has
+  wilson_block<Store, CT>(jb.g, jb.U, jb.rmin, jb.rmax, jb.tmin, jb.tmax, jb.cols, jb.rows,
+                          colblock, nu,
+                          jb.partials + ((size_t)nu * colblocks + colblock) * ne, smem_raw);
+}
+
+// Fixed-order reduction of several lattices' partials; block = (lattice,
+// entry), the same tree as reduce_partials_kernel.
+__global__ void __launch_bounds__(256)
+    reduce_batch_kernel(const RJob *__restrict__ jobs, int njobs) {
+  __shared__ double sh[256];
+  int lo = 0, hi = njobs - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (jobs[mid].entry_start <= (int)blockIdx.x)
+      lo = mid;
+    else
+      hi = mid - 1;
+  }
+  const RJob &jb = jobs[lo];
+  const int e = blockIdx.x - jb.entry_start;
+  const int nentries = jb.nr * jb.nt;
+  double s = 0.0;
+  for (int b = threadIdx.x; b < jb.nblocks; b += blockDim.x)
+    s += jb.partials[(size_t)b * nentries + e];
+  sh[threadIdx.x] = s;
+  __syncthreads();
+  for (int w = blockDim.x / 2; w > 0; w >>= 1) {
+    if (threadIdx.x < w)
+      sh[threadIdx.x] += sh[threadIdx.x + w];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    const int ir = e / jb.nt, it = e % jb.nt;
+    jb.out[it * jb.nr + ir] = sh[0] * jb.scale;
   }
 }
 
@@ -358,12 +429,46 @@ int launch_plaquette(const Geom &g, const Fields4 &U, double *partials,
   return launch_check("reduce_partials_kernel");
 }
 
+size_t wilson_job_smem(const WJob &j, int nc, int ct_bytes) {
+  const int nwarps = 256 / 32;
+  const int ncomp = (nc == 3) ? 18 : 4;
+  return (size_t)nwarps * (j.rmax - j.rmin + 1) * (j.tmax - j.tmin + 1) * sizeof(double) +
+         3 * (size_t)ncomp * j.g.L[3] * j.cols * ct_bytes;
+}
+
+template <class Store, class CT>
+int launch_wilson_batch(const WJob *jobs, int njobs, int blocks, size_t smem,
+                        cudaStream_t s) {
+  if (njobs <= 0 || blocks <= 0)
+    return GC_OK;
+  if (smem > 227 * 1024)
+    return plan_error("wilson_batch_kernel: shared memory above 227 KB");
+  if (smem > 48 * 1024) {
+    cudaError_t e = cudaFuncSetAttribute(wilson_batch_kernel<Store, CT>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)smem);
+    if (e != cudaSuccess)
+      return launch_check("wilson_batch_kernel smem attribute");
+  }
+  wilson_batch_kernel<Store, CT><<<blocks, 256, smem, s>>>(jobs, njobs);
+  return launch_check("wilson_batch_kernel");
+}
+
+int launch_reduce_batch(const RJob *jobs, int njobs, int entries, cudaStream_t s) {
+  if (njobs <= 0 || entries <= 0)
+    return GC_OK;
+  reduce_batch_kernel<<<entries, 256, 0, s>>>(jobs, njobs);
+  return launch_check("reduce_batch_kernel");
+}
+
 #define GC_INSTANTIATE_W(STORE, CT)                                            \
   template int launch_wilson<STORE, CT>(const Geom &, const Fields4 &, int,   \
                                         int, int, int, double *, double *,    \
                                         cudaStream_t);                        \
   template int launch_plaquette<STORE, CT>(const Geom &, const Fields4 &,     \
-                                           double *, double *, cudaStream_t);
+                                           double *, double *, cudaStream_t);  \
+  template int launch_wilson_batch<STORE, CT>(const WJob *, int, int, size_t, \
+                                              cudaStream_t);
 
 GC_INSTANTIATE_W(StoreF64SU3, double)
 GC_INSTANTIATE_W(StoreF64SU2, double)
