@@ -68,6 +68,29 @@ SIGNATURES = {
     "gc_job_device_bytes": (ctypes.c_longlong, [_pint, _c_int, _c_int, _c_int, _c_int]),
 }
 
+class GcJob(ctypes.Structure):
+    """gc_job (include/gc_lattice.h)."""
+    _fields_ = [("dims", ctypes.c_int * 4), ("nc", ctypes.c_int), ("hyp_steps", ctypes.c_int),
+                ("hyp_alpha", ctypes.c_double * 3), ("ape_steps", ctypes.c_int),
+                ("ape_alpha", ctypes.c_double), ("r_min", ctypes.c_int), ("r_max", ctypes.c_int),
+                ("time_min", ctypes.c_int), ("time_max", ctypes.c_int)]
+
+
+_pjob = ctypes.POINTER(GcJob)
+SIGNATURES.update({
+    "gc_batch_create": (_c_int, [_pjob, _c_int, _c_int, ctypes.POINTER(_p)]),
+    "gc_batch_destroy": (_c_int, [_p]),
+    "gc_batch_upload": (_c_int, [_p, _c_int, _pdbl, _c_int]),
+    "gc_batch_generate": (_c_int, [_p, _c_dbl, _c_dbl, _c_uint, _c_uint]),
+    "gc_batch_autotune": (_c_int, [_p]),
+    "gc_batch_run": (_c_int, [_p, _p]),
+    "gc_batch_synchronize": (_c_int, [_p]),
+    "gc_batch_wilson": (_c_int, [_p, _c_int, _pdbl]),
+    "gc_batch_download": (_c_int, [_p, _c_int, _pdbl, _c_int]),
+    "gc_batch_info": (_c_int, [_p, ctypes.POINTER(ctypes.c_longlong), _pint, _pint]),
+    "gc_batch_job_shape": (_c_int, [_p, _c_int, _pint, _pint]),
+})
+
 _lib = None
 
 

@@ -98,6 +98,15 @@ int launch_wilson(const Geom &g, const Fields4 &U, int rmin, int rmax,
                   int tmin, int tmax, double *partials, double *out_dev,
                   cudaStream_t s);
 
+// An explicit block shape (rows must divide Lt, rows*cols <= 256).
+WilsonPlan wilson_plan_shape(const Geom &g, int nr, int nt, int nc, int ct_bytes, int rows,
+                             int cols);
+// W with an explicit plan; out_dev == nullptr skips the reduction.
+template <class Store, class CT>
+int launch_wilson_plan(const Geom &g, const Fields4 &U, int rmin, int rmax, int tmin,
+                       int tmax, const WilsonPlan &p, double *partials, double *out_dev,
+                       cudaStream_t s);
+
 template <class Store, class CT>
 int launch_plaquette(const Geom &g, const Fields4 &U, double *partials,
                      double *out_dev, cudaStream_t s);

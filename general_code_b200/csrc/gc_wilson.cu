@@ -429,6 +429,46 @@ int launch_plaquette(const Geom &g, const Fields4 &U, double *partials,
   return launch_check("reduce_partials_kernel");
 }
 
+WilsonPlan wilson_plan_shape(const Geom &g, int nr, int nt, int nc, int ct_bytes, int rows,
+                             int cols) {
+  WilsonPlan p;
+  const int ncomp = (nc == 3) ? 18 : 4;
+  p.rows = rows;
+  p.cols_per_block = cols;
+  p.threads = ((rows * cols + 31) / 32) * 32;
+  p.blocks = ((g.Vs + cols - 1) / cols) * 3;
+  const int nwarps = p.threads / 32;
+  p.smem = (size_t)nwarps * nr * nt * sizeof(double) +
+           3 * (size_t)ncomp * g.L[3] * cols * ct_bytes;
+  p.fits = (g.L[3] % rows == 0) && rows * cols <= 256 && p.smem <= 227 * 1024;
+  return p;
+}
+
+template <class Store, class CT>
+int launch_wilson_plan(const Geom &g, const Fields4 &U, int rmin, int rmax, int tmin,
+                       int tmax, const WilsonPlan &p, double *partials, double *out_dev,
+                       cudaStream_t s) {
+  const int nr = rmax - rmin + 1, nt = tmax - tmin + 1;
+  if (!p.fits)
+    return plan_error("wilson_kernel: block shape does not fit");
+  if (p.smem > 48 * 1024) {
+    cudaError_t e = cudaFuncSetAttribute(
+        wilson_kernel<Store, CT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)p.smem);
+    if (e != cudaSuccess)
+      return launch_check("wilson_kernel smem attribute");
+  }
+  wilson_kernel<Store, CT><<<dim3(p.blocks / 3, 3), p.threads, p.smem, s>>>(
+      g, U, rmin, rmax, tmin, tmax, p.cols_per_block, p.rows, partials);
+  int rc = launch_check("wilson_kernel");
+  if (rc)
+    return rc;
+  if (!out_dev)
+    return GC_OK;
+  reduce_partials_kernel<<<nr * nt, 256, 0, s>>>(
+      partials, p.blocks, nr * nt, nr, nt, 1.0 / (3.0 * (double)g.V), out_dev);
+  return launch_check("reduce_partials_kernel");
+}
+
 size_t wilson_job_smem(const WJob &j, int nc, int ct_bytes) {
   const int nwarps = 256 / 32;
   const int ncomp = (nc == 3) ? 18 : 4;
@@ -443,7 +483,11 @@ int launch_wilson_batch(const WJob *jobs, int njobs, int blocks, size_t smem,
     return GC_OK;
   if (smem > 227 * 1024)
     return plan_error("wilson_batch_kernel: shared memory above 227 KB");
-  if (smem > 48 * 1024) {
+  cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+  cudaStreamIsCapturing(s, &cap);
+  // (while a stream is captured the attribute set by an earlier eager launch
+  // of the same schedule stays in force)
+  if (smem > 48 * 1024 && cap == cudaStreamCaptureStatusNone) {
     cudaError_t e = cudaFuncSetAttribute(wilson_batch_kernel<Store, CT>,
                                          cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          (int)smem);
@@ -468,7 +512,11 @@ int launch_reduce_batch(const RJob *jobs, int njobs, int entries, cudaStream_t s
   template int launch_plaquette<STORE, CT>(const Geom &, const Fields4 &,     \
                                            double *, double *, cudaStream_t);  \
   template int launch_wilson_batch<STORE, CT>(const WJob *, int, int, size_t, \
-                                              cudaStream_t);
+                                              cudaStream_t);                  \
+  template int launch_wilson_plan<STORE, CT>(const Geom &, const Fields4 &,   \
+                                             int, int, int, int,              \
+                                             const WilsonPlan &, double *,    \
+                                             double *, cudaStream_t);
 
 GC_INSTANTIATE_W(StoreF64SU3, double)
 GC_INSTANTIATE_W(StoreF64SU2, double)

@@ -182,6 +182,61 @@ int gc_generate(gc_lattice *h, double eps, unsigned int seed,
 int gc_generate_host(const int dims[4], int nc, double eps, unsigned int seed,
                      unsigned int config_index, int gauge, double *host_links);
 
+/* ---------------------------------------------------------------- batches
+ * Many independent smear-and-measure jobs of uneven sizes (SU(2) and SU(3)
+ * mixed), run together. The reference runs one configuration per program
+ * invocation (apps/smearing/smearing.cpp:228-301); a batch is that loop for
+ * many configurations at once: HYP x hyp_steps, APE x ape_steps, then the
+ * W(R,T) table, per job. Each phase is one launch over all jobs of a group;
+ * the first gc_batch_run captures the schedule into a CUDA graph and later
+ * runs replay it. */
+typedef struct gc_batch gc_batch;
+
+typedef struct {
+  int dims[4];          /* Lx, Ly, Lz, Lt */
+  int nc;               /* 2 or 3 */
+  int hyp_steps;        /* >= 0 */
+  double hyp_alpha[3];  /* alpha1, alpha2, alpha3 */
+  int ape_steps;        /* >= 0 */
+  double ape_alpha;
+  int r_min, r_max;     /* W ranges; r_max = time_max = 0: no W table */
+  int time_min, time_max;
+} gc_job;
+
+/* Plans the batch and allocates all its device memory (links, working
+ * fields, W partial sums and tables). */
+int gc_batch_create(const gc_job *jobs, int njobs, int precision,
+                    gc_batch **out);
+int gc_batch_destroy(gc_batch *b);
+/* Sets job j's input links (host array, GC_LAYOUT_*). Every run starts from
+ * the inputs. */
+int gc_batch_upload(gc_batch *b, int job, const double *host_links,
+                    int layout);
+/* Sets every job's input to the seeded synthetic configuration of
+ * gc_generate (eps by group), config index first_index + job. */
+int gc_batch_generate(gc_batch *b, double eps_su2, double eps_su3,
+                      unsigned int seed, unsigned int first_index);
+/* Optional: times the candidate W block shapes for each distinct (time
+ * extent, group, R/T range) of the batch on this GPU and keeps the fastest. */
+int gc_batch_autotune(gc_batch *b);
+/* Runs the whole batch on cuda_stream (NULL: the batch's own stream) and
+ * returns after enqueueing. The first run executes eagerly and captures the
+ * schedule into a CUDA graph; later runs launch the graph. */
+int gc_batch_run(gc_batch *b, void *cuda_stream);
+/* Waits for the last run. */
+int gc_batch_synchronize(gc_batch *b);
+/* Job j's W table of the last run (waits for it), laid out like
+ * gc_wilson_onaxis's output. */
+int gc_batch_wilson(gc_batch *b, int job, double *out);
+/* Job j's smeared links of the last run (host array, GC_LAYOUT_*). */
+int gc_batch_download(gc_batch *b, int job, double *host_links, int layout);
+/* Device bytes of the batch, kernel nodes of its graph (0 before the first
+ * run) and kernel launches per run. */
+int gc_batch_info(const gc_batch *b, long long *device_bytes, int *graph_nodes,
+                  int *launches);
+/* The W block shape (threads per column, columns per block) used for job j. */
+int gc_batch_job_shape(const gc_batch *b, int job, int *rows, int *cols);
+
 /* Bytes of device memory a handle of this shape uses for links plus working
  * buffers of a full HYP + APE + W job (for admission control). */
 long long gc_job_device_bytes(const int dims[4], int nc, int precision,
