@@ -183,6 +183,120 @@ def cpu_baseline(wl, workload, host_links, steps=1, warmup=0):
                                "seconds": total}
 
 
+def bench_batch(steps: int):
+    """64 configurations of uneven sizes ({8^4, 12^4, 16^4, 16^3x32, 24^4,
+    24^3x48}, SU(2)/SU(3) 50/50, APE 5..30, R,T up to L_s/2) as one batch:
+    autotuned W shapes, one CUDA graph launch per run. Times `steps` graph
+    launches with CUDA events after the capture run."""
+    import torch
+    from general_code_b200.batch import Batch, uneven_jobs
+    out = {}
+    jobs = uneven_jobs(64)
+    sites = sum(j.sites for j in jobs)
+    for form in ("mixed", "fp64"):
+        with Batch(jobs, form) as b:
+            b.generate(0.3, 0.25, SEED, 1000)
+            b.autotune()
+            b.run()
+            b.synchronize()
+            s = torch.cuda.Stream()
+            ms = []
+            for _ in range(steps):
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                e0.record(s)
+                b.run(s.cuda_stream)
+                e1.record(s)
+                s.synchronize()
+                ms.append(e0.elapsed_time(e1))
+            info = b.info()
+        out[form] = {"sites_per_s": sites / (sum(ms) / len(ms) * 1e-3),
+                     "ms_per_batch": sum(ms) / len(ms), "graph_nodes": info["graph_nodes"],
+                     "kernel_launches_per_batch": info["launches_per_run"],
+                     "device_bytes": info["device_bytes"]}
+    return {"workload": "64 uneven configurations, one CUDA graph per run", "jobs": 64,
+            "sites": sites, "total_ape_steps": sum(j.ape_steps for j in jobs),
+            "value": out["mixed"]["sites_per_s"], "unit": "sites/s", "forms": out}
+
+
+def bench_serving(duration_s: float, rate: float = 200.0, slots: int = 8):
+    """Poisson stream of smear-and-measure requests: V log-uniform in
+    [8^4, 32^4], L = round(V^(1/4)), SU(2)/SU(3) 50/50, APE 5..40, R,T up to
+    L/2, mixed precision, admission by free device memory. Reports the
+    submit-to-result latency percentiles and the completed sites/s, and the
+    largest W error of a sample of requests against the FP64 form run alone."""
+    from general_code_b200 import Lattice, generate_config
+    from general_code_b200.batch import Job
+    from general_code_b200.server import Server
+    rng = np.random.default_rng(SEED + 5)
+    n = max(1, int(duration_s * rate))
+    gaps = rng.exponential(1.0 / rate, n)
+    reqs = []
+    for _ in range(n):
+        v = float(np.exp(rng.uniform(np.log(8 ** 4), np.log(32 ** 4))))
+        L = int(min(32, max(8, round(v ** 0.25))))
+        nc = int(rng.choice([2, 3]))
+        reqs.append(Job(dims=(L, L, L, L), nc=nc, ape_steps=int(rng.integers(5, 41)),
+                        r_max=L // 2, t_max=L // 2))
+    pool = {}
+    for j in reqs:
+        key = (j.dims[0], j.nc)
+        if key not in pool:
+            pool[key] = generate_config(j.dims, j.nc, 0.3 if j.nc == 2 else 0.25, SEED, len(pool))
+    results = {}
+    with Server(slots=slots, precision="mixed") as srv:
+        ids = []
+
+        def collect():
+            for k, rid in enumerate(ids_ready()):
+                results[k] = srv.wait(rid, timeout=600)
+
+        import queue
+        import threading
+        q = queue.Queue()
+
+        def ids_ready():
+            while True:
+                item = q.get()
+                if item is None:
+                    return
+                yield item
+
+        t = threading.Thread(target=collect)
+        t.start()
+        t0 = time.perf_counter()
+        next_t = t0
+        for k, j in enumerate(reqs):
+            next_t += gaps[k]
+            dt = next_t - time.perf_counter()
+            if dt > 0:
+                time.sleep(dt)
+            rid = srv.submit(j, pool[(j.dims[0], j.nc)])
+            ids.append(rid)
+            q.put(rid)
+        q.put(None)
+        t.join()
+        wall = time.perf_counter() - t0
+        st = srv.stats()
+    # accuracy of the served (mixed) results against FP64 alone, on a sample
+    sample = sorted(set(int(i) for i in rng.choice(n, min(8, n), replace=False)))
+    err = 0.0
+    for k in sample:
+        j = reqs[k]
+        with Lattice(j.dims, j.nc, "fp64") as lat:
+            lat.upload(pool[(j.dims[0], j.nc)])
+            lat.hyp(*j.hyp_alpha, 1)
+            lat.ape(j.ape_alpha, j.ape_steps)
+            w = lat.wilson_loop(1, j.r_max, 1, j.t_max)
+        err = max(err, float(np.max(np.abs(results[k] - w) / np.abs(w))))
+    return {"workload": f"Poisson {rate:g} req/s for {duration_s:g} s, L^4 with L 8..32",
+            "requests": n, "completed": st["completed"], "offered_rate": rate,
+            "wall_s": wall, "p50_ms": st["p50_ms"], "p99_ms": st["p99_ms"],
+            "mean_ms": st["mean_ms"], "value": st["sites_per_s"], "unit": "sites/s",
+            "slots": slots, "peak_inflight": st["peak_inflight"],
+            "peak_device_bytes": st["peak_bytes"], "mixed_vs_fp64_max_rel_err_W": err,
+            "checked_requests": len(sample)}
+
+
 def run_reference(args, wl, rank):
     if rank != 0:
         return 0
@@ -216,6 +330,9 @@ def main():
     ap.add_argument("--form", choices=["both", "fp64", "mixed"], default="both")
     ap.add_argument("--workload", choices=sorted(WORKLOADS), default="su3_24")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--sections", default="batch,serving",
+                    help="extra single-GPU measurements: batch, serving (comma list, or none)")
+    ap.add_argument("--serving-seconds", type=float, default=10.0)
     args = ap.parse_args()
     if args.warmup < 3:
         ap.error("--warmup must be >= 3")
@@ -404,6 +521,11 @@ def main():
                              "ms_per_step": sums[f]["ms_per_step"],
                              "phases_ms": sums[f]["phases_ms"],
                              "roofline": sums[f]["roofline"]} for f in forms}
+    sections = [x for x in args.sections.split(",") if x and x != "none"]
+    if world == 1 and "batch" in sections:
+        line["batch"] = bench_batch(args.steps)
+    if world == 1 and "serving" in sections:
+        line["serving"] = bench_serving(args.serving_seconds)
     if world == 1 and not args.no_cpu_baseline:
         v, info = cpu_baseline(wl, args.workload, host)
         line["cpu_baseline"] = {"value": v, "unit": "sites/s", "cores": info["cores"],

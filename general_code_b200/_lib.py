@@ -91,6 +91,39 @@ SIGNATURES.update({
     "gc_batch_job_shape": (_c_int, [_p, _c_int, _pint, _pint]),
 })
 
+FREE_BYTES_FN = ctypes.CFUNCTYPE(ctypes.c_longlong, ctypes.c_void_p)
+
+
+class ServerOpts(ctypes.Structure):
+    """gc_server_opts (include/gc_lattice.h)."""
+    _fields_ = [("slots", ctypes.c_int), ("precision", ctypes.c_int),
+                ("memory_budget", ctypes.c_longlong), ("queue_capacity", ctypes.c_int),
+                ("free_bytes", FREE_BYTES_FN), ("free_bytes_ctx", ctypes.c_void_p),
+                ("simulate_us", ctypes.c_int)]
+
+
+class ServerMetrics(ctypes.Structure):
+    """gc_server_metrics (include/gc_lattice.h)."""
+    _fields_ = [("submitted", ctypes.c_longlong), ("completed", ctypes.c_longlong),
+                ("rejected", ctypes.c_longlong), ("failed", ctypes.c_longlong),
+                ("pending", ctypes.c_longlong), ("inflight", ctypes.c_int),
+                ("peak_inflight", ctypes.c_int), ("peak_bytes", ctypes.c_longlong),
+                ("budget", ctypes.c_longlong), ("p50_ms", ctypes.c_double),
+                ("p99_ms", ctypes.c_double), ("mean_ms", ctypes.c_double),
+                ("sites_per_s", ctypes.c_double)]
+
+
+SIGNATURES.update({
+    "gc_lattice_create_on_stream": (_c_int, [_pint, _c_int, _c_int, _p, ctypes.POINTER(_p)]),
+    "gc_server_create": (_c_int, [ctypes.POINTER(ServerOpts), ctypes.POINTER(_p)]),
+    "gc_server_submit": (_c_int, [_p, _pjob, _pdbl, _c_int,
+                                  ctypes.POINTER(ctypes.c_ulonglong)]),
+    "gc_server_wait": (_c_int, [_p, ctypes.c_ulonglong, _pdbl, _c_dbl]),
+    "gc_server_cancel": (_c_int, [_p, ctypes.c_ulonglong]),
+    "gc_server_stats": (_c_int, [_p, ctypes.POINTER(ServerMetrics)]),
+    "gc_server_destroy": (_c_int, [_p]),
+})
+
 _lib = None
 
 

@@ -65,6 +65,7 @@ struct gc_lattice {
   size_t dev_out_cap = 0;   // doubles
   cudaStream_t own_stream = nullptr;
   cudaStream_t stream = nullptr;
+  bool stream_ordered = false; // device memory from cudaMallocAsync on `stream`
   bool has_links = false;
   std::string err;
   std::mutex mu;
@@ -95,6 +96,22 @@ int launch_fail(gc_lattice *h, int rc) {
   return fail(h, rc, g_launch_error);
 }
 
+// Device allocations of a handle: ordinary, or stream-ordered on the handle's
+// stream (no device-wide synchronisation when freed).
+cudaError_t dev_alloc(gc_lattice *h, void **p, size_t n) {
+  if (h->stream_ordered)
+    return cudaMallocAsync(p, n, h->stream);
+  return cudaMalloc(p, n);
+}
+void dev_free(gc_lattice *h, void *p) {
+  if (!p)
+    return;
+  if (h->stream_ordered)
+    cudaFreeAsync(p, h->stream);
+  else
+    cudaFree(p);
+}
+
 size_t bytes_per_link(int nc, int prec) {
   if (nc == 3)
     return prec == GC_PREC_FP64 ? 144 : 48;
@@ -123,7 +140,7 @@ int ensure_staging(gc_lattice *h) {
   if (h->staging)
     return GC_OK;
   const size_t per = (h->nc == 3 ? 18 : 4) * sizeof(double);
-  cudaError_t e = cudaMalloc(&h->staging, per * 4 * (size_t)h->g.V);
+  cudaError_t e = dev_alloc(h, (void **)&h->staging, per * 4 * (size_t)h->g.V);
   if (e != cudaSuccess) {
     h->staging = nullptr;
     return cuda_fail(h, "cudaMalloc(staging)", e);
@@ -134,11 +151,10 @@ int ensure_staging(gc_lattice *h) {
 int ensure_partials(gc_lattice *h, size_t n) {
   if (h->partials_cap >= n)
     return GC_OK;
-  if (h->partials)
-    cudaFree(h->partials);
+  dev_free(h, h->partials);
   h->partials = nullptr;
   h->partials_cap = 0;
-  cudaError_t e = cudaMalloc(&h->partials, n * sizeof(double));
+  cudaError_t e = dev_alloc(h, (void **)&h->partials, n * sizeof(double));
   if (e != cudaSuccess) {
     h->partials = nullptr;
     return cuda_fail(h, "cudaMalloc(partials)", e);
@@ -150,11 +166,10 @@ int ensure_partials(gc_lattice *h, size_t n) {
 int ensure_dev_out(gc_lattice *h, size_t n) {
   if (h->dev_out_cap >= n)
     return GC_OK;
-  if (h->dev_out)
-    cudaFree(h->dev_out);
+  dev_free(h, h->dev_out);
   h->dev_out = nullptr;
   h->dev_out_cap = 0;
-  cudaError_t e = cudaMalloc(&h->dev_out, n * sizeof(double));
+  cudaError_t e = dev_alloc(h, (void **)&h->dev_out, n * sizeof(double));
   if (e != cudaSuccess) {
     h->dev_out = nullptr;
     return cuda_fail(h, "cudaMalloc(result)", e);
@@ -166,7 +181,7 @@ int ensure_dev_out(gc_lattice *h, size_t n) {
 int ensure_hyp(gc_lattice *h) {
   if (h->hyp)
     return GC_OK;
-  cudaError_t e = cudaMalloc(&h->hyp, 15 * h->field_bytes);
+  cudaError_t e = dev_alloc(h, &h->hyp, 15 * h->field_bytes);
   if (e != cudaSuccess) {
     h->hyp = nullptr;
     return cuda_fail(h, "cudaMalloc(HYP decorated links)", e);
@@ -205,8 +220,23 @@ const char *gc_last_error(const gc_lattice *h) {
   return copy.c_str();
 }
 
+static int create_impl(const int dims[4], int nc, int precision, cudaStream_t ordered,
+                       gc_lattice **out);
+
 int gc_lattice_create(const int dims[4], int nc, int precision,
                       gc_lattice **out) {
+  return create_impl(dims, nc, precision, nullptr, out);
+}
+
+int gc_lattice_create_on_stream(const int dims[4], int nc, int precision,
+                                void *cuda_stream, gc_lattice **out) {
+  if (!cuda_stream)
+    return fail(nullptr, GC_ERR_ARG, "gc_lattice_create_on_stream: null stream");
+  return create_impl(dims, nc, precision, (cudaStream_t)cuda_stream, out);
+}
+
+static int create_impl(const int dims[4], int nc, int precision, cudaStream_t ordered,
+                       gc_lattice **out) {
   if (!out || !dims)
     return fail(nullptr, GC_ERR_ARG, "null argument");
   *out = nullptr;
@@ -240,8 +270,22 @@ int gc_lattice_create(const int dims[4], int nc, int precision,
   h->g.Vs = dims[0] * dims[1] * dims[2];
   // 256-byte aligned fields
   h->field_bytes = ((bytes_per_link(nc, precision) * (size_t)V + 255) / 256) * 256;
-  cudaError_t e = cudaMalloc(&h->links, 8 * h->field_bytes);
+  cudaError_t e;
+  if (ordered) {
+    h->stream_ordered = true;
+    h->stream = ordered;
+  } else {
+    e = cudaStreamCreateWithFlags(&h->own_stream, cudaStreamNonBlocking);
+    if (e != cudaSuccess) {
+      delete h;
+      return cuda_fail(nullptr, "cudaStreamCreate", e);
+    }
+    h->stream = h->own_stream;
+  }
+  e = dev_alloc(h, &h->links, 8 * h->field_bytes);
   if (e != cudaSuccess) {
+    if (h->own_stream)
+      cudaStreamDestroy(h->own_stream);
     delete h;
     return cuda_fail(nullptr, "cudaMalloc(links)", e);
   }
@@ -249,13 +293,6 @@ int gc_lattice_create(const int dims[4], int nc, int precision,
     h->cur.f[d] = (char *)h->links + d * h->field_bytes;
     h->alt.f[d] = (char *)h->links + (4 + d) * h->field_bytes;
   }
-  e = cudaStreamCreateWithFlags(&h->own_stream, cudaStreamNonBlocking);
-  if (e != cudaSuccess) {
-    cudaFree(h->links);
-    delete h;
-    return cuda_fail(nullptr, "cudaStreamCreate", e);
-  }
-  h->stream = h->own_stream;
   *out = h;
   return GC_OK;
 }
@@ -265,16 +302,14 @@ int gc_lattice_destroy(gc_lattice *h) {
     return GC_OK;
   {
     std::lock_guard<std::mutex> lk(h->mu);
-    cudaStreamSynchronize(h->stream);
-    cudaFree(h->links);
-    if (h->hyp)
-      cudaFree(h->hyp);
-    if (h->staging)
-      cudaFree(h->staging);
-    if (h->partials)
-      cudaFree(h->partials);
-    if (h->dev_out)
-      cudaFree(h->dev_out);
+    // stream-ordered memory is released in the stream's order, without waiting
+    if (!h->stream_ordered)
+      cudaStreamSynchronize(h->stream);
+    dev_free(h, h->links);
+    dev_free(h, h->hyp);
+    dev_free(h, h->staging);
+    dev_free(h, h->partials);
+    dev_free(h, h->dev_out);
     if (h->own_stream)
       cudaStreamDestroy(h->own_stream);
   }
@@ -286,6 +321,9 @@ int gc_set_stream(gc_lattice *h, void *stream) {
   if (!h)
     return fail(nullptr, GC_ERR_ARG, "null handle");
   std::lock_guard<std::mutex> lk(h->mu);
+  if (h->stream_ordered)
+    return fail(h, GC_ERR_STATE,
+                "a handle made by gc_lattice_create_on_stream stays on its stream");
   h->stream = stream ? (cudaStream_t)stream : h->own_stream;
   return GC_OK;
 }

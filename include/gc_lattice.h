@@ -67,6 +67,15 @@ const char *gc_last_error(const gc_lattice *h);
 int gc_lattice_create(const int dims[4], int nc, int precision,
                       gc_lattice **out);
 
+/* As gc_lattice_create, but all of the handle's device memory is allocated
+ * and freed stream-ordered (cudaMallocAsync/cudaFreeAsync) on cuda_stream
+ * (a cudaStream_t as void*), and all its work runs there: creating and
+ * destroying handles then never synchronises the device, so handles of
+ * concurrent jobs on different streams overlap. gc_set_stream is refused for
+ * such a handle. */
+int gc_lattice_create_on_stream(const int dims[4], int nc, int precision,
+                                void *cuda_stream, gc_lattice **out);
+
 /* Frees all device memory of h. NULL is accepted. */
 int gc_lattice_destroy(gc_lattice *h);
 
@@ -236,6 +245,55 @@ int gc_batch_info(const gc_batch *b, long long *device_bytes, int *graph_nodes,
                   int *launches);
 /* The W block shape (threads per column, columns per block) used for job j. */
 int gc_batch_job_shape(const gc_batch *b, int job, int *rows, int *cols);
+
+/* ---------------------------------------------------------------- serving
+ * A request loop: each request is one configuration (a gc_job and its host
+ * links). Requests wait in a FIFO queue; `slots` workers, each on its own
+ * CUDA stream, take the head as soon as a worker is free and the head's
+ * device memory (gc_job_device_bytes) fits in the rest of the memory budget
+ * (and, if a free-memory provider is given, in the free memory it reports).
+ * Requests run concurrently on the GPU with stream-ordered memory; a
+ * request's result is bitwise the same alone and among others. No
+ * counterpart in the reference (its programs process one configuration per
+ * invocation). */
+typedef struct gc_server gc_server;
+
+typedef struct {
+  int slots;                 /* requests on the GPU at once (1..256) */
+  int precision;             /* GC_PREC_FP64 or GC_PREC_MIXED */
+  long long memory_budget;   /* bytes admitted requests may hold together;
+                                0: 90% of the free device memory at creation */
+  int queue_capacity;        /* pending requests before GC_ERR_BUSY; 0: no limit */
+  long long (*free_bytes)(void *ctx); /* optional free-memory provider */
+  void *free_bytes_ctx;
+  int simulate_us;           /* > 0: no GPU work, each request sleeps this many
+                                microseconds (tests of the admission logic) */
+} gc_server_opts;
+
+typedef struct {
+  long long submitted, completed, rejected, failed, pending;
+  int inflight, peak_inflight;
+  long long peak_bytes, budget;
+  double p50_ms, p99_ms, mean_ms; /* submit-to-result latency of completed requests */
+  double sites_per_s;             /* completed sites / (last result - first submit) */
+} gc_server_metrics;
+
+int gc_server_create(const gc_server_opts *opts, gc_server **out);
+/* Queues a request. host_links (4V links, GC_LAYOUT_*) must stay valid until
+ * the request completes. GC_ERR_NOMEM: the job alone exceeds the memory
+ * budget; GC_ERR_BUSY: the queue is full. */
+int gc_server_submit(gc_server *s, const gc_job *job, const double *host_links,
+                     int layout, unsigned long long *id);
+/* Waits up to timeout_s seconds for request id and copies its W table to
+ * out_w (as gc_wilson_onaxis lays it out). GC_ERR_TIMEOUT leaves the request
+ * in place (wait again); any other return releases it. */
+int gc_server_wait(gc_server *s, unsigned long long id, double *out_w,
+                   double timeout_s);
+/* Removes a request that has not started (GC_ERR_STATE if it has). */
+int gc_server_cancel(gc_server *s, unsigned long long id);
+int gc_server_stats(gc_server *s, gc_server_metrics *stats);
+/* Cancels pending requests, waits for running ones, frees everything. */
+int gc_server_destroy(gc_server *s);
 
 /* Bytes of device memory a handle of this shape uses for links plus working
  * buffers of a full HYP + APE + W job (for admission control). */
