@@ -72,9 +72,9 @@ def algorithmic(wl, form):
     return {
         "ape": {"bytes": 6 * b, "flops": 3 * (8 * mm + proj)},
         "hyp": {"bytes": 5 * b, "flops": 96 * mm + 16 * proj},
-        # the fused W kernel reads the 4 link fields once per R (lines stay on
-        # chip); two products + a dot per (x, nu, R, T)
-        "wilson": {"bytes": 4 * b * nr, "flops": 3 * nr * nt * (2 * mm + (36 if nc == 3 else 8))},
+        # the fused W kernel needs the 4 link fields once (space and time
+        # lines stay on chip); two products + a dot per (x, nu, R, T)
+        "wilson": {"bytes": 4 * b, "flops": 3 * nr * nt * (2 * mm + (36 if nc == 3 else 8))},
     }
 
 

@@ -85,6 +85,11 @@ struct WilsonPlan {
   size_t smem;        // dynamic shared memory bytes
   bool fits;          // false when even one column exceeds the budget
 };
+// Doubles of a W block's per-warp accumulators in shared memory, rounded up
+// to an even count so the 16-byte arrays placed after them stay aligned.
+__host__ __device__ inline size_t wacc_doubles(int nwarps, int nr, int nt) {
+  return ((size_t)nwarps * nr * nt + 1) & ~(size_t)1;
+}
 // At most this many (R,T) entries per launch (callers split R into chunks).
 constexpr int kWilsonMaxEntries = 1024;
 // Shared-memory budget for the column storage of one block (bytes), sized

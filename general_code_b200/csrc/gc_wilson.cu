@@ -121,7 +121,9 @@ __device__ __forceinline__ void wilson_block(const Geom &g, const Fields4 &U, in
   double *wacc = reinterpret_cast<double *>(smem_raw);         // [nwarps][nr*nt]
   const int sstride = Lt * cols;                                // matrices per set
   // space lines S(s,t,R) of the block's columns
-  VT *scol = reinterpret_cast<VT *>(wacc + (size_t)nwarps * nr * nt);
+  // (the accumulator block is rounded up to an even number of doubles so the
+  // 16-byte double2 arrays after it stay 16-byte aligned)
+  VT *scol = reinterpret_cast<VT *>(wacc + wacc_doubles(nwarps, nr, nt));
   // the block's own time links U_t(s, t), reused for every R and T
   VT *ucol = scol + (size_t)NE * sstride;
   // the time links of the neighbour columns U_t(s + R nu, t), one R at a time
@@ -377,7 +379,7 @@ WilsonPlan wilson_plan(const Geom &g, int nr, int nt, int nc, int ct_bytes) {
   p.blocks = colblocks * 3;
   const int nwarps = p.threads / 32;
   // per-warp accumulators + space lines + own and neighbour time links
-  p.smem = (size_t)nwarps * nr * nt * sizeof(double) +
+  p.smem = wacc_doubles(nwarps, nr, nt) * sizeof(double) +
            3 * (size_t)ncomp * Lt * p.cols_per_block * ct_bytes;
   p.fits = p.cols_per_block * col_bytes <= kWilsonColumnBudget;
   return p;
@@ -438,7 +440,7 @@ WilsonPlan wilson_plan_shape(const Geom &g, int nr, int nt, int nc, int ct_bytes
   p.threads = ((rows * cols + 31) / 32) * 32;
   p.blocks = ((g.Vs + cols - 1) / cols) * 3;
   const int nwarps = p.threads / 32;
-  p.smem = (size_t)nwarps * nr * nt * sizeof(double) +
+  p.smem = wacc_doubles(nwarps, nr, nt) * sizeof(double) +
            3 * (size_t)ncomp * g.L[3] * cols * ct_bytes;
   p.fits = (g.L[3] % rows == 0) && rows * cols <= 256 && p.smem <= 227 * 1024;
   return p;
@@ -472,7 +474,7 @@ int launch_wilson_plan(const Geom &g, const Fields4 &U, int rmin, int rmax, int 
 size_t wilson_job_smem(const WJob &j, int nc, int ct_bytes) {
   const int nwarps = 256 / 32;
   const int ncomp = (nc == 3) ? 18 : 4;
-  return (size_t)nwarps * (j.rmax - j.rmin + 1) * (j.tmax - j.tmin + 1) * sizeof(double) +
+  return wacc_doubles(nwarps, j.rmax - j.rmin + 1, j.tmax - j.tmin + 1) * sizeof(double) +
          3 * (size_t)ncomp * j.g.L[3] * j.cols * ct_bytes;
 }
 

@@ -46,6 +46,9 @@ def test_fp64_matches_reference_fixture(name, meta):
     (3, (8, 8, 8, 12), 0.25, (1.0, 0.75, 0.6), 5, (1, 4, 1, 6)),
     (3, (6, 10, 4, 12), 0.25, (1.0, 1.0, 0.5), 3, (2, 3, 3, 6)),
     (2, (5, 7, 3, 9), 0.3, (0.8, 0.6, 0.4), 4, (1, 3, 1, 5)),
+    # 7 warps x 25 (R,T) entries: an odd number of FP64 accumulators in the W
+    # kernel's shared memory ahead of its 16-byte column arrays
+    (3, (10, 10, 10, 10), 0.25, (1.0, 0.75, 0.6), 2, (1, 5, 1, 5)),
 ])
 def test_fp64_matches_oracle_seeded(port, nc, dims, eps, hyp, n_ape, rng):
     links = generate_config(dims, nc, eps, 20261203, 7)
