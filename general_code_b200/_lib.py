@@ -53,6 +53,7 @@ SIGNATURES = {
     "gc_ape": (_c_int, [_p, _c_dbl, _c_int]),
     "gc_hyp": (_c_int, [_p, _c_dbl, _c_dbl, _c_dbl, _c_int]),
     "gc_wilson_onaxis": (_c_int, [_p, _c_int, _c_int, _c_int, _c_int, _pdbl]),
+    "gc_wilson_adjoint_onaxis": (_c_int, [_p, _c_int, _c_int, _c_int, _c_int, _pdbl]),
     "gc_plaquette": (_c_int, [_p, _pdbl]),
     "gc_wilson_onaxis_noalloc": (_c_int, [_pint, _c_int, _c_int, ctypes.POINTER(_p), _c_int,
                                           _c_int, _c_int, _c_int, _p, _p]),

@@ -465,8 +465,8 @@ int gc_hyp(gc_lattice *h, double a1, double a2, double a3, int steps) {
   return GC_OK;
 }
 
-int gc_wilson_onaxis(gc_lattice *h, int rmin, int rmax, int tmin, int tmax,
-                     double *out) {
+static int wilson_impl(gc_lattice *h, int rmin, int rmax, int tmin, int tmax,
+                       double *out, bool adjoint) {
   int rc = check_ready(h);
   if (rc)
     return rc;
@@ -493,7 +493,7 @@ int gc_wilson_onaxis(gc_lattice *h, int rmin, int rmax, int tmin, int tmax,
     const int r1 = std::min(rmax, r0 + rchunk - 1);
     const int ncr = r1 - r0 + 1;
     rc = GC_DISPATCH(h, launch_wilson, h->g, h->cur, r0, r1, tmin, tmax,
-                     h->partials, chunk_out, h->stream);
+                     h->partials, chunk_out, h->stream, adjoint);
     if (rc)
       return launch_fail(h, rc);
     // chunk_out[(T-tmin)*ncr + (R-r0)] -> dev_out[(T-tmin)*nr + (R-rmin)]
@@ -512,6 +512,16 @@ int gc_wilson_onaxis(gc_lattice *h, int rmin, int rmax, int tmin, int tmax,
   if (e != cudaSuccess)
     return cuda_fail(h, "wilson synchronize", e);
   return GC_OK;
+}
+
+int gc_wilson_onaxis(gc_lattice *h, int rmin, int rmax, int tmin, int tmax,
+                     double *out) {
+  return wilson_impl(h, rmin, rmax, tmin, tmax, out, false);
+}
+
+int gc_wilson_adjoint_onaxis(gc_lattice *h, int rmin, int rmax, int tmin, int tmax,
+                             double *out) {
+  return wilson_impl(h, rmin, rmax, tmin, tmax, out, true);
 }
 
 int gc_plaquette(gc_lattice *h, double *out) {

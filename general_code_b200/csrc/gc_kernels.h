@@ -98,10 +98,11 @@ constexpr size_t kWilsonColumnBudget = 96 * 1024;
 
 WilsonPlan wilson_plan(const Geom &g, int nr, int nt, int nc, int ct_bytes);
 
+// adjoint: the adjoint-representation loop |Tr W|^2 - 1 instead of Re Tr W/N.
 template <class Store, class CT>
 int launch_wilson(const Geom &g, const Fields4 &U, int rmin, int rmax,
                   int tmin, int tmax, double *partials, double *out_dev,
-                  cudaStream_t s);
+                  cudaStream_t s, bool adjoint = false);
 
 // An explicit block shape (rows must divide Lt, rows*cols <= 256).
 WilsonPlan wilson_plan_shape(const Geom &g, int nr, int nt, int nc, int ct_bytes, int rows,

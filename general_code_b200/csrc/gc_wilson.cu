@@ -105,9 +105,37 @@ template <class T> __device__ __forceinline__ double conj_tr_d(const SU2<T> &a, 
   return double(s);
 }
 
+// The per-loop quantity, from the loop's trace Tr[S K^dag]: the fundamental
+// Re Tr W / N (multiply_conj_tr, matrix.h:54-56, 260-262) or, with ADJ, the
+// adjoint character |Tr W|^2 - 1 (multiply_conj_tr_adjoint / tr_adjoint,
+// matrix.h:62-65, 264-270; SU(2): 4 (a.b)^2 - 1).
+template <bool ADJ, class T>
+__device__ __forceinline__ double loop_value(const SU3<T> &a, const SU3<T> &b) {
+  if (!ADJ)
+    return conj_tr_d(a, b);
+  T re = a.e[0][0].re * b.e[0][0].re;
+  T im = a.e[0][0].im * b.e[0][0].re;
+  re = GC_FMA(a.e[0][0].im, b.e[0][0].im, re);
+  im = GC_FMA(-a.e[0][0].re, b.e[0][0].im, im);
+#pragma unroll
+  for (int k = 1; k < 9; k++) {
+    re = GC_FMA(a.e[k / 3][k % 3].re, b.e[k / 3][k % 3].re, re);
+    re = GC_FMA(a.e[k / 3][k % 3].im, b.e[k / 3][k % 3].im, re);
+    im = GC_FMA(a.e[k / 3][k % 3].im, b.e[k / 3][k % 3].re, im);
+    im = GC_FMA(-a.e[k / 3][k % 3].re, b.e[k / 3][k % 3].im, im);
+  }
+  const double r = double(re), i = double(im);
+  return r * r + i * i - 1.0;
+}
+template <bool ADJ, class T>
+__device__ __forceinline__ double loop_value(const SU2<T> &a, const SU2<T> &b) {
+  const double d = conj_tr_d(a, b);
+  return ADJ ? 4.0 * d * d - 1.0 : d;
+}
+
 // One block of the W computation: `cols` spatial columns starting at
 // colblock*cols, direction nu; writes its nr*nt partial sums to part.
-template <class Store, class CT>
+template <class Store, class CT, bool ADJ = false>
 __device__ __forceinline__ void wilson_block(const Geom &g, const Fields4 &U, int rmin,
                                              int rmax, int tmin, int tmax, int cols,
                                              int rows, int colblock, int nu,
@@ -193,7 +221,7 @@ __device__ __forceinline__ void wilson_block(const Geom &g, const Fields4 &U, in
           }
           if (T >= tmin) {
             double term = active
-                ? conj_tr_d(sm_load(scol, sstride, tu * cols + c, (M *)nullptr), K)
+                ? loop_value<ADJ>(sm_load(scol, sstride, tu * cols + c, (M *)nullptr), K)
                 : 0.0;
             term = warp_sum(term);
             if (lane == 0)
@@ -215,14 +243,14 @@ __device__ __forceinline__ void wilson_block(const Geom &g, const Fields4 &U, in
   }
 }
 
-template <class Store, class CT>
+template <class Store, class CT, bool ADJ>
 __global__ void __launch_bounds__(256)
     wilson_kernel(Geom g, const __grid_constant__ Fields4 U, int rmin, int rmax, int tmin,
                   int tmax, int cols, int rows, double *partials) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const size_t blk = (size_t)blockIdx.y * gridDim.x + blockIdx.x;
   const int ne = (rmax - rmin + 1) * (tmax - tmin + 1);
-  wilson_block<Store, CT>(g, U, rmin, rmax, tmin, tmax, cols, rows, blockIdx.x, blockIdx.y,
+  wilson_block<Store, CT, ADJ>(g, U, rmin, rmax, tmin, tmax, cols, rows, blockIdx.x, blockIdx.y,
                           partials + blk * ne, smem_raw);
 }
 
@@ -394,7 +422,7 @@ int plaquette_partials_count(const Geom &g) { return (g.V + 255) / 256; }
 template <class Store, class CT>
 int launch_wilson(const Geom &g, const Fields4 &U, int rmin, int rmax,
                   int tmin, int tmax, double *partials, double *out_dev,
-                  cudaStream_t s) {
+                  cudaStream_t s, bool adjoint) {
   const int nr = rmax - rmin + 1, nt = tmax - tmin + 1;
   WilsonPlan p = wilson_plan(g, nr, nt, Store::NC, (int)sizeof(CT));
   if (!p.fits || nr * nt > kWilsonMaxEntries)
@@ -402,13 +430,14 @@ int launch_wilson(const Geom &g, const Fields4 &U, int rmin, int rmax,
                       "one block's shared memory");
   if (p.smem > 48 * 1024) {
     cudaError_t e = cudaFuncSetAttribute(
-        wilson_kernel<Store, CT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-        (int)p.smem);
+        adjoint ? wilson_kernel<Store, CT, true> : wilson_kernel<Store, CT, false>,
+        cudaFuncAttributeMaxDynamicSharedMemorySize, (int)p.smem);
     if (e != cudaSuccess)
       return launch_check("wilson_kernel smem attribute");
   }
   dim3 grid(p.blocks / 3, 3);
-  wilson_kernel<Store, CT><<<grid, p.threads, p.smem, s>>>(
+  auto kern = adjoint ? wilson_kernel<Store, CT, true> : wilson_kernel<Store, CT, false>;
+  kern<<<grid, p.threads, p.smem, s>>>(
       g, U, rmin, rmax, tmin, tmax, p.cols_per_block, p.rows, partials);
   int rc = launch_check("wilson_kernel");
   if (rc)
@@ -455,11 +484,12 @@ int launch_wilson_plan(const Geom &g, const Fields4 &U, int rmin, int rmax, int 
     return plan_error("wilson_kernel: block shape does not fit");
   if (p.smem > 48 * 1024) {
     cudaError_t e = cudaFuncSetAttribute(
-        wilson_kernel<Store, CT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)p.smem);
+        wilson_kernel<Store, CT, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+        (int)p.smem);
     if (e != cudaSuccess)
       return launch_check("wilson_kernel smem attribute");
   }
-  wilson_kernel<Store, CT><<<dim3(p.blocks / 3, 3), p.threads, p.smem, s>>>(
+  wilson_kernel<Store, CT, false><<<dim3(p.blocks / 3, 3), p.threads, p.smem, s>>>(
       g, U, rmin, rmax, tmin, tmax, p.cols_per_block, p.rows, partials);
   int rc = launch_check("wilson_kernel");
   if (rc)
@@ -510,7 +540,7 @@ int launch_reduce_batch(const RJob *jobs, int njobs, int entries, cudaStream_t s
 #define GC_INSTANTIATE_W(STORE, CT)                                            \
   template int launch_wilson<STORE, CT>(const Geom &, const Fields4 &, int,   \
                                         int, int, int, double *, double *,    \
-                                        cudaStream_t);                        \
+                                        cudaStream_t, bool);                  \
   template int launch_plaquette<STORE, CT>(const Geom &, const Fields4 &,     \
                                            double *, double *, cudaStream_t);  \
   template int launch_wilson_batch<STORE, CT>(const WJob *, int, int, size_t, \

@@ -157,6 +157,14 @@ class Lattice:
                                            int(time_max), dbl_ptr(out)))
         return out
 
+    def wilson_loop_adjoint(self, r_min: int, r_max: int, time_min: int,
+                            time_max: int) -> np.ndarray:
+        """Adjoint-representation W table (wilson_loops.h:1173-1200), same layout."""
+        out = np.empty((time_max - time_min + 1, r_max - r_min + 1), dtype=np.float64)
+        self._check(lib().gc_wilson_adjoint_onaxis(self._h, int(r_min), int(r_max),
+                                                   int(time_min), int(time_max), dbl_ptr(out)))
+        return out
+
     def plaquette(self) -> float:
         out = ctypes.c_double()
         self._check(lib().gc_plaquette(self._h, ctypes.byref(out)))

@@ -18,6 +18,7 @@
 //   smearing_APE(LatticeData&, double)                    smearing.h:115-117
 //   smearing_HYP(LatticeData&, double, double, double)    smearing.h:480-482
 //   wilson_loop(const LatticeData&, int, int, int, int)   wilson_loops.h:1047-1050
+//   wilson_loop_adjoint(const LatticeData&, int x4)       wilson_loops.h:1173-1176
 //   wilson_loop(const std::vector<T>&, int, int, int, int)
 //                                              basic_observables.h:108-111
 //   plaket(const LatticeData&)                            plaket.h:83-84
@@ -99,15 +100,19 @@ void hyp(Data::LatticeData<DataPatternLexicographical, MT> &conf, double a1,
 template <class MT>
 std::map<std::tuple<int, int>, double>
 wilson(const std::array<int, 4> &dims, const MT *links, int r_min, int r_max,
-       int time_min, int time_max) {
+       int time_min, int time_max, bool adjoint = false) {
   std::map<std::tuple<int, int>, double> result;
   if (r_max < r_min || time_max < time_min)
     return result;
   Session<MT> s(dims, links);
   const int nr = r_max - r_min + 1, nt = time_max - time_min + 1;
   std::vector<double> w((size_t)nr * nt);
-  check(gc_wilson_onaxis(s.get(), r_min, r_max, time_min, time_max, w.data()),
-        s.get(), "wilson_loop");
+  if (adjoint)
+    check(gc_wilson_adjoint_onaxis(s.get(), r_min, r_max, time_min, time_max, w.data()),
+          s.get(), "wilson_loop_adjoint");
+  else
+    check(gc_wilson_onaxis(s.get(), r_min, r_max, time_min, time_max, w.data()),
+          s.get(), "wilson_loop");
   for (int t = time_min; t <= time_max; t++)
     for (int r = r_min; r <= r_max; r++)
       result[std::tuple<int, int>(t, r)] = w[(t - time_min) * nr + (r - r_min)];
@@ -152,6 +157,19 @@ wilson_loop(const Data::LatticeData<DataPatternLexicographical, su3> &conf,
             int r_min, int r_max, int time_min, int time_max) {
   return gc_dropin::wilson(conf.lat_dim, conf.array.data(), r_min, r_max,
                            time_min, time_max);
+}
+// Adjoint representation (wilson_loops.h:1173-1200).
+inline std::map<std::tuple<int, int>, double>
+wilson_loop_adjoint(const Data::LatticeData<DataPatternLexicographical, su2> &conf,
+                    int r_min, int r_max, int time_min, int time_max) {
+  return gc_dropin::wilson(conf.lat_dim, conf.array.data(), r_min, r_max,
+                           time_min, time_max, true);
+}
+inline std::map<std::tuple<int, int>, double>
+wilson_loop_adjoint(const Data::LatticeData<DataPatternLexicographical, su3> &conf,
+                    int r_min, int r_max, int time_min, int time_max) {
+  return gc_dropin::wilson(conf.lat_dim, conf.array.data(), r_min, r_max,
+                           time_min, time_max, true);
 }
 // Legacy vector form (basic_observables.h:108-111). The reference reads the
 // lattice size from the globals x_size, y_size, z_size, t_size

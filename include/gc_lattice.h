@@ -122,6 +122,14 @@ int gc_hyp(gc_lattice *h, double alpha1, double alpha2, double alpha3,
 int gc_wilson_onaxis(gc_lattice *h, int r_min, int r_max, int time_min,
                      int time_max, double *out);
 
+/* On-axis Wilson loops in the adjoint representation: per loop W,
+ * |Tr W|^2 - 1 (SU(2): 4 (Re Tr W / 2)^2 - 1), averaged like
+ * gc_wilson_onaxis, same output layout.
+ * Replaces: wilson_loop_adjoint(conf, r_min, r_max, time_min, time_max)
+ * (wilson_loops.h:1173-1200, plane sums :793-861). */
+int gc_wilson_adjoint_onaxis(gc_lattice *h, int r_min, int r_max, int time_min,
+                             int time_max, double *out);
+
 /* The W(R,T) table of gc_wilson_onaxis for callers that cannot allocate
  * device memory (an application whose allocator owns the whole device budget,
  * or a timing-critical loop where cudaMalloc/cudaFree would synchronise the

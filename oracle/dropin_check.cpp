@@ -1,6 +1,7 @@
 // Drop-in check (TEST INFRASTRUCTURE ONLY): compiles the reference's own
 // headers together with include/gc_dropin.hpp, then runs the sequence of
-// apps/smearing/smearing.cpp:186-301 (plaket, HYP, APE, wilson_loop) twice on
+// apps/smearing/smearing.cpp:186-301 (plaket, HYP, APE, wilson_loop, and
+// wilson_loop_adjoint as apps/smearing/smearing_wilson_gevp.cpp uses it) twice on
 // the same seeded configuration:
 //   - with unqualified calls, exactly as the app writes them, which overload
 //     resolution binds to the drop-in (GPU) functions;
@@ -61,13 +62,14 @@ int run(const std::array<int, 4> &dims, int ape_steps, int rmax, int tmax) {
     b.array[i] = MT(buf);
   }
   double pa, pb;
-  std::map<std::tuple<int, int>, double> wa, wb;
+  std::map<std::tuple<int, int>, double> wa, wb, aa, ab;
   try {
     pa = plaket(a); // drop-in
     smearing_HYP(a, 1, 0.75, 0.6);
     for (int i = 0; i < ape_steps; i++)
       smearing_APE(a, 0.5);
     wa = wilson_loop(a, 1, rmax, 1, tmax);
+    aa = wilson_loop_adjoint(a, 1, rmax, 1, tmax);
   } catch (const std::exception &e) {
     std::printf("drop-in raised: %s\n", e.what());
     return 3;
@@ -77,6 +79,7 @@ int run(const std::array<int, 4> &dims, int ape_steps, int rmax, int tmax) {
   for (int i = 0; i < ape_steps; i++)
     ::smearing_APE<DP, MT>(b, 0.5);
   wb = ::wilson_loop<DP, MT>(b, 1, rmax, 1, tmax);
+  ab = ::wilson_loop_adjoint<DP, MT>(b, 1, rmax, 1, tmax);
   double dl = 0;
   for (size_t i = 0; i < a.array.size(); i++) {
     std::vector<double> x = a.array[i].get_data(), y = b.array[i].get_data();
@@ -87,6 +90,11 @@ int run(const std::array<int, 4> &dims, int ape_steps, int rmax, int tmax) {
   bool ok = dl <= 1e-12 && std::fabs(pa - pb) <= 1e-12 * std::fabs(pb) + 1e-14;
   for (auto &kv : wb) {
     double d = std::fabs(wa.at(kv.first) - kv.second);
+    dw = std::fmax(dw, d / (std::fabs(kv.second) + 1e-300));
+    ok = ok && d <= 1e-12 * std::fabs(kv.second) + 1e-14;
+  }
+  for (auto &kv : ab) {
+    double d = std::fabs(aa.at(kv.first) - kv.second);
     dw = std::fmax(dw, d / (std::fabs(kv.second) + 1e-300));
     ok = ok && d <= 1e-12 * std::fabs(kv.second) + 1e-14;
   }

@@ -431,8 +431,12 @@ static double *lines_indexed(const group_t *G, const geom_t *g,
   return l;
 }
 
-int or_wilson(int nc, const int dims[4], const double *links, int rmin,
-              int rmax, int tmin, int tmax, double *out) {
+/* adjoint = 0: wilson_loop (wilson_loops.h:1047-1074, plane sums :719-791);
+ * adjoint = 1: wilson_loop_adjoint (:1173-1200, plane sums :793-861), i.e.
+ * per loop |Tr W|^2 - 1 (su3 tr_adjoint, matrix.h:264) or 4 (w.s)^2 - 1
+ * (su2 multiply_conj_tr_adjoint, matrix.h:62-65). */
+static int wilson_impl(int nc, const int dims[4], const double *links, int rmin,
+                       int rmax, int tmin, int tmax, double *out, int adjoint) {
   const group_t *G = group_of(nc);
   if (!G || rmin < 1 || tmin < 1 || rmax < rmin || tmax < tmin)
     return -1;
@@ -465,12 +469,19 @@ int or_wilson(int nc, const int dims[4], const double *links, int rmin,
             su3_mul(w, L + x * ds, sl[nu] + x2 * ds);
             su3_mul_ad(w, w, L + x3 * ds);
             su3_mul_ad(w, w, sl[nu] + x * ds);
-            result += su3_tr_real(w);
+            if (adjoint) {
+              double tr = RE(w, 0, 0) + RE(w, 1, 1) + RE(w, 2, 2);
+              double ti = IM(w, 0, 0) + IM(w, 1, 1) + IM(w, 2, 2);
+              result += tr * tr + ti * ti - 1;
+            } else {
+              result += su3_tr_real(w);
+            }
           } else {
             /* generic form (:735-748) */
             su2_mul(w, L + x * ds, sl[nu] + x2 * ds);
             su2_mul_ad(w, w, L + x3 * ds);
-            result += su2_conj_tr(w, sl[nu] + x * ds);
+            double d = su2_conj_tr(w, sl[nu] + x * ds);
+            result += adjoint ? 4 * d * d - 1 : d;
           }
         }
       }
@@ -485,6 +496,16 @@ int or_wilson(int nc, const int dims[4], const double *links, int rmin,
   for (int mu = 0; mu < 3; mu++)
     free(sl[mu]);
   return 0;
+}
+
+int or_wilson(int nc, const int dims[4], const double *links, int rmin,
+              int rmax, int tmin, int tmax, double *out) {
+  return wilson_impl(nc, dims, links, rmin, rmax, tmin, tmax, out, 0);
+}
+
+int or_wilson_adjoint(int nc, const int dims[4], const double *links, int rmin,
+                      int rmax, int tmin, int tmax, double *out) {
+  return wilson_impl(nc, dims, links, rmin, rmax, tmin, tmax, out, 1);
 }
 
 /* ------------------------------------------------------------ plaquette */

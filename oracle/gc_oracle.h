@@ -23,6 +23,8 @@ int or_hyp(int nc, const int dims[4], double *links, double alpha1,
            double alpha2, double alpha3, int steps);
 int or_wilson(int nc, const int dims[4], const double *links, int r_min,
               int r_max, int time_min, int time_max, double *out);
+int or_wilson_adjoint(int nc, const int dims[4], const double *links, int r_min,
+                      int r_max, int time_min, int time_max, double *out);
 double or_plaquette(int nc, const int dims[4], const double *links);
 /* Applies proj() to every link (test helper for the projection alone). */
 int or_proj_all(int nc, long long nlinks, double *links);

@@ -45,6 +45,8 @@ class _Checker:
             f"{p}ape": (_c_int, [_c_int, _pint, _pdbl, _c_dbl, _c_int]),
             f"{p}hyp": (_c_int, [_c_int, _pint, _pdbl, _c_dbl, _c_dbl, _c_dbl, _c_int]),
             f"{p}wilson": (_c_int, [_c_int, _pint, _pdbl, _c_int, _c_int, _c_int, _c_int, _pdbl]),
+            f"{p}wilson_adjoint": (_c_int, [_c_int, _pint, _pdbl, _c_int, _c_int, _c_int, _c_int,
+                                            _pdbl]),
             f"{p}plaquette": (_c_dbl, [_c_int, _pint, _pdbl]),
         }
         for name, (res, args) in sig.items():
@@ -64,6 +66,12 @@ class _Checker:
         out = np.empty((tmax - tmin + 1, rmax - rmin + 1), dtype=np.float64)
         assert self._fn("wilson")(nc, _dims(dims), _ptr(links), rmin, rmax, tmin, tmax,
                                   _ptr(out)) == 0
+        return out
+
+    def wilson_adjoint(self, nc, dims, links, rmin, rmax, tmin, tmax):
+        out = np.empty((tmax - tmin + 1, rmax - rmin + 1), dtype=np.float64)
+        assert self._fn("wilson_adjoint")(nc, _dims(dims), _ptr(links), rmin, rmax, tmin,
+                                          tmax, _ptr(out)) == 0
         return out
 
     def plaquette(self, nc, dims, links):

@@ -7,6 +7,7 @@
 //   smearing_APE          lib/cpu/include/smearing.h:115-161
 //   smearing_HYP          lib/cpu/include/smearing.h:480-516
 //   wilson_loop           lib/cpu/include/wilson_loops.h:1047-1074
+//   wilson_loop_adjoint   lib/cpu/include/wilson_loops.h:1173-1200
 //   plaket_site           lib/cpu/include/plaket.h:24-42
 //   Data::read_data_convert / write_data   lib/cpu/include/data.h:193-205,265-338
 //
@@ -191,6 +192,25 @@ int ref_wilson(int nc, const int *dims, const double *links, int rmin,
     Data::LatticeData<DP, su3> conf = make_conf<su3>(dims, links);
     wilson_to_table<su3>(wilson_loop(conf, rmin, rmax, tmin, tmax), rmin, rmax,
                          tmin, tmax, out);
+    return 0;
+  }
+  return -1;
+}
+
+// wilson_loop_adjoint (wilson_loops.h:1173-1200)
+int ref_wilson_adjoint(int nc, const int *dims, const double *links, int rmin,
+                       int rmax, int tmin, int tmax, double *out) {
+  set_globals(dims);
+  if (nc == 2) {
+    Data::LatticeData<DP, su2> conf = make_conf<su2>(dims, links);
+    wilson_to_table<su2>(wilson_loop_adjoint(conf, rmin, rmax, tmin, tmax), rmin,
+                         rmax, tmin, tmax, out);
+    return 0;
+  }
+  if (nc == 3) {
+    Data::LatticeData<DP, su3> conf = make_conf<su3>(dims, links);
+    wilson_to_table<su3>(wilson_loop_adjoint(conf, rmin, rmax, tmin, tmax), rmin,
+                         rmax, tmin, tmax, out);
     return 0;
   }
   return -1;

@@ -1,6 +1,6 @@
 """Generates the golden fixtures in tests/golden/ from the REFERENCE's own CPU
 code (oracle/_ref/libref_parity.so: lib/cpu smearing_HYP, smearing_APE,
-wilson_loop and plaket_site compiled from the reference sources with -O2 and
+wilson_loop, wilson_loop_adjoint and plaket_site compiled from the reference sources with -O2 and
 no fast-math by oracle/Makefile).
 
 Each case: a seeded synthetic configuration (the product's generator,
@@ -52,19 +52,21 @@ def main() -> None:
         links_ape = links_hyp.copy()
         ref.ape(nc, dims, links_ape, alpha, n_ape)
         w = ref.wilson(nc, dims, links_ape, r0, r1, t0, t1)
+        wa = ref.wilson_adjoint(nc, dims, links_ape, r0, r1, t0, t1)
         plaq1 = ref.plaquette(nc, dims, links_ape)
         np.savez_compressed(OUT / f"{name}.npz", links0=links0, links_hyp=links_hyp,
-                            links_ape=links_ape, wilson=w,
+                            links_ape=links_ape, wilson=w, wilson_adjoint=wa,
                             plaquettes=np.array([plaq0, plaq1]))
         index[name] = {"nc": nc, "dims": list(dims), "eps": eps, "seed": seed,
                        "config_index": cfg, "hyp_alpha": [a1, a2, a3], "ape_steps": n_ape,
                        "ape_alpha": alpha, "r_min": r0, "r_max": r1, "time_min": t0,
                        "time_max": t1, "plaquette_in": plaq0, "plaquette_out": plaq1,
-                       "wilson": w.tolist()}
+                       "wilson": w.tolist(), "wilson_adjoint": wa.tolist()}
         print(name, "plaq", plaq0, "->", plaq1, "W[0,0]", w[0, 0])
     meta = {"generated_by": "tests/golden/make_golden.py",
             "reference_code": "oracle/_ref/libref_parity.so (lib/cpu smearing_HYP, "
-                              "smearing_APE, wilson_loop, plaket_site; -O2 -fno-fast-math)",
+                              "smearing_APE, wilson_loop, wilson_loop_adjoint, plaket_site; "
+                              "-O2 -fno-fast-math)",
             "link_layout": "4*V links, link index 4*site+mu, row-major (get_data order)",
             "cases": index}
     (OUT / "index.json").write_text(json.dumps(meta, indent=1))

@@ -38,6 +38,9 @@ def test_fp64_matches_reference_fixture(name, meta):
         assert max_abs(lat.download(), g["links_ape"]) <= LINK_ATOL
         w = lat.wilson_loop(meta["r_min"], meta["r_max"], meta["time_min"], meta["time_max"])
         assert_w_close(w, g["wilson"])
+        wa = lat.wilson_loop_adjoint(meta["r_min"], meta["r_max"], meta["time_min"],
+                                     meta["time_max"])
+        assert_w_close(wa, g["wilson_adjoint"])
         assert lat.plaquette() == pytest.approx(g["plaquettes"][1], rel=1e-12)
 
 
@@ -62,6 +65,7 @@ def test_fp64_matches_oracle_seeded(port, nc, dims, eps, hyp, n_ape, rng):
         lat.ape(0.5, n_ape)
         assert max_abs(lat.download(), ref) <= LINK_ATOL
         assert_w_close(lat.wilson_loop(*rng), w_ref)
+        assert_w_close(lat.wilson_loop_adjoint(*rng), port.wilson_adjoint(nc, dims, ref, *rng))
         assert lat.plaquette() == pytest.approx(port.plaquette(nc, dims, ref), rel=1e-12)
 
 

@@ -28,6 +28,9 @@ def test_port_matches_reference_fixture(port, name, meta):
     assert max_abs(links, g["links_ape"]) <= 1e-13
     w = port.wilson(nc, dims, links, meta["r_min"], meta["r_max"], meta["time_min"], meta["time_max"])
     np.testing.assert_allclose(w, g["wilson"], rtol=1e-12, atol=0)
+    wa = port.wilson_adjoint(nc, dims, links, meta["r_min"], meta["r_max"], meta["time_min"],
+                             meta["time_max"])
+    np.testing.assert_allclose(wa, g["wilson_adjoint"], rtol=1e-12, atol=1e-14)
     assert abs(port.plaquette(nc, dims, links) - g["plaquettes"][1]) <= 1e-12
 
 
@@ -47,6 +50,9 @@ def test_reference_reproduces_fixture(name, meta):
     assert max_abs(links, g["links_ape"]) == 0.0
     w = ref.wilson(nc, dims, links, meta["r_min"], meta["r_max"], meta["time_min"], meta["time_max"])
     np.testing.assert_allclose(w, g["wilson"], rtol=1e-13, atol=0)
+    wa = ref.wilson_adjoint(nc, dims, links, meta["r_min"], meta["r_max"], meta["time_min"],
+                            meta["time_max"])
+    np.testing.assert_allclose(wa, g["wilson_adjoint"], rtol=1e-13, atol=0)
 
 
 @pytest.mark.parametrize("nc", [2, 3])
