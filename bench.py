@@ -294,7 +294,6 @@ def bench_serving(duration_s: float, rate: float = 200.0, slots: int = 8):
             lat.ape(j.ape_alpha, j.ape_steps)
             w = lat.wilson_loop(1, j.r_max, 1, j.t_max)
         err = max(err, float(np.max(np.abs(results[k] - w) / np.abs(w))))
-    worst = max(sample, key=lambda k: 0) if sample else None
     return {"workload": f"Poisson {rate:g} req/s for {duration_s:g} s, L^4 with L 8..32",
             "requests": n, "completed": st["completed"], "offered_rate": rate,
             "wall_s": wall, "p50_ms": st["p50_ms"], "p99_ms": st["p99_ms"],
