@@ -178,10 +178,15 @@ int ensure_dev_out(gc_lattice *h, size_t n) {
   return GC_OK;
 }
 
+// One HYP decorated-link field (256-byte aligned).
+size_t hyp_field_bytes(const gc_lattice *h) {
+  return ((inter_link_bytes(h->nc, h->prec) * (size_t)h->g.V + 255) / 256) * 256;
+}
+
 int ensure_hyp(gc_lattice *h) {
   if (h->hyp)
     return GC_OK;
-  cudaError_t e = dev_alloc(h, &h->hyp, 15 * h->field_bytes);
+  cudaError_t e = dev_alloc(h, &h->hyp, 15 * hyp_field_bytes(h));
   if (e != cudaSuccess) {
     h->hyp = nullptr;
     return cuda_fail(h, "cudaMalloc(HYP decorated links)", e);
@@ -451,10 +456,11 @@ int gc_hyp(gc_lattice *h, double a1, double a2, double a3, int steps) {
     return rc;
   HypL1 l1;
   HypL2 l2;
+  const size_t hb = hyp_field_bytes(h);
   for (int i = 0; i < 9; i++)
-    l1.f[i] = (char *)h->hyp + i * h->field_bytes;
+    l1.f[i] = (char *)h->hyp + i * hb;
   for (int i = 0; i < 6; i++)
-    l2.f[i] = (char *)h->hyp + (9 + i) * h->field_bytes;
+    l2.f[i] = (char *)h->hyp + (9 + i) * hb;
   for (int s = 0; s < steps; s++) {
     rc = GC_DISPATCH(h, launch_hyp, h->g, h->cur, l1, l2, h->alt.f[3], a1, a2, a3,
                      h->stream);
@@ -665,7 +671,9 @@ long long gc_job_device_bytes(const int dims[4], int nc, int precision,
   const int nr = std::max(1, rmax), nt = std::max(1, tmax);
   const long long partials =
       (long long)wilson_partials_count(g, std::min(nr, std::max(1, 1024 / nt)), nt, nc) * 8;
-  return 8 * field + 15 * field + staging + partials + 64LL * 1024;
+  const long long hfield =
+      ((long long)inter_link_bytes(nc, precision) * V + 255) / 256 * 256;
+  return 8 * field + 15 * hfield + staging + partials + 64LL * 1024;
 }
 
 } // extern "C"

@@ -80,6 +80,7 @@ struct JobState {
   gc_job desc;
   Geom g;
   size_t field_bytes;
+  size_t hyp_bytes; // one HYP decorated-link field
   void *input[4];  // the job's configuration (kept between runs)
   void *setA[4], *setB[4];
   void *hyp[15];
@@ -563,7 +564,8 @@ int gc_batch_create(const gc_job *jobs, int njobs, int precision, gc_batch **out
     const bool w = !(j.desc.r_max == 0 && j.desc.time_max == 0);
     j.nr = w ? j.desc.r_max - j.desc.r_min + 1 : 0;
     j.nt = w ? j.desc.time_max - j.desc.time_min + 1 : 0;
-    total += (12 + (j.desc.hyp_steps > 0 ? 15 : 0)) * j.field_bytes;
+    j.hyp_bytes = align256(inter_link_bytes(j.desc.nc, precision) * (size_t)j.g.V);
+    total += 12 * j.field_bytes + (j.desc.hyp_steps > 0 ? 15 * j.hyp_bytes : 0);
     staging = std::max(staging, (size_t)(j.desc.nc == 3 ? 18 : 4) * 8 * 4 * (size_t)j.g.V);
     outs += (size_t)j.nr * j.nt;
     if (w)
@@ -586,8 +588,8 @@ int gc_batch_create(const gc_job *jobs, int njobs, int precision, gc_batch **out
     }
     const int nh = j.desc.hyp_steps > 0 ? 15 : 0;
     for (int f = 0; f < 15; f++)
-      j.hyp[f] = nh ? base + (12 + f) * j.field_bytes : nullptr;
-    off += (12 + nh) * j.field_bytes;
+      j.hyp[f] = nh ? base + 12 * j.field_bytes + f * j.hyp_bytes : nullptr;
+    off += 12 * j.field_bytes + nh * j.hyp_bytes;
   }
   b->outs_count = std::max<size_t>(outs, 1);
   bool ok = cudaMalloc(&b->outs, b->outs_count * sizeof(double)) == cudaSuccess &&

@@ -134,6 +134,37 @@ struct StoreF32SU3 {
   }
 };
 
+// FP32 SU(3) with all 18 reals: 9 planes of float2 (element (k/3, k%3)).
+// Used for fields that may hold matrices that are not in SU(3) -- HYP's
+// decorated links, whose projection (six Newton-Schulz steps, as in the
+// reference) need not converge -- where rebuilding the third row would
+// change the matrix.
+struct StoreF32SU3Full {
+  static constexpr int NC = 3;
+  static constexpr int kBytes = 72;
+  template <class CT> using M = SU3<CT>;
+  template <class CT>
+  __device__ __forceinline__ static SU3<CT> load(const void *f, size_t V,
+                                                 int site) {
+    const float2 *p = reinterpret_cast<const float2 *>(f) + site;
+    SU3<CT> u;
+#pragma unroll
+    for (int k = 0; k < 9; k++) {
+      float2 v = __ldg(p + k * V);
+      u.e[k / 3][k % 3] = {CT(v.x), CT(v.y)};
+    }
+    return u;
+  }
+  template <class CT>
+  __device__ __forceinline__ static void store(void *f, size_t V, int site,
+                                               const SU3<CT> &u) {
+    float2 *p = reinterpret_cast<float2 *>(f) + site;
+#pragma unroll
+    for (int k = 0; k < 9; k++)
+      p[k * V] = make_float2(float(u.e[k / 3][k % 3].re), float(u.e[k / 3][k % 3].im));
+  }
+};
+
 struct StoreF32SU2 {
   static constexpr int NC = 2;
   static constexpr int kBytes = 16;
@@ -151,6 +182,21 @@ struct StoreF32SU2 {
         make_float4(float(u.a0), float(u.a1), float(u.a2), float(u.a3));
   }
 };
+
+// Storage of HYP's decorated-link fields for a link storage type: the same,
+// except that 12-real SU(3) becomes the full 18-real form.
+template <class Store> struct InterStore {
+  using type = Store;
+};
+template <> struct InterStore<StoreF32SU3> {
+  using type = StoreF32SU3Full;
+};
+// Bytes per link of HYP's decorated-link fields.
+inline size_t inter_link_bytes(int nc, int prec) {
+  if (nc == 3)
+    return prec == 0 ? 144 : 72;
+  return prec == 0 ? 32 : 16;
+}
 
 // Conversion between compute types (identity when equal).
 template <class TO, class FROM>

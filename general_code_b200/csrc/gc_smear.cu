@@ -41,6 +41,10 @@ __device__ __forceinline__ void add_staples(M &S, const void *fmu,
 template <class Store> struct ProjTol {
   static constexpr double value = (Store::kBytes == 144 || Store::kBytes == 32) ? 1e-14 : 1e-9;
 };
+// HYP's decorated links of the mixed form are kept in FP32 with all 18 reals
+// (InterStore): the reference's six-step projection of a level-1 or level-2
+// sum need not reach SU(3) (e.g. 0.4 U + 0.3 x staples can be nearly
+// singular), and the 12-real form would replace such a matrix's third row.
 
 template <class Store, class CT, class M>
 __device__ __forceinline__ void proj_store(void *out, size_t V, int site,
@@ -111,7 +115,7 @@ __device__ __forceinline__ void hyp_l1_site(const Geom &g, const Fields4 &U,
   Nbr n = neighbours(g, site, x, mu, eta);
   add_staples<Store, CT>(S, U.f[mu], U.f[eta], V, site, n.pnu, n.pmu, n.mnu,
                          n.mnu_pmu, CT(alpha3 / 2));
-  proj_store<Store, CT>(out.f[f], V, site, S);
+  proj_store<typename InterStore<Store>::type, CT>(out.f[f], V, site, S);
 }
 
 // Level-1 field holding Vbar_{mu; nu, t} for spatial mu != nu.
@@ -145,10 +149,10 @@ __device__ __forceinline__ void hyp_l2_site(const Geom &g, const Fields4 &U,
                                : l1.f[l1_spatial(nu, rho)];
     const void *fnu = l1.f[l1_spatial(rho, nu)];
     Nbr n = neighbours(g, site, x, mu, rho);
-    add_staples<Store, CT>(S, fmu, fnu, V, site, n.pnu, n.pmu, n.mnu,
-                           n.mnu_pmu, c);
+    add_staples<typename InterStore<Store>::type, CT>(S, fmu, fnu, V, site, n.pnu, n.pmu,
+                                                      n.mnu, n.mnu_pmu, c);
   }
-  proj_store<Store, CT>(out.f[f], V, site, S);
+  proj_store<typename InterStore<Store>::type, CT>(out.f[f], V, site, S);
 }
 
 // Level 3: the new temporal link (smearing.h:484-503).
@@ -165,8 +169,8 @@ __device__ __forceinline__ void hyp_l3_site(const Geom &g, const void *Ut,
 #pragma unroll 1
   for (int nu = 0; nu < 3; nu++) {
     Nbr n = neighbours(g, site, x, 3, nu);
-    add_staples<Store, CT>(S, l2.f[nu], l2.f[3 + nu], V, site, n.pnu, n.pmu,
-                           n.mnu, n.mnu_pmu, c);
+    add_staples<typename InterStore<Store>::type, CT>(S, l2.f[nu], l2.f[3 + nu], V, site,
+                                                      n.pnu, n.pmu, n.mnu, n.mnu_pmu, c);
   }
   proj_store<Store, CT>(out_t, V, site, S);
 }

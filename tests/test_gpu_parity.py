@@ -166,3 +166,21 @@ def test_results_are_deterministic(precision):
             out.append((lat.wilson_loop(1, 4, 1, 4), lat.plaquette()))
     assert np.array_equal(out[0][0], out[1][0])
     assert out[0][1] == out[1][1]
+
+
+@pytest.mark.parametrize("nc", [2, 3])
+@pytest.mark.parametrize("precision,atol", [("fp64", 1e-14), ("mixed", 1e-6)])
+def test_abelian_flux_closed_form(nc, precision, atol):
+    """Closed-form W(R,T) and plaquette of a constant-flux diagonal
+    configuration, before and after APE (for which it is a fixed point)."""
+    from conftest import abelian_flux_config
+    dims = (6, 5, 4, 8)
+    links, wf, plaq = abelian_flux_config(dims, nc)
+    expect = np.array([[wf(r, t) for r in range(1, 4)] for t in range(1, 5)])
+    with Lattice(dims, nc, precision) as lat:
+        lat.upload(links)
+        assert lat.plaquette() == pytest.approx(plaq, abs=atol)
+        np.testing.assert_allclose(lat.wilson_loop(1, 3, 1, 4), expect, atol=atol)
+        lat.ape(0.5, 3)
+        assert max_abs(lat.download(), links) <= (1e-14 if precision == "fp64" else 1e-6)
+        np.testing.assert_allclose(lat.wilson_loop(1, 3, 1, 4), expect, atol=atol)

@@ -91,3 +91,17 @@ def test_smeared_links_are_special_unitary(port, nc, eps):
     port.hyp(nc, dims, a, 1.0, 0.75, 0.6, 1)
     port.ape(nc, dims, a, 0.5, 2)
     assert unitarity_error(nc, a) < 1e-12
+
+
+@pytest.mark.parametrize("nc", [2, 3])
+def test_abelian_flux_closed_form(port, nc):
+    from conftest import abelian_flux_config
+    dims = (6, 5, 4, 8)
+    links, wf, plaq = abelian_flux_config(dims, nc)
+    assert port.plaquette(nc, dims, links) == pytest.approx(plaq, abs=1e-14)
+    expect = np.array([[wf(r, t) for r in range(1, 4)] for t in range(1, 5)])
+    np.testing.assert_allclose(port.wilson(nc, dims, links, 1, 3, 1, 4), expect, atol=1e-14)
+    v = links.copy()
+    port.ape(nc, dims, v, 0.5, 3)  # fixed point
+    assert max_abs(v, links) <= 1e-14
+    np.testing.assert_allclose(port.wilson(nc, dims, v, 1, 3, 1, 4), expect, atol=1e-14)
