@@ -353,6 +353,35 @@ template <class T> GC_HD SU3<T> proj(const SU3<T> &A, T tol) {
 }
 template <class T> GC_HD SU2<T> proj(const SU2<T> &A, T) { return proj(A); }
 
+// Newton-Schulz steps from A until a step changes no element by more than
+// tol, at most max_steps of them; *steps receives the number taken. Used
+// by the mixed-precision projection: FP32 steps while the iteration still
+// moves, then one FP64 step (ns_step<double>), which removes the FP32
+// rounding of a converged iterate (the error after a step is O(d^2) for an
+// input error d, so an FP32-converged iterate, d ~ 1e-7, lands at FP64
+// rounding). Together at most six steps, like the reference's projection.
+template <class T> GC_HD SU3<T> ns_until(SU3<T> B, T tol, int max_steps, int *steps) {
+  int n = 0;
+#pragma unroll 1
+  while (n < max_steps) {
+    SU3<T> N = ns_step(B);
+    n++;
+    T d = T(0);
+#pragma unroll
+    for (int i = 0; i < 3; i++)
+#pragma unroll
+      for (int j = 0; j < 3; j++) {
+        d = fmax(d, fabs(N.e[i][j].re - B.e[i][j].re));
+        d = fmax(d, fabs(N.e[i][j].im - B.e[i][j].im));
+      }
+    B = N;
+    if (d <= tol)
+      break;
+  }
+  *steps = n;
+  return B;
+}
+
 // Gram-Schmidt reunitarisation: rows 0 and 1 orthonormalised, row 2 =
 // conj(row0 x row1). Used by the configuration generator (not on the
 // reference path).

@@ -270,7 +270,7 @@ int build_schedule(gc_batch *b) {
     {
       std::vector<WJob> t;
       std::vector<RJob> r;
-      int blocks = 0, entries = 0;
+      int blocks = 0, entries = 0, threads = 32;
       size_t smem = 0;
       const int ct = prec == GC_PREC_FP64 ? 8 : 4;
       for (int i : ids) {
@@ -290,21 +290,24 @@ int build_schedule(gc_batch *b) {
         w.block_start = blocks;
         w.blocks = j.w_blocks;
         blocks += j.w_blocks;
-        smem = std::max(smem, wilson_job_smem(w, nc, ct));
+        threads = std::max(threads, wilson_threads(j.cols, j.rows, wilson_lanes(nc, ct)));
         t.push_back(w);
         RJob q;
         q.partials = j.partials;
         q.nblocks = j.w_blocks;
         q.nr = j.nr;
         q.nt = j.nt;
-        q.scale = 1.0 / (3.0 * (double)j.g.V);
+        q.scale = wilson_scale(j.g.V, j.desc.nc, false);
         q.out = j.out_dev;
         q.entry_start = entries;
         entries += j.nr * j.nt;
         r.push_back(q);
       }
+      for (const WJob &w : t)
+        smem = std::max(smem, wilson_job_smem(w, nc, ct, threads));
       if (!t.empty()) {
-        Launch L{Launch::W, cls, push_table(arena, t), (int)t.size(), {blocks, 0, 0}, smem};
+        // blocks[1]: threads per block (the widest job shape of the launch)
+        Launch L{Launch::W, cls, push_table(arena, t), (int)t.size(), {blocks, threads, 0}, smem};
         b->launches.push_back(L);
         Launch R{Launch::REDUCE, cls, push_table(arena, r), (int)r.size(), {entries, 0, 0}, 0};
         b->launches.push_back(R);
@@ -347,7 +350,8 @@ int enqueue_class(gc_batch *b, int cls, cudaStream_t s) {
       rc = launch_ape_batch<Store, CT>((const ApeJob *)tab, L.njobs, L.blocks[0], s);
       break;
     case Launch::W:
-      rc = launch_wilson_batch<Store, CT>((const WJob *)tab, L.njobs, L.blocks[0], L.smem, s);
+      rc = launch_wilson_batch<Store, CT>((const WJob *)tab, L.njobs, L.blocks[0], L.blocks[1],
+                                          L.smem, s);
       break;
     case Launch::REDUCE:
       rc = launch_reduce_batch((const RJob *)tab, L.njobs, L.blocks[0], s);
@@ -438,7 +442,7 @@ int tune_job(gc_batch *b, JobState &j, double *scratch, cudaStream_t s, int *row
     if (Lt % rows || rows < std::min(4, Lt))
       continue;
     for (int threads : {128, 256}) {
-      const int cols = threads / rows;
+      const int cols = wilson_lanes(j.desc.nc, b->prec == GC_PREC_FP64 ? 8 : 4) * (threads / rows);
       if (cols < 1)
         continue;
       float ms = 0;

@@ -36,17 +36,24 @@ __host__ __device__ inline void site_coords(const Geom &g, int site, int x[4]) {
   x[3] = r / g.L[2];
 }
 
+// a[d] for a direction d known only at run time, as selects (a dynamically
+// indexed array would be placed in local memory).
+__host__ __device__ __forceinline__ int sel4(const int a[4], int d) {
+  return d == 0 ? a[0] : d == 1 ? a[1] : d == 2 ? a[2] : a[3];
+}
+
 // Offset of a one-step move in direction mu (+1 or -1) from coordinate xm.
 __host__ __device__ inline int step_off(const Geom &g, int xm, int mu, int dir) {
+  const int L = sel4(g.L, mu), st = sel4(g.stride, mu);
   if (dir > 0)
-    return (xm == g.L[mu] - 1) ? -(g.L[mu] - 1) * g.stride[mu] : g.stride[mu];
-  return (xm == 0) ? (g.L[mu] - 1) * g.stride[mu] : -g.stride[mu];
+    return (xm == L - 1) ? -(L - 1) * st : st;
+  return (xm == 0) ? (L - 1) * st : -st;
 }
 
 // Offset of an n-step forward move (n >= 0, any size) from coordinate xm.
 __host__ __device__ inline int fwd_off(const Geom &g, int xm, int mu, int n) {
-  int xn = (xm + n) % g.L[mu];
-  return (xn - xm) * g.stride[mu];
+  int xn = (xm + n) % sel4(g.L, mu);
+  return (xn - xm) * sel4(g.stride, mu);
 }
 
 // ------------------------------------------------------------- storage

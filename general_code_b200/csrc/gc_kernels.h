@@ -68,11 +68,11 @@ struct RJob {           // fixed-order reduction of one lattice's partials
   int entry_start;      // first block of the reduction launch
 };
 template <class Store, class CT>
-int launch_wilson_batch(const WJob *jobs, int njobs, int blocks, size_t smem,
+int launch_wilson_batch(const WJob *jobs, int njobs, int blocks, int threads, size_t smem,
                         cudaStream_t s);
 int launch_reduce_batch(const RJob *jobs, int njobs, int entries, cudaStream_t s);
 // Shared memory one lattice's W blocks need.
-size_t wilson_job_smem(const WJob &j, int nc, int ct_bytes);
+size_t wilson_job_smem(const WJob &j, int nc, int ct_bytes, int threads);
 
 // Wilson loops: per-block partial sums into `partials` (device, sized by
 // wilson_partials_count), then a fixed-order reduction into `out_dev`
@@ -80,7 +80,7 @@ size_t wilson_job_smem(const WJob &j, int nc, int ct_bytes);
 struct WilsonPlan {
   int cols_per_block; // spatial columns per block
   int rows;           // threads per column (a divisor of Lt, <= 32)
-  int threads;        // cols_per_block * rows
+  int threads;        // ceil(cols_per_block / lanes) * rows, whole warps
   int blocks;         // ceil(Vs / cols_per_block) * 3
   size_t smem;        // dynamic shared memory bytes
   bool fits;          // false when even one column exceeds the budget
@@ -89,6 +89,30 @@ struct WilsonPlan {
 // to an even count so the 16-byte arrays placed after them stay aligned.
 __host__ __device__ inline size_t wacc_doubles(int nwarps, int nr, int nt) {
   return ((size_t)nwarps * nr * nt + 1) & ~(size_t)1;
+}
+// Spatial columns one W thread carries: two adjacent columns (packed FP32x2
+// arithmetic) for FP32 SU(3), one otherwise.
+__host__ __device__ constexpr int wilson_lanes(int nc, int ct_bytes) {
+  return (nc == 3 && ct_bytes == 4) ? 2 : 1;
+}
+// The W kernels sum raw traces Re Tr W (SU(3)) or a.b = Re Tr W / 2 (SU(2),
+// quaternion form); the fundamental normalisation 1/N of the reference's
+// multiply_conj_tr is applied once, with the 1/(3V) average, to the sums.
+__host__ __device__ inline double wilson_trace_norm(int nc) { return nc == 3 ? 3.0 : 1.0; }
+// Scale of the summed per-block partials: 1/(3V) over sites and the three
+// spatial directions, times 1/N for the fundamental SU(3) trace (the adjoint
+// character |Tr W|^2 - 1 is summed as is).
+inline double wilson_scale(long long V, int nc, bool adjoint) {
+  return 1.0 / (3.0 * (double)V * (adjoint ? 1.0 : wilson_trace_norm(nc)));
+}
+// Row stride of a W block's shared column arrays: cols rounded up to a
+// multiple of the lane count.
+__host__ __device__ inline int wilson_col_stride(int cols, int lanes) {
+  return (cols + lanes - 1) / lanes * lanes;
+}
+// Threads of a W block shape (whole warps).
+__host__ __device__ inline int wilson_threads(int cols, int rows, int lanes) {
+  return ((wilson_col_stride(cols, lanes) / lanes * rows + 31) / 32) * 32;
 }
 // At most this many (R,T) entries per launch (callers split R into chunks).
 constexpr int kWilsonMaxEntries = 1024;
@@ -104,7 +128,7 @@ int launch_wilson(const Geom &g, const Fields4 &U, int rmin, int rmax,
                   int tmin, int tmax, double *partials, double *out_dev,
                   cudaStream_t s, bool adjoint = false);
 
-// An explicit block shape (rows must divide Lt, rows*cols <= 256).
+// An explicit block shape (rows must divide Lt, at most 256 threads).
 WilsonPlan wilson_plan_shape(const Geom &g, int nr, int nt, int nc, int ct_bytes, int rows,
                              int cols);
 // W with an explicit plan; out_dev == nullptr skips the reduction.

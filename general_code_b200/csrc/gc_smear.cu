@@ -34,24 +34,39 @@ __device__ __forceinline__ void add_staples(M &S, const void *fmu,
   S = add(S, mul(scale(b, c), Store::template load<CT>(fnu, V, x_mnu_pmu)));
 }
 
-// Projection tolerance: an update below it ends the iteration early (see
-// proj in gc_algebra.cuh). FP64 links: 1e-14, so the result equals the full
-// six-step iteration to rounding. FP32-stored links: 1e-9, far below the
-// 6e-8 rounding of the stored result.
+// Projection tolerance of the FP64 iteration: an update below it ends the
+// iteration early (see proj in gc_algebra.cuh); 1e-14, so the result equals
+// the full six-step iteration to rounding. (SU(2) projection is a single
+// normalisation and FP32-stored SU(3) uses proj_store's split iteration.)
 template <class Store> struct ProjTol {
-  static constexpr double value = (Store::kBytes == 144 || Store::kBytes == 32) ? 1e-14 : 1e-9;
+  static constexpr double value = 1e-14;
 };
 // HYP's decorated links of the mixed form are kept in FP32 with all 18 reals
 // (InterStore): the reference's six-step projection of a level-1 or level-2
 // sum need not reach SU(3) (e.g. 0.4 U + 0.3 x staples can be nearly
 // singular), and the 12-real form would replace such a matrix's third row.
 
+// FP32-stored SU(3) (the mixed form): Newton-Schulz steps in FP32 while a
+// step still changes an element by more than 1e-5 (at most five), then one
+// FP64 step, whose result is stored (ns_until). Other storage: the
+// reference's iteration in FP64 with the early exit of proj(A, tol).
+template <class Store> struct SplitProj {
+  static constexpr bool value = Store::NC == 3 && (Store::kBytes == 48 || Store::kBytes == 72);
+};
+
 template <class Store, class CT, class M>
 __device__ __forceinline__ void proj_store(void *out, size_t V, int site,
                                            const M &S) {
   using MD = typename Store::template M<double>;
-  MD d = convert(S, (MD *)nullptr);
-  Store::template store<double>(out, V, site, proj(d, ProjTol<Store>::value));
+  if constexpr (SplitProj<Store>::value) {
+    using MF = typename Store::template M<float>;
+    int n;
+    const MF f = ns_until(convert(S, (MF *)nullptr), 1e-5f, 5, &n);
+    Store::template store<double>(out, V, site, ns_step(convert(f, (MD *)nullptr)));
+  } else {
+    MD d = convert(S, (MD *)nullptr);
+    Store::template store<double>(out, V, site, proj(d, ProjTol<Store>::value));
+  }
 }
 
 struct Nbr {
@@ -61,9 +76,9 @@ struct Nbr {
 __device__ __forceinline__ Nbr neighbours(const Geom &g, int site,
                                           const int x[4], int mu, int nu) {
   Nbr n;
-  const int dpn = step_off(g, x[nu], nu, +1);
-  const int dmn = step_off(g, x[nu], nu, -1);
-  const int dpm = step_off(g, x[mu], mu, +1);
+  const int dpn = step_off(g, sel4(x, nu), nu, +1);
+  const int dmn = step_off(g, sel4(x, nu), nu, -1);
+  const int dpm = step_off(g, sel4(x, mu), mu, +1);
   n.pnu = site + dpn;
   n.pmu = site + dpm;
   n.mnu = site + dmn;

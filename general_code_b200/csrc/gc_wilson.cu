@@ -24,15 +24,70 @@
 // (R,T), then a fixed-order tree over blocks.
 #include "gc_internal.cuh"
 #include "gc_kernels.h"
+#include "gc_pair.cuh"
+
+#include <type_traits>
 
 namespace gc {
 
 namespace {
 
-// Shared-memory matrices are stored element-major as 2-vectors: complex
-// element k (or quaternion pair k) of matrix i at sm[k*stride + i], one
-// 8-byte (FP32) or 16-byte (FP64) load per element, consecutive threads on
-// consecutive addresses.
+// ------------------------------------------------------ shared column storage
+// A block keeps three sets of matrices in shared memory (space lines, own
+// time links, neighbour time links), one slot per (t, column unit), slot
+// index t * cs + u. SU(3) slots are contiguous 144-byte records, read and
+// written as 16-byte vectors at immediate offsets from one address per slot:
+//   SU3<double>: element k at double2 [9 i + k]  = (re, im)
+//   SU3<f2>    : element k at float4  [9 i + k]  = (re lane0, re lane1,
+//                                                   im lane0, im lane1)
+// Consecutive threads hold consecutive slots (a 144-byte = 36-word stride),
+// so each quarter-warp phase of a 16-byte access covers all 32 banks once.
+// SU(2) slots (16 or 32 bytes) stay element-major planes of 2-vectors,
+// element pair k of slot i at [k * nslots + i].
+template <class M> struct ColSet;
+template <> struct ColSet<SU3<double>> {
+  static constexpr int kBytes = 144;
+  __device__ __forceinline__ static void store(unsigned char *set, int, int i,
+                                               const SU3<double> &m) {
+    double2 *p = reinterpret_cast<double2 *>(set) + 9 * i;
+#pragma unroll
+    for (int k = 0; k < 9; k++)
+      p[k] = make_double2(m.e[k / 3][k % 3].re, m.e[k / 3][k % 3].im);
+  }
+  __device__ __forceinline__ static SU3<double> load(const unsigned char *set, int, int i) {
+    const double2 *p = reinterpret_cast<const double2 *>(set) + 9 * i;
+    SU3<double> m;
+#pragma unroll
+    for (int k = 0; k < 9; k++) {
+      const double2 v = p[k];
+      m.e[k / 3][k % 3] = {v.x, v.y};
+    }
+    return m;
+  }
+};
+template <> struct ColSet<SU3<f2>> {
+  static constexpr int kBytes = 144;
+  __device__ __forceinline__ static void store(unsigned char *set, int, int i,
+                                               const SU3<f2> &m) {
+    float4 *p = reinterpret_cast<float4 *>(set) + 9 * i;
+#pragma unroll
+    for (int k = 0; k < 9; k++) {
+      const float2 re = m.e[k / 3][k % 3].re.v, im = m.e[k / 3][k % 3].im.v;
+      p[k] = make_float4(re.x, re.y, im.x, im.y);
+    }
+  }
+  __device__ __forceinline__ static SU3<f2> load(const unsigned char *set, int, int i) {
+    const float4 *p = reinterpret_cast<const float4 *>(set) + 9 * i;
+    SU3<f2> m;
+#pragma unroll
+    for (int k = 0; k < 9; k++) {
+      const float4 v = p[k];
+      m.e[k / 3][k % 3].re = f2(make_float2(v.x, v.y));
+      m.e[k / 3][k % 3].im = f2(make_float2(v.z, v.w));
+    }
+    return m;
+  }
+};
 template <class T> struct V2;
 template <> struct V2<double> {
   using type = double2;
@@ -40,43 +95,20 @@ template <> struct V2<double> {
 template <> struct V2<float> {
   using type = float2;
 };
-
-template <class T>
-__device__ __forceinline__ void sm_store(typename V2<T>::type *sm, int stride,
-                                         int i, const SU3<T> &m) {
-#pragma unroll
-  for (int k = 0; k < 9; k++)
-    sm[k * stride + i] = {m.e[k / 3][k % 3].re, m.e[k / 3][k % 3].im};
-}
-template <class T>
-__device__ __forceinline__ SU3<T> sm_load(const typename V2<T>::type *sm,
-                                          int stride, int i, SU3<T> *) {
-  SU3<T> m;
-#pragma unroll
-  for (int k = 0; k < 9; k++) {
-    const auto v = sm[k * stride + i];
-    m.e[k / 3][k % 3] = {v.x, v.y};
+template <class T> struct ColSet<SU2<T>> {
+  using VT = typename V2<T>::type;
+  static constexpr int kBytes = 2 * sizeof(VT);
+  __device__ __forceinline__ static void store(unsigned char *set, int nslots, int i,
+                                               const SU2<T> &m) {
+    VT *p = reinterpret_cast<VT *>(set);
+    p[i] = {m.a0, m.a1};
+    p[nslots + i] = {m.a2, m.a3};
   }
-  return m;
-}
-template <class T>
-__device__ __forceinline__ void sm_store(typename V2<T>::type *sm, int stride,
-                                         int i, const SU2<T> &m) {
-  sm[i] = {m.a0, m.a1};
-  sm[stride + i] = {m.a2, m.a3};
-}
-template <class T>
-__device__ __forceinline__ SU2<T> sm_load(const typename V2<T>::type *sm,
-                                          int stride, int i, SU2<T> *) {
-  const auto a = sm[i], b = sm[stride + i];
-  return {a.x, a.y, b.x, b.y};
-}
-template <class M> struct Elems;
-template <class T> struct Elems<SU3<T>> {
-  static constexpr int n = 9;
-};
-template <class T> struct Elems<SU2<T>> {
-  static constexpr int n = 2;
+  __device__ __forceinline__ static SU2<T> load(const unsigned char *set, int nslots, int i) {
+    const VT *p = reinterpret_cast<const VT *>(set);
+    const VT a = p[i], b = p[nslots + i];
+    return {a.x, a.y, b.x, b.y};
+  }
 };
 
 __device__ __forceinline__ double warp_sum(double v) {
@@ -86,33 +118,25 @@ __device__ __forceinline__ double warp_sum(double v) {
   return v;
 }
 
-// Re Tr(A B^dag)/N in the compute type, returned in FP64 for accumulation.
-template <class T> __device__ __forceinline__ double conj_tr_d(const SU3<T> &a, const SU3<T> &b) {
-  T s = a.e[0][0].re * b.e[0][0].re;
-  s = GC_FMA(a.e[0][0].im, b.e[0][0].im, s);
-#pragma unroll
-  for (int k = 1; k < 9; k++) {
-    s = GC_FMA(a.e[k / 3][k % 3].re, b.e[k / 3][k % 3].re, s);
-    s = GC_FMA(a.e[k / 3][k % 3].im, b.e[k / 3][k % 3].im, s);
-  }
-  return double(s) / 3.0;
-}
-template <class T> __device__ __forceinline__ double conj_tr_d(const SU2<T> &a, const SU2<T> &b) {
-  T s = a.a0 * b.a0;
-  s = GC_FMA(a.a1, b.a1, s);
-  s = GC_FMA(a.a2, b.a2, s);
-  s = GC_FMA(a.a3, b.a3, s);
-  return double(s);
-}
-
-// The per-loop quantity, from the loop's trace Tr[S K^dag]: the fundamental
-// Re Tr W / N (multiply_conj_tr, matrix.h:54-56, 260-262) or, with ADJ, the
-// adjoint character |Tr W|^2 - 1 (multiply_conj_tr_adjoint / tr_adjoint,
-// matrix.h:62-65, 264-270; SU(2): 4 (a.b)^2 - 1).
+// ------------------------------------------------------------ loop values
+// The per-loop quantity from the loop's trace Tr[S K^dag], summed over the
+// thread's active lanes in FP64: the fundamental Re Tr W (multiply_conj_tr,
+// matrix.h:54-56, 260-262; the 1/N normalisation is applied once to the
+// final sums) or, with ADJ, the adjoint character |Tr W|^2 - 1
+// (multiply_conj_tr_adjoint / tr_adjoint, matrix.h:62-65, 264-270; SU(2):
+// 4 (a.b)^2 - 1).
 template <bool ADJ, class T>
-__device__ __forceinline__ double loop_value(const SU3<T> &a, const SU3<T> &b) {
-  if (!ADJ)
-    return conj_tr_d(a, b);
+__device__ __forceinline__ double loop_value(const SU3<T> &a, const SU3<T> &b, bool) {
+  if (!ADJ) {
+    T s = a.e[0][0].re * b.e[0][0].re;
+    s = GC_FMA(a.e[0][0].im, b.e[0][0].im, s);
+#pragma unroll
+    for (int k = 1; k < 9; k++) {
+      s = GC_FMA(a.e[k / 3][k % 3].re, b.e[k / 3][k % 3].re, s);
+      s = GC_FMA(a.e[k / 3][k % 3].im, b.e[k / 3][k % 3].im, s);
+    }
+    return double(s);
+  }
   T re = a.e[0][0].re * b.e[0][0].re;
   T im = a.e[0][0].im * b.e[0][0].re;
   re = GC_FMA(a.e[0][0].im, b.e[0][0].im, re);
@@ -128,48 +152,108 @@ __device__ __forceinline__ double loop_value(const SU3<T> &a, const SU3<T> &b) {
   return r * r + i * i - 1.0;
 }
 template <bool ADJ, class T>
-__device__ __forceinline__ double loop_value(const SU2<T> &a, const SU2<T> &b) {
-  const double d = conj_tr_d(a, b);
+__device__ __forceinline__ double loop_value(const SU2<T> &a, const SU2<T> &b, bool) {
+  T s = a.a0 * b.a0;
+  s = GC_FMA(a.a1, b.a1, s);
+  s = GC_FMA(a.a2, b.a2, s);
+  s = GC_FMA(a.a3, b.a3, s);
+  const double d = double(s);
   return ADJ ? 4.0 * d * d - 1.0 : d;
 }
+// Two lanes (lane 1 counted only when active).
+template <bool ADJ>
+__device__ __forceinline__ double loop_value(const SU3<f2> &a, const SU3<f2> &b, bool lane1) {
+  if (!ADJ) {
+    f2 s = a.e[0][0].re * b.e[0][0].re;
+    s = fma(a.e[0][0].im, b.e[0][0].im, s);
+#pragma unroll
+    for (int k = 1; k < 9; k++) {
+      s = fma(a.e[k / 3][k % 3].re, b.e[k / 3][k % 3].re, s);
+      s = fma(a.e[k / 3][k % 3].im, b.e[k / 3][k % 3].im, s);
+    }
+    const double v0 = double(s.v.x);
+    return lane1 ? v0 + double(s.v.y) : v0;
+  }
+  f2 re = a.e[0][0].re * b.e[0][0].re;
+  f2 im = a.e[0][0].im * b.e[0][0].re;
+  re = fma(a.e[0][0].im, b.e[0][0].im, re);
+  im = fma(-a.e[0][0].re, b.e[0][0].im, im);
+#pragma unroll
+  for (int k = 1; k < 9; k++) {
+    re = fma(a.e[k / 3][k % 3].re, b.e[k / 3][k % 3].re, re);
+    re = fma(a.e[k / 3][k % 3].im, b.e[k / 3][k % 3].im, re);
+    im = fma(a.e[k / 3][k % 3].im, b.e[k / 3][k % 3].re, im);
+    im = fma(-a.e[k / 3][k % 3].re, b.e[k / 3][k % 3].im, im);
+  }
+  const double r0 = double(re.v.x), i0 = double(im.v.x);
+  const double v0 = r0 * r0 + i0 * i0 - 1.0;
+  if (!lane1)
+    return v0;
+  const double r1 = double(re.v.y), i1 = double(im.v.y);
+  return v0 + (r1 * r1 + i1 * i1 - 1.0);
+}
 
+// Matrix of `lanes` adjacent sites from a link field (lane 1 = site s1).
+template <class Store, class CT, int LANES> struct LaneLoad {
+  using M = typename Store::template M<CT>;
+  __device__ __forceinline__ static M load(const void *f, size_t V, int s0, int) {
+    return Store::template load<CT>(f, V, s0);
+  }
+};
+template <> struct LaneLoad<StoreF32SU3, float, 2> {
+  using M = SU3<f2>;
+  __device__ __forceinline__ static M load(const void *f, size_t V, int s0, int s1) {
+    return zip(StoreF32SU3::load<float>(f, V, s0), StoreF32SU3::load<float>(f, V, s1));
+  }
+};
+
+// ---------------------------------------------------------------- W block
 // One block of the W computation: `cols` spatial columns starting at
-// colblock*cols, direction nu; writes its nr*nt partial sums to part.
+// colblock*cols, direction nu; writes its nr*nt partial sums to part. Each
+// thread carries LANES adjacent columns: LANES = 2 for FP32 SU(3), whose
+// matrices are SU3<f2> so that every product and dot-product term is one
+// packed FP32x2 instruction for both columns. Lane 1 of a pair that runs past
+// the block's columns or the lattice duplicates lane 0's site and contributes
+// nothing.
 template <class Store, class CT, bool ADJ = false>
 __device__ __forceinline__ void wilson_block(const Geom &g, const Fields4 &U, int rmin,
                                              int rmax, int tmin, int tmax, int cols,
                                              int rows, int colblock, int nu,
                                              double *part, unsigned char *smem_raw) {
-  using M = typename Store::template M<CT>;
-  using VT = typename V2<CT>::type;
-  constexpr int NE = Elems<M>::n;
+  constexpr int LANES = wilson_lanes(Store::NC, sizeof(CT));
+  using LL = LaneLoad<Store, CT, LANES>;
+  using M = typename LL::M;
+  using CS = ColSet<M>;
   const int Lt = g.L[3];
   const int nr = rmax - rmin + 1, nt = tmax - tmin + 1;
   const int nwarps = blockDim.x >> 5;
-  double *wacc = reinterpret_cast<double *>(smem_raw);         // [nwarps][nr*nt]
-  const int sstride = Lt * cols;                                // matrices per set
-  // space lines S(s,t,R) of the block's columns
+  const int cs = wilson_col_stride(cols, LANES); // slot units per t (x LANES columns)
+  const int units = cs / LANES;
+  const int nslots = Lt * units;
+  double *wacc = reinterpret_cast<double *>(smem_raw); // [nwarps][nr*nt]
   // (the accumulator block is rounded up to an even number of doubles so the
-  // 16-byte double2 arrays after it stay 16-byte aligned)
-  VT *scol = reinterpret_cast<VT *>(wacc + wacc_doubles(nwarps, nr, nt));
-  // the block's own time links U_t(s, t), reused for every R and T
-  VT *ucol = scol + (size_t)NE * sstride;
-  // the time links of the neighbour columns U_t(s + R nu, t), one R at a time
-  VT *ncol = ucol + (size_t)NE * sstride;
+  // 16-byte vectors after it stay 16-byte aligned; set sizes are multiples of
+  // 16 bytes)
+  unsigned char *scol = reinterpret_cast<unsigned char *>(wacc + wacc_doubles(nwarps, nr, nt));
+  unsigned char *ucol = scol + (size_t)CS::kBytes * nslots; // own time links U_t(s, t)
+  unsigned char *ncol = ucol + (size_t)CS::kBytes * nslots; // U_t(s + R nu, t), per R
 
   const int tid = threadIdx.x;
   const int warp = tid >> 5, lane = tid & 31;
   for (int i = tid; i < nwarps * nr * nt; i += blockDim.x)
     wacc[i] = 0.0;
 
-  const int c = tid % cols;
-  const int row = tid / cols;
-  const int s = colblock * cols + c;
-  const bool active = (row < rows) && (s < g.Vs);
+  const int u = tid % units;
+  const int row = tid / units;
+  const int s0 = colblock * cols + LANES * u;
+  const bool active = (row < rows) && (s0 < g.Vs);
+  const bool lane1 = LANES == 2 && active && (LANES * u + 1 < cols) && (s0 + 1 < g.Vs);
+  const int s1 = lane1 ? s0 + 1 : s0;
   const int kt = Lt / rows;
-  int xs[4] = {0, 0, 0, 0};
-  if (active)
-    site_coords(g, s, xs);
+  // coordinates of the columns along nu, and the lattice's extent and stride
+  // along nu (scalars: no dynamically indexed local arrays)
+  const int Ln = sel4(g.L, nu), stn = sel4(g.stride, nu);
+  const int xn0 = (s0 / stn) % Ln, xn1 = (s1 / stn) % Ln;
   const size_t V = g.V;
   const void *Unu = U.f[nu];
   const void *Ut = U.f[3];
@@ -177,8 +261,7 @@ __device__ __forceinline__ void wilson_block(const Geom &g, const Fields4 &U, in
 #pragma unroll 1
     for (int k = 0; k < kt; k++) {
       const int t0 = row + k * rows;
-      sm_store(ucol, sstride, t0 * cols + c,
-               Store::template load<CT>(Ut, V, s + t0 * g.Vs));
+      CS::store(ucol, nslots, t0 * units + u, LL::load(Ut, V, s0 + t0 * g.Vs, s1 + t0 * g.Vs));
     }
   }
   __syncthreads();
@@ -186,19 +269,21 @@ __device__ __forceinline__ void wilson_block(const Geom &g, const Fields4 &U, in
 #pragma unroll 1
   for (int R = 1; R <= rmax; R++) {
     // Extend the space lines of this thread's corners by one link, and stage
-    // the neighbour column's time links for this R.
+    // the neighbour columns' time links for this R.
     if (active) {
-      const int sl = s + fwd_off(g, xs[nu], nu, R - 1);
-      const int sR = s + fwd_off(g, xs[nu], nu, R);
+      const int l0 = s0 + ((xn0 + R - 1) % Ln - xn0) * stn;
+      const int l1 = s1 + ((xn1 + R - 1) % Ln - xn1) * stn;
+      const int r0 = s0 + ((xn0 + R) % Ln - xn0) * stn;
+      const int r1 = s1 + ((xn1 + R) % Ln - xn1) * stn;
 #pragma unroll 1
       for (int k = 0; k < kt; k++) {
         const int t0 = row + k * rows;
-        M u = Store::template load<CT>(Unu, V, sl + t0 * g.Vs);
-        M sn = (R == 1) ? u : mul(sm_load(scol, sstride, t0 * cols + c, (M *)nullptr), u);
-        sm_store(scol, sstride, t0 * cols + c, sn);
+        const int i = t0 * units + u;
+        M lnk = LL::load(Unu, V, l0 + t0 * g.Vs, l1 + t0 * g.Vs);
+        M sn = (R == 1) ? lnk : mul(CS::load(scol, nslots, i), lnk);
+        CS::store(scol, nslots, i, sn);
         if (R >= rmin)
-          sm_store(ncol, sstride, t0 * cols + c,
-                   Store::template load<CT>(Ut, V, sR + t0 * g.Vs));
+          CS::store(ncol, nslots, i, LL::load(Ut, V, r0 + t0 * g.Vs, r1 + t0 * g.Vs));
       }
     }
     __syncthreads();
@@ -207,21 +292,19 @@ __device__ __forceinline__ void wilson_block(const Geom &g, const Fields4 &U, in
 #pragma unroll 1
       for (int k = 0; k < kt; k++) {
         const int t0 = row + k * rows;
-        M K = active ? sm_load(scol, sstride, t0 * cols + c, (M *)nullptr)
-                     : unit(M());
+        M K = active ? CS::load(scol, nslots, t0 * units + u) : unit(M());
         int tt = t0; // (t0 + T - 1) mod Lt
 #pragma unroll 1
         for (int T = 1; T <= tmax; T++) {
           int tu = tt + 1; // (t0 + T) mod Lt
           tu = (tu == Lt) ? 0 : tu;
           if (active) {
-            M a = sm_load(ucol, sstride, tt * cols + c, (M *)nullptr);
-            M b = sm_load(ncol, sstride, tt * cols + c, (M *)nullptr);
-            K = mul(mul_da(a, K), b);
+            const int i = tt * units + u;
+            K = mul(mul_da(CS::load(ucol, nslots, i), K), CS::load(ncol, nslots, i));
           }
           if (T >= tmin) {
             double term = active
-                ? loop_value<ADJ>(sm_load(scol, sstride, tu * cols + c, (M *)nullptr), K)
+                ? loop_value<ADJ>(CS::load(scol, nslots, tu * units + u), K, lane1)
                 : 0.0;
             term = warp_sum(term);
             if (lane == 0)
@@ -245,13 +328,14 @@ __device__ __forceinline__ void wilson_block(const Geom &g, const Fields4 &U, in
 
 template <class Store, class CT, bool ADJ>
 __global__ void __launch_bounds__(256)
-    wilson_kernel(Geom g, const __grid_constant__ Fields4 U, int rmin, int rmax, int tmin,
+    wilson_kernel(const __grid_constant__ Geom g, const __grid_constant__ Fields4 U, int rmin,
+                  int rmax, int tmin,
                   int tmax, int cols, int rows, double *partials) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const size_t blk = (size_t)blockIdx.y * gridDim.x + blockIdx.x;
   const int ne = (rmax - rmin + 1) * (tmax - tmin + 1);
-  wilson_block<Store, CT, ADJ>(g, U, rmin, rmax, tmin, tmax, cols, rows, blockIdx.x, blockIdx.y,
-                          partials + blk * ne, smem_raw);
+  wilson_block<Store, CT, ADJ>(g, U, rmin, rmax, tmin, tmax, cols, rows, blockIdx.x,
+                               blockIdx.y, partials + blk * ne, smem_raw);
 }
 
 // Several lattices in one launch. A block finds its lattice by binary search
@@ -275,11 +359,12 @@ __global__ void __launch_bounds__(256)
   const int nu = local % 3, colblock = local / 3;
   const int colblocks = jb.blocks / 3;
   const int ne = (jb.rmax - jb.rmin + 1) * (jb.tmax - jb.tmin + 1);
-  if (jb.cols * jb.rows > (int)blockDim.x)
+  if (wilson_threads(jb.cols, jb.rows, wilson_lanes(Store::NC, sizeof(CT))) > (int)blockDim.x)
     return; // a lattice whose shape needs more threads than the launch has
-  wilson_block<Store, CT>(jb.g, jb.U, jb.rmin, jb.rmax, jb.tmin, jb.tmax, jb.cols, jb.rows,
-                          colblock, nu,
-                          jb.partials + ((size_t)nu * colblocks + colblock) * ne, smem_raw);
+  wilson_block<Store, CT, false>(jb.g, jb.U, jb.rmin, jb.rmax, jb.tmin, jb.tmax, jb.cols,
+                                 jb.rows, colblock, nu,
+                                 jb.partials + ((size_t)nu * colblocks + colblock) * ne,
+                                 smem_raw);
 }
 
 // Fixed-order reduction of several lattices' partials; block = (lattice,
@@ -354,15 +439,15 @@ __global__ void __launch_bounds__(256)
     for (int mu = 0; mu < 3; mu++) {
 #pragma unroll 1
       for (int nu = mu + 1; nu < 4; nu++) {
-        const int pm = site + step_off(g, x[mu], mu, +1);
-        const int pn = site + step_off(g, x[nu], nu, +1);
+        const int pm = site + step_off(g, sel4(x, mu), mu, +1);
+        const int pn = site + step_off(g, sel4(x, nu), nu, +1);
         M a = mul(Store::template load<CT>(U.f[mu], V, site),
                   Store::template load<CT>(U.f[nu], V, pm));
         a = mul_ad(a, Store::template load<CT>(U.f[mu], V, pn));
-        acc += conj_tr_d(a, Store::template load<CT>(U.f[nu], V, site));
+        acc += loop_value<false>(a, Store::template load<CT>(U.f[nu], V, site), false);
       }
     }
-    p = acc / 6.0;
+    p = acc / (6.0 * wilson_trace_norm(Store::NC));
   }
   sh[threadIdx.x] = p;
   __syncthreads();
@@ -384,32 +469,33 @@ int largest_divisor_upto(int n, int cap) {
 
 } // namespace
 
-// The block shape depends only on Lt and the group, never on the R/T ranges
-// or the compute type, so every caller that sizes the per-block partials
-// from a plan gets the same block count as the launch. Columns per block are
-// limited so that the shared column storage (FP64 worst case) plus the
-// largest per-warp accumulator set (8 warps x 1024 (R,T) entries) fits in a
-// block's shared memory.
+// The block shape depends only on Lt, the group and the compute type, never
+// on the R/T ranges. A block has about 128 threads (rows = the largest divisor
+// of Lt up to 32, each thread carrying `lanes` columns); columns are limited
+// so that the shared column storage fits kWilsonColumnBudget. The FP64 plan
+// has the fewest columns per block and so the most blocks: callers that size
+// per-block partials before the compute type is known use it.
 WilsonPlan wilson_plan(const Geom &g, int nr, int nt, int nc, int ct_bytes) {
   WilsonPlan p;
   const int Lt = g.L[3];
   const int ncomp = (nc == 3) ? 18 : 4;
+  const int lanes = wilson_lanes(nc, ct_bytes);
   p.rows = largest_divisor_upto(Lt, 32);
-  p.cols_per_block = 256 / p.rows;
+  p.cols_per_block = lanes * (128 / p.rows);
   if (p.cols_per_block < 1)
     p.cols_per_block = 1;
-  const size_t col_bytes = 3 * (size_t)ncomp * Lt * sizeof(double);
-  while (p.cols_per_block > 1 && p.cols_per_block * col_bytes > kWilsonColumnBudget)
+  const size_t col_bytes = 3 * (size_t)ncomp * Lt * ct_bytes;
+  while (p.cols_per_block > 1 &&
+         wilson_col_stride(p.cols_per_block, lanes) * col_bytes > kWilsonColumnBudget)
     p.cols_per_block--;
-  const int active = p.cols_per_block * p.rows;
-  p.threads = ((active + 31) / 32) * 32;
+  p.threads = wilson_threads(p.cols_per_block, p.rows, lanes);
   const int colblocks = (g.Vs + p.cols_per_block - 1) / p.cols_per_block;
   p.blocks = colblocks * 3;
   const int nwarps = p.threads / 32;
   // per-warp accumulators + space lines + own and neighbour time links
   p.smem = wacc_doubles(nwarps, nr, nt) * sizeof(double) +
-           3 * (size_t)ncomp * Lt * p.cols_per_block * ct_bytes;
-  p.fits = p.cols_per_block * col_bytes <= kWilsonColumnBudget;
+           wilson_col_stride(p.cols_per_block, lanes) * col_bytes;
+  p.fits = wilson_col_stride(p.cols_per_block, lanes) * col_bytes <= kWilsonColumnBudget;
   return p;
 }
 
@@ -443,7 +529,7 @@ int launch_wilson(const Geom &g, const Fields4 &U, int rmin, int rmax,
   if (rc)
     return rc;
   reduce_partials_kernel<<<nr * nt, 256, 0, s>>>(
-      partials, p.blocks, nr * nt, nr, nt, 1.0 / (3.0 * (double)g.V), out_dev);
+      partials, p.blocks, nr * nt, nr, nt, wilson_scale(g.V, Store::NC, adjoint), out_dev);
   return launch_check("reduce_partials_kernel");
 }
 
@@ -464,14 +550,15 @@ WilsonPlan wilson_plan_shape(const Geom &g, int nr, int nt, int nc, int ct_bytes
                              int cols) {
   WilsonPlan p;
   const int ncomp = (nc == 3) ? 18 : 4;
+  const int lanes = wilson_lanes(nc, ct_bytes);
   p.rows = rows;
   p.cols_per_block = cols;
-  p.threads = ((rows * cols + 31) / 32) * 32;
+  p.threads = wilson_threads(cols, rows, lanes);
   p.blocks = ((g.Vs + cols - 1) / cols) * 3;
   const int nwarps = p.threads / 32;
   p.smem = wacc_doubles(nwarps, nr, nt) * sizeof(double) +
-           3 * (size_t)ncomp * g.L[3] * cols * ct_bytes;
-  p.fits = (g.L[3] % rows == 0) && rows * cols <= 256 && p.smem <= 227 * 1024;
+           3 * (size_t)ncomp * g.L[3] * wilson_col_stride(cols, lanes) * ct_bytes;
+  p.fits = (g.L[3] % rows == 0) && p.threads <= 256 && p.smem <= 227 * 1024;
   return p;
 }
 
@@ -497,22 +584,27 @@ int launch_wilson_plan(const Geom &g, const Fields4 &U, int rmin, int rmax, int 
   if (!out_dev)
     return GC_OK;
   reduce_partials_kernel<<<nr * nt, 256, 0, s>>>(
-      partials, p.blocks, nr * nt, nr, nt, 1.0 / (3.0 * (double)g.V), out_dev);
+      partials, p.blocks, nr * nt, nr, nt, wilson_scale(g.V, Store::NC, false), out_dev);
   return launch_check("reduce_partials_kernel");
 }
 
-size_t wilson_job_smem(const WJob &j, int nc, int ct_bytes) {
-  const int nwarps = 256 / 32;
+// (for a launch of `threads` threads: the per-warp accumulators are sized by
+// the launch's warps)
+size_t wilson_job_smem(const WJob &j, int nc, int ct_bytes, int threads) {
+  const int nwarps = threads / 32;
   const int ncomp = (nc == 3) ? 18 : 4;
+  const int lanes = wilson_lanes(nc, ct_bytes);
   return wacc_doubles(nwarps, j.rmax - j.rmin + 1, j.tmax - j.tmin + 1) * sizeof(double) +
-         3 * (size_t)ncomp * j.g.L[3] * j.cols * ct_bytes;
+         3 * (size_t)ncomp * j.g.L[3] * wilson_col_stride(j.cols, lanes) * ct_bytes;
 }
 
 template <class Store, class CT>
-int launch_wilson_batch(const WJob *jobs, int njobs, int blocks, size_t smem,
+int launch_wilson_batch(const WJob *jobs, int njobs, int blocks, int threads, size_t smem,
                         cudaStream_t s) {
   if (njobs <= 0 || blocks <= 0)
     return GC_OK;
+  if (threads <= 0 || threads > 256 || threads % 32)
+    return plan_error("wilson_batch_kernel: thread count");
   if (smem > 227 * 1024)
     return plan_error("wilson_batch_kernel: shared memory above 227 KB");
   cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
@@ -526,7 +618,7 @@ int launch_wilson_batch(const WJob *jobs, int njobs, int blocks, size_t smem,
     if (e != cudaSuccess)
       return launch_check("wilson_batch_kernel smem attribute");
   }
-  wilson_batch_kernel<Store, CT><<<blocks, 256, smem, s>>>(jobs, njobs);
+  wilson_batch_kernel<Store, CT><<<blocks, threads, smem, s>>>(jobs, njobs);
   return launch_check("wilson_batch_kernel");
 }
 
@@ -543,8 +635,8 @@ int launch_reduce_batch(const RJob *jobs, int njobs, int entries, cudaStream_t s
                                         cudaStream_t, bool);                  \
   template int launch_plaquette<STORE, CT>(const Geom &, const Fields4 &,     \
                                            double *, double *, cudaStream_t);  \
-  template int launch_wilson_batch<STORE, CT>(const WJob *, int, int, size_t, \
-                                              cudaStream_t);                  \
+  template int launch_wilson_batch<STORE, CT>(const WJob *, int, int, int,     \
+                                              size_t, cudaStream_t);          \
   template int launch_wilson_plan<STORE, CT>(const Geom &, const Fields4 &,   \
                                              int, int, int, int,              \
                                              const WilsonPlan &, double *,    \
