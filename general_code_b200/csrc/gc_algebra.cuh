@@ -258,8 +258,8 @@ template <class T> GC_HD cx<T> det(const SU3<T> &m) {
 // A <- (1 - (det A - 1)/3) A.  H = A A^dag is Hermitian: its upper triangle
 // is computed and mirrored. The factor -1/2 is folded into H (exact: a power
 // of two), so B = 3/2 A + (-H/2) A is one fused chain per element.
-template <class T> GC_HD SU3<T> ns_step(const SU3<T> &A) {
-  cx<T> H[3][3];
+// H = -1/2 A A^dag (Hermitian; entries below the diagonal mirrored).
+template <class T> GC_HD void ns_gram(const SU3<T> &A, cx<T> H[3][3]) {
 #pragma unroll
   for (int i = 0; i < 3; i++) {
     T d = A.e[i][0].re * A.e[i][0].re;
@@ -286,6 +286,10 @@ template <class T> GC_HD SU3<T> ns_step(const SU3<T> &A) {
       H[j][i] = {T(-0.5) * re, T(0.5) * im};
     }
   }
+}
+
+// B = 3/2 A + H A with H from ns_gram, then the determinant phase fix.
+template <class T> GC_HD SU3<T> ns_finish(const SU3<T> &A, const cx<T> H[3][3]) {
   SU3<T> B;
 #pragma unroll
   for (int i = 0; i < 3; i++)
@@ -312,6 +316,12 @@ template <class T> GC_HD SU3<T> ns_step(const SU3<T> &A) {
     for (int j = 0; j < 3; j++)
       B.e[i][j] = cmul(c, B.e[i][j]);
   return B;
+}
+
+template <class T> GC_HD SU3<T> ns_step(const SU3<T> &A) {
+  cx<T> H[3][3];
+  ns_gram(A, H);
+  return ns_finish(A, H);
 }
 
 template <class T> GC_HD SU3<T> proj(const SU3<T> &A) {
@@ -353,30 +363,33 @@ template <class T> GC_HD SU3<T> proj(const SU3<T> &A, T tol) {
 }
 template <class T> GC_HD SU2<T> proj(const SU2<T> &A, T) { return proj(A); }
 
-// Newton-Schulz steps from A until a step changes no element by more than
-// tol, at most max_steps of them; *steps receives the number taken. Used
-// by the mixed-precision projection: FP32 steps while the iteration still
-// moves, then one FP64 step (ns_step<double>), which removes the FP32
-// rounding of a converged iterate (the error after a step is O(d^2) for an
-// input error d, so an FP32-converged iterate, d ~ 1e-7, lands at FP64
-// rounding). Together at most six steps, like the reference's projection.
+// Newton-Schulz steps from B while its unitarity defect max|A A^dag - 1|
+// (read off the step's own Gram matrix) exceeds tol, at most max_steps of
+// them; *steps receives the number taken. The mixed-precision projection
+// takes these in FP32 and then one step in FP64 (ns_step<double>): a step
+// maps a defect d to O(d^2) (A = U(1 + E) becomes U(1 - 3/2 E^2 + ...),
+// d = 2|E|), so from d <= 2e-5 the FP64 step lands below 1e-9, under the
+// FP32 rounding of the stored link, and removes the FP32 rounding of the
+// iterate. Together at most six steps, like the reference's projection.
 template <class T> GC_HD SU3<T> ns_until(SU3<T> B, T tol, int max_steps, int *steps) {
   int n = 0;
 #pragma unroll 1
   while (n < max_steps) {
-    SU3<T> N = ns_step(B);
-    n++;
+    cx<T> H[3][3];
+    ns_gram(B, H);
+    // A A^dag = -2 H
     T d = T(0);
 #pragma unroll
-    for (int i = 0; i < 3; i++)
+    for (int i = 0; i < 3; i++) {
+      d = fmax(d, fabs(T(-2) * H[i][i].re - T(1)));
 #pragma unroll
-      for (int j = 0; j < 3; j++) {
-        d = fmax(d, fabs(N.e[i][j].re - B.e[i][j].re));
-        d = fmax(d, fabs(N.e[i][j].im - B.e[i][j].im));
-      }
-    B = N;
+      for (int j = i + 1; j < 3; j++)
+        d = fmax(d, fmax(fabs(H[i][j].re), fabs(H[i][j].im)) * T(2));
+    }
     if (d <= tol)
       break;
+    B = ns_finish(B, H);
+    n++;
   }
   *steps = n;
   return B;

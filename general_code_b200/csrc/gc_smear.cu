@@ -46,10 +46,10 @@ template <class Store> struct ProjTol {
 // sum need not reach SU(3) (e.g. 0.4 U + 0.3 x staples can be nearly
 // singular), and the 12-real form would replace such a matrix's third row.
 
-// FP32-stored SU(3) (the mixed form): Newton-Schulz steps in FP32 while a
-// step still changes an element by more than 1e-5 (at most five), then one
-// FP64 step, whose result is stored (ns_until). Other storage: the
-// reference's iteration in FP64 with the early exit of proj(A, tol).
+// FP32-stored SU(3) (the mixed form): Newton-Schulz steps in FP32 while the
+// unitarity defect exceeds 2e-5 (at most five), then one FP64 step, whose
+// result is stored (ns_until). Other storage: the reference's iteration in
+// FP64 with the early exit of proj(A, tol).
 template <class Store> struct SplitProj {
   static constexpr bool value = Store::NC == 3 && (Store::kBytes == 48 || Store::kBytes == 72);
 };
@@ -61,7 +61,7 @@ __device__ __forceinline__ void proj_store(void *out, size_t V, int site,
   if constexpr (SplitProj<Store>::value) {
     using MF = typename Store::template M<float>;
     int n;
-    const MF f = ns_until(convert(S, (MF *)nullptr), 1e-5f, 5, &n);
+    const MF f = ns_until(convert(S, (MF *)nullptr), 2e-5f, 5, &n);
     Store::template store<double>(out, V, site, ns_step(convert(f, (MD *)nullptr)));
   } else {
     MD d = convert(S, (MD *)nullptr);
