@@ -5,9 +5,16 @@ The compute path is libgc_b200.so (hand-written CUDA kernels behind the C ABI
 in include/gc_lattice.h); this package is a thin ctypes host layer over it.
 """
 from .lattice import (GCError, Lattice, LatticeData, generate_config, job_device_bytes,
-                      link_size, plaket, probe_config, read_data_convert, smearing_APE,
-                      smearing_HYP, unit_config, volume, wilson_loop)
+                      link_size, plaket, plaket_space, plaket_time, polyakov_average_directions,
+                      polyakov_loop, polyakov_loop_correlator_color_average,
+                      polyakov_loop_correlator_singlet, probe_config, read_data_convert,
+                      smearing_APE, smearing_HYP, unit_config, volume, wilson_gevp_adjoint_indexed,
+                      wilson_gevp_indexed, wilson_loop, wilson_loop_adjoint)
 
 __all__ = ["GCError", "Lattice", "LatticeData", "generate_config", "job_device_bytes",
-           "link_size", "plaket", "probe_config", "read_data_convert", "smearing_APE",
-           "smearing_HYP", "unit_config", "volume", "wilson_loop"]
+           "link_size", "plaket", "plaket_space", "plaket_time", "polyakov_average_directions",
+           "polyakov_loop", "polyakov_loop_correlator_color_average",
+           "polyakov_loop_correlator_singlet", "probe_config", "read_data_convert",
+           "smearing_APE", "smearing_HYP", "unit_config", "volume",
+           "wilson_gevp_adjoint_indexed", "wilson_gevp_indexed", "wilson_loop",
+           "wilson_loop_adjoint"]

@@ -55,6 +55,12 @@ SIGNATURES = {
     "gc_wilson_onaxis": (_c_int, [_p, _c_int, _c_int, _c_int, _c_int, _pdbl]),
     "gc_wilson_adjoint_onaxis": (_c_int, [_p, _c_int, _c_int, _c_int, _c_int, _pdbl]),
     "gc_plaquette": (_c_int, [_p, _pdbl]),
+    "gc_plaquette_space": (_c_int, [_p, _pdbl]),
+    "gc_plaquette_time": (_c_int, [_p, _pdbl]),
+    "gc_wilson_gevp_onaxis": (_c_int, [_p, _p, _c_int, _c_int, _c_int, _c_int, _pdbl]),
+    "gc_wilson_gevp_adjoint_onaxis": (_c_int, [_p, _p, _c_int, _c_int, _c_int, _c_int, _pdbl]),
+    "gc_polyakov_loop": (_c_int, [_p, _pdbl]),
+    "gc_polyakov_correlator": (_c_int, [_p, _c_int, _c_int, _pdbl]),
     "gc_wilson_onaxis_noalloc": (_c_int, [_pint, _c_int, _c_int, ctypes.POINTER(_p), _c_int,
                                           _c_int, _c_int, _c_int, _p, _p]),
     "gc_read_config": (_c_int, [_p, ctypes.c_char_p, ctypes.c_char_p, ctypes.c_longlong,

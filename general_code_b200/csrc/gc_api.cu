@@ -5,10 +5,13 @@
 #include "gc_internal.cuh"
 #include "gc_kernels.h"
 
+#include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <functional>
 #include <mutex>
 #include <string>
+#include <vector>
 
 namespace gc {
 int generate_host(const int dims[4], int nc, double eps, unsigned seed,
@@ -63,6 +66,8 @@ struct gc_lattice {
   size_t partials_cap = 0;  // doubles
   double *dev_out = nullptr;
   size_t dev_out_cap = 0;   // doubles
+  void *aux = nullptr;      // Polyakov lines and offset tables
+  size_t aux_cap = 0;       // bytes
   cudaStream_t own_stream = nullptr;
   cudaStream_t stream = nullptr;
   bool stream_ordered = false; // device memory from cudaMallocAsync on `stream`
@@ -175,6 +180,21 @@ int ensure_dev_out(gc_lattice *h, size_t n) {
     return cuda_fail(h, "cudaMalloc(result)", e);
   }
   h->dev_out_cap = n;
+  return GC_OK;
+}
+
+int ensure_aux(gc_lattice *h, size_t bytes) {
+  if (h->aux_cap >= bytes)
+    return GC_OK;
+  dev_free(h, h->aux);
+  h->aux = nullptr;
+  h->aux_cap = 0;
+  cudaError_t e = dev_alloc(h, &h->aux, bytes);
+  if (e != cudaSuccess) {
+    h->aux = nullptr;
+    return cuda_fail(h, "cudaMalloc(Polyakov scratch)", e);
+  }
+  h->aux_cap = bytes;
   return GC_OK;
 }
 
@@ -315,6 +335,7 @@ int gc_lattice_destroy(gc_lattice *h) {
     dev_free(h, h->staging);
     dev_free(h, h->partials);
     dev_free(h, h->dev_out);
+    dev_free(h, h->aux);
     if (h->own_stream)
       cudaStreamDestroy(h->own_stream);
   }
@@ -471,8 +492,10 @@ int gc_hyp(gc_lattice *h, double a1, double a2, double a3, int steps) {
   return GC_OK;
 }
 
+// W(R,T) of h, or with `second` the GEVP loops of the pair (h, second):
+// h's time lines, space lines of both (wilson_gevp_indexed).
 static int wilson_impl(gc_lattice *h, int rmin, int rmax, int tmin, int tmax,
-                       double *out, bool adjoint) {
+                       double *out, bool adjoint, gc_lattice *second = nullptr) {
   int rc = check_ready(h);
   if (rc)
     return rc;
@@ -480,7 +503,39 @@ static int wilson_impl(gc_lattice *h, int rmin, int rmax, int tmin, int tmax,
     return fail(h, GC_ERR_ARG, "null output");
   if (rmin < 1 || tmin < 1 || rmax < rmin || tmax < tmin)
     return fail(h, GC_ERR_ARG, "need 1 <= r_min <= r_max and 1 <= time_min <= time_max");
-  std::lock_guard<std::mutex> lk(h->mu);
+  if (second && second != h) {
+    rc = check_ready(second);
+    if (rc)
+      return fail(h, rc, std::string("second configuration: ") + gc_last_error(second));
+    for (int d = 0; d < 4; d++)
+      if (second->g.L[d] != h->g.L[d])
+        return fail(h, GC_ERR_ARG, "the two configurations have different lattice sizes");
+    if (second->nc != h->nc || second->prec != h->prec)
+      return fail(h, GC_ERR_ARG, "the two configurations differ in group or precision");
+  }
+  // both handles locked (in a fixed order, so two calls on the same pair in
+  // opposite roles cannot deadlock)
+  std::unique_lock<std::mutex> lk1, lk2;
+  if (second && second != h) {
+    gc_lattice *a = std::less<gc_lattice *>()(h, second) ? h : second;
+    gc_lattice *b = a == h ? second : h;
+    lk1 = std::unique_lock<std::mutex>(a->mu);
+    lk2 = std::unique_lock<std::mutex>(b->mu);
+    // h's stream waits for the work queued on the second handle
+    cudaEvent_t ev;
+    cudaError_t e = cudaEventCreateWithFlags(&ev, cudaEventDisableTiming);
+    if (e != cudaSuccess)
+      return cuda_fail(h, "cudaEventCreate(second configuration)", e);
+    e = cudaEventRecord(ev, second->stream);
+    if (e == cudaSuccess)
+      e = cudaStreamWaitEvent(h->stream, ev, 0);
+    cudaEventDestroy(ev);
+    if (e != cudaSuccess)
+      return cuda_fail(h, "ordering after the second configuration", e);
+  } else {
+    lk1 = std::unique_lock<std::mutex>(h->mu);
+  }
+  const gc::Fields4 *u2 = second ? &second->cur : nullptr;
   const int nr = rmax - rmin + 1, nt = tmax - tmin + 1;
   // The per-warp accumulators live in shared memory; split R into chunks so
   // that a block's accumulators stay small.
@@ -491,7 +546,8 @@ static int wilson_impl(gc_lattice *h, int rmin, int rmax, int tmin, int tmax,
   rc = ensure_dev_out(h, (size_t)nr * nt + (size_t)rchunk * nt);
   if (rc)
     return rc;
-  rc = ensure_partials(h, wilson_partials_count(h->g, std::min(rchunk, nr), nt, h->nc));
+  rc = ensure_partials(h, wilson_partials_count(h->g, std::min(rchunk, nr), nt, h->nc,
+                                                second ? 4 : 3));
   if (rc)
     return rc;
   double *chunk_out = h->dev_out + (size_t)nr * nt;
@@ -499,7 +555,7 @@ static int wilson_impl(gc_lattice *h, int rmin, int rmax, int tmin, int tmax,
     const int r1 = std::min(rmax, r0 + rchunk - 1);
     const int ncr = r1 - r0 + 1;
     rc = GC_DISPATCH(h, launch_wilson, h->g, h->cur, r0, r1, tmin, tmax,
-                     h->partials, chunk_out, h->stream, adjoint);
+                     h->partials, chunk_out, h->stream, adjoint, u2);
     if (rc)
       return launch_fail(h, rc);
     // chunk_out[(T-tmin)*ncr + (R-r0)] -> dev_out[(T-tmin)*nr + (R-rmin)]
@@ -530,7 +586,110 @@ int gc_wilson_adjoint_onaxis(gc_lattice *h, int rmin, int rmax, int tmin, int tm
   return wilson_impl(h, rmin, rmax, tmin, tmax, out, true);
 }
 
+int gc_wilson_gevp_onaxis(gc_lattice *h1, gc_lattice *h2, int rmin, int rmax, int tmin,
+                          int tmax, double *out) {
+  if (!h2)
+    return fail(h1, GC_ERR_ARG, "null second configuration");
+  return wilson_impl(h1, rmin, rmax, tmin, tmax, out, false, h2);
+}
+
+int gc_wilson_gevp_adjoint_onaxis(gc_lattice *h1, gc_lattice *h2, int rmin, int rmax,
+                                  int tmin, int tmax, double *out) {
+  if (!h2)
+    return fail(h1, GC_ERR_ARG, "null second configuration");
+  return wilson_impl(h1, rmin, rmax, tmin, tmax, out, true, h2);
+}
+
+// Both plaquette averages: out2[0] spatial planes, out2[1] (mu, t) planes.
+static int plaquettes(gc_lattice *h, double out2[2]) {
+  int rc = check_ready(h);
+  if (rc)
+    return rc;
+  std::lock_guard<std::mutex> lk(h->mu);
+  rc = ensure_dev_out(h, 2);
+  if (rc)
+    return rc;
+  rc = ensure_partials(h, plaquette_partials_count(h->g));
+  if (rc)
+    return rc;
+  rc = GC_DISPATCH(h, launch_plaquette, h->g, h->cur, h->partials, h->dev_out, h->stream);
+  if (rc)
+    return launch_fail(h, rc);
+  cudaError_t e = cudaMemcpyAsync(out2, h->dev_out, 2 * sizeof(double),
+                                  cudaMemcpyDeviceToHost, h->stream);
+  if (e != cudaSuccess)
+    return cuda_fail(h, "cudaMemcpyAsync(plaquette)", e);
+  e = cudaStreamSynchronize(h->stream);
+  if (e != cudaSuccess)
+    return cuda_fail(h, "plaquette synchronize", e);
+  return GC_OK;
+}
+
 int gc_plaquette(gc_lattice *h, double *out) {
+  if (!out)
+    return fail(h, GC_ERR_ARG, "null output");
+  double v[2];
+  int rc = plaquettes(h, v);
+  if (rc)
+    return rc;
+  *out = 0.5 * (v[0] + v[1]);
+  return GC_OK;
+}
+
+int gc_plaquette_space(gc_lattice *h, double *out) {
+  if (!out)
+    return fail(h, GC_ERR_ARG, "null output");
+  double v[2];
+  int rc = plaquettes(h, v);
+  if (rc)
+    return rc;
+  *out = v[0];
+  return GC_OK;
+}
+
+int gc_plaquette_time(gc_lattice *h, double *out) {
+  if (!out)
+    return fail(h, GC_ERR_ARG, "null output");
+  double v[2];
+  int rc = plaquettes(h, v);
+  if (rc)
+    return rc;
+  *out = v[1];
+  return GC_OK;
+}
+
+// Offsets (Dx, Dy, Dz) that polyakov_loop_correlator_{singlet,color_average}
+// visit (polyakov_loops.h:100-113, 163-176): Dz, Dy in [-D, D]; Dx from 0 when
+// Dy and Dz are both non-zero, else from -D; |D| <= D_max. w = the entry's
+// place in the (2 D_max + 1)^3 table.
+static std::vector<int4> correlator_offsets(int D) {
+  std::vector<int4> v;
+  const int n = 2 * D + 1;
+  for (int dz = -D; dz <= D; dz++)
+    for (int dy = -D; dy <= D; dy++) {
+      const int dx_min = (dy != 0 && dz != 0) ? 0 : -D;
+      for (int dx = dx_min; dx <= D; dx++)
+        if (std::sqrt((double)(dx * dx + dy * dy + dz * dz)) <= D)
+          v.push_back(make_int4(dx, dy, dz, (dz + D) * n * n + (dy + D) * n + dx + D));
+    }
+  return v;
+}
+
+// Polyakov lines into h->aux (FP64 planes); optionally the loop average.
+static int polyakov_lines(gc_lattice *h, size_t extra_bytes, double *loop_dev) {
+  const size_t lines_bytes = (size_t)(h->nc == 3 ? 9 : 2) * h->g.Vs * sizeof(double2);
+  int rc = ensure_aux(h, ((lines_bytes + 255) / 256) * 256 + extra_bytes);
+  if (rc)
+    return rc;
+  rc = ensure_partials(h, (h->g.Vs + 255) / 256);
+  if (rc)
+    return rc;
+  rc = GC_DISPATCH(h, launch_polyakov_lines, h->g, h->cur, (double2 *)h->aux, h->partials,
+                   loop_dev, h->stream);
+  return rc ? launch_fail(h, rc) : GC_OK;
+}
+
+int gc_polyakov_loop(gc_lattice *h, double *out) {
   int rc = check_ready(h);
   if (rc)
     return rc;
@@ -540,20 +699,54 @@ int gc_plaquette(gc_lattice *h, double *out) {
   rc = ensure_dev_out(h, 1);
   if (rc)
     return rc;
-  rc = ensure_partials(h, plaquette_partials_count(h->g));
+  rc = polyakov_lines(h, 0, h->dev_out);
   if (rc)
     return rc;
-  rc = GC_DISPATCH(h, launch_plaquette, h->g, h->cur, h->partials, h->dev_out, h->stream);
+  cudaError_t e = cudaMemcpyAsync(out, h->dev_out, sizeof(double), cudaMemcpyDeviceToHost,
+                                  h->stream);
+  if (e == cudaSuccess)
+    e = cudaStreamSynchronize(h->stream);
+  return e == cudaSuccess ? GC_OK : cuda_fail(h, "Polyakov loop result", e);
+}
+
+int gc_polyakov_correlator(gc_lattice *h, int d_max, int kind, double *out) {
+  int rc = check_ready(h);
+  if (rc)
+    return rc;
+  if (!out)
+    return fail(h, GC_ERR_ARG, "null output");
+  if (d_max < 0)
+    return fail(h, GC_ERR_ARG, "D_max must be >= 0");
+  if (kind != GC_POLYAKOV_COLOR_AVERAGE && kind != GC_POLYAKOV_SINGLET)
+    return fail(h, GC_ERR_ARG, "unknown correlator kind");
+  const size_t n = (size_t)(2 * d_max + 1) * (2 * d_max + 1) * (2 * d_max + 1);
+  if (n > (size_t)1 << 24)
+    return fail(h, GC_ERR_ARG, "D_max too large");
+  std::lock_guard<std::mutex> lk(h->mu);
+  const std::vector<int4> offs = correlator_offsets(d_max);
+  rc = ensure_dev_out(h, n);
+  if (rc)
+    return rc;
+  rc = polyakov_lines(h, offs.size() * sizeof(int4), nullptr);
+  if (rc)
+    return rc;
+  const size_t lines_bytes = (size_t)(h->nc == 3 ? 9 : 2) * h->g.Vs * sizeof(double2);
+  int4 *dev_offs = (int4 *)((char *)h->aux + ((lines_bytes + 255) / 256) * 256);
+  cudaError_t e = cudaMemcpyAsync(dev_offs, offs.data(), offs.size() * sizeof(int4),
+                                  cudaMemcpyHostToDevice, h->stream);
+  if (e == cudaSuccess)
+    e = cudaMemsetAsync(h->dev_out, 0, n * sizeof(double), h->stream);
+  if (e != cudaSuccess)
+    return cuda_fail(h, "Polyakov correlator setup", e);
+  rc = launch_polyakov_correlator(h->g, h->nc, (const double2 *)h->aux, dev_offs,
+                                  (int)offs.size(), kind == GC_POLYAKOV_SINGLET, h->dev_out,
+                                  h->stream);
   if (rc)
     return launch_fail(h, rc);
-  cudaError_t e = cudaMemcpyAsync(out, h->dev_out, sizeof(double),
-                                  cudaMemcpyDeviceToHost, h->stream);
-  if (e != cudaSuccess)
-    return cuda_fail(h, "cudaMemcpyAsync(plaquette)", e);
-  e = cudaStreamSynchronize(h->stream);
-  if (e != cudaSuccess)
-    return cuda_fail(h, "plaquette synchronize", e);
-  return GC_OK;
+  e = cudaMemcpyAsync(out, h->dev_out, n * sizeof(double), cudaMemcpyDeviceToHost, h->stream);
+  if (e == cudaSuccess)
+    e = cudaStreamSynchronize(h->stream);
+  return e == cudaSuccess ? GC_OK : cuda_fail(h, "Polyakov correlator result", e);
 }
 
 int gc_read_config(gc_lattice *h, const char *path, const char *format,

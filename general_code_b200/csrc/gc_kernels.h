@@ -120,13 +120,17 @@ constexpr int kWilsonMaxEntries = 1024;
 // so that two blocks fit on an SM with their per-warp accumulators.
 constexpr size_t kWilsonColumnBudget = 96 * 1024;
 
-WilsonPlan wilson_plan(const Geom &g, int nr, int nt, int nc, int ct_bytes);
+// sets: shared column sets of the block (3; 4 for the two-configuration
+// GEVP loops).
+WilsonPlan wilson_plan(const Geom &g, int nr, int nt, int nc, int ct_bytes, int sets = 3);
 
 // adjoint: the adjoint-representation loop |Tr W|^2 - 1 instead of Re Tr W/N.
+// second: a second configuration of the same lattice for the GEVP loops
+// (wilson_gevp_indexed): its space lines pair with U's, time lines from U.
 template <class Store, class CT>
 int launch_wilson(const Geom &g, const Fields4 &U, int rmin, int rmax,
                   int tmin, int tmax, double *partials, double *out_dev,
-                  cudaStream_t s, bool adjoint = false);
+                  cudaStream_t s, bool adjoint = false, const Fields4 *second = nullptr);
 
 // An explicit block shape (rows must divide Lt, at most 256 threads).
 WilsonPlan wilson_plan_shape(const Geom &g, int nr, int nt, int nc, int ct_bytes, int rows,
@@ -142,7 +146,23 @@ int launch_plaquette(const Geom &g, const Fields4 &U, double *partials,
                      double *out_dev, cudaStream_t s);
 
 int plaquette_partials_count(const Geom &g);
-size_t wilson_partials_count(const Geom &g, int nr, int nt, int nc);
+
+// out_dev[0] = scale * (fixed-order sum of partials[0..n)).
+int launch_reduce_sum(const double *partials, int n, double scale, double *out_dev,
+                      cudaStream_t s);
+
+// Polyakov lines P(s) of every spatial site into `lines` (FP64 element
+// planes: 9 (SU(3)) or 2 (SU(2)) double2 planes of Vs entries), block sums of
+// Re Tr P / N into partials ((Vs + 255) / 256 of them) and, if out_dev is
+// given, the Polyakov loop (their mean) into out_dev[0].
+template <class Store, class CT>
+int launch_polyakov_lines(const Geom &g, const Fields4 &U, double2 *lines, double *partials,
+                          double *out_dev, cudaStream_t s);
+// Correlator entries out_dev[offsets[i].w] for the offsets (x, y, z) of the
+// table; singlet: Re Tr(P P'^dag)/N, else Re(tr P conj(tr P')).
+int launch_polyakov_correlator(const Geom &g, int nc, const double2 *lines, const int4 *offsets,
+                               int noffsets, bool singlet, double *out_dev, cudaStream_t s);
+size_t wilson_partials_count(const Geom &g, int nr, int nt, int nc, int sets = 3);
 
 // Host AoS (uploaded raw to a device staging buffer) <-> device SoA fields.
 int launch_aos_to_soa(const Geom &g, int nc, int prec, int layout,

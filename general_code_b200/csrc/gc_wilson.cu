@@ -215,9 +215,15 @@ template <> struct LaneLoad<StoreF32SU3, float, 2> {
 // packed FP32x2 instruction for both columns. Lane 1 of a pair that runs past
 // the block's columns or the lattice duplicates lane 0's site and contributes
 // nothing.
-template <class Store, class CT, bool ADJ = false>
-__device__ __forceinline__ void wilson_block(const Geom &g, const Fields4 &U, int rmin,
-                                             int rmax, int tmin, int tmax, int cols,
+//
+// GEVP (wilson_gevp_indexed, wilson_loops.h:1202-1233; per-plane sums
+// :867-955, adjoint :957-1045): the space lines come from two
+// configurations, U (S1) and U2 (S2), the time links from U, and every loop
+// is counted twice, with S1 on top and S2 at the bottom and the other way
+// round. The block keeps a fourth set (S2) and walks T once per ordering.
+template <class Store, class CT, bool ADJ = false, bool GEVP = false>
+__device__ __forceinline__ void wilson_block(const Geom &g, const Fields4 &U, const Fields4 &U2,
+                                             int rmin, int rmax, int tmin, int tmax, int cols,
                                              int rows, int colblock, int nu,
                                              double *part, unsigned char *smem_raw) {
   constexpr int LANES = wilson_lanes(Store::NC, sizeof(CT));
@@ -237,6 +243,7 @@ __device__ __forceinline__ void wilson_block(const Geom &g, const Fields4 &U, in
   unsigned char *scol = reinterpret_cast<unsigned char *>(wacc + wacc_doubles(nwarps, nr, nt));
   unsigned char *ucol = scol + (size_t)CS::kBytes * nslots; // own time links U_t(s, t)
   unsigned char *ncol = ucol + (size_t)CS::kBytes * nslots; // U_t(s + R nu, t), per R
+  unsigned char *scol2 = ncol + (size_t)CS::kBytes * nslots; // GEVP: S2 lines
 
   const int tid = threadIdx.x;
   const int warp = tid >> 5, lane = tid & 31;
@@ -282,6 +289,11 @@ __device__ __forceinline__ void wilson_block(const Geom &g, const Fields4 &U, in
         M lnk = LL::load(Unu, V, l0 + t0 * g.Vs, l1 + t0 * g.Vs);
         M sn = (R == 1) ? lnk : mul(CS::load(scol, nslots, i), lnk);
         CS::store(scol, nslots, i, sn);
+        if (GEVP) {
+          M lnk2 = LL::load(U2.f[nu], V, l0 + t0 * g.Vs, l1 + t0 * g.Vs);
+          M sn2 = (R == 1) ? lnk2 : mul(CS::load(scol2, nslots, i), lnk2);
+          CS::store(scol2, nslots, i, sn2);
+        }
         if (R >= rmin)
           CS::store(ncol, nslots, i, LL::load(Ut, V, r0 + t0 * g.Vs, r1 + t0 * g.Vs));
       }
@@ -290,27 +302,34 @@ __device__ __forceinline__ void wilson_block(const Geom &g, const Fields4 &U, in
     if (R >= rmin) {
       double *wrow = wacc + (size_t)warp * nr * nt + (R - rmin) * nt;
 #pragma unroll 1
-      for (int k = 0; k < kt; k++) {
-        const int t0 = row + k * rows;
-        M K = active ? CS::load(scol, nslots, t0 * units + u) : unit(M());
-        int tt = t0; // (t0 + T - 1) mod Lt
+      for (int pass = 0; pass < (GEVP ? 2 : 1); pass++) {
+        // bottom and top space lines of this pass (GEVP: S2 below S1, then S1
+        // below S2)
+        const unsigned char *sbot = (GEVP && pass == 0) ? scol2 : scol;
+        const unsigned char *stop = (GEVP && pass == 1) ? scol2 : scol;
 #pragma unroll 1
-        for (int T = 1; T <= tmax; T++) {
-          int tu = tt + 1; // (t0 + T) mod Lt
-          tu = (tu == Lt) ? 0 : tu;
-          if (active) {
-            const int i = tt * units + u;
-            K = mul(mul_da(CS::load(ucol, nslots, i), K), CS::load(ncol, nslots, i));
+        for (int k = 0; k < kt; k++) {
+          const int t0 = row + k * rows;
+          M K = active ? CS::load(sbot, nslots, t0 * units + u) : unit(M());
+          int tt = t0; // (t0 + T - 1) mod Lt
+#pragma unroll 1
+          for (int T = 1; T <= tmax; T++) {
+            int tu = tt + 1; // (t0 + T) mod Lt
+            tu = (tu == Lt) ? 0 : tu;
+            if (active) {
+              const int i = tt * units + u;
+              K = mul(mul_da(CS::load(ucol, nslots, i), K), CS::load(ncol, nslots, i));
+            }
+            if (T >= tmin) {
+              double term = active
+                  ? loop_value<ADJ>(CS::load(stop, nslots, tu * units + u), K, lane1)
+                  : 0.0;
+              term = warp_sum(term);
+              if (lane == 0)
+                wrow[T - tmin] += term;
+            }
+            tt = tu;
           }
-          if (T >= tmin) {
-            double term = active
-                ? loop_value<ADJ>(CS::load(scol, nslots, tu * units + u), K, lane1)
-                : 0.0;
-            term = warp_sum(term);
-            if (lane == 0)
-              wrow[T - tmin] += term;
-          }
-          tt = tu;
         }
       }
     }
@@ -326,16 +345,16 @@ __device__ __forceinline__ void wilson_block(const Geom &g, const Fields4 &U, in
   }
 }
 
-template <class Store, class CT, bool ADJ>
+template <class Store, class CT, bool ADJ, bool GEVP>
 __global__ void __launch_bounds__(256)
-    wilson_kernel(const __grid_constant__ Geom g, const __grid_constant__ Fields4 U, int rmin,
-                  int rmax, int tmin,
-                  int tmax, int cols, int rows, double *partials) {
+    wilson_kernel(const __grid_constant__ Geom g, const __grid_constant__ Fields4 U,
+                  const __grid_constant__ Fields4 U2, int rmin, int rmax, int tmin, int tmax,
+                  int cols, int rows, double *partials) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const size_t blk = (size_t)blockIdx.y * gridDim.x + blockIdx.x;
   const int ne = (rmax - rmin + 1) * (tmax - tmin + 1);
-  wilson_block<Store, CT, ADJ>(g, U, rmin, rmax, tmin, tmax, cols, rows, blockIdx.x,
-                               blockIdx.y, partials + blk * ne, smem_raw);
+  wilson_block<Store, CT, ADJ, GEVP>(g, U, U2, rmin, rmax, tmin, tmax, cols, rows, blockIdx.x,
+                                     blockIdx.y, partials + blk * ne, smem_raw);
 }
 
 // Several lattices in one launch. A block finds its lattice by binary search
@@ -361,7 +380,7 @@ __global__ void __launch_bounds__(256)
   const int ne = (jb.rmax - jb.rmin + 1) * (jb.tmax - jb.tmin + 1);
   if (wilson_threads(jb.cols, jb.rows, wilson_lanes(Store::NC, sizeof(CT))) > (int)blockDim.x)
     return; // a lattice whose shape needs more threads than the launch has
-  wilson_block<Store, CT, false>(jb.g, jb.U, jb.rmin, jb.rmax, jb.tmin, jb.tmax, jb.cols,
+  wilson_block<Store, CT, false>(jb.g, jb.U, jb.U, jb.rmin, jb.rmax, jb.tmin, jb.tmax, jb.cols,
                                  jb.rows, colblock, nu,
                                  jb.partials + ((size_t)nu * colblocks + colblock) * ne,
                                  smem_raw);
@@ -421,20 +440,22 @@ __global__ void __launch_bounds__(256)
   }
 }
 
-// Average plaquette: thread per site, six planes (plaket.h:24-42), fixed-order
-// block sums.
+// Plaquette sums: thread per site over the six planes (plaket.h:24-42),
+// split into the three spatial planes (plaket_site_space, :63-81) and the
+// three (mu, t) planes (plaket_site_time, :44-61); raw traces, fixed-order
+// block sums into partials[2 * block + {0: space, 1: time}].
 template <class Store, class CT>
 __global__ void __launch_bounds__(256)
-    plaquette_kernel(Geom g, const __grid_constant__ Fields4 U, double *partials) {
+    plaquette_kernel(const __grid_constant__ Geom g, const __grid_constant__ Fields4 U,
+                     double *partials) {
   using M = typename Store::template M<CT>;
-  __shared__ double sh[256];
+  __shared__ double sh[2][256];
   const int site = blockIdx.x * blockDim.x + threadIdx.x;
-  double p = 0.0;
+  double sp = 0.0, tm = 0.0;
   if (site < g.V) {
     int x[4];
     site_coords(g, site, x);
     const size_t V = g.V;
-    double acc = 0.0;
 #pragma unroll 1
     for (int mu = 0; mu < 3; mu++) {
 #pragma unroll 1
@@ -444,20 +465,28 @@ __global__ void __launch_bounds__(256)
         M a = mul(Store::template load<CT>(U.f[mu], V, site),
                   Store::template load<CT>(U.f[nu], V, pm));
         a = mul_ad(a, Store::template load<CT>(U.f[mu], V, pn));
-        acc += loop_value<false>(a, Store::template load<CT>(U.f[nu], V, site), false);
+        const double v = loop_value<false>(a, Store::template load<CT>(U.f[nu], V, site), false);
+        if (nu == 3)
+          tm += v;
+        else
+          sp += v;
       }
     }
-    p = acc / (6.0 * wilson_trace_norm(Store::NC));
   }
-  sh[threadIdx.x] = p;
+  sh[0][threadIdx.x] = sp;
+  sh[1][threadIdx.x] = tm;
   __syncthreads();
   for (int w = blockDim.x / 2; w > 0; w >>= 1) {
-    if (threadIdx.x < w)
-      sh[threadIdx.x] += sh[threadIdx.x + w];
+    if (threadIdx.x < w) {
+      sh[0][threadIdx.x] += sh[0][threadIdx.x + w];
+      sh[1][threadIdx.x] += sh[1][threadIdx.x + w];
+    }
     __syncthreads();
   }
-  if (threadIdx.x == 0)
-    partials[blockIdx.x] = sh[0];
+  if (threadIdx.x == 0) {
+    partials[2 * blockIdx.x] = sh[0][0];
+    partials[2 * blockIdx.x + 1] = sh[1][0];
+  }
 }
 
 int largest_divisor_upto(int n, int cap) {
@@ -475,7 +504,7 @@ int largest_divisor_upto(int n, int cap) {
 // so that the shared column storage fits kWilsonColumnBudget. The FP64 plan
 // has the fewest columns per block and so the most blocks: callers that size
 // per-block partials before the compute type is known use it.
-WilsonPlan wilson_plan(const Geom &g, int nr, int nt, int nc, int ct_bytes) {
+WilsonPlan wilson_plan(const Geom &g, int nr, int nt, int nc, int ct_bytes, int sets) {
   WilsonPlan p;
   const int Lt = g.L[3];
   const int ncomp = (nc == 3) ? 18 : 4;
@@ -484,7 +513,7 @@ WilsonPlan wilson_plan(const Geom &g, int nr, int nt, int nc, int ct_bytes) {
   p.cols_per_block = lanes * (128 / p.rows);
   if (p.cols_per_block < 1)
     p.cols_per_block = 1;
-  const size_t col_bytes = 3 * (size_t)ncomp * Lt * ct_bytes;
+  const size_t col_bytes = (size_t)sets * ncomp * Lt * ct_bytes;
   while (p.cols_per_block > 1 &&
          wilson_col_stride(p.cols_per_block, lanes) * col_bytes > kWilsonColumnBudget)
     p.cols_per_block--;
@@ -493,56 +522,75 @@ WilsonPlan wilson_plan(const Geom &g, int nr, int nt, int nc, int ct_bytes) {
   p.blocks = colblocks * 3;
   const int nwarps = p.threads / 32;
   // per-warp accumulators + space lines + own and neighbour time links
+  // (+ the second configuration's space lines)
   p.smem = wacc_doubles(nwarps, nr, nt) * sizeof(double) +
            wilson_col_stride(p.cols_per_block, lanes) * col_bytes;
   p.fits = wilson_col_stride(p.cols_per_block, lanes) * col_bytes <= kWilsonColumnBudget;
   return p;
 }
 
-size_t wilson_partials_count(const Geom &g, int nr, int nt, int nc) {
-  return (size_t)wilson_plan(g, nr, nt, nc, 8).blocks * nr * nt;
+size_t wilson_partials_count(const Geom &g, int nr, int nt, int nc, int sets) {
+  return (size_t)wilson_plan(g, nr, nt, nc, 8, sets).blocks * nr * nt;
 }
 
-int plaquette_partials_count(const Geom &g) { return (g.V + 255) / 256; }
+int plaquette_partials_count(const Geom &g) { return 2 * ((g.V + 255) / 256); }
 
-template <class Store, class CT>
-int launch_wilson(const Geom &g, const Fields4 &U, int rmin, int rmax,
-                  int tmin, int tmax, double *partials, double *out_dev,
-                  cudaStream_t s, bool adjoint) {
+template <class Store, class CT, bool ADJ, bool GEVP>
+int launch_wilson_mode(const Geom &g, const Fields4 &U, const Fields4 &U2, int rmin, int rmax,
+                       int tmin, int tmax, double *partials, double *out_dev, cudaStream_t s) {
   const int nr = rmax - rmin + 1, nt = tmax - tmin + 1;
-  WilsonPlan p = wilson_plan(g, nr, nt, Store::NC, (int)sizeof(CT));
+  WilsonPlan p = wilson_plan(g, nr, nt, Store::NC, (int)sizeof(CT), GEVP ? 4 : 3);
   if (!p.fits || nr * nt > kWilsonMaxEntries)
     return plan_error("wilson_kernel: time extent or (R,T) range too large for "
                       "one block's shared memory");
   if (p.smem > 48 * 1024) {
-    cudaError_t e = cudaFuncSetAttribute(
-        adjoint ? wilson_kernel<Store, CT, true> : wilson_kernel<Store, CT, false>,
-        cudaFuncAttributeMaxDynamicSharedMemorySize, (int)p.smem);
+    cudaError_t e = cudaFuncSetAttribute(wilson_kernel<Store, CT, ADJ, GEVP>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)p.smem);
     if (e != cudaSuccess)
       return launch_check("wilson_kernel smem attribute");
   }
-  dim3 grid(p.blocks / 3, 3);
-  auto kern = adjoint ? wilson_kernel<Store, CT, true> : wilson_kernel<Store, CT, false>;
-  kern<<<grid, p.threads, p.smem, s>>>(
-      g, U, rmin, rmax, tmin, tmax, p.cols_per_block, p.rows, partials);
+  wilson_kernel<Store, CT, ADJ, GEVP><<<dim3(p.blocks / 3, 3), p.threads, p.smem, s>>>(
+      g, U, U2, rmin, rmax, tmin, tmax, p.cols_per_block, p.rows, partials);
   int rc = launch_check("wilson_kernel");
   if (rc)
     return rc;
-  reduce_partials_kernel<<<nr * nt, 256, 0, s>>>(
-      partials, p.blocks, nr * nt, nr, nt, wilson_scale(g.V, Store::NC, adjoint), out_dev);
+  // GEVP counts every loop twice (the / (6 V) of wilson_loops.h:910, 954)
+  const double scale = wilson_scale(g.V, Store::NC, ADJ) / (GEVP ? 2.0 : 1.0);
+  reduce_partials_kernel<<<nr * nt, 256, 0, s>>>(partials, p.blocks, nr * nt, nr, nt, scale,
+                                                 out_dev);
   return launch_check("reduce_partials_kernel");
 }
 
 template <class Store, class CT>
+int launch_wilson(const Geom &g, const Fields4 &U, int rmin, int rmax,
+                  int tmin, int tmax, double *partials, double *out_dev,
+                  cudaStream_t s, bool adjoint, const Fields4 *second) {
+  if (second)
+    return adjoint ? launch_wilson_mode<Store, CT, true, true>(g, U, *second, rmin, rmax, tmin,
+                                                               tmax, partials, out_dev, s)
+                   : launch_wilson_mode<Store, CT, false, true>(g, U, *second, rmin, rmax,
+                                                                tmin, tmax, partials, out_dev, s);
+  return adjoint ? launch_wilson_mode<Store, CT, true, false>(g, U, U, rmin, rmax, tmin, tmax,
+                                                              partials, out_dev, s)
+                 : launch_wilson_mode<Store, CT, false, false>(g, U, U, rmin, rmax, tmin, tmax,
+                                                               partials, out_dev, s);
+}
+
+// out_dev[0] = spatial-plane average (plaket_space), out_dev[1] = (mu, t)
+// average (plaket_time); the full plaquette is their mean.
+template <class Store, class CT>
 int launch_plaquette(const Geom &g, const Fields4 &U, double *partials,
                      double *out_dev, cudaStream_t s) {
-  const int nb = plaquette_partials_count(g);
+  const int nb = (g.V + 255) / 256;
   plaquette_kernel<Store, CT><<<nb, 256, 0, s>>>(g, U, partials);
   int rc = launch_check("plaquette_kernel");
   if (rc)
     return rc;
-  reduce_partials_kernel<<<1, 256, 0, s>>>(partials, nb, 1, 1, 1,
-                                           1.0 / (double)g.V, out_dev);
+  reduce_partials_kernel<<<2, 256, 0, s>>>(partials, nb, 2, 2, 1,
+                                           1.0 / (3.0 * (double)g.V *
+                                                  wilson_trace_norm(Store::NC)),
+                                           out_dev);
   return launch_check("reduce_partials_kernel");
 }
 
@@ -571,13 +619,13 @@ int launch_wilson_plan(const Geom &g, const Fields4 &U, int rmin, int rmax, int 
     return plan_error("wilson_kernel: block shape does not fit");
   if (p.smem > 48 * 1024) {
     cudaError_t e = cudaFuncSetAttribute(
-        wilson_kernel<Store, CT, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+        wilson_kernel<Store, CT, false, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
         (int)p.smem);
     if (e != cudaSuccess)
       return launch_check("wilson_kernel smem attribute");
   }
-  wilson_kernel<Store, CT, false><<<dim3(p.blocks / 3, 3), p.threads, p.smem, s>>>(
-      g, U, rmin, rmax, tmin, tmax, p.cols_per_block, p.rows, partials);
+  wilson_kernel<Store, CT, false, false><<<dim3(p.blocks / 3, 3), p.threads, p.smem, s>>>(
+      g, U, U, rmin, rmax, tmin, tmax, p.cols_per_block, p.rows, partials);
   int rc = launch_check("wilson_kernel");
   if (rc)
     return rc;
@@ -622,6 +670,12 @@ int launch_wilson_batch(const WJob *jobs, int njobs, int blocks, int threads, si
   return launch_check("wilson_batch_kernel");
 }
 
+int launch_reduce_sum(const double *partials, int n, double scale, double *out_dev,
+                      cudaStream_t s) {
+  reduce_partials_kernel<<<1, 256, 0, s>>>(partials, n, 1, 1, 1, scale, out_dev);
+  return launch_check("reduce_partials_kernel");
+}
+
 int launch_reduce_batch(const RJob *jobs, int njobs, int entries, cudaStream_t s) {
   if (njobs <= 0 || entries <= 0)
     return GC_OK;
@@ -632,7 +686,7 @@ int launch_reduce_batch(const RJob *jobs, int njobs, int entries, cudaStream_t s
 #define GC_INSTANTIATE_W(STORE, CT)                                            \
   template int launch_wilson<STORE, CT>(const Geom &, const Fields4 &, int,   \
                                         int, int, int, double *, double *,    \
-                                        cudaStream_t, bool);                  \
+                                        cudaStream_t, bool, const Fields4 *); \
   template int launch_plaquette<STORE, CT>(const Geom &, const Fields4 &,     \
                                            double *, double *, cudaStream_t);  \
   template int launch_wilson_batch<STORE, CT>(const WJob *, int, int, int,     \

@@ -15,12 +15,13 @@ device-resident form: links stay in HBM between calls.
 from __future__ import annotations
 
 import ctypes
+import math
 from typing import Dict, Sequence, Tuple
 
 import numpy as np
 
 from . import _lib
-from ._lib import (GC_LAYOUT_EIGEN_COLMAJOR, GC_LAYOUT_ROWMAJOR, GC_PREC_FP64,
+from ._lib import (GC_ERR_ARG, GC_LAYOUT_EIGEN_COLMAJOR, GC_LAYOUT_ROWMAJOR, GC_PREC_FP64,
                    GC_PREC_MIXED, GCError, check, dbl_ptr, dims_arg, lib)
 
 _PREC = {"fp64": GC_PREC_FP64, "mixed": GC_PREC_MIXED}
@@ -170,6 +171,47 @@ class Lattice:
         self._check(lib().gc_plaquette(self._h, ctypes.byref(out)))
         return out.value
 
+    def plaquette_time(self) -> float:
+        """Average of the (mu, t) plaquettes (plaket.h:103-121)."""
+        out = ctypes.c_double()
+        self._check(lib().gc_plaquette_time(self._h, ctypes.byref(out)))
+        return out.value
+
+    def plaquette_space(self) -> float:
+        """Average of the spatial plaquettes (plaket.h:123-141)."""
+        out = ctypes.c_double()
+        self._check(lib().gc_plaquette_space(self._h, ctypes.byref(out)))
+        return out.value
+
+    def wilson_gevp(self, other: "Lattice", r_min: int, r_max: int, time_min: int,
+                    time_max: int, adjoint: bool = False) -> np.ndarray:
+        """Two-configuration loops (wilson_gevp_indexed / wilson_gevp_adjoint_indexed,
+        wilson_loops.h:1202-1266): time lines from self, space lines from self and
+        other; same table layout as wilson_loop."""
+        out = np.empty((time_max - time_min + 1, r_max - r_min + 1), dtype=np.float64)
+        fn = lib().gc_wilson_gevp_adjoint_onaxis if adjoint else lib().gc_wilson_gevp_onaxis
+        self._check(fn(self._h, other._h, int(r_min), int(r_max), int(time_min), int(time_max),
+                       dbl_ptr(out)))
+        return out
+
+    def polyakov_loop(self) -> float:
+        """Mean of Re Tr P / N over spatial sites (polyakov_loops.h:24-41)."""
+        out = ctypes.c_double()
+        self._check(lib().gc_polyakov_loop(self._h, ctypes.byref(out)))
+        return out.value
+
+    def polyakov_correlator(self, d_max: int, singlet: bool) -> np.ndarray:
+        """(2 d_max + 1)^3 table of polyakov_loop_correlator_singlet (singlet) or
+        _color_average (polyakov_loops.h:83-206), entry
+        (Dz+d)(2d+1)^2 + (Dy+d)(2d+1) + Dx+d."""
+        if int(d_max) < 0:
+            raise GCError(GC_ERR_ARG, "D_max must be >= 0")
+        n = 2 * int(d_max) + 1
+        out = np.empty(n ** 3, dtype=np.float64)
+        self._check(lib().gc_polyakov_correlator(self._h, int(d_max), 1 if singlet else 0,
+                                                 dbl_ptr(out)))
+        return out
+
 
 class LatticeData:
     """Host-side configuration, like Data::LatticeData<DataPatternLexicographical, MT>.
@@ -224,6 +266,94 @@ def plaket(conf: LatticeData) -> float:
     with Lattice(conf.lat_dim, conf.nc) as lat:
         lat.upload(conf.array)
         return lat.plaquette()
+
+
+def plaket_time(conf: LatticeData) -> float:
+    """Average (mu, t) plaquette (plaket.h:103-121)."""
+    with Lattice(conf.lat_dim, conf.nc) as lat:
+        lat.upload(conf.array)
+        return lat.plaquette_time()
+
+
+def plaket_space(conf: LatticeData) -> float:
+    """Average spatial plaquette (plaket.h:123-141)."""
+    with Lattice(conf.lat_dim, conf.nc) as lat:
+        lat.upload(conf.array)
+        return lat.plaquette_space()
+
+
+def _gevp(conf1: LatticeData, conf2: LatticeData, r_min, r_max, time_min, time_max, adjoint):
+    if conf1.lat_dim != conf2.lat_dim or conf1.nc != conf2.nc:
+        raise GCError(GC_ERR_ARG, "the two configurations differ in size or group")
+    with Lattice(conf1.lat_dim, conf1.nc) as a, Lattice(conf2.lat_dim, conf2.nc) as b:
+        a.upload(conf1.array)
+        b.upload(conf2.array)
+        w = a.wilson_gevp(b, r_min, r_max, time_min, time_max, adjoint)
+    return {(t, r): float(w[t - time_min, r - r_min])
+            for t in range(time_min, time_max + 1) for r in range(r_min, r_max + 1)}
+
+
+def wilson_gevp_indexed(conf1: LatticeData, conf2: LatticeData, r_min: int, r_max: int,
+                        time_min: int, time_max: int) -> Dict[Tuple[int, int], float]:
+    """Two-configuration W(R,T) keyed (T, R) (wilson_loops.h:1202-1233)."""
+    return _gevp(conf1, conf2, r_min, r_max, time_min, time_max, False)
+
+
+def wilson_gevp_adjoint_indexed(conf1: LatticeData, conf2: LatticeData, r_min: int,
+                                r_max: int, time_min: int,
+                                time_max: int) -> Dict[Tuple[int, int], float]:
+    """Adjoint two-configuration W(R,T) keyed (T, R) (wilson_loops.h:1235-1266)."""
+    return _gevp(conf1, conf2, r_min, r_max, time_min, time_max, True)
+
+
+def wilson_loop_adjoint(conf: LatticeData, r_min: int, r_max: int, time_min: int,
+                        time_max: int) -> Dict[Tuple[int, int], float]:
+    """Adjoint-representation W(R,T) keyed (T, R) (wilson_loops.h:1173-1200)."""
+    with Lattice(conf.lat_dim, conf.nc) as lat:
+        lat.upload(conf.array)
+        w = lat.wilson_loop_adjoint(r_min, r_max, time_min, time_max)
+    return {(t, r): float(w[t - time_min, r - r_min])
+            for t in range(time_min, time_max + 1) for r in range(r_min, r_max + 1)}
+
+
+def polyakov_loop(conf: LatticeData) -> float:
+    """Polyakov loop (polyakov_loops.h:24-41)."""
+    with Lattice(conf.lat_dim, conf.nc) as lat:
+        lat.upload(conf.array)
+        return lat.polyakov_loop()
+
+
+def polyakov_loop_correlator_singlet(conf: LatticeData, D_max: int) -> np.ndarray:
+    """Singlet correlator table (polyakov_loops.h:147-206)."""
+    with Lattice(conf.lat_dim, conf.nc) as lat:
+        lat.upload(conf.array)
+        return lat.polyakov_correlator(D_max, True)
+
+
+def polyakov_loop_correlator_color_average(conf: LatticeData, D_max: int) -> np.ndarray:
+    """Color-averaged correlator table (polyakov_loops.h:83-145)."""
+    with Lattice(conf.lat_dim, conf.nc) as lat:
+        lat.upload(conf.array)
+        return lat.polyakov_correlator(D_max, False)
+
+
+def polyakov_average_directions(correlators: np.ndarray, D_max: int) -> Dict[float, float]:
+    """Average of a correlator table over offsets of equal length, origin
+    excluded (the reference's polyakov_average_directions,
+    lib/cpu/src/polyakov_loops.cpp:6-40): {distance: mean}, ascending."""
+    n = 2 * int(D_max) + 1
+    c = np.asarray(correlators, dtype=np.float64).reshape(n, n, n)  # [Dz][Dy][Dx]
+    sums: Dict[float, float] = {}
+    counts: Dict[float, int] = {}
+    for dz in range(-D_max, D_max + 1):
+        for dy in range(-D_max, D_max + 1):
+            dx_min = 0 if (dy != 0 and dz != 0) else -D_max
+            for dx in range(dx_min, D_max + 1):
+                d = math.sqrt(dx * dx + dy * dy + dz * dz)
+                if d <= D_max and not (dx == 0 and dy == 0 and dz == 0):
+                    sums[d] = sums.get(d, 0.0) + float(c[dz + D_max, dy + D_max, dx + D_max])
+                    counts[d] = counts.get(d, 0) + 1
+    return {d: sums[d] / counts[d] for d in sorted(sums)}
 
 
 def read_data_convert(conf: LatticeData, file_path, conf_format: str, bytes_skip: int,

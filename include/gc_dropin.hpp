@@ -22,6 +22,12 @@
 //   wilson_loop(const std::vector<T>&, int, int, int, int)
 //                                              basic_observables.h:108-111
 //   plaket(const LatticeData&)                            plaket.h:83-84
+//   plaket_time / plaket_space(const LatticeData&)        plaket.h:103-141
+//   wilson_gevp_indexed / wilson_gevp_adjoint_indexed(const LatticeData&,
+//       const LatticeData&, int, int, int, int)           wilson_loops.h:1202-1266
+//   polyakov_loop(const LatticeData&)                     polyakov_loops.h:24-41
+//   polyakov_loop_correlator_color_average / _singlet(const LatticeData&, int)
+//                                                         polyakov_loops.h:83-206
 #pragma once
 
 #include "gc_lattice.h"
@@ -119,12 +125,64 @@ wilson(const std::array<int, 4> &dims, const MT *links, int r_min, int r_max,
   return result;
 }
 
+// which: 0 all planes, 1 (mu, t) planes, 2 spatial planes.
 template <class MT>
-double plaquette(const Data::LatticeData<DataPatternLexicographical, MT> &conf) {
+double plaquette(const Data::LatticeData<DataPatternLexicographical, MT> &conf, int which = 0) {
   Session<MT> s(conf.lat_dim, conf.array.data());
   double p = 0;
-  check(gc_plaquette(s.get(), &p), s.get(), "plaket");
+  if (which == 1)
+    check(gc_plaquette_time(s.get(), &p), s.get(), "plaket_time");
+  else if (which == 2)
+    check(gc_plaquette_space(s.get(), &p), s.get(), "plaket_space");
+  else
+    check(gc_plaquette(s.get(), &p), s.get(), "plaket");
   return p;
+}
+
+template <class MT>
+std::map<std::tuple<int, int>, double>
+gevp(const Data::LatticeData<DataPatternLexicographical, MT> &conf1,
+     const Data::LatticeData<DataPatternLexicographical, MT> &conf2, int r_min, int r_max,
+     int time_min, int time_max, bool adjoint) {
+  std::map<std::tuple<int, int>, double> result;
+  if (r_max < r_min || time_max < time_min)
+    return result;
+  if (conf1.lat_dim != conf2.lat_dim)
+    throw std::runtime_error("general_code_b200 wilson_gevp: lattice sizes differ");
+  Session<MT> a(conf1.lat_dim, conf1.array.data()), b(conf2.lat_dim, conf2.array.data());
+  const int nr = r_max - r_min + 1, nt = time_max - time_min + 1;
+  std::vector<double> w((size_t)nr * nt);
+  if (adjoint)
+    check(gc_wilson_gevp_adjoint_onaxis(a.get(), b.get(), r_min, r_max, time_min, time_max,
+                                        w.data()),
+          a.get(), "wilson_gevp_adjoint_indexed");
+  else
+    check(gc_wilson_gevp_onaxis(a.get(), b.get(), r_min, r_max, time_min, time_max, w.data()),
+          a.get(), "wilson_gevp_indexed");
+  for (int t = time_min; t <= time_max; t++)
+    for (int r = r_min; r <= r_max; r++)
+      result[std::tuple<int, int>(t, r)] = w[(t - time_min) * nr + (r - r_min)];
+  return result;
+}
+
+template <class MT>
+double polyakov(const Data::LatticeData<DataPatternLexicographical, MT> &conf) {
+  Session<MT> s(conf.lat_dim, conf.array.data());
+  double p = 0;
+  check(gc_polyakov_loop(s.get(), &p), s.get(), "polyakov_loop");
+  return p;
+}
+
+template <class MT>
+std::vector<double> polyakov_correlator(const Data::LatticeData<DataPatternLexicographical, MT> &conf,
+                                        int D_max, int kind) {
+  Session<MT> s(conf.lat_dim, conf.array.data());
+  const size_t n = (size_t)(2 * D_max + 1) * (2 * D_max + 1) * (2 * D_max + 1);
+  std::vector<double> out(n);
+  check(gc_polyakov_correlator(s.get(), D_max, kind, out.data()), s.get(),
+        kind == GC_POLYAKOV_SINGLET ? "polyakov_loop_correlator_singlet"
+                                    : "polyakov_loop_correlator_color_average");
+  return out;
 }
 
 } // namespace gc_dropin
@@ -191,4 +249,68 @@ inline double plaket(const Data::LatticeData<DataPatternLexicographical, su2> &c
 }
 inline double plaket(const Data::LatticeData<DataPatternLexicographical, su3> &conf) {
   return gc_dropin::plaquette(conf);
+}
+inline double plaket_time(const Data::LatticeData<DataPatternLexicographical, su2> &conf) {
+  return gc_dropin::plaquette(conf, 1);
+}
+inline double plaket_time(const Data::LatticeData<DataPatternLexicographical, su3> &conf) {
+  return gc_dropin::plaquette(conf, 1);
+}
+inline double plaket_space(const Data::LatticeData<DataPatternLexicographical, su2> &conf) {
+  return gc_dropin::plaquette(conf, 2);
+}
+inline double plaket_space(const Data::LatticeData<DataPatternLexicographical, su3> &conf) {
+  return gc_dropin::plaquette(conf, 2);
+}
+// Two-configuration loops (wilson_loops.h:1202-1266), as
+// apps/smearing/smearing_wilson_gevp.cpp:200-203 calls them.
+inline std::map<std::tuple<int, int>, double>
+wilson_gevp_indexed(const Data::LatticeData<DataPatternLexicographical, su2> &conf1,
+                    const Data::LatticeData<DataPatternLexicographical, su2> &conf2, int r_min,
+                    int r_max, int time_min, int time_max) {
+  return gc_dropin::gevp(conf1, conf2, r_min, r_max, time_min, time_max, false);
+}
+inline std::map<std::tuple<int, int>, double>
+wilson_gevp_indexed(const Data::LatticeData<DataPatternLexicographical, su3> &conf1,
+                    const Data::LatticeData<DataPatternLexicographical, su3> &conf2, int r_min,
+                    int r_max, int time_min, int time_max) {
+  return gc_dropin::gevp(conf1, conf2, r_min, r_max, time_min, time_max, false);
+}
+inline std::map<std::tuple<int, int>, double>
+wilson_gevp_adjoint_indexed(const Data::LatticeData<DataPatternLexicographical, su2> &conf1,
+                            const Data::LatticeData<DataPatternLexicographical, su2> &conf2,
+                            int r_min, int r_max, int time_min, int time_max) {
+  return gc_dropin::gevp(conf1, conf2, r_min, r_max, time_min, time_max, true);
+}
+inline std::map<std::tuple<int, int>, double>
+wilson_gevp_adjoint_indexed(const Data::LatticeData<DataPatternLexicographical, su3> &conf1,
+                            const Data::LatticeData<DataPatternLexicographical, su3> &conf2,
+                            int r_min, int r_max, int time_min, int time_max) {
+  return gc_dropin::gevp(conf1, conf2, r_min, r_max, time_min, time_max, true);
+}
+// Polyakov loops (polyakov_loops.h:24-41, 83-206); with polyakov_loops.h
+// included before this header, as apps/smearing/smearing.cpp:5 does.
+inline double polyakov_loop(const Data::LatticeData<DataPatternLexicographical, su2> &conf) {
+  return gc_dropin::polyakov(conf);
+}
+inline double polyakov_loop(const Data::LatticeData<DataPatternLexicographical, su3> &conf) {
+  return gc_dropin::polyakov(conf);
+}
+inline std::vector<double>
+polyakov_loop_correlator_singlet(const Data::LatticeData<DataPatternLexicographical, su2> &conf,
+                                 int D_max) {
+  return gc_dropin::polyakov_correlator(conf, D_max, GC_POLYAKOV_SINGLET);
+}
+inline std::vector<double>
+polyakov_loop_correlator_singlet(const Data::LatticeData<DataPatternLexicographical, su3> &conf,
+                                 int D_max) {
+  return gc_dropin::polyakov_correlator(conf, D_max, GC_POLYAKOV_SINGLET);
+}
+inline std::vector<double> polyakov_loop_correlator_color_average(
+    const Data::LatticeData<DataPatternLexicographical, su2> &conf, int D_max) {
+  return gc_dropin::polyakov_correlator(conf, D_max, GC_POLYAKOV_COLOR_AVERAGE);
+}
+inline std::vector<double> polyakov_loop_correlator_color_average(
+    const Data::LatticeData<DataPatternLexicographical, su3> &conf, int D_max) {
+  return gc_dropin::polyakov_correlator(conf, D_max, GC_POLYAKOV_COLOR_AVERAGE);
 }

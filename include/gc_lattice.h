@@ -130,6 +130,23 @@ int gc_wilson_onaxis(gc_lattice *h, int r_min, int r_max, int time_min,
 int gc_wilson_adjoint_onaxis(gc_lattice *h, int r_min, int r_max, int time_min,
                              int time_max, double *out);
 
+/* On-axis Wilson loops between two configurations of the same lattice (for
+ * a generalised eigenvalue problem over smearing levels): time lines from
+ * h1, and each loop counted with h1's space line on top and h2's at the
+ * bottom and the other way round, averaged over 6V. h1 and h2 must have the
+ * same sizes, group and precision (h2 == h1 is allowed); h1's stream waits
+ * for h2's queued work. Same output layout as gc_wilson_onaxis.
+ * Replaces: wilson_gevp_indexed(conf1, conf2, r_min, r_max, time_min,
+ * time_max) (wilson_loops.h:1202-1233, plane sums :867-955). */
+int gc_wilson_gevp_onaxis(gc_lattice *h1, gc_lattice *h2, int r_min, int r_max,
+                          int time_min, int time_max, double *out);
+
+/* The same in the adjoint representation (|Tr W|^2 - 1 per loop).
+ * Replaces: wilson_gevp_adjoint_indexed (wilson_loops.h:1235-1266, plane
+ * sums :957-1045). */
+int gc_wilson_gevp_adjoint_onaxis(gc_lattice *h1, gc_lattice *h2, int r_min, int r_max,
+                                  int time_min, int time_max, double *out);
+
 /* The W(R,T) table of gc_wilson_onaxis for callers that cannot allocate
  * device memory (an application whose allocator owns the whole device budget,
  * or a timing-critical loop where cudaMalloc/cudaFree would synchronise the
@@ -157,6 +174,31 @@ int gc_wilson_onaxis_noalloc(const int dims[4], int nc, int precision,
 /* Average plaquette over the 6 planes (1 for unit links).
  * Replaces: plaket(conf) (plaket.h:83-101). */
 int gc_plaquette(gc_lattice *h, double *out);
+
+/* Average of the three spatial plaquettes per site.
+ * Replaces: plaket_space(conf) (plaket.h:123-141, sites :63-81). */
+int gc_plaquette_space(gc_lattice *h, double *out);
+
+/* Average of the three (mu, t) plaquettes per site.
+ * Replaces: plaket_time(conf) (plaket.h:103-121, sites :44-61). */
+int gc_plaquette_time(gc_lattice *h, double *out);
+
+/* Polyakov loop: mean over spatial sites of Re Tr P / N, P the product of
+ * the Lt time links of the site's column.
+ * Replaces: polyakov_loop(conf) (polyakov_loops.h:24-41, lines :10-22). */
+int gc_polyakov_loop(gc_lattice *h, double *out);
+
+#define GC_POLYAKOV_COLOR_AVERAGE 0
+#define GC_POLYAKOV_SINGLET 1
+/* Polyakov-loop correlator table of (2 d_max + 1)^3 doubles, entry
+ * (Dz+d_max)(2d_max+1)^2 + (Dy+d_max)(2d_max+1) + Dx+d_max, for the offsets
+ * the reference visits (|D| <= d_max; Dx >= 0 when Dy, Dz are both non-zero),
+ * other entries 0. kind GC_POLYAKOV_COLOR_AVERAGE: mean of
+ * Re[tr P(s) conj(tr P(s+D))], tr = Tr/N; GC_POLYAKOV_SINGLET: mean of
+ * Re Tr[P(s) P(s+D)^dag]/N.
+ * Replaces: polyakov_loop_correlator_color_average (polyakov_loops.h:83-145)
+ * and polyakov_loop_correlator_singlet (:147-206). */
+int gc_polyakov_correlator(gc_lattice *h, int d_max, int kind, double *out);
 
 /* Reads a configuration file straight into h's device links.
  * format: "lexicographical" (link index 4*site+mu, get_data element order),

@@ -1,8 +1,11 @@
 // Drop-in check (TEST INFRASTRUCTURE ONLY): compiles the reference's own
 // headers together with include/gc_dropin.hpp, then runs the sequence of
-// apps/smearing/smearing.cpp:186-301 (plaket, HYP, APE, wilson_loop, and
-// wilson_loop_adjoint as apps/smearing/smearing_wilson_gevp.cpp uses it) twice on
-// the same seeded configuration:
+// apps/smearing/smearing.cpp:186-301 (plaket, Polyakov loop and correlators,
+// HYP, APE, wilson_loop), and the observables of
+// apps/smearing/smearing_wilson_gevp.cpp (wilson_loop_adjoint,
+// wilson_gevp_indexed, wilson_gevp_adjoint_indexed of the HYP and HYP+APE
+// configurations) and plaket_time / plaket_space, twice on the same seeded
+// configuration:
 //   - with unqualified calls, exactly as the app writes them, which overload
 //     resolution binds to the drop-in (GPU) functions;
 //   - with the reference templates named explicitly (CPU).
@@ -16,6 +19,7 @@
 #include "indexing.h"
 #include "matrix.h"
 #include "plaket.h"
+#include "polyakov_loops.h"
 #include "smearing.h"
 #include "wilson_loops.h"
 
@@ -31,7 +35,10 @@ namespace {
 
 typedef DataPatternLexicographical DP;
 
-template <class MT> double ref_plaquette(const Data::LatticeData<DP, MT> &conf) {
+// which: 0 plaket_site, 1 plaket_site_time, 2 plaket_site_space, summed into
+// a zeroed accumulator (the reference's plaket / plaket_time / plaket_space
+// leave theirs uninitialised, plaket.h:85, 105, 125).
+template <class MT> double ref_plaquette(const Data::LatticeData<DP, MT> &conf, int which = 0) {
   DP dp(conf.lat_dim);
   double sum = 0;
   for (int t = 0; t < dp.lat_dim[3]; t++)
@@ -39,9 +46,47 @@ template <class MT> double ref_plaquette(const Data::LatticeData<DP, MT> &conf) 
       for (int y = 0; y < dp.lat_dim[1]; y++)
         for (int x = 0; x < dp.lat_dim[0]; x++) {
           dp.lat_coord = {x, y, z, t};
-          sum += plaket_site(conf, dp);
+          sum += which == 1   ? plaket_site_time(conf, dp)
+                 : which == 2 ? plaket_site_space(conf, dp)
+                              : plaket_site(conf, dp);
         }
   return sum / dp.get_lattice_size();
+}
+
+// polyakov_loop (polyakov_loops.h:24-41) with a zeroed accumulator (the
+// reference's is uninitialised).
+template <class MT> double ref_polyakov(const Data::LatticeData<DP, MT> &conf) {
+  DP dp(conf.lat_dim);
+  double sum = 0;
+  for (int z = 0; z < dp.lat_dim[2]; z++)
+    for (int y = 0; y < dp.lat_dim[1]; y++)
+      for (int x = 0; x < dp.lat_dim[0]; x++) {
+        dp.lat_coord = {x, y, z, 0};
+        sum += get_polyakov_loop(conf, dp).tr_real();
+      }
+  return sum / (dp.lat_dim[0] * dp.lat_dim[1] * dp.lat_dim[2]);
+}
+
+double max_rel(const std::map<std::tuple<int, int>, double> &a,
+               const std::map<std::tuple<int, int>, double> &b, bool *ok) {
+  double d = 0;
+  for (auto &kv : b) {
+    const double e = std::fabs(a.at(kv.first) - kv.second);
+    d = std::fmax(d, e / (std::fabs(kv.second) + 1e-300));
+    *ok = *ok && e <= 1e-12 * std::fabs(kv.second) + 1e-14;
+  }
+  return d;
+}
+
+double max_abs_vec(const std::vector<double> &a, const std::vector<double> &b, bool *ok) {
+  double d = 0;
+  for (size_t i = 0; i < b.size(); i++) {
+    const double e = std::fabs(a.at(i) - b[i]);
+    d = std::fmax(d, e);
+    *ok = *ok && e <= 1e-12 * std::fabs(b[i]) + 1e-14;
+  }
+  *ok = *ok && a.size() == b.size();
+  return d;
 }
 
 template <class MT>
@@ -61,46 +106,62 @@ int run(const std::array<int, 4> &dims, int ape_steps, int rmax, int tmax) {
     a.array[i] = MT(buf);
     b.array[i] = MT(buf);
   }
-  double pa, pb;
-  std::map<std::tuple<int, int>, double> wa, wb, aa, ab;
+  double pa, pb, pta, ptb, psa, psb, la, lb;
+  std::map<std::tuple<int, int>, double> wa, wb, aa, ab, ga, gb, gaa, gab;
+  std::vector<double> csa, csb, cca, ccb;
+  const int D = 2;
+  Data::LatticeData<DP, MT> ha(dims), hb(dims); // configurations after HYP
   try {
     pa = plaket(a); // drop-in
     smearing_HYP(a, 1, 0.75, 0.6);
+    ha.array = a.array;
+    la = polyakov_loop(a);
+    csa = polyakov_loop_correlator_singlet(a, D);
+    cca = polyakov_loop_correlator_color_average(a, D);
     for (int i = 0; i < ape_steps; i++)
       smearing_APE(a, 0.5);
     wa = wilson_loop(a, 1, rmax, 1, tmax);
     aa = wilson_loop_adjoint(a, 1, rmax, 1, tmax);
+    ga = wilson_gevp_indexed(a, ha, 1, rmax, 1, tmax);
+    gaa = wilson_gevp_adjoint_indexed(a, ha, 1, rmax, 1, tmax);
+    pta = plaket_time(a);
+    psa = plaket_space(a);
   } catch (const std::exception &e) {
     std::printf("drop-in raised: %s\n", e.what());
     return 3;
   }
   pb = ref_plaquette(b);
   ::smearing_HYP<DP, MT>(b, 1, 0.75, 0.6);
+  hb.array = b.array;
+  lb = ref_polyakov(b);
+  csb = ::polyakov_loop_correlator_singlet<DP, MT>(b, D);
+  ccb = ::polyakov_loop_correlator_color_average<DP, MT>(b, D);
   for (int i = 0; i < ape_steps; i++)
     ::smearing_APE<DP, MT>(b, 0.5);
   wb = ::wilson_loop<DP, MT>(b, 1, rmax, 1, tmax);
   ab = ::wilson_loop_adjoint<DP, MT>(b, 1, rmax, 1, tmax);
+  gb = ::wilson_gevp_indexed<DP, MT>(b, hb, 1, rmax, 1, tmax);
+  gab = ::wilson_gevp_adjoint_indexed<DP, MT>(b, hb, 1, rmax, 1, tmax);
+  ptb = ref_plaquette(b, 1);
+  psb = ref_plaquette(b, 2);
   double dl = 0;
   for (size_t i = 0; i < a.array.size(); i++) {
     std::vector<double> x = a.array[i].get_data(), y = b.array[i].get_data();
     for (int k = 0; k < ds; k++)
       dl = std::fmax(dl, std::fabs(x[k] - y[k]));
   }
-  double dw = 0;
-  bool ok = dl <= 1e-12 && std::fabs(pa - pb) <= 1e-12 * std::fabs(pb) + 1e-14;
-  for (auto &kv : wb) {
-    double d = std::fabs(wa.at(kv.first) - kv.second);
-    dw = std::fmax(dw, d / (std::fabs(kv.second) + 1e-300));
-    ok = ok && d <= 1e-12 * std::fabs(kv.second) + 1e-14;
-  }
-  for (auto &kv : ab) {
-    double d = std::fabs(aa.at(kv.first) - kv.second);
-    dw = std::fmax(dw, d / (std::fabs(kv.second) + 1e-300));
-    ok = ok && d <= 1e-12 * std::fabs(kv.second) + 1e-14;
-  }
-  std::printf("links max|diff| %.3e  plaquette diff %.3e  W max rel diff %.3e  "
-              "entries %zu  %s\n",
-              dl, std::fabs(pa - pb), dw, wb.size(), ok ? "OK" : "MISMATCH");
+  bool ok = dl <= 1e-12;
+  for (auto pr : {std::make_pair(pa, pb), std::make_pair(pta, ptb), std::make_pair(psa, psb),
+                  std::make_pair(la, lb)})
+    ok = ok && std::fabs(pr.first - pr.second) <= 1e-12 * std::fabs(pr.second) + 1e-14;
+  double dw = max_rel(wa, wb, &ok);
+  dw = std::fmax(dw, max_rel(aa, ab, &ok));
+  const double dg = std::fmax(max_rel(ga, gb, &ok), max_rel(gaa, gab, &ok));
+  const double dc = std::fmax(max_abs_vec(csa, csb, &ok), max_abs_vec(cca, ccb, &ok));
+  std::printf("links max|diff| %.3e  plaquette diff %.3e (time %.3e space %.3e)  W max rel "
+              "diff %.3e  GEVP %.3e  Polyakov %.3e, correlators %.3e  entries %zu  %s\n",
+              dl, std::fabs(pa - pb), std::fabs(pta - ptb), std::fabs(psa - psb), dw, dg,
+              std::fabs(la - lb), dc, wb.size(), ok ? "OK" : "MISMATCH");
   return ok ? 0 : 1;
 }
 

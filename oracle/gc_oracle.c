@@ -431,12 +431,40 @@ static double *lines_indexed(const group_t *G, const geom_t *g,
   return l;
 }
 
+/* Value of one loop: L(x) * S_top(x+T) * L(x+R)^dag * S_bot(x)^dag, its
+ * real trace / N, or the adjoint |Tr|^2 - 1 (su3 tr_adjoint, matrix.h:258)
+ * / 4 (w.s)^2 - 1 (su2 multiply_conj_tr_adjoint, matrix.h:62-65). */
+static double loop_value(int nc, int ds, const double *L, const double *stop,
+                         const double *L3, const double *sbot, int adjoint) {
+  double w[18];
+  if (nc == 3) {
+    /* (L(x) * S(x+T) * L(x+R)^dag * S(x)^dag).tr_real()  (:781-784) */
+    su3_mul(w, L, stop);
+    su3_mul_ad(w, w, L3);
+    su3_mul_ad(w, w, sbot);
+    if (adjoint) {
+      double tr = RE(w, 0, 0) + RE(w, 1, 1) + RE(w, 2, 2);
+      double ti = IM(w, 0, 0) + IM(w, 1, 1) + IM(w, 2, 2);
+      return tr * tr + ti * ti - 1;
+    }
+    return su3_tr_real(w);
+  }
+  (void)ds;
+  /* generic form (:735-748) */
+  su2_mul(w, L, stop);
+  su2_mul_ad(w, w, L3);
+  double d = su2_conj_tr(w, sbot);
+  return adjoint ? 4 * d * d - 1 : d;
+}
+
 /* adjoint = 0: wilson_loop (wilson_loops.h:1047-1074, plane sums :719-791);
- * adjoint = 1: wilson_loop_adjoint (:1173-1200, plane sums :793-861), i.e.
- * per loop |Tr W|^2 - 1 (su3 tr_adjoint, matrix.h:264) or 4 (w.s)^2 - 1
- * (su2 multiply_conj_tr_adjoint, matrix.h:62-65). */
-static int wilson_impl(int nc, const int dims[4], const double *links, int rmin,
-                       int rmax, int tmin, int tmax, double *out, int adjoint) {
+ * adjoint = 1: wilson_loop_adjoint (:1173-1200, plane sums :793-861).
+ * links2 != NULL: wilson_gevp_indexed / wilson_gevp_adjoint_indexed
+ * (:1202-1266, plane sums :867-1045): time lines from links, space lines S1
+ * from links and S2 from links2, each loop taken as (top S1, bottom S2) and
+ * (top S2, bottom S1), the sum divided by 6V. */
+static int wilson_impl(int nc, const int dims[4], const double *links, const double *links2,
+                       int rmin, int rmax, int tmin, int tmax, double *out, int adjoint) {
   const group_t *G = group_of(nc);
   if (!G || rmin < 1 || tmin < 1 || rmax < rmin || tmax < tmin)
     return -1;
@@ -451,9 +479,12 @@ static int wilson_impl(int nc, const int dims[4], const double *links, int rmin,
     memcpy(tl[t - tmin], tl[t - tmin - 1], (size_t)g.V * ds * sizeof(double));
     prolong(G, &g, links, tl[t - tmin], t - 1, 3);
   }
-  double *sl[3];
-  for (int mu = 0; mu < 3; mu++)
+  double *sl[3], *sl2[3] = {NULL, NULL, NULL};
+  for (int mu = 0; mu < 3; mu++) {
     sl[mu] = lines_indexed(G, &g, links, rmin, mu);
+    if (links2)
+      sl2[mu] = lines_indexed(G, &g, links2, rmin, mu);
+  }
   for (int r = rmin; r <= rmax; r++) {
     for (int t = tmin; t <= tmax; t++) {
       const double *L = tl[t - tmin];
@@ -463,52 +494,184 @@ static int wilson_impl(int nc, const int dims[4], const double *links, int rmin,
         long long x2 = shift(&g, x, 3, t);
         for (int nu = 0; nu < 3; nu++) {
           long long x3 = shift(&g, x, nu, r);
-          double w[18];
-          if (nc == 3) {
-            /* (L(x) * S(x+T) * L(x+R)^dag * S(x)^dag).tr_real()  (:781-784) */
-            su3_mul(w, L + x * ds, sl[nu] + x2 * ds);
-            su3_mul_ad(w, w, L + x3 * ds);
-            su3_mul_ad(w, w, sl[nu] + x * ds);
-            if (adjoint) {
-              double tr = RE(w, 0, 0) + RE(w, 1, 1) + RE(w, 2, 2);
-              double ti = IM(w, 0, 0) + IM(w, 1, 1) + IM(w, 2, 2);
-              result += tr * tr + ti * ti - 1;
-            } else {
-              result += su3_tr_real(w);
-            }
+          if (!links2) {
+            result += loop_value(nc, ds, L + x * ds, sl[nu] + x2 * ds, L + x3 * ds,
+                                 sl[nu] + x * ds, adjoint);
           } else {
-            /* generic form (:735-748) */
-            su2_mul(w, L + x * ds, sl[nu] + x2 * ds);
-            su2_mul_ad(w, w, L + x3 * ds);
-            double d = su2_conj_tr(w, sl[nu] + x * ds);
-            result += adjoint ? 4 * d * d - 1 : d;
+            result += loop_value(nc, ds, L + x * ds, sl[nu] + x2 * ds, L + x3 * ds,
+                                 sl2[nu] + x * ds, adjoint);
+            result += loop_value(nc, ds, L + x * ds, sl2[nu] + x2 * ds, L + x3 * ds,
+                                 sl[nu] + x * ds, adjoint);
           }
         }
       }
-      out[(t - tmin) * nr + (r - rmin)] = result / (g.V * 3);
+      out[(t - tmin) * nr + (r - rmin)] = result / (g.V * (links2 ? 6 : 3));
     }
-    for (int mu = 0; mu < 3; mu++)
+    for (int mu = 0; mu < 3; mu++) {
       prolong(G, &g, links, sl[mu], r, mu);
+      if (links2)
+        prolong(G, &g, links2, sl2[mu], r, mu);
+    }
   }
   for (int i = 0; i < nt; i++)
     free(tl[i]);
   free(tl);
-  for (int mu = 0; mu < 3; mu++)
+  for (int mu = 0; mu < 3; mu++) {
     free(sl[mu]);
+    free(sl2[mu]);
+  }
   return 0;
 }
 
 int or_wilson(int nc, const int dims[4], const double *links, int rmin,
               int rmax, int tmin, int tmax, double *out) {
-  return wilson_impl(nc, dims, links, rmin, rmax, tmin, tmax, out, 0);
+  return wilson_impl(nc, dims, links, NULL, rmin, rmax, tmin, tmax, out, 0);
 }
 
 int or_wilson_adjoint(int nc, const int dims[4], const double *links, int rmin,
                       int rmax, int tmin, int tmax, double *out) {
-  return wilson_impl(nc, dims, links, rmin, rmax, tmin, tmax, out, 1);
+  return wilson_impl(nc, dims, links, NULL, rmin, rmax, tmin, tmax, out, 1);
+}
+
+int or_wilson_gevp(int nc, const int dims[4], const double *links1, const double *links2,
+                   int rmin, int rmax, int tmin, int tmax, int adjoint, double *out) {
+  if (!links2)
+    return -1;
+  return wilson_impl(nc, dims, links1, links2, rmin, rmax, tmin, tmax, out, adjoint);
 }
 
 /* ------------------------------------------------------------ plaquette */
+/* which = 0: all six planes / 6 (plaket_site, plaket.h:24-42);
+ * 1: (mu, t) planes / 3 (plaket_site_time, :44-61);
+ * 2: spatial planes / 3 (plaket_site_space, :63-81). */
+static double plaquette_kind(int nc, const int dims[4], const double *links, int which) {
+  const group_t *G = group_of(nc);
+  if (!G)
+    return 0;
+  geom_t g;
+  geom_init(&g, dims);
+  const int ds = G->ds;
+  double sum = 0;
+#pragma omp parallel for reduction(+ : sum)
+  for (long long x = 0; x < g.V; x++) {
+    double p = 0, a[18];
+    for (int mu = 0; mu < 3; mu++)
+      for (int nu = mu + 1; nu < 4; nu++) {
+        if ((which == 1 && nu != 3) || (which == 2 && nu == 3))
+          continue;
+        long long xm = shift(&g, x, mu, 1), xn = shift(&g, x, nu, 1);
+        G->mul(a, links + (4 * x + mu) * ds, links + (4 * xm + nu) * ds);
+        G->mul_ad(a, a, links + (4 * xn + mu) * ds);
+        p += (nc == 3) ? su3_conj_tr(a, links + (4 * x + nu) * ds)
+                       : su2_conj_tr(a, links + (4 * x + nu) * ds);
+      }
+    sum += p / (which == 0 ? 6 : 3);
+  }
+  return sum / g.V;
+}
+
+double or_plaquette_time(int nc, const int dims[4], const double *links) {
+  return plaquette_kind(nc, dims, links, 1);
+}
+
+double or_plaquette_space(int nc, const int dims[4], const double *links) {
+  return plaquette_kind(nc, dims, links, 2);
+}
+
+/* ------------------------------------------------------------ Polyakov loops */
+/* P(s) = U_t(s,0) ... U_t(s,Lt-1) for spatial site s (get_polyakov_loop,
+ * polyakov_loops.h:10-22); lines: Vs matrices. */
+static double *polyakov_lines(const group_t *G, const geom_t *g, const double *links) {
+  const int ds = G->ds;
+  const long long Vs = g->V / g->L[3];
+  double *P = (double *)malloc((size_t)Vs * ds * sizeof(double));
+#pragma omp parallel for
+  for (long long s = 0; s < Vs; s++) {
+    double *A = P + s * ds;
+    memcpy(A, links + (4 * s + 3) * ds, ds * sizeof(double));
+    for (int t = 1; t < g->L[3]; t++)
+      G->mul(A, A, links + (4 * (s + t * Vs) + 3) * ds);
+  }
+  return P;
+}
+
+/* tr P = Tr P / N (su3 tr(), matrix.h:256; su2 a0): re, im. */
+static void norm_trace(int nc, const double *m, double *re, double *im) {
+  if (nc == 3) {
+    *re = (RE(m, 0, 0) + RE(m, 1, 1) + RE(m, 2, 2)) / 3;
+    *im = (IM(m, 0, 0) + IM(m, 1, 1) + IM(m, 2, 2)) / 3;
+  } else {
+    *re = m[0];
+    *im = 0;
+  }
+}
+
+/* polyakov_loop (polyakov_loops.h:24-41) */
+double or_polyakov_loop(int nc, const int dims[4], const double *links) {
+  const group_t *G = group_of(nc);
+  if (!G)
+    return 0;
+  geom_t g;
+  geom_init(&g, dims);
+  const long long Vs = g.V / g.L[3];
+  double *P = polyakov_lines(G, &g, links);
+  double sum = 0;
+  for (long long s = 0; s < Vs; s++) {
+    double re, im;
+    norm_trace(nc, P + s * G->ds, &re, &im);
+    sum += re;
+  }
+  free(P);
+  return sum / Vs;
+}
+
+/* polyakov_loop_correlator_color_average (kind 0, polyakov_loops.h:83-145)
+ * and polyakov_loop_correlator_singlet (kind 1, :147-206): out has
+ * (2 D + 1)^3 entries, zero where the reference visits no offset. */
+int or_polyakov_correlator(int nc, const int dims[4], const double *links, int D, int kind,
+                           double *out) {
+  const group_t *G = group_of(nc);
+  if (!G || D < 0)
+    return -1;
+  geom_t g;
+  geom_init(&g, dims);
+  const int ds = G->ds;
+  const long long Vs = g.V / g.L[3];
+  const int n = 2 * D + 1;
+  double *P = polyakov_lines(G, &g, links);
+  memset(out, 0, (size_t)n * n * n * sizeof(double));
+  for (int dz = -D; dz <= D; dz++)
+    for (int dy = -D; dy <= D; dy++) {
+      const int dx_min = (dy != 0 && dz != 0) ? 0 : -D;
+      for (int dx = dx_min; dx <= D; dx++) {
+        if (sqrt((double)(dx * dx + dy * dy + dz * dz)) > D)
+          continue;
+        double acc = 0;
+#pragma omp parallel for reduction(+ : acc)
+        for (long long s = 0; s < Vs; s++) {
+          const int x = (int)(s % g.L[0]), y = (int)((s / g.L[0]) % g.L[1]),
+                    z = (int)(s / ((long long)g.L[0] * g.L[1]));
+          const int x2 = ((x + dx) % g.L[0] + g.L[0]) % g.L[0];
+          const int y2 = ((y + dy) % g.L[1] + g.L[1]) % g.L[1];
+          const int z2 = ((z + dz) % g.L[2] + g.L[2]) % g.L[2];
+          const long long s2 = x2 + (long long)g.L[0] * (y2 + (long long)g.L[1] * z2);
+          const double *a = P + s * ds, *b = P + s2 * ds;
+          if (kind == 1) {
+            acc += (nc == 3) ? su3_conj_tr(a, b) : su2_conj_tr(a, b);
+          } else {
+            double pr, pi, qr, qi;
+            norm_trace(nc, a, &pr, &pi);
+            norm_trace(nc, b, &qr, &qi);
+            acc += pr * qr + pi * qi;
+          }
+        }
+        out[(dz + D) * n * n + (dy + D) * n + dx + D] = acc / Vs;
+      }
+    }
+  free(P);
+  return 0;
+}
+
 double or_plaquette(int nc, const int dims[4], const double *links) {
   const group_t *G = group_of(nc);
   if (!G)

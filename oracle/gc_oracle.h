@@ -25,7 +25,17 @@ int or_wilson(int nc, const int dims[4], const double *links, int r_min,
               int r_max, int time_min, int time_max, double *out);
 int or_wilson_adjoint(int nc, const int dims[4], const double *links, int r_min,
                       int r_max, int time_min, int time_max, double *out);
+/* Two-configuration (GEVP) loops; adjoint selects the adjoint trace. */
+int or_wilson_gevp(int nc, const int dims[4], const double *links1, const double *links2,
+                   int r_min, int r_max, int time_min, int time_max, int adjoint,
+                   double *out);
 double or_plaquette(int nc, const int dims[4], const double *links);
+double or_plaquette_time(int nc, const int dims[4], const double *links);
+double or_plaquette_space(int nc, const int dims[4], const double *links);
+double or_polyakov_loop(int nc, const int dims[4], const double *links);
+/* kind 0: color average, 1: singlet; out: (2 D + 1)^3 doubles. */
+int or_polyakov_correlator(int nc, const int dims[4], const double *links, int D, int kind,
+                           double *out);
 /* Applies proj() to every link (test helper for the projection alone). */
 int or_proj_all(int nc, long long nlinks, double *links);
 void or_set_threads(int n);

@@ -77,18 +77,56 @@ class _Checker:
     def plaquette(self, nc, dims, links):
         return float(self._fn("plaquette")(nc, _dims(dims), _ptr(links)))
 
+    def _setup_observables(self):
+        p = self.prefix
+        sig = {
+            f"{p}wilson_gevp": (_c_int, [_c_int, _pint, _pdbl, _pdbl, _c_int, _c_int, _c_int,
+                                         _c_int, _c_int, _pdbl]),
+            f"{p}polyakov_loop": (_c_dbl, [_c_int, _pint, _pdbl]),
+            f"{p}polyakov_correlator": (_c_int, [_c_int, _pint, _pdbl, _c_int, _c_int, _pdbl]),
+        }
+        for name, (res, args) in sig.items():
+            fn = getattr(self.lib, name)
+            fn.restype, fn.argtypes = res, args
+
+    def wilson_gevp(self, nc, dims, links1, links2, rmin, rmax, tmin, tmax, adjoint=False):
+        out = np.empty((tmax - tmin + 1, rmax - rmin + 1), dtype=np.float64)
+        assert self._fn("wilson_gevp")(nc, _dims(dims), _ptr(links1), _ptr(links2), rmin, rmax,
+                                       tmin, tmax, int(adjoint), _ptr(out)) == 0
+        return out
+
+    def polyakov_loop(self, nc, dims, links):
+        return float(self._fn("polyakov_loop")(nc, _dims(dims), _ptr(links)))
+
+    def polyakov_correlator(self, nc, dims, links, d_max, singlet):
+        n = 2 * d_max + 1
+        out = np.empty(n ** 3, dtype=np.float64)
+        assert self._fn("polyakov_correlator")(nc, _dims(dims), _ptr(links), d_max,
+                                               int(singlet), _ptr(out)) == 0
+        return out
+
 
 class Port(_Checker):
     prefix = "or_"
 
     def __init__(self, path=PORT_LIB):
         super().__init__(path)
+        self._setup_observables()
+        for name in ("or_plaquette_time", "or_plaquette_space"):
+            fn = getattr(self.lib, name)
+            fn.restype, fn.argtypes = _c_dbl, [_c_int, _pint, _pdbl]
         self.lib.or_set_threads.argtypes = [_c_int]
         self.lib.or_proj_all.argtypes = [_c_int, ctypes.c_longlong, _pdbl]
         self.lib.or_proj_all.restype = _c_int
 
     def set_threads(self, n):
         self.lib.or_set_threads(int(n))
+
+    def plaquette_time(self, nc, dims, links):
+        return float(self.lib.or_plaquette_time(nc, _dims(dims), _ptr(links)))
+
+    def plaquette_space(self, nc, dims, links):
+        return float(self.lib.or_plaquette_space(nc, _dims(dims), _ptr(links)))
 
     def proj_all(self, nc, links):
         assert self.lib.or_proj_all(nc, links.shape[0], _ptr(links)) == 0
@@ -99,6 +137,11 @@ class Ref(_Checker):
 
     def __init__(self, path):
         super().__init__(path)
+        self._setup_observables()
+        self.lib.ref_plaquette_part.restype = _c_dbl
+        self.lib.ref_plaquette_part.argtypes = [_c_int, _pint, _pdbl, _c_int]
+        self.lib.ref_polyakov_average_directions.restype = _c_int
+        self.lib.ref_polyakov_average_directions.argtypes = [_pdbl, _c_int, _pdbl, _pdbl, _c_int]
         self.lib.ref_job.restype = _c_int
         self.lib.ref_job.argtypes = [_c_int, _pint, _pdbl, _c_int, _c_dbl, _c_dbl, _c_dbl,
                                      _c_int, _c_dbl, _c_int, _c_int, _c_int, _c_int, _pdbl,
@@ -113,6 +156,22 @@ class Ref(_Checker):
 
     def num_threads(self):
         return int(self.lib.ref_num_threads())
+
+    def plaquette_time(self, nc, dims, links):
+        return float(self.lib.ref_plaquette_part(nc, _dims(dims), _ptr(links), 1))
+
+    def plaquette_space(self, nc, dims, links):
+        return float(self.lib.ref_plaquette_part(nc, _dims(dims), _ptr(links), 2))
+
+    def polyakov_average_directions(self, table, d_max):
+        """The reference's distance average: {distance: mean} (ascending)."""
+        table = np.ascontiguousarray(table, dtype=np.float64)
+        cap = table.size
+        dist = np.empty(cap, dtype=np.float64)
+        avg = np.empty(cap, dtype=np.float64)
+        n = self.lib.ref_polyakov_average_directions(_ptr(table), d_max, _ptr(dist), _ptr(avg),
+                                                     cap)
+        return dict(zip(dist[:n].tolist(), avg[:n].tolist()))
 
     def set_threads(self, n):
         self.lib.ref_set_threads(int(n))

@@ -9,6 +9,11 @@
 //   wilson_loop           lib/cpu/include/wilson_loops.h:1047-1074
 //   wilson_loop_adjoint   lib/cpu/include/wilson_loops.h:1173-1200
 //   plaket_site           lib/cpu/include/plaket.h:24-42
+//   plaket_site_time / plaket_site_space   plaket.h:44-61, 63-81
+//   wilson_gevp_indexed / wilson_gevp_adjoint_indexed  wilson_loops.h:1202-1266
+//   get_polyakov_loop, polyakov_loop_correlator_{color_average,singlet}
+//                         lib/cpu/include/polyakov_loops.h:10-22, 83-206
+//   polyakov_average_directions            lib/cpu/src/polyakov_loops.cpp:6-40
 //   Data::read_data_convert / write_data   lib/cpu/include/data.h:193-205,265-338
 //
 // Link exchange layout ("row-major"): link index 4*site+mu with
@@ -19,6 +24,7 @@
 #include "indexing.h"
 #include "matrix.h"
 #include "plaket.h"
+#include "polyakov_loops.h"
 #include "smearing.h"
 #include "wilson_loops.h"
 
@@ -97,6 +103,36 @@ template <class MT> double plaquette(const Data::LatticeData<DP, MT> &conf) {
           sum += plaket_site(conf, dp);
         }
   return sum / dp.get_lattice_size();
+}
+
+// plaket_time / plaket_space (plaket.h:103-141) and polyakov_loop
+// (polyakov_loops.h:24-41) have the same uninitialised reduction variable;
+// the harness sums the reference's per-site functions into zeroed
+// accumulators. which: 1 time, 2 space.
+template <class MT> double plaquette_part(const Data::LatticeData<DP, MT> &conf, int which) {
+  DP dp(conf.lat_dim);
+  double sum = 0;
+#pragma omp parallel for collapse(4) firstprivate(dp) reduction(+ : sum)
+  for (int t = 0; t < dp.lat_dim[3]; t++)
+    for (int z = 0; z < dp.lat_dim[2]; z++)
+      for (int y = 0; y < dp.lat_dim[1]; y++)
+        for (int x = 0; x < dp.lat_dim[0]; x++) {
+          dp.lat_coord = {x, y, z, t};
+          sum += which == 1 ? plaket_site_time(conf, dp) : plaket_site_space(conf, dp);
+        }
+  return sum / dp.get_lattice_size();
+}
+
+template <class MT> double polyakov_mean(const Data::LatticeData<DP, MT> &conf) {
+  DP dp(conf.lat_dim);
+  double sum = 0;
+  for (int z = 0; z < dp.lat_dim[2]; z++)
+    for (int y = 0; y < dp.lat_dim[1]; y++)
+      for (int x = 0; x < dp.lat_dim[0]; x++) {
+        dp.lat_coord = {x, y, z, 0};
+        sum += get_polyakov_loop(conf, dp).tr_real();
+      }
+  return sum / (dp.lat_dim[0] * dp.lat_dim[1] * dp.lat_dim[2]);
 }
 
 double now() {
@@ -214,6 +250,79 @@ int ref_wilson_adjoint(int nc, const int *dims, const double *links, int rmin,
     return 0;
   }
   return -1;
+}
+
+int ref_wilson_gevp(int nc, const int *dims, const double *links1, const double *links2,
+                    int rmin, int rmax, int tmin, int tmax, int adjoint, double *out) {
+  set_globals(dims);
+  if (nc == 2) {
+    Data::LatticeData<DP, su2> c1 = make_conf<su2>(dims, links1), c2 = make_conf<su2>(dims, links2);
+    wilson_to_table<su2>(adjoint ? wilson_gevp_adjoint_indexed(c1, c2, rmin, rmax, tmin, tmax)
+                                 : wilson_gevp_indexed(c1, c2, rmin, rmax, tmin, tmax),
+                         rmin, rmax, tmin, tmax, out);
+    return 0;
+  }
+  if (nc == 3) {
+    Data::LatticeData<DP, su3> c1 = make_conf<su3>(dims, links1), c2 = make_conf<su3>(dims, links2);
+    wilson_to_table<su3>(adjoint ? wilson_gevp_adjoint_indexed(c1, c2, rmin, rmax, tmin, tmax)
+                                 : wilson_gevp_indexed(c1, c2, rmin, rmax, tmin, tmax),
+                         rmin, rmax, tmin, tmax, out);
+    return 0;
+  }
+  return -1;
+}
+
+double ref_plaquette_part(int nc, const int *dims, const double *links, int which) {
+  set_globals(dims);
+  if (nc == 2)
+    return plaquette_part(make_conf<su2>(dims, links), which);
+  if (nc == 3)
+    return plaquette_part(make_conf<su3>(dims, links), which);
+  return 0.0;
+}
+
+double ref_polyakov_loop(int nc, const int *dims, const double *links) {
+  set_globals(dims);
+  if (nc == 2)
+    return polyakov_mean(make_conf<su2>(dims, links));
+  if (nc == 3)
+    return polyakov_mean(make_conf<su3>(dims, links));
+  return 0.0;
+}
+
+// kind 0: color average, 1: singlet; out: (2 D + 1)^3 doubles.
+int ref_polyakov_correlator(int nc, const int *dims, const double *links, int D, int kind,
+                            double *out) {
+  set_globals(dims);
+  std::vector<double> v;
+  if (nc == 2) {
+    Data::LatticeData<DP, su2> c = make_conf<su2>(dims, links);
+    v = kind ? polyakov_loop_correlator_singlet(c, D) : polyakov_loop_correlator_color_average(c, D);
+  } else if (nc == 3) {
+    Data::LatticeData<DP, su3> c = make_conf<su3>(dims, links);
+    v = kind ? polyakov_loop_correlator_singlet(c, D) : polyakov_loop_correlator_color_average(c, D);
+  } else {
+    return -1;
+  }
+  std::memcpy(out, v.data(), v.size() * sizeof(double));
+  return 0;
+}
+
+// polyakov_average_directions: distances (ascending) and averages; returns
+// the number of distances (at most cap).
+int ref_polyakov_average_directions(const double *table, int D, double *dist, double *avg,
+                                    int cap) {
+  const int n = (2 * D + 1) * (2 * D + 1) * (2 * D + 1);
+  std::map<double, double> m = polyakov_average_directions(std::vector<double>(table, table + n), D);
+  int i = 0;
+  for (auto &kv : m) {
+    if (i >= cap)
+      break;
+    dist[i] = kv.first;
+    avg[i] = kv.second;
+    i++;
+  }
+  return i;
 }
 
 double ref_plaquette(int nc, const int *dims, const double *links) {

@@ -8,6 +8,11 @@ gc_generate_host), one HYP step, then APE steps, then a W(R,T) table, with
 the plaquette of the input and of the result. The fixture stores the input
 links, the links after HYP, the links after HYP+APE, the W table and the
 plaquettes, so the tests do not depend on the generator staying unchanged.
+Also from the reference, on the same links: the adjoint W table; the
+two-configuration (GEVP) tables of (HYP+APE, HYP) (wilson_gevp_indexed and
+wilson_gevp_adjoint_indexed); the time and space plaquettes after HYP+APE;
+the Polyakov loop and both correlator tables (D_max = 2) after HYP, with the
+reference's distance averages of the tables.
 
 Run here (needs the reference sources and oracle/_ref):
     make -C oracle ref && python tests/golden/make_golden.py
@@ -54,19 +59,41 @@ def main() -> None:
         w = ref.wilson(nc, dims, links_ape, r0, r1, t0, t1)
         wa = ref.wilson_adjoint(nc, dims, links_ape, r0, r1, t0, t1)
         plaq1 = ref.plaquette(nc, dims, links_ape)
+        gevp = ref.wilson_gevp(nc, dims, links_ape, links_hyp, r0, r1, t0, t1, False)
+        gevp_adj = ref.wilson_gevp(nc, dims, links_ape, links_hyp, r0, r1, t0, t1, True)
+        plaq_t = ref.plaquette_time(nc, dims, links_ape)
+        plaq_s = ref.plaquette_space(nc, dims, links_ape)
+        poly = ref.polyakov_loop(nc, dims, links_hyp)
+        d_max = 2
+        corr_s = ref.polyakov_correlator(nc, dims, links_hyp, d_max, True)
+        corr_c = ref.polyakov_correlator(nc, dims, links_hyp, d_max, False)
+        avg_s = ref.polyakov_average_directions(corr_s, d_max)
+        avg_c = ref.polyakov_average_directions(corr_c, d_max)
         np.savez_compressed(OUT / f"{name}.npz", links0=links0, links_hyp=links_hyp,
                             links_ape=links_ape, wilson=w, wilson_adjoint=wa,
-                            plaquettes=np.array([plaq0, plaq1]))
+                            plaquettes=np.array([plaq0, plaq1]), gevp=gevp,
+                            gevp_adjoint=gevp_adj, plaquettes_time_space=np.array([plaq_t, plaq_s]),
+                            polyakov_loop=np.array([poly]), polyakov_singlet=corr_s,
+                            polyakov_color_average=corr_c)
         index[name] = {"nc": nc, "dims": list(dims), "eps": eps, "seed": seed,
                        "config_index": cfg, "hyp_alpha": [a1, a2, a3], "ape_steps": n_ape,
                        "ape_alpha": alpha, "r_min": r0, "r_max": r1, "time_min": t0,
                        "time_max": t1, "plaquette_in": plaq0, "plaquette_out": plaq1,
-                       "wilson": w.tolist(), "wilson_adjoint": wa.tolist()}
+                       "wilson": w.tolist(), "wilson_adjoint": wa.tolist(),
+                       "gevp": gevp.tolist(), "gevp_adjoint": gevp_adj.tolist(),
+                       "plaquette_time": plaq_t, "plaquette_space": plaq_s,
+                       "polyakov_loop": poly, "polyakov_d_max": d_max,
+                       "polyakov_singlet_by_distance": [[k, v] for k, v in avg_s.items()],
+                       "polyakov_color_average_by_distance": [[k, v] for k, v in avg_c.items()]}
         print(name, "plaq", plaq0, "->", plaq1, "W[0,0]", w[0, 0])
     meta = {"generated_by": "tests/golden/make_golden.py",
             "reference_code": "oracle/_ref/libref_parity.so (lib/cpu smearing_HYP, "
-                              "smearing_APE, wilson_loop, wilson_loop_adjoint, plaket_site; "
-                              "-O2 -fno-fast-math)",
+                              "smearing_APE, wilson_loop, wilson_loop_adjoint, "
+                              "wilson_gevp_indexed, wilson_gevp_adjoint_indexed, plaket_site, "
+                              "plaket_site_time, plaket_site_space, get_polyakov_loop, "
+                              "polyakov_loop_correlator_singlet, "
+                              "polyakov_loop_correlator_color_average, "
+                              "polyakov_average_directions; -O2 -fno-fast-math)",
             "link_layout": "4*V links, link index 4*site+mu, row-major (get_data order)",
             "cases": index}
     (OUT / "index.json").write_text(json.dumps(meta, indent=1))

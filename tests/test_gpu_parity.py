@@ -184,3 +184,78 @@ def test_abelian_flux_closed_form(nc, precision, atol):
         lat.ape(0.5, 3)
         assert max_abs(lat.download(), links) <= (1e-14 if precision == "fp64" else 1e-6)
         np.testing.assert_allclose(lat.wilson_loop(1, 3, 1, 4), expect, atol=atol)
+
+
+@pytest.mark.parametrize("name,meta", CASES, ids=[c[0] for c in CASES])
+def test_fp64_observables_match_reference_fixture(name, meta):
+    """GEVP tables (two handles), time/space plaquettes, Polyakov loop and
+    correlators against the reference's values."""
+    g = load_golden(name)
+    nc, dims = meta["nc"], meta["dims"]
+    r0, r1, t0, t1 = meta["r_min"], meta["r_max"], meta["time_min"], meta["time_max"]
+    with Lattice(dims, nc, "fp64") as a, Lattice(dims, nc, "fp64") as b:
+        a.upload(g["links_ape"])
+        b.upload(g["links_hyp"])
+        assert_w_close(a.wilson_gevp(b, r0, r1, t0, t1), g["gevp"])
+        assert_w_close(a.wilson_gevp(b, r0, r1, t0, t1, adjoint=True), g["gevp_adjoint"])
+        pt, ps = g["plaquettes_time_space"]
+        assert a.plaquette_time() == pytest.approx(pt, rel=1e-12)
+        assert a.plaquette_space() == pytest.approx(ps, rel=1e-12)
+        assert b.polyakov_loop() == pytest.approx(float(g["polyakov_loop"][0]), rel=1e-12,
+                                                  abs=1e-14)
+        d = meta["polyakov_d_max"]
+        np.testing.assert_allclose(b.polyakov_correlator(d, True), g["polyakov_singlet"],
+                                   rtol=1e-12, atol=1e-15)
+        np.testing.assert_allclose(b.polyakov_correlator(d, False),
+                                   g["polyakov_color_average"], rtol=1e-12, atol=1e-15)
+
+
+@pytest.mark.parametrize("nc,eps", [(2, 0.3), (3, 0.25)])
+def test_observables_match_oracle_seeded(port, nc, eps):
+    """Larger lattices (several W blocks, several Polyakov blocks) in both
+    forms: FP64 within 1e-12, mixed within 1e-6 relative / 1e-7 absolute."""
+    dims = (8, 6, 10, 12)
+    a = generate_config(dims, nc, eps, 20261203, 31)
+    b = generate_config(dims, nc, eps, 20261203, 32)
+    want = {"gevp": port.wilson_gevp(nc, dims, a, b, 1, 4, 1, 6),
+            "gevp_adj": port.wilson_gevp(nc, dims, a, b, 1, 4, 1, 6, True),
+            "pt": port.plaquette_time(nc, dims, a), "ps": port.plaquette_space(nc, dims, a),
+            "poly": port.polyakov_loop(nc, dims, a),
+            "sing": port.polyakov_correlator(nc, dims, a, 3, True),
+            "col": port.polyakov_correlator(nc, dims, a, 3, False)}
+    for precision, rtol, atol in (("fp64", 1e-12, 1e-14), ("mixed", 1e-6, 1e-7)):
+        with Lattice(dims, nc, precision) as la, Lattice(dims, nc, precision) as lb:
+            la.upload(a)
+            lb.upload(b)
+            np.testing.assert_allclose(la.wilson_gevp(lb, 1, 4, 1, 6), want["gevp"], rtol=rtol,
+                                       atol=atol)
+            np.testing.assert_allclose(la.wilson_gevp(lb, 1, 4, 1, 6, True), want["gevp_adj"],
+                                       rtol=rtol, atol=atol)
+            assert la.plaquette_time() == pytest.approx(want["pt"], rel=rtol, abs=atol)
+            assert la.plaquette_space() == pytest.approx(want["ps"], rel=rtol, abs=atol)
+            assert la.plaquette() == pytest.approx(0.5 * (want["pt"] + want["ps"]), rel=rtol)
+            assert la.polyakov_loop() == pytest.approx(want["poly"], rel=rtol, abs=atol)
+            np.testing.assert_allclose(la.polyakov_correlator(3, True), want["sing"], rtol=rtol,
+                                       atol=atol)
+            np.testing.assert_allclose(la.polyakov_correlator(3, False), want["col"], rtol=rtol,
+                                       atol=atol)
+
+
+@pytest.mark.parametrize("nc", [2, 3])
+def test_gevp_with_itself_and_argument_errors(nc):
+    dims = (4, 4, 4, 6)
+    links = generate_config(dims, nc, 0.3 if nc == 2 else 0.25, 5, 0)
+    with Lattice(dims, nc, "fp64") as a, Lattice((4, 4, 4, 8), nc, "fp64") as other, \
+            Lattice(dims, nc, "mixed") as m:
+        a.upload(links)
+        other.upload(generate_config((4, 4, 4, 8), nc, 0.3, 5, 0))
+        m.upload(links)
+        # the same handle as both configurations gives the ordinary table
+        np.testing.assert_allclose(a.wilson_gevp(a, 1, 2, 1, 3), a.wilson_loop(1, 2, 1, 3),
+                                   rtol=1e-13, atol=1e-15)
+        with pytest.raises(GCError):
+            a.wilson_gevp(other, 1, 2, 1, 3)  # different sizes
+        with pytest.raises(GCError):
+            a.wilson_gevp(m, 1, 2, 1, 3)  # different precision
+        with pytest.raises(GCError):
+            a.polyakov_correlator(-1, True)

@@ -105,3 +105,88 @@ def test_abelian_flux_closed_form(port, nc):
     port.ape(nc, dims, v, 0.5, 3)  # fixed point
     assert max_abs(v, links) <= 1e-14
     np.testing.assert_allclose(port.wilson(nc, dims, v, 1, 3, 1, 4), expect, atol=1e-14)
+
+
+@pytest.mark.parametrize("name,meta", CASES, ids=[c[0] for c in CASES])
+def test_port_observables_match_reference_fixture(port, name, meta):
+    """GEVP tables, time/space plaquettes, Polyakov loop and correlators."""
+    g = load_golden(name)
+    nc, dims = meta["nc"], meta["dims"]
+    r0, r1, t0, t1 = meta["r_min"], meta["r_max"], meta["time_min"], meta["time_max"]
+    for adjoint, key in ((False, "gevp"), (True, "gevp_adjoint")):
+        w = port.wilson_gevp(nc, dims, g["links_ape"], g["links_hyp"], r0, r1, t0, t1, adjoint)
+        np.testing.assert_allclose(w, g[key], rtol=1e-12, atol=1e-14)
+    pt, ps = g["plaquettes_time_space"]
+    assert port.plaquette_time(nc, dims, g["links_ape"]) == pytest.approx(pt, rel=1e-12)
+    assert port.plaquette_space(nc, dims, g["links_ape"]) == pytest.approx(ps, rel=1e-12)
+    assert port.polyakov_loop(nc, dims, g["links_hyp"]) == pytest.approx(
+        float(g["polyakov_loop"][0]), rel=1e-12, abs=1e-14)
+    d = meta["polyakov_d_max"]
+    for singlet, key in ((True, "polyakov_singlet"), (False, "polyakov_color_average")):
+        c = port.polyakov_correlator(nc, dims, g["links_hyp"], d, singlet)
+        np.testing.assert_allclose(c, g[key], rtol=1e-12, atol=1e-15)
+
+
+@pytest.mark.parametrize("name,meta", CASES, ids=[c[0] for c in CASES])
+def test_reference_reproduces_observable_fixture(name, meta):
+    from oracle import py_oracle
+    if not py_oracle.ref_available("parity"):
+        pytest.skip("reference not compiled in this checkout (oracle/_ref)")
+    ref = py_oracle.ref("parity")
+    g = load_golden(name)
+    nc, dims = meta["nc"], meta["dims"]
+    r0, r1, t0, t1 = meta["r_min"], meta["r_max"], meta["time_min"], meta["time_max"]
+    w = ref.wilson_gevp(nc, dims, g["links_ape"], g["links_hyp"], r0, r1, t0, t1, False)
+    np.testing.assert_allclose(w, g["gevp"], rtol=1e-13, atol=0)
+    assert ref.polyakov_loop(nc, dims, g["links_hyp"]) == float(g["polyakov_loop"][0])
+    c = ref.polyakov_correlator(nc, dims, g["links_hyp"], meta["polyakov_d_max"], True)
+    np.testing.assert_allclose(c, g["polyakov_singlet"], rtol=1e-13, atol=1e-16)
+
+
+@pytest.mark.parametrize("name,meta", CASES, ids=[c[0] for c in CASES])
+def test_polyakov_distance_average_matches_reference(name, meta):
+    """Host-side polyakov_average_directions against the reference's output."""
+    from general_code_b200 import polyakov_average_directions
+    g = load_golden(name)
+    d = meta["polyakov_d_max"]
+    for key in ("polyakov_singlet", "polyakov_color_average"):
+        got = polyakov_average_directions(g[key], d)
+        want = meta[f"{key}_by_distance"]
+        assert [k for k in got] == pytest.approx([k for k, _ in want], abs=0)
+        np.testing.assert_allclose(list(got.values()), [v for _, v in want], rtol=1e-15,
+                                   atol=1e-17)
+
+
+@pytest.mark.parametrize("nc", [2, 3])
+def test_gevp_of_identical_configurations_is_the_wilson_table(port, nc):
+    dims = (4, 4, 3, 6)
+    a = generate_config(dims, nc, 0.3 if nc == 2 else 0.25, 21, 0)
+    for adjoint in (False, True):
+        w = port.wilson_gevp(nc, dims, a, a, 1, 2, 1, 3, adjoint)
+        ref = (port.wilson_adjoint if adjoint else port.wilson)(nc, dims, a, 1, 2, 1, 3)
+        np.testing.assert_allclose(w, ref, rtol=1e-13, atol=1e-15)
+
+
+def visited_offsets(d):
+    """Offsets the reference's correlators visit (polyakov_loops.h:100-113)."""
+    out = []
+    for dz in range(-d, d + 1):
+        for dy in range(-d, d + 1):
+            for dx in range(0 if (dy and dz) else -d, d + 1):
+                if (dx * dx + dy * dy + dz * dz) ** 0.5 <= d:
+                    out.append((dx, dy, dz))
+    return out
+
+
+@pytest.mark.parametrize("nc", [2, 3])
+def test_polyakov_of_unit_and_abelian_configurations(port, nc):
+    """Unit links: P = 1, loop 1, all visited correlator entries 1. The
+    constant-flux configuration has unit time links, so the same holds."""
+    from conftest import abelian_flux_config
+    dims = (6, 5, 4, 8)
+    for links in (unit_config(dims, nc), abelian_flux_config(dims, nc)[0]):
+        assert port.polyakov_loop(nc, dims, links) == pytest.approx(1.0, abs=1e-14)
+        for singlet in (True, False):
+            c = port.polyakov_correlator(nc, dims, links, 2, singlet)
+            assert set(np.round(c[c != 0], 12)) == {1.0}
+            assert np.count_nonzero(c) == len(visited_offsets(2))
