@@ -138,6 +138,12 @@ def load_peaks():
     return 6650.0, "fallback"
 
 
+# Nominal vector-pipe peaks of one B200 (148 SMs at 1965 MHz): FP64 64 and
+# FP32 128 fused multiply-adds per SM per clock. Not measured on this pool
+# (the measured peaks cover HBM copy and bf16 GEMM only).
+FP_PEAK_TFLOPS = {"fp64": 148 * 64 * 2 * 1.965e9 / 1e12, "fp32": 148 * 128 * 2 * 1.965e9 / 1e12}
+
+
 def load_traffic():
     p = ROOT / "profiles" / "roofline_traffic.json"
     if p.exists():
@@ -297,7 +303,9 @@ def bench_serving(duration_s: float, rate: float = 200.0, slots: int = 8):
     return {"workload": f"Poisson {rate:g} req/s for {duration_s:g} s, L^4 with L 8..32",
             "requests": n, "completed": st["completed"], "offered_rate": rate,
             "wall_s": wall, "p50_ms": st["p50_ms"], "p99_ms": st["p99_ms"],
-            "mean_ms": st["mean_ms"], "value": st["sites_per_s"], "unit": "sites/s",
+            "mean_ms": st["mean_ms"], "queue_p50_ms": st["queue_p50_ms"],
+            "queue_p99_ms": st["queue_p99_ms"], "run_p50_ms": st["run_p50_ms"],
+            "run_p99_ms": st["run_p99_ms"], "value": st["sites_per_s"], "unit": "sites/s",
             "slots": slots, "peak_inflight": st["peak_inflight"],
             "peak_device_bytes": st["peak_bytes"], "mixed_vs_fp64_max_rel_err_W": err,
             "checked_requests": len(sample)}
@@ -483,6 +491,7 @@ def main():
         ms = per_launch[dom]
         achieved = alg[dom]["bytes"] * V / (ms * 1e-3) / 1e9
         tr = traffic.get(f"{dom}:{args.workload}:{form}")
+        pipe = "fp64" if form == "fp64" else "fp32"
         return {
             "value": world * V * args.steps / (r["total_ms"] * 1e-3),
             "e2e_value": world * V * args.steps / (r["total_e2e_ms"] * 1e-3),
@@ -494,7 +503,14 @@ def main():
                          "traffic": (tr["dram_bytes_per_site"] * V if tr else None),
                          "alg_bytes_per_launch": alg[dom]["bytes"] * V,
                          "fp_flops_per_launch": alg[dom]["flops"] * V,
-                         "fp_tflops": alg[dom]["flops"] * V / (ms * 1e-3) / 1e12},
+                         "fp_tflops": alg[dom]["flops"] * V / (ms * 1e-3) / 1e12,
+                         # the kernels are bound by the vector FP pipes, not HBM:
+                         # algorithmic FLOPs over the pipe the form computes in
+                         "compute": {"pipe": pipe,
+                                     "achieved_tflops": alg[dom]["flops"] * V / (ms * 1e-3) / 1e12,
+                                     "peak_tflops": FP_PEAK_TFLOPS[pipe], "peak_kind": "nominal",
+                                     "frac": alg[dom]["flops"] * V / (ms * 1e-3) / 1e12
+                                     / FP_PEAK_TFLOPS[pipe]}},
         }
 
     sums = {f: summary(f, results[f]) for f in forms}

@@ -117,7 +117,9 @@ class ServerMetrics(ctypes.Structure):
                 ("peak_inflight", ctypes.c_int), ("peak_bytes", ctypes.c_longlong),
                 ("budget", ctypes.c_longlong), ("p50_ms", ctypes.c_double),
                 ("p99_ms", ctypes.c_double), ("mean_ms", ctypes.c_double),
-                ("sites_per_s", ctypes.c_double)]
+                ("sites_per_s", ctypes.c_double), ("queue_p50_ms", ctypes.c_double),
+                ("queue_p99_ms", ctypes.c_double), ("run_p50_ms", ctypes.c_double),
+                ("run_p99_ms", ctypes.c_double)]
 
 
 SIGNATURES.update({

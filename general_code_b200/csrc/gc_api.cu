@@ -123,21 +123,27 @@ size_t bytes_per_link(int nc, int prec) {
   return prec == GC_PREC_FP64 ? 32 : 16;
 }
 
+// (an attribute query, not cudaGetDeviceProperties, which is slow and is
+// otherwise paid by every handle a request loop creates)
 int check_device(gc_lattice *h) {
   int n = 0;
   cudaError_t e = cudaGetDeviceCount(&n);
   if (e != cudaSuccess || n == 0)
     return fail(h, GC_ERR_NODEVICE, "no CUDA device available");
-  int dev = 0;
+  int dev = 0, major = 0;
   cudaGetDevice(&dev);
-  cudaDeviceProp p;
-  e = cudaGetDeviceProperties(&p, dev);
+  e = cudaDeviceGetAttribute(&major, cudaDevAttrComputeCapabilityMajor, dev);
   if (e != cudaSuccess)
-    return cuda_fail(h, "cudaGetDeviceProperties", e);
-  if (p.major != 10)
+    return cuda_fail(h, "cudaDeviceGetAttribute", e);
+  if (major != 10) {
+    char name[256] = "?";
+    cudaDeviceProp p;
+    if (cudaGetDeviceProperties(&p, dev) == cudaSuccess)
+      std::snprintf(name, sizeof name, "%s", p.name);
     return fail(h, GC_ERR_NODEVICE,
-                "device " + std::string(p.name) +
+                "device " + std::string(name) +
                     " is not sm_100 (this library is built for sm_100a only)");
+  }
   return GC_OK;
 }
 

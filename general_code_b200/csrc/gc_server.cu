@@ -83,7 +83,7 @@ struct gc_server {
   long long submitted = 0, completed = 0, rejected = 0, failed = 0;
   long long sites_done = 0;
   double t_first = 0, t_last = 0;
-  std::vector<double> latencies_ms;
+  std::vector<double> latencies_ms, queue_ms, run_ms;
 };
 
 namespace {
@@ -169,6 +169,8 @@ void worker(gc_server *s, int slot) {
       s->completed++;
       s->sites_done += r.sites;
       s->latencies_ms.push_back(1e3 * (r.t_done - r.t_submit));
+      s->queue_ms.push_back(1e3 * (r.t_start - r.t_submit));
+      s->run_ms.push_back(1e3 * (r.t_done - r.t_start));
       s->t_last = std::max(s->t_last, r.t_done);
     }
     s->cv_done.notify_all();
@@ -339,6 +341,10 @@ int gc_server_stats(gc_server *s, gc_server_metrics *st) {
   for (double v : s->latencies_ms)
     sum += v;
   st->mean_ms = s->latencies_ms.empty() ? 0 : sum / s->latencies_ms.size();
+  st->queue_p50_ms = percentile(s->queue_ms, 0.50);
+  st->queue_p99_ms = percentile(s->queue_ms, 0.99);
+  st->run_p50_ms = percentile(s->run_ms, 0.50);
+  st->run_p99_ms = percentile(s->run_ms, 0.99);
   const double span = s->t_last - s->t_first;
   st->sites_per_s = span > 0 ? (double)s->sites_done / span : 0;
   return GC_OK;

@@ -26,7 +26,10 @@
 #include "gc_kernels.h"
 #include "gc_pair.cuh"
 
+#include <mutex>
+#include <set>
 #include <type_traits>
+#include <utility>
 
 namespace gc {
 
@@ -489,6 +492,36 @@ __global__ void __launch_bounds__(256)
   }
 }
 
+// Lets `kernel` use up to the device's opt-in shared memory per block. Set
+// once per (kernel, device) rather than before every launch: concurrent
+// request threads would otherwise call cudaFuncSetAttribute on every W
+// launch. The attribute only raises the allowed maximum; each launch still
+// asks for the shared memory it needs.
+template <class K> int allow_large_smem(K *kernel, size_t smem, bool capturing = false) {
+  if (smem <= 48 * 1024)
+    return GC_OK;
+  static std::mutex mu;
+  static std::set<std::pair<const void *, int>> done;
+  int dev = 0;
+  cudaGetDevice(&dev);
+  std::lock_guard<std::mutex> lk(mu);
+  if (done.count({(const void *)kernel, dev}))
+    return GC_OK;
+  // (while a stream is captured the attribute set by an earlier eager launch
+  // of the same schedule stays in force)
+  if (capturing)
+    return GC_OK;
+  int optin = 0;
+  cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+  if ((size_t)optin < smem)
+    return plan_error("W kernel: shared memory above the device's limit");
+  if (cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, optin) !=
+      cudaSuccess)
+    return launch_check("wilson kernel shared-memory attribute");
+  done.insert({(const void *)kernel, dev});
+  return GC_OK;
+}
+
 int largest_divisor_upto(int n, int cap) {
   for (int d = cap < n ? cap : n; d > 1; d--)
     if (n % d == 0)
@@ -543,16 +576,12 @@ int launch_wilson_mode(const Geom &g, const Fields4 &U, const Fields4 &U2, int r
   if (!p.fits || nr * nt > kWilsonMaxEntries)
     return plan_error("wilson_kernel: time extent or (R,T) range too large for "
                       "one block's shared memory");
-  if (p.smem > 48 * 1024) {
-    cudaError_t e = cudaFuncSetAttribute(wilson_kernel<Store, CT, ADJ, GEVP>,
-                                         cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         (int)p.smem);
-    if (e != cudaSuccess)
-      return launch_check("wilson_kernel smem attribute");
-  }
+  int rc = allow_large_smem(wilson_kernel<Store, CT, ADJ, GEVP>, p.smem);
+  if (rc)
+    return rc;
   wilson_kernel<Store, CT, ADJ, GEVP><<<dim3(p.blocks / 3, 3), p.threads, p.smem, s>>>(
       g, U, U2, rmin, rmax, tmin, tmax, p.cols_per_block, p.rows, partials);
-  int rc = launch_check("wilson_kernel");
+  rc = launch_check("wilson_kernel");
   if (rc)
     return rc;
   // GEVP counts every loop twice (the / (6 V) of wilson_loops.h:910, 954)
@@ -617,16 +646,12 @@ int launch_wilson_plan(const Geom &g, const Fields4 &U, int rmin, int rmax, int 
   const int nr = rmax - rmin + 1, nt = tmax - tmin + 1;
   if (!p.fits)
     return plan_error("wilson_kernel: block shape does not fit");
-  if (p.smem > 48 * 1024) {
-    cudaError_t e = cudaFuncSetAttribute(
-        wilson_kernel<Store, CT, false, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-        (int)p.smem);
-    if (e != cudaSuccess)
-      return launch_check("wilson_kernel smem attribute");
-  }
+  int rc = allow_large_smem(wilson_kernel<Store, CT, false, false>, p.smem);
+  if (rc)
+    return rc;
   wilson_kernel<Store, CT, false, false><<<dim3(p.blocks / 3, 3), p.threads, p.smem, s>>>(
       g, U, U, rmin, rmax, tmin, tmax, p.cols_per_block, p.rows, partials);
-  int rc = launch_check("wilson_kernel");
+  rc = launch_check("wilson_kernel");
   if (rc)
     return rc;
   if (!out_dev)
@@ -657,15 +682,10 @@ int launch_wilson_batch(const WJob *jobs, int njobs, int blocks, int threads, si
     return plan_error("wilson_batch_kernel: shared memory above 227 KB");
   cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
   cudaStreamIsCapturing(s, &cap);
-  // (while a stream is captured the attribute set by an earlier eager launch
-  // of the same schedule stays in force)
-  if (smem > 48 * 1024 && cap == cudaStreamCaptureStatusNone) {
-    cudaError_t e = cudaFuncSetAttribute(wilson_batch_kernel<Store, CT>,
-                                         cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         (int)smem);
-    if (e != cudaSuccess)
-      return launch_check("wilson_batch_kernel smem attribute");
-  }
+  int rc = allow_large_smem(wilson_batch_kernel<Store, CT>, smem,
+                            cap != cudaStreamCaptureStatusNone);
+  if (rc)
+    return rc;
   wilson_batch_kernel<Store, CT><<<blocks, threads, smem, s>>>(jobs, njobs);
   return launch_check("wilson_batch_kernel");
 }

@@ -326,6 +326,8 @@ typedef struct {
   long long peak_bytes, budget;
   double p50_ms, p99_ms, mean_ms; /* submit-to-result latency of completed requests */
   double sites_per_s;             /* completed sites / (last result - first submit) */
+  double queue_p50_ms, queue_p99_ms; /* submit-to-admission part of the latency */
+  double run_p50_ms, run_p99_ms;     /* admission-to-result part */
 } gc_server_metrics;
 
 int gc_server_create(const gc_server_opts *opts, gc_server **out);
