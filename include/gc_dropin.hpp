@@ -28,6 +28,8 @@
 //   polyakov_loop(const LatticeData&)                     polyakov_loops.h:24-41
 //   polyakov_loop_correlator_color_average / _singlet(const LatticeData&, int)
 //                                                         polyakov_loops.h:83-206
+//   Data::read_data_convert(LatticeData&, std::string, std::string, int,
+//       std::string, bool)                                data.h:265-338
 #pragma once
 
 #include "gc_lattice.h"
@@ -64,6 +66,11 @@ template <class MT> class Session {
 public:
   static_assert(sizeof(MT) == (traits<MT>::nc == 3 ? 18 : 4) * sizeof(double),
                 "link type must be a plain array of doubles");
+  // an empty FP64 handle (links to be read from a file)
+  explicit Session(const std::array<int, 4> &dims) {
+    check(gc_lattice_create(dims.data(), traits<MT>::nc, GC_PREC_FP64, &h_),
+          nullptr, "create");
+  }
   Session(const std::array<int, 4> &dims, const MT *links) {
     check(gc_lattice_create(dims.data(), traits<MT>::nc, GC_PREC_FP64, &h_),
           nullptr, "create");
@@ -163,6 +170,19 @@ gevp(const Data::LatticeData<DataPatternLexicographical, MT> &conf1,
     for (int r = r_min; r <= r_max; r++)
       result[std::tuple<int, int>(t, r)] = w[(t - time_min) * nr + (r - r_min)];
   return result;
+}
+
+// The file is read by the library's reader straight into device links
+// (gc_read_config), then copied into conf.array.
+template <class MT>
+void read(Data::LatticeData<DataPatternLexicographical, MT> &conf, const std::string &path,
+          const std::string &format, int bytes_skip, const std::string &precision,
+          bool convert) {
+  Session<MT> s(conf.lat_dim);
+  check(gc_read_config(s.get(), path.c_str(), format.c_str(), bytes_skip, precision.c_str(),
+                       convert ? 1 : 0),
+        s.get(), "read_data_convert");
+  s.download(conf.array.data());
 }
 
 template <class MT>
@@ -314,3 +334,17 @@ inline std::vector<double> polyakov_loop_correlator_color_average(
     const Data::LatticeData<DataPatternLexicographical, su3> &conf, int D_max) {
   return gc_dropin::polyakov_correlator(conf, D_max, GC_POLYAKOV_COLOR_AVERAGE);
 }
+// Configuration reader (data.h:265-338), as apps/smearing/smearing.cpp:188
+// calls it (qualified, Data::read_data_convert).
+namespace Data {
+inline void read_data_convert(LatticeData<DataPatternLexicographical, su2> &conf,
+                              std::string file_path, std::string conf_format, int bytes_skip,
+                              std::string file_precision, bool convert) {
+  gc_dropin::read(conf, file_path, conf_format, bytes_skip, file_precision, convert);
+}
+inline void read_data_convert(LatticeData<DataPatternLexicographical, su3> &conf,
+                              std::string file_path, std::string conf_format, int bytes_skip,
+                              std::string file_precision, bool convert) {
+  gc_dropin::read(conf, file_path, conf_format, bytes_skip, file_precision, convert);
+}
+} // namespace Data

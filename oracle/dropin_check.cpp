@@ -28,6 +28,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
+#include <unistd.h>
 
 int x_size, y_size, z_size, t_size, size1, size2;
 
@@ -133,6 +134,35 @@ int run(const std::array<int, 4> &dims, int ape_steps, int rmax, int tmax) {
   pb = ref_plaquette(b);
   ::smearing_HYP<DP, MT>(b, 1, 0.75, 0.6);
   hb.array = b.array;
+  // reader: the HYP-smeared links written as the app writes them
+  // (smearing.cpp:336-339), read back through the drop-in (qualified call, as
+  // smearing.cpp:188) and through the reference's template
+  double dread = -1;
+  {
+    char path[] = "/tmp/gc_dropin_conf_XXXXXX";
+    const int fd = mkstemp(path);
+    if (fd >= 0) {
+      close(fd);
+      FilePatternLexicographical<4, MT> fp;
+      hb.write_data(std::string(path), fp);
+      Data::LatticeData<DP, MT> ra(dims), rb(dims);
+      try {
+        Data::read_data_convert(ra, std::string(path), "lexicographical", 0, "double", false);
+      } catch (const std::exception &e) {
+        std::printf("drop-in reader raised: %s\n", e.what());
+        std::remove(path);
+        return 3;
+      }
+      Data::read_data_convert<DP>(rb, std::string(path), "lexicographical", 0, "double", false);
+      std::remove(path);
+      dread = 0;
+      for (size_t i = 0; i < ra.array.size(); i++) {
+        std::vector<double> x = ra.array[i].get_data(), y = rb.array[i].get_data();
+        for (size_t k = 0; k < x.size(); k++)
+          dread = std::fmax(dread, std::fabs(x[k] - y[k]));
+      }
+    }
+  }
   lb = ref_polyakov(b);
   csb = ::polyakov_loop_correlator_singlet<DP, MT>(b, D);
   ccb = ::polyakov_loop_correlator_color_average<DP, MT>(b, D);
@@ -150,7 +180,7 @@ int run(const std::array<int, 4> &dims, int ape_steps, int rmax, int tmax) {
     for (int k = 0; k < ds; k++)
       dl = std::fmax(dl, std::fabs(x[k] - y[k]));
   }
-  bool ok = dl <= 1e-12;
+  bool ok = dl <= 1e-12 && dread == 0.0;
   for (auto pr : {std::make_pair(pa, pb), std::make_pair(pta, ptb), std::make_pair(psa, psb),
                   std::make_pair(la, lb)})
     ok = ok && std::fabs(pr.first - pr.second) <= 1e-12 * std::fabs(pr.second) + 1e-14;
@@ -159,9 +189,10 @@ int run(const std::array<int, 4> &dims, int ape_steps, int rmax, int tmax) {
   const double dg = std::fmax(max_rel(ga, gb, &ok), max_rel(gaa, gab, &ok));
   const double dc = std::fmax(max_abs_vec(csa, csb, &ok), max_abs_vec(cca, ccb, &ok));
   std::printf("links max|diff| %.3e  plaquette diff %.3e (time %.3e space %.3e)  W max rel "
-              "diff %.3e  GEVP %.3e  Polyakov %.3e, correlators %.3e  entries %zu  %s\n",
+              "diff %.3e  GEVP %.3e  Polyakov %.3e, correlators %.3e  reader %.3e  "
+              "entries %zu  %s\n",
               dl, std::fabs(pa - pb), std::fabs(pta - ptb), std::fabs(psa - psb), dw, dg,
-              std::fabs(la - lb), dc, wb.size(), ok ? "OK" : "MISMATCH");
+              std::fabs(la - lb), dc, dread, wb.size(), ok ? "OK" : "MISMATCH");
   return ok ? 0 : 1;
 }
 

@@ -135,8 +135,9 @@ def test_device_generator_matches_host(nc, eps):
 
 @pytest.mark.parametrize("nc,eps", [(2, 0.3), (3, 0.25)])
 def test_mixed_precision_error_budget(port, nc, eps):
-    """Mixed form (FP32 links, FP64 projection and sums) against the FP64
-    oracle: links within 1e-5 and W within 1e-5 relative after HYP + 5 APE."""
+    """Mixed form (FP32 links, FP64 final projection step and sums) against
+    the FP64 oracle: links within 1e-5 and W within 1e-6 relative (the mixed
+    form's bar) after HYP + 5 APE."""
     dims = (8, 8, 8, 8)
     links = generate_config(dims, nc, eps, 11, 0)
     ref = links.copy()
@@ -151,7 +152,25 @@ def test_mixed_precision_error_budget(port, nc, eps):
         assert max_abs(got, ref) < 1e-5
         assert unitarity_error(nc, got) < 1e-6
         w = lat.wilson_loop(1, 4, 1, 4)
-    np.testing.assert_allclose(w, w_ref, rtol=1e-5)
+    np.testing.assert_allclose(w, w_ref, rtol=1e-6)
+
+
+@pytest.mark.parametrize("nc,eps", [(2, 0.3), (3, 0.25)])
+def test_mixed_w_within_1e6_after_long_smearing(port, nc, eps):
+    """Every W(R,T) of the mixed form within 1e-6 relative of the FP64 oracle
+    after HYP + 20 APE steps on a 12^4 lattice, R, T up to 6."""
+    dims = (12, 12, 12, 12)
+    links = generate_config(dims, nc, eps, 20261203, 41)
+    ref = links.copy()
+    port.hyp(nc, dims, ref, 1.0, 0.75, 0.6, 1)
+    port.ape(nc, dims, ref, 0.5, 20)
+    w_ref = port.wilson(nc, dims, ref, 1, 6, 1, 6)
+    with Lattice(dims, nc, "mixed") as lat:
+        lat.upload(links)
+        lat.hyp(1.0, 0.75, 0.6, 1)
+        lat.ape(0.5, 20)
+        w = lat.wilson_loop(1, 6, 1, 6)
+    np.testing.assert_allclose(w, w_ref, rtol=1e-6, atol=0)
 
 
 @pytest.mark.parametrize("precision", ["fp64", "mixed"])
