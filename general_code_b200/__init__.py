@@ -9,7 +9,9 @@ from .lattice import (GCError, Lattice, LatticeData, generate_config, job_device
                       polyakov_loop, polyakov_loop_correlator_color_average,
                       polyakov_loop_correlator_singlet, probe_config, read_data_convert,
                       smearing_APE, smearing_HYP, unit_config, volume, wilson_gevp_adjoint_indexed,
-                      wilson_gevp_indexed, wilson_loop, wilson_loop_adjoint)
+                      wilson_gevp_indexed, wilson_loop, wilson_loop_adjoint, wilson_offaxis,
+                      wilson_offaxis_adjoint, wilson_offaxis_adjoint_result,
+                      wilson_offaxis_result)
 
 __all__ = ["GCError", "Lattice", "LatticeData", "generate_config", "job_device_bytes",
            "link_size", "plaket", "plaket_space", "plaket_time", "polyakov_average_directions",
@@ -17,4 +19,5 @@ __all__ = ["GCError", "Lattice", "LatticeData", "generate_config", "job_device_b
            "polyakov_loop_correlator_singlet", "probe_config", "read_data_convert",
            "smearing_APE", "smearing_HYP", "unit_config", "volume",
            "wilson_gevp_adjoint_indexed", "wilson_gevp_indexed", "wilson_loop",
-           "wilson_loop_adjoint"]
+           "wilson_loop_adjoint", "wilson_offaxis", "wilson_offaxis_adjoint",
+           "wilson_offaxis_adjoint_result", "wilson_offaxis_result"]

@@ -60,6 +60,10 @@ SIGNATURES = {
     "gc_wilson_gevp_onaxis": (_c_int, [_p, _p, _c_int, _c_int, _c_int, _c_int, _pdbl]),
     "gc_wilson_gevp_adjoint_onaxis": (_c_int, [_p, _p, _c_int, _c_int, _c_int, _c_int, _pdbl]),
     "gc_polyakov_loop": (_c_int, [_p, _pdbl]),
+    "gc_wilson_offaxis": (_c_int, [_p, _pint, _c_int, _c_dbl, _c_dbl, _c_int, _c_int, _c_int,
+                                   _p, _c_int, _pint]),
+    "gc_wilson_offaxis_result": (_c_int, [_p, _c_dbl, _c_dbl, _c_int, _c_int, _c_int, _p,
+                                          _c_int, _pint]),
     "gc_polyakov_correlator": (_c_int, [_p, _c_int, _c_int, _pdbl]),
     "gc_wilson_onaxis_noalloc": (_c_int, [_pint, _c_int, _c_int, ctypes.POINTER(_p), _c_int,
                                           _c_int, _c_int, _c_int, _p, _p]),
@@ -134,6 +138,12 @@ SIGNATURES.update({
 })
 
 _lib = None
+
+
+class WilsonResult(ctypes.Structure):
+    """gc_wilson_result (include/gc_lattice.h)."""
+    _fields_ = [("wilson_loop", ctypes.c_double), ("time_size", ctypes.c_int),
+                ("space_size", ctypes.c_double), ("statistics_size", ctypes.c_int)]
 
 
 class GCError(RuntimeError):

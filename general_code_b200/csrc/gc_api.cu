@@ -5,6 +5,7 @@
 #include "gc_internal.cuh"
 #include "gc_kernels.h"
 
+#include <array>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -662,6 +663,116 @@ int gc_plaquette_time(gc_lattice *h, double *out) {
     return rc;
   *out = v[1];
   return GC_OK;
+}
+
+// Off-axis loops: one space-line field and one loop launch per line of the
+// plan, all loop averages copied back once, then averaged per (direction,
+// multiplier, T) in the plan's order (a left-to-right sum from 0, as
+// std::accumulate).
+static int offaxis_impl(gc_lattice *h, const std::vector<std::array<int, 3>> &dirs,
+                        double r_min, double r_max, int tmin, int tmax, bool adjoint,
+                        std::vector<gc_wilson_result> &res) {
+  int rc = check_ready(h);
+  if (rc)
+    return rc;
+  if (tmin < 1 || tmax < tmin)
+    return fail(h, GC_ERR_ARG, "need 1 <= time_min <= time_max");
+  const int nt = tmax - tmin + 1;
+  if (nt > kWilsonMaxEntries)
+    return fail(h, GC_ERR_ARG, "time range too large (at most 1024 values of T)");
+  for (const auto &d : dirs)
+    if (d[0] < 1 || d[1] < 0 || d[2] < 0 || d[0] < d[1] || d[1] < d[2])
+      return fail(h, GC_ERR_ARG, "directions need a1 >= a2 >= a3 >= 0 and a1 >= 1");
+  const OffaxisPlan plan = offaxis_plan(dirs, r_min, r_max);
+  for (const auto &line : plan.lines)
+    if ((int)line.pattern.size() > kOffaxisMaxSteps)
+      return fail(h, GC_ERR_ARG, "off-axis line longer than 256 links (reduce r_max)");
+  res.clear();
+  if (plan.lines.empty())
+    return GC_OK;
+  std::lock_guard<std::mutex> lk(h->mu);
+  const size_t line_bytes =
+      ((inter_link_bytes(h->nc, h->prec) * (size_t)h->g.V + 255) / 256) * 256;
+  rc = ensure_aux(h, line_bytes);
+  if (rc)
+    return rc;
+  rc = ensure_partials(h, offaxis_partials_count(h->g, nt));
+  if (rc)
+    return rc;
+  rc = ensure_dev_out(h, plan.lines.size() * (size_t)nt);
+  if (rc)
+    return rc;
+  for (size_t i = 0; i < plan.lines.size(); i++) {
+    OffaxisSteps steps;
+    steps.n = (int)plan.lines[i].pattern.size();
+    for (int k = 0; k < steps.n; k++)
+      steps.s[k] = (signed char)plan.lines[i].pattern[k];
+    rc = GC_DISPATCH(h, launch_offaxis_line, h->g, h->cur, steps, h->aux, h->stream);
+    if (!rc)
+      rc = GC_DISPATCH(h, launch_offaxis_loops, h->g, h->cur, h->aux, plan.lines[i].disp, tmin,
+                       tmax, adjoint, h->partials, h->dev_out + i * nt, h->stream);
+    if (rc)
+      return launch_fail(h, rc);
+  }
+  std::vector<double> vals(plan.lines.size() * (size_t)nt);
+  cudaError_t e = cudaMemcpyAsync(vals.data(), h->dev_out, vals.size() * sizeof(double),
+                                  cudaMemcpyDeviceToHost, h->stream);
+  if (e == cudaSuccess)
+    e = cudaStreamSynchronize(h->stream);
+  if (e != cudaSuccess)
+    return cuda_fail(h, "off-axis results", e);
+  for (const auto &grp : plan.groups)
+    for (int T = tmin; T <= tmax; T++) {
+      double sum = 0.0;
+      for (int li : grp.lines)
+        sum += vals[(size_t)li * nt + (T - tmin)];
+      gc_wilson_result r;
+      r.statistics_size = (int)grp.lines.size();
+      r.wilson_loop = sum / r.statistics_size;
+      r.time_size = T;
+      r.space_size = grp.length * grp.multiplier;
+      res.push_back(r);
+    }
+  return GC_OK;
+}
+
+static int offaxis_out(gc_lattice *h, const std::vector<gc_wilson_result> &res,
+                       gc_wilson_result *out, int capacity, int *count) {
+  *count = (int)res.size();
+  if ((int)res.size() > capacity)
+    return fail(h, GC_ERR_ARG, "output capacity too small (*count holds the size needed)");
+  if (!res.empty())
+    std::memcpy(out, res.data(), res.size() * sizeof(gc_wilson_result));
+  return GC_OK;
+}
+
+int gc_wilson_offaxis(gc_lattice *h, const int *directions, int ndirections, double r_min,
+                      double r_max, int time_min, int time_max, int adjoint,
+                      gc_wilson_result *out, int capacity, int *count) {
+  if (!count || (capacity > 0 && !out) || ndirections < 0 || (ndirections > 0 && !directions))
+    return fail(h, GC_ERR_ARG, "null or negative argument");
+  std::vector<std::array<int, 3>> dirs(ndirections);
+  for (int i = 0; i < ndirections; i++)
+    dirs[i] = {directions[3 * i], directions[3 * i + 1], directions[3 * i + 2]};
+  std::vector<gc_wilson_result> res;
+  int rc = offaxis_impl(h, dirs, r_min, r_max, time_min, time_max, adjoint != 0, res);
+  if (rc)
+    return rc;
+  return offaxis_out(h, res, out, capacity, count);
+}
+
+int gc_wilson_offaxis_result(gc_lattice *h, double r_min, double r_max, int time_min,
+                             int time_max, int adjoint, gc_wilson_result *out, int capacity,
+                             int *count) {
+  if (!count || (capacity > 0 && !out))
+    return fail(h, GC_ERR_ARG, "null argument");
+  std::vector<gc_wilson_result> res;
+  int rc = offaxis_impl(h, offaxis_directions(4), r_min - 0.1, r_max + 0.1, time_min, time_max,
+                        adjoint != 0, res);
+  if (rc)
+    return rc;
+  offaxis_reduce(res);
+  return offaxis_out(h, res, out, capacity, count);
 }
 
 // Offsets (Dx, Dy, Dz) that polyakov_loop_correlator_{singlet,color_average}

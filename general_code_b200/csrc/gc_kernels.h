@@ -4,6 +4,9 @@
 #include "../../include/gc_lattice.h"
 #include "gc_internal.cuh"
 
+#include <array>
+#include <vector>
+
 namespace gc {
 
 struct HypL1 {
@@ -150,6 +153,50 @@ int plaquette_partials_count(const Geom &g);
 // out_dev[0] = scale * (fixed-order sum of partials[0..n)).
 int launch_reduce_sum(const double *partials, int n, double scale, double *out_dev,
                       cudaStream_t s);
+
+// out_dev[e] = scale * (fixed-order sum over blocks b of partials[b * n + e]),
+// e < n.
+int launch_reduce_rows(const double *partials, int blocks, int n, double scale,
+                       double *out_dev, cudaStream_t s);
+
+// ------------------------------------------------------------ off-axis loops
+constexpr int kOffaxisMaxSteps = 256;
+// A space line's links, in order: +a steps forward along axis a-1 (1..3), -a
+// steps back and takes the link's adjoint.
+struct OffaxisSteps {
+  signed char s[kOffaxisMaxSteps];
+  int n;
+};
+struct OffaxisLine {
+  std::vector<int> pattern;
+  int disp[3];
+};
+// The lines of one (direction, length multiplier), in the order whose
+// values are averaged.
+struct OffaxisGroup {
+  double length; // |direction|
+  int multiplier;
+  std::vector<int> lines;
+};
+struct OffaxisPlan {
+  std::vector<OffaxisLine> lines;
+  std::vector<OffaxisGroup> groups; // output order
+};
+std::vector<std::array<int, 3>> offaxis_directions(int length_max);
+OffaxisPlan offaxis_plan(const std::vector<std::array<int, 3>> &directions, double r_min,
+                         double r_max);
+void offaxis_reduce(std::vector<gc_wilson_result> &results);
+int offaxis_partials_count(const Geom &g, int nt);
+// The space line of `steps` from every site into S (V matrices in the
+// decorated-link storage of Store).
+template <class Store, class CT>
+int launch_offaxis_line(const Geom &g, const Fields4 &U, const OffaxisSteps &steps, void *S,
+                        cudaStream_t s);
+// out_dev[T - tmin] = the loop average for the line S with displacement disp.
+template <class Store, class CT>
+int launch_offaxis_loops(const Geom &g, const Fields4 &U, const void *S, const int disp[3],
+                         int tmin, int tmax, bool adjoint, double *partials, double *out_dev,
+                         cudaStream_t s);
 
 // Polyakov lines P(s) of every spatial site into `lines` (FP64 element
 // planes: 9 (SU(3)) or 2 (SU(2)) double2 planes of Vs entries), block sums of

@@ -696,6 +696,12 @@ int launch_reduce_sum(const double *partials, int n, double scale, double *out_d
   return launch_check("reduce_partials_kernel");
 }
 
+int launch_reduce_rows(const double *partials, int blocks, int n, double scale,
+                       double *out_dev, cudaStream_t s) {
+  reduce_partials_kernel<<<n, 256, 0, s>>>(partials, blocks, n, 1, n, scale, out_dev);
+  return launch_check("reduce_partials_kernel");
+}
+
 int launch_reduce_batch(const RJob *jobs, int njobs, int entries, cudaStream_t s) {
   if (njobs <= 0 || entries <= 0)
     return GC_OK;

@@ -22,7 +22,7 @@ import numpy as np
 
 from . import _lib
 from ._lib import (GC_ERR_ARG, GC_LAYOUT_EIGEN_COLMAJOR, GC_LAYOUT_ROWMAJOR, GC_PREC_FP64,
-                   GC_PREC_MIXED, GCError, check, dbl_ptr, dims_arg, lib)
+                   GC_PREC_MIXED, GCError, WilsonResult, check, dbl_ptr, dims_arg, lib)
 
 _PREC = {"fp64": GC_PREC_FP64, "mixed": GC_PREC_MIXED}
 _LAYOUT = {"rowmajor": GC_LAYOUT_ROWMAJOR, "eigen": GC_LAYOUT_EIGEN_COLMAJOR}
@@ -194,6 +194,40 @@ class Lattice:
                        dbl_ptr(out)))
         return out
 
+    def _offaxis(self, fn, *args):
+        count = ctypes.c_int(0)
+        cap = 4096
+        while True:
+            out = (WilsonResult * cap)()
+            rc = fn(self._h, *args, ctypes.cast(out, ctypes.c_void_p), cap, ctypes.byref(count))
+            if rc == GC_ERR_ARG and count.value > cap:
+                cap = count.value
+                continue
+            self._check(rc)
+            return [(r.wilson_loop, r.time_size, r.space_size, r.statistics_size)
+                    for r in out[:count.value]]
+
+    def wilson_offaxis(self, directions, r_min: float, r_max: float, time_min: int,
+                       time_max: int, adjoint: bool = False):
+        """Off-axis loops for the given directions (wilson_offaxis[_adjoint],
+        wilson_loops.h:313-645): [(W, T, size, orientations)] in the
+        reference's order, one per (direction, length multiple, T)."""
+        d = np.ascontiguousarray(directions, dtype=np.int32).reshape(-1, 3)
+        return self._offaxis(lib().gc_wilson_offaxis, d.ctypes.data_as(ctypes.POINTER(ctypes.c_int)),
+                             int(d.shape[0]), float(r_min), float(r_max), int(time_min),
+                             int(time_max), 1 if adjoint else 0)
+
+    def wilson_offaxis_result(self, r_min: float, r_max: float, time_min: int,
+                              time_max: int, adjoint: bool = False) -> Dict[Tuple[int, float], float]:
+        """Merged off-axis loops {(T, size): W} (wilson_offaxis[_adjoint]_result,
+        wilson_loops.h:470-485, 648-663)."""
+        entries = self._offaxis(lib().gc_wilson_offaxis_result, float(r_min), float(r_max),
+                                int(time_min), int(time_max), 1 if adjoint else 0)
+        out: Dict[Tuple[int, float], float] = {}
+        for w, t, size, _ in entries:
+            out[(t, size)] = w
+        return out
+
     def polyakov_loop(self) -> float:
         """Mean of Re Tr P / N over spatial sites (polyakov_loops.h:24-41)."""
         out = ctypes.c_double()
@@ -314,6 +348,45 @@ def wilson_loop_adjoint(conf: LatticeData, r_min: int, r_max: int, time_min: int
         w = lat.wilson_loop_adjoint(r_min, r_max, time_min, time_max)
     return {(t, r): float(w[t - time_min, r - r_min])
             for t in range(time_min, time_max + 1) for r in range(r_min, r_max + 1)}
+
+
+def _wilson_result_list(entries):
+    return [{"wilson_loop": w, "time_size": t, "space_size": size, "statistics_size": n}
+            for w, t, size, n in entries]
+
+
+def wilson_offaxis(conf: LatticeData, directions, r_min: float, r_max: float, time_min: int,
+                   time_max: int):
+    """Off-axis loops (wilson_loops.h:313-467) as a list of wilson_result dicts."""
+    with Lattice(conf.lat_dim, conf.nc) as lat:
+        lat.upload(conf.array)
+        return _wilson_result_list(lat.wilson_offaxis(directions, r_min, r_max, time_min,
+                                                      time_max))
+
+
+def wilson_offaxis_adjoint(conf: LatticeData, directions, r_min: float, r_max: float,
+                           time_min: int, time_max: int):
+    """Adjoint off-axis loops (wilson_loops.h:487-645)."""
+    with Lattice(conf.lat_dim, conf.nc) as lat:
+        lat.upload(conf.array)
+        return _wilson_result_list(lat.wilson_offaxis(directions, r_min, r_max, time_min,
+                                                      time_max, adjoint=True))
+
+
+def wilson_offaxis_result(conf: LatticeData, r_min: float, r_max: float, time_min: int,
+                          time_max: int) -> Dict[Tuple[int, float], float]:
+    """Merged off-axis loops keyed (T, size) (wilson_loops.h:470-485)."""
+    with Lattice(conf.lat_dim, conf.nc) as lat:
+        lat.upload(conf.array)
+        return lat.wilson_offaxis_result(r_min, r_max, time_min, time_max)
+
+
+def wilson_offaxis_adjoint_result(conf: LatticeData, r_min: float, r_max: float, time_min: int,
+                                  time_max: int) -> Dict[Tuple[int, float], float]:
+    """Merged adjoint off-axis loops keyed (T, size) (wilson_loops.h:648-663)."""
+    with Lattice(conf.lat_dim, conf.nc) as lat:
+        lat.upload(conf.array)
+        return lat.wilson_offaxis_result(r_min, r_max, time_min, time_max, adjoint=True)
 
 
 def polyakov_loop(conf: LatticeData) -> float:

@@ -30,6 +30,13 @@
 //                                                         polyakov_loops.h:83-206
 //   Data::read_data_convert(LatticeData&, std::string, std::string, int,
 //       std::string, bool)                                data.h:265-338
+//   wilson_offaxis / wilson_offaxis_adjoint(const LatticeData&,
+//       std::vector<std::vector<int>>, double, double, int, int)
+//                                                         wilson_loops.h:313-317, 487-491
+//   wilson_offaxis_result / wilson_offaxis_adjoint_result(const LatticeData&,
+//       double, double, int, int)                         wilson_loops.h:470-473, 648-651
+//   wilson_offaxis_result / wilson_offaxis_adjoint_result(const std::vector<T>&,
+//       double, double, int, int)                         basic_observables.h:34-36, 45-48
 #pragma once
 
 #include "gc_lattice.h"
@@ -185,6 +192,58 @@ void read(Data::LatticeData<DataPatternLexicographical, MT> &conf, const std::st
   s.download(conf.array.data());
 }
 
+// Off-axis entries of one call (gc_wilson_offaxis[_result]) as the
+// reference's wilson_result list.
+template <class MT>
+std::vector<wilson_result> offaxis(const std::array<int, 4> &dims, const MT *links,
+                                   const std::vector<std::vector<int>> *directions,
+                                   double r_min, double r_max, int time_min, int time_max,
+                                   bool adjoint) {
+  Session<MT> s(dims, links);
+  std::vector<int> flat;
+  if (directions)
+    for (const auto &d : *directions) {
+      if (d.size() != 3)
+        throw std::runtime_error("general_code_b200 wilson_offaxis: directions need 3 ints");
+      flat.insert(flat.end(), d.begin(), d.end());
+    }
+  std::vector<gc_wilson_result> out(4096);
+  int count = 0;
+  for (int attempt = 0; attempt < 2; attempt++) {
+    const int rc =
+        directions ? gc_wilson_offaxis(s.get(), flat.data(), (int)directions->size(), r_min,
+                                       r_max, time_min, time_max, adjoint ? 1 : 0, out.data(),
+                                       (int)out.size(), &count)
+                   : gc_wilson_offaxis_result(s.get(), r_min, r_max, time_min, time_max,
+                                              adjoint ? 1 : 0, out.data(), (int)out.size(),
+                                              &count);
+    if (rc == GC_ERR_ARG && count > (int)out.size()) {
+      out.resize(count);
+      continue;
+    }
+    check(rc, s.get(), "wilson_offaxis");
+    break;
+  }
+  std::vector<wilson_result> res(count);
+  for (int i = 0; i < count; i++) {
+    res[i].wilson_loop = out[i].wilson_loop;
+    res[i].time_size = out[i].time_size;
+    res[i].space_size = out[i].space_size;
+    res[i].statistics_size = out[i].statistics_size;
+  }
+  return res;
+}
+
+// The merged entries keyed (T, size), later entries replacing earlier ones
+// (as the reference builds its map).
+inline std::map<std::tuple<int, double>, double>
+offaxis_map(const std::vector<wilson_result> &entries) {
+  std::map<std::tuple<int, double>, double> m;
+  for (const auto &e : entries)
+    m[std::tuple<int, double>(e.time_size, e.space_size)] = e.wilson_loop;
+  return m;
+}
+
 template <class MT>
 double polyakov(const Data::LatticeData<DataPatternLexicographical, MT> &conf) {
   Session<MT> s(conf.lat_dim, conf.array.data());
@@ -334,6 +393,55 @@ inline std::vector<double> polyakov_loop_correlator_color_average(
     const Data::LatticeData<DataPatternLexicographical, su3> &conf, int D_max) {
   return gc_dropin::polyakov_correlator(conf, D_max, GC_POLYAKOV_COLOR_AVERAGE);
 }
+// Off-axis loops (wilson_loops.h:313-663), and the legacy vector form of the
+// merged results that apps/observables/wilson_loops/wilson_loops.cpp:135-140
+// calls (basic_observables.h:34-36, 45-48; lattice size from the globals
+// x_size, y_size, z_size, t_size, which the program must set).
+#define GC_DROPIN_OFFAXIS(MT)                                                                  \
+  inline std::vector<wilson_result> wilson_offaxis(                                            \
+      const Data::LatticeData<DataPatternLexicographical, MT> &conf,                           \
+      const std::vector<std::vector<int>> directions, double r_min, double r_max,              \
+      int time_min, int time_max) {                                                            \
+    return gc_dropin::offaxis(conf.lat_dim, conf.array.data(), &directions, r_min, r_max,      \
+                              time_min, time_max, false);                                      \
+  }                                                                                            \
+  inline std::vector<wilson_result> wilson_offaxis_adjoint(                                    \
+      const Data::LatticeData<DataPatternLexicographical, MT> &conf,                           \
+      const std::vector<std::vector<int>> directions, double r_min, double r_max,              \
+      int time_min, int time_max) {                                                            \
+    return gc_dropin::offaxis(conf.lat_dim, conf.array.data(), &directions, r_min, r_max,      \
+                              time_min, time_max, true);                                       \
+  }                                                                                            \
+  inline std::map<std::tuple<int, double>, double> wilson_offaxis_result(                      \
+      const Data::LatticeData<DataPatternLexicographical, MT> &conf, double r_min,             \
+      double r_max, int time_min, int time_max) {                                              \
+    return gc_dropin::offaxis_map(gc_dropin::offaxis(conf.lat_dim, conf.array.data(),          \
+                                                     nullptr, r_min, r_max, time_min,          \
+                                                     time_max, false));                        \
+  }                                                                                            \
+  inline std::map<std::tuple<int, double>, double> wilson_offaxis_adjoint_result(              \
+      const Data::LatticeData<DataPatternLexicographical, MT> &conf, double r_min,             \
+      double r_max, int time_min, int time_max) {                                              \
+    return gc_dropin::offaxis_map(gc_dropin::offaxis(conf.lat_dim, conf.array.data(),          \
+                                                     nullptr, r_min, r_max, time_min,          \
+                                                     time_max, true));                         \
+  }                                                                                            \
+  inline std::map<std::tuple<int, double>, double> wilson_offaxis_result(                      \
+      const std::vector<MT> &array, double r_min, double r_max, int time_min, int time_max) {  \
+    return gc_dropin::offaxis_map(gc_dropin::offaxis(                                          \
+        std::array<int, 4>{x_size, y_size, z_size, t_size}, array.data(), nullptr, r_min,      \
+        r_max, time_min, time_max, false));                                                    \
+  }                                                                                            \
+  inline std::map<std::tuple<int, double>, double> wilson_offaxis_adjoint_result(              \
+      const std::vector<MT> &array, double r_min, double r_max, int time_min, int time_max) {  \
+    return gc_dropin::offaxis_map(gc_dropin::offaxis(                                          \
+        std::array<int, 4>{x_size, y_size, z_size, t_size}, array.data(), nullptr, r_min,      \
+        r_max, time_min, time_max, true));                                                     \
+  }
+GC_DROPIN_OFFAXIS(su2)
+GC_DROPIN_OFFAXIS(su3)
+#undef GC_DROPIN_OFFAXIS
+
 // Configuration reader (data.h:265-338), as apps/smearing/smearing.cpp:188
 // calls it (qualified, Data::read_data_convert).
 namespace Data {

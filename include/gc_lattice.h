@@ -175,6 +175,39 @@ int gc_wilson_onaxis_noalloc(const int dims[4], int nc, int precision,
  * Replaces: plaket(conf) (plaket.h:83-101). */
 int gc_plaquette(gc_lattice *h, double *out);
 
+/* One off-axis Wilson-loop entry (the reference's wilson_result,
+ * basic_observables.h:18-23). */
+typedef struct {
+  double wilson_loop;  /* average over the orientations of the entry */
+  int time_size;       /* T */
+  double space_size;   /* |direction| * multiplier */
+  int statistics_size; /* orientations averaged */
+} gc_wilson_result;
+
+/* Off-axis Wilson loops for the given spatial directions (ndirections x 3
+ * ints, each a1 >= a2 >= a3 >= 0, a1 > 0): every permuted and reflected
+ * orientation of each direction's staircase, lengths |d| m in
+ * [r_min, r_max] (m rounded inwards), T in [time_min, time_max]; one entry per
+ * (direction, m, T) in the reference's order. adjoint != 0: |Tr W|^2 - 1 per
+ * loop. out has room for capacity entries; *count receives the number of
+ * entries (GC_ERR_ARG, with *count set, when capacity is too small). A line
+ * may have at most 256 links.
+ * Replaces: wilson_offaxis / wilson_offaxis_adjoint (wilson_loops.h:313-467,
+ * 487-645). */
+int gc_wilson_offaxis(gc_lattice *h, const int *directions, int ndirections, double r_min,
+                      double r_max, int time_min, int time_max, int adjoint,
+                      gc_wilson_result *out, int capacity, int *count);
+
+/* gc_wilson_offaxis over the directions of length up to 4 with the range
+ * widened by 0.1 on each side, then entries of equal (T, size) merged as
+ * the reference's wilson_offaxis_reduce does; a caller keys the entries by
+ * (time_size, space_size) in order, later entries replacing earlier ones.
+ * Replaces: wilson_offaxis_result / wilson_offaxis_adjoint_result
+ * (wilson_loops.h:470-485, 648-663; reduce basic_observables.cpp:167-186). */
+int gc_wilson_offaxis_result(gc_lattice *h, double r_min, double r_max, int time_min,
+                             int time_max, int adjoint, gc_wilson_result *out, int capacity,
+                             int *count);
+
 /* Average of the three spatial plaquettes per site.
  * Replaces: plaket_space(conf) (plaket.h:123-141, sites :63-81). */
 int gc_plaquette_space(gc_lattice *h, double *out);

@@ -4,7 +4,9 @@
 // HYP, APE, wilson_loop), and the observables of
 // apps/smearing/smearing_wilson_gevp.cpp (wilson_loop_adjoint,
 // wilson_gevp_indexed, wilson_gevp_adjoint_indexed of the HYP and HYP+APE
-// configurations) and plaket_time / plaket_space, twice on the same seeded
+// configurations), plaket_time / plaket_space, the reader, and the merged
+// off-axis loops of apps/observables/wilson_loops (wilson_offaxis_result and,
+// for su3, wilson_offaxis_adjoint_result), twice on the same seeded
 // configuration:
 //   - with unqualified calls, exactly as the app writes them, which overload
 //     resolution binds to the drop-in (GPU) functions;
@@ -109,6 +111,7 @@ int run(const std::array<int, 4> &dims, int ape_steps, int rmax, int tmax) {
   }
   double pa, pb, pta, ptb, psa, psb, la, lb;
   std::map<std::tuple<int, int>, double> wa, wb, aa, ab, ga, gb, gaa, gab;
+  std::map<std::tuple<int, double>, double> oa, ob, ooa, oob;
   std::vector<double> csa, csb, cca, ccb;
   const int D = 2;
   Data::LatticeData<DP, MT> ha(dims), hb(dims); // configurations after HYP
@@ -125,6 +128,9 @@ int run(const std::array<int, 4> &dims, int ape_steps, int rmax, int tmax) {
     aa = wilson_loop_adjoint(a, 1, rmax, 1, tmax);
     ga = wilson_gevp_indexed(a, ha, 1, rmax, 1, tmax);
     gaa = wilson_gevp_adjoint_indexed(a, ha, 1, rmax, 1, tmax);
+    oa = wilson_offaxis_result(a, 1, rmax, 1, tmax);
+    if (ds == 18)
+      ooa = wilson_offaxis_adjoint_result(a, 1, rmax, 1, tmax);
     pta = plaket_time(a);
     psa = plaket_space(a);
   } catch (const std::exception &e) {
@@ -172,6 +178,9 @@ int run(const std::array<int, 4> &dims, int ape_steps, int rmax, int tmax) {
   ab = ::wilson_loop_adjoint<DP, MT>(b, 1, rmax, 1, tmax);
   gb = ::wilson_gevp_indexed<DP, MT>(b, hb, 1, rmax, 1, tmax);
   gab = ::wilson_gevp_adjoint_indexed<DP, MT>(b, hb, 1, rmax, 1, tmax);
+  ob = ::wilson_offaxis_result<DP, MT>(b, 1, rmax, 1, tmax);
+  if (ds == 18)
+    oob = ::wilson_offaxis_adjoint_result<DP, MT>(b, 1, rmax, 1, tmax);
   ptb = ref_plaquette(b, 1);
   psb = ref_plaquette(b, 2);
   double dl = 0;
@@ -188,11 +197,26 @@ int run(const std::array<int, 4> &dims, int ape_steps, int rmax, int tmax) {
   dw = std::fmax(dw, max_rel(aa, ab, &ok));
   const double dg = std::fmax(max_rel(ga, gb, &ok), max_rel(gaa, gab, &ok));
   const double dc = std::fmax(max_abs_vec(csa, csb, &ok), max_abs_vec(cca, ccb, &ok));
+  double doff = 0;
+  for (const auto *pr : {&oa, &ooa}) {
+    const auto &got = *pr, &want = (pr == &oa) ? ob : oob;
+    ok = ok && got.size() == want.size();
+    for (auto &kv : want) {
+      auto it = got.find(kv.first);
+      if (it == got.end()) {
+        ok = false;
+        continue;
+      }
+      const double e = std::fabs(it->second - kv.second);
+      doff = std::fmax(doff, e / (std::fabs(kv.second) + 1e-300));
+      ok = ok && e <= 1e-12 * std::fabs(kv.second) + 1e-14;
+    }
+  }
   std::printf("links max|diff| %.3e  plaquette diff %.3e (time %.3e space %.3e)  W max rel "
               "diff %.3e  GEVP %.3e  Polyakov %.3e, correlators %.3e  reader %.3e  "
-              "entries %zu  %s\n",
+              "off-axis %.3e (%zu entries)  entries %zu  %s\n",
               dl, std::fabs(pa - pb), std::fabs(pta - ptb), std::fabs(psa - psb), dw, dg,
-              std::fabs(la - lb), dc, dread, wb.size(), ok ? "OK" : "MISMATCH");
+              std::fabs(la - lb), dc, dread, doff, ob.size(), wb.size(), ok ? "OK" : "MISMATCH");
   return ok ? 0 : 1;
 }
 

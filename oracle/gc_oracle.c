@@ -540,6 +540,268 @@ int or_wilson_gevp(int nc, const int dims[4], const double *links1, const double
   return wilson_impl(nc, dims, links1, links2, rmin, rmax, tmin, tmax, out, adjoint);
 }
 
+/* ------------------------------------------------------------ off-axis loops */
+/* wilson_offaxis (wilson_loops.h:313-467) and the _adjoint / _result forms
+ * (:470-485, 487-663) with the helpers of basic_observables.cpp:167-186,
+ * 543-623, 754-840, restated for host arrays. */
+
+/* generate_directions: a1 >= a2 >= a3, one per slope; returns the count. */
+static int offaxis_dirs(int lmax, int (*dirs)[3], int cap) {
+  int n = 0;
+  for (int a1 = 1; a1 <= lmax; a1++)
+    for (int a2 = 0; a2 <= lmax; a2++)
+      for (int a3 = 0; a3 <= lmax; a3++) {
+        if (!(a1 >= a2 && a2 >= a3))
+          continue;
+        int fresh = 1;
+        for (int i = 0; i < n; i++)
+          if (dirs[i][0] * a2 == dirs[i][1] * a1 && dirs[i][0] * a3 == dirs[i][2] * a1)
+            fresh = 0;
+        if (fresh && n < cap) {
+          dirs[n][0] = a1;
+          dirs[n][1] = a2;
+          dirs[n][2] = a3;
+          n++;
+        }
+      }
+  return n;
+}
+
+/* make_offaxis_pattern (Bresenham): returns the pattern length. */
+static int offaxis_pattern(const int d[3], int *p) {
+  int n = 0, e1 = -d[1], e2 = -d[2];
+  for (int i = 0; i < d[0]; i++) {
+    e1 += 2 * d[1];
+    e2 += 2 * d[2];
+    if (e1 >= d[0]) {
+      p[n++] = 2;
+      e1 -= 2 * d[0];
+    }
+    if (e2 >= d[0]) {
+      p[n++] = 3;
+      e2 -= 2 * d[0];
+    }
+    p[n++] = 1;
+  }
+  return n;
+}
+
+static int nzeros(const int d[3]) { return (d[0] == 0) + (d[1] == 0) + (d[2] == 0); }
+
+/* generate_permutations */
+static int offaxis_perms(const int d[3], int (*perm)[3]) {
+  if (nzeros(d) == 2) {
+    const int q[3][3] = {{1, 2, 3}, {2, 1, 3}, {3, 1, 2}};
+    memcpy(perm, q, sizeof q);
+    return 3;
+  }
+  int n = 0;
+  for (int p1 = 1; p1 <= 3; p1++)
+    for (int p2 = 1; p2 <= 3; p2++)
+      for (int p3 = 1; p3 <= 3; p3++)
+        if (p1 != p2 && p2 != p3 && p3 != p1) {
+          perm[n][0] = p1;
+          perm[n][1] = p2;
+          perm[n][2] = p3;
+          n++;
+        }
+  return n;
+}
+
+/* generate_reflections */
+static int offaxis_refls(const int d[3], int (*refl)[3]) {
+  const int z = nzeros(d);
+  if (z == 0) {
+    /* the four sign choices of axes 2, 3, then the identity again (the
+     * reference's else branch of its one-zero test also runs here) */
+    int n = 0;
+    for (int r1 = 0; r1 < 2; r1++)
+      for (int r2 = 0; r2 < 2; r2++) {
+        refl[n][0] = 1;
+        refl[n][1] = r1 ? -1 : 1;
+        refl[n][2] = r2 ? -1 : 1;
+        n++;
+      }
+    refl[n][0] = refl[n][1] = refl[n][2] = 1;
+    return n + 1;
+  }
+  if (z == 1) {
+    int k = 0;
+    while (d[k] == 0)
+      k++;
+    for (int r1 = 0; r1 < 2; r1++) {
+      refl[r1][0] = refl[r1][1] = refl[r1][2] = 1;
+      refl[r1][k] = r1 ? -1 : 1;
+    }
+    return 2;
+  }
+  refl[0][0] = refl[0][1] = refl[0][2] = 1;
+  return 1;
+}
+
+/* wilson_lines_offaxis: product of the pattern's links from every site
+ * (starting from the identity, as wilson_line_offaxis does) */
+static void offaxis_lines(const group_t *G, const geom_t *g, const double *links,
+                          const int *pat, int n, double *S) {
+  const int ds = G->ds;
+#pragma omp parallel for
+  for (long long x = 0; x < g->V; x++) {
+    double A[18];
+    memset(A, 0, sizeof A);
+    if (ds == 4)
+      A[0] = 1;
+    else
+      A[0] = A[8] = A[16] = 1;
+    long long cur = x;
+    for (int i = 0; i < n; i++) {
+      const int mu = abs(pat[i]) - 1;
+      if (pat[i] > 0) {
+        G->mul(A, A, links + (4 * cur + mu) * ds);
+        cur = shift(g, cur, mu, 1);
+      } else {
+        cur = shift(g, cur, mu, -1);
+        G->mul_ad(A, A, links + (4 * cur + mu) * ds);
+      }
+    }
+    memcpy(S + x * ds, A, ds * sizeof(double));
+  }
+}
+
+/* calculate_wilson_loop_offaxis[_adjoint]: mean over x of the loop
+ * L(x,T) S(x+T) L(x+D,T)^dag S(x)^dag (tr_real or tr_adjoint). */
+static double offaxis_loop(int nc, const group_t *G, const geom_t *g, const double *L,
+                           int T, const double *S, const int D[3], int adjoint) {
+  const int ds = G->ds;
+  double result = 0;
+#pragma omp parallel for reduction(+ : result)
+  for (long long x = 0; x < g->V; x++) {
+    long long xT = shift(g, x, 3, T), xD = x;
+    for (int i = 0; i < 3; i++)
+      xD = shift(g, xD, i, D[i]);
+    double w[18];
+    G->mul(w, L + x * ds, S + xT * ds);
+    G->mul_ad(w, w, L + xD * ds);
+    G->mul_ad(w, w, S + x * ds);
+    if (nc == 3) {
+      if (adjoint) {
+        double tr = RE(w, 0, 0) + RE(w, 1, 1) + RE(w, 2, 2);
+        double ti = IM(w, 0, 0) + IM(w, 1, 1) + IM(w, 2, 2);
+        result += tr * tr + ti * ti - 1;
+      } else {
+        result += su3_tr_real(w);
+      }
+    } else {
+      result += adjoint ? 4 * w[0] * w[0] - 1 : w[0];
+    }
+  }
+  return result / g->V;
+}
+
+/* One entry per (direction, multiplier, T); returns the count (or -1). */
+static int offaxis_raw(int nc, const int dims[4], const double *links, const int (*dirs)[3],
+                       int ndirs, double rmin, double rmax, int tmin, int tmax, int adjoint,
+                       or_wilson_result *out, int cap) {
+  const group_t *G = group_of(nc);
+  if (!G || tmin < 1 || tmax < tmin)
+    return -1;
+  geom_t g;
+  geom_init(&g, dims);
+  const int ds = G->ds, nt = tmax - tmin + 1;
+  double **tl = (double **)malloc(nt * sizeof(double *));
+  for (int t = tmin; t <= tmax; t++)
+    tl[t - tmin] = lines_indexed(G, &g, links, t, 3);
+  double *S = (double *)malloc((size_t)g.V * ds * sizeof(double));
+  int count = 0;
+  for (int di = 0; di < ndirs; di++) {
+    const int *d = dirs[di];
+    const double len0 = sqrt((double)(d[0] * d[0] + d[1] * d[1] + d[2] * d[2]));
+    int base[64], perm[6][3], refl[5][3];
+    const int nb = offaxis_pattern(d, base);
+    const int np = offaxis_perms(d, perm), nrf = offaxis_refls(d, refl);
+    const int mlo = (int)round(rmin / len0 + 0.5), mhi = (int)round(rmax / len0 - 0.5);
+    const int nm = mhi - mlo + 1;
+    if (nm <= 0)
+      continue;
+    /* sums[m][T] over the orientations, in the reference's order */
+    double *sums = (double *)calloc((size_t)nm * nt, sizeof(double));
+    int stats = 0;
+    for (int p = 0; p < np; p++) {
+      int pp[64], dp[3];
+      for (int i = 0; i < nb; i++)
+        pp[i] = perm[p][base[i] - 1];
+      for (int k = 0; k < 3; k++)
+        dp[perm[p][k] - 1] = d[k];
+      for (int r = 0; r < nrf; r++) {
+        int pr[64], dr[3];
+        for (int i = 0; i < nb; i++)
+          pr[i] = pp[i] * refl[r][pp[i] - 1];
+        for (int k = 0; k < 3; k++)
+          dr[k] = dp[k] * refl[r][k];
+        stats++;
+        for (int m = mlo; m <= mhi; m++) {
+          int *pat = (int *)malloc((size_t)nb * m * sizeof(int)), D[3];
+          for (int rep = 0; rep < m; rep++)
+            memcpy(pat + rep * nb, pr, nb * sizeof(int));
+          for (int k = 0; k < 3; k++)
+            D[k] = dr[k] * m;
+          offaxis_lines(G, &g, links, pat, nb * m, S);
+          free(pat);
+          for (int t = tmin; t <= tmax; t++)
+            sums[(m - mlo) * nt + (t - tmin)] +=
+                offaxis_loop(nc, G, &g, tl[t - tmin], t, S, D, adjoint);
+        }
+      }
+    }
+    for (int m = mlo; m <= mhi; m++)
+      for (int t = tmin; t <= tmax; t++) {
+        if (count < cap) {
+          out[count].wilson_loop = sums[(m - mlo) * nt + (t - tmin)] / stats;
+          out[count].time_size = t;
+          out[count].space_size = len0 * m;
+          out[count].statistics_size = stats;
+        }
+        count++;
+      }
+    free(sums);
+  }
+  free(S);
+  for (int i = 0; i < nt; i++)
+    free(tl[i]);
+  free(tl);
+  return count;
+}
+
+int or_wilson_offaxis(int nc, const int dims[4], const double *links, const int *directions,
+                      int ndirections, double r_min, double r_max, int time_min, int time_max,
+                      int adjoint, or_wilson_result *out, int capacity) {
+  return offaxis_raw(nc, dims, links, (const int(*)[3])directions, ndirections, r_min, r_max,
+                     time_min, time_max, adjoint, out, capacity);
+}
+
+/* wilson_offaxis_result: length-4 directions, range widened by 0.1, then
+ * wilson_offaxis_reduce (step for step, basic_observables.cpp:167-186). */
+int or_wilson_offaxis_result(int nc, const int dims[4], const double *links, double r_min,
+                             double r_max, int time_min, int time_max, int adjoint,
+                             or_wilson_result *out, int capacity) {
+  int dirs[128][3];
+  const int nd = offaxis_dirs(4, dirs, 128);
+  int n = offaxis_raw(nc, dims, links, (const int(*)[3])dirs, nd, r_min - 0.1, r_max + 0.1,
+                      time_min, time_max, adjoint, out, capacity);
+  if (n < 0 || n > capacity)
+    return n;
+  for (int i = 0; i < n; i++)
+    for (int j = 0; j < n; j++)
+      if (out[i].space_size == out[j].space_size && out[i].time_size == out[j].time_size &&
+          i != j) {
+        out[i].wilson_loop = (out[i].wilson_loop * out[i].statistics_size +
+                              out[j].wilson_loop * out[j].statistics_size) /
+                             (out[i].statistics_size + out[j].statistics_size);
+        memmove(out + j, out + j + 1, (size_t)(n - j - 1) * sizeof(or_wilson_result));
+        n--;
+      }
+  return n;
+}
+
 /* ------------------------------------------------------------ plaquette */
 /* which = 0: all six planes / 6 (plaket_site, plaket.h:24-42);
  * 1: (mu, t) planes / 3 (plaket_site_time, :44-61);

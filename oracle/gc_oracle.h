@@ -29,6 +29,20 @@ int or_wilson_adjoint(int nc, const int dims[4], const double *links, int r_min,
 int or_wilson_gevp(int nc, const int dims[4], const double *links1, const double *links2,
                    int r_min, int r_max, int time_min, int time_max, int adjoint,
                    double *out);
+/* Off-axis Wilson loops; entries as the reference's wilson_result. Return
+ * the entry count (entries past capacity are not written) or -1. */
+typedef struct {
+  double wilson_loop;
+  int time_size;
+  double space_size;
+  int statistics_size;
+} or_wilson_result;
+int or_wilson_offaxis(int nc, const int dims[4], const double *links, const int *directions,
+                      int ndirections, double r_min, double r_max, int time_min, int time_max,
+                      int adjoint, or_wilson_result *out, int capacity);
+int or_wilson_offaxis_result(int nc, const int dims[4], const double *links, double r_min,
+                             double r_max, int time_min, int time_max, int adjoint,
+                             or_wilson_result *out, int capacity);
 double or_plaquette(int nc, const int dims[4], const double *links);
 double or_plaquette_time(int nc, const int dims[4], const double *links);
 double or_plaquette_space(int nc, const int dims[4], const double *links);

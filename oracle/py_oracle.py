@@ -106,6 +106,20 @@ class _Checker:
         return out
 
 
+class WilsonResult(ctypes.Structure):
+    """or_wilson_result / gc_wilson_result."""
+    _fields_ = [("wilson_loop", ctypes.c_double), ("time_size", ctypes.c_int),
+                ("space_size", ctypes.c_double), ("statistics_size", ctypes.c_int)]
+
+
+def _as_dict(entries):
+    """{(T, size): W} built in order, later entries replacing earlier ones."""
+    out = {}
+    for w, t, size, _ in entries:
+        out[(t, size)] = w
+    return out
+
+
 class Port(_Checker):
     prefix = "or_"
 
@@ -121,6 +135,34 @@ class Port(_Checker):
 
     def set_threads(self, n):
         self.lib.or_set_threads(int(n))
+
+    def wilson_offaxis(self, nc, dims, links, directions, rmin, rmax, tmin, tmax,
+                       adjoint=False, capacity=20000):
+        """Unmerged off-axis entries [(W, T, size, statistics)] in order."""
+        d = np.ascontiguousarray(directions, dtype=np.int32).reshape(-1, 3)
+        fn = self.lib.or_wilson_offaxis
+        fn.restype = _c_int
+        fn.argtypes = [_c_int, _pint, _pdbl, _pint, _c_int, _c_dbl, _c_dbl, _c_int, _c_int,
+                       _c_int, ctypes.POINTER(WilsonResult), _c_int]
+        out = (WilsonResult * capacity)()
+        n = fn(nc, _dims(dims), _ptr(links), d.ctypes.data_as(_pint), d.shape[0], rmin, rmax,
+               tmin, tmax, int(adjoint), out, capacity)
+        assert 0 <= n <= capacity
+        return [(r.wilson_loop, r.time_size, r.space_size, r.statistics_size) for r in out[:n]]
+
+    def wilson_offaxis_result(self, nc, dims, links, rmin, rmax, tmin, tmax, adjoint=False,
+                              capacity=20000):
+        """Merged off-axis loops {(T, size): W} (wilson_offaxis_result)."""
+        fn = self.lib.or_wilson_offaxis_result
+        fn.restype = _c_int
+        fn.argtypes = [_c_int, _pint, _pdbl, _c_dbl, _c_dbl, _c_int, _c_int, _c_int,
+                       ctypes.POINTER(WilsonResult), _c_int]
+        out = (WilsonResult * capacity)()
+        n = fn(nc, _dims(dims), _ptr(links), rmin, rmax, tmin, tmax, int(adjoint), out,
+               capacity)
+        assert 0 <= n <= capacity
+        return _as_dict((r.wilson_loop, r.time_size, r.space_size, r.statistics_size)
+                        for r in out[:n])
 
     def plaquette_time(self, nc, dims, links):
         return float(self.lib.or_plaquette_time(nc, _dims(dims), _ptr(links)))
@@ -156,6 +198,34 @@ class Ref(_Checker):
 
     def num_threads(self):
         return int(self.lib.ref_num_threads())
+
+    def _offaxis(self, nc, dims, links, mode, directions, rmin, rmax, tmin, tmax, adjoint,
+                 capacity=20000):
+        fn = self.lib.ref_wilson_offaxis
+        fn.restype = _c_int
+        fn.argtypes = [_c_int, _pint, _pdbl, _c_int, _pint, _c_int, _c_dbl, _c_dbl, _c_int,
+                       _c_int, _c_int, _pdbl, _pint, _pdbl, _pint, _c_int]
+        d = np.ascontiguousarray(directions if directions is not None else np.zeros((0, 3)),
+                                 dtype=np.int32).reshape(-1, 3)
+        w = np.zeros(capacity)
+        t = np.zeros(capacity, dtype=np.int32)
+        sz = np.zeros(capacity)
+        st = np.zeros(capacity, dtype=np.int32)
+        n = fn(nc, _dims(dims), _ptr(links), mode, d.ctypes.data_as(_pint), d.shape[0], rmin,
+               rmax, tmin, tmax, int(adjoint), _ptr(w), t.ctypes.data_as(_pint), _ptr(sz),
+               st.ctypes.data_as(_pint), capacity)
+        assert 0 <= n <= capacity
+        return [(float(w[i]), int(t[i]), float(sz[i]), int(st[i])) for i in range(n)]
+
+    def wilson_offaxis(self, nc, dims, links, directions, rmin, rmax, tmin, tmax,
+                       adjoint=False):
+        """The reference's wilson_offaxis[_adjoint]: [(W, T, size, statistics)]."""
+        return self._offaxis(nc, dims, links, 0, directions, rmin, rmax, tmin, tmax, adjoint)
+
+    def wilson_offaxis_result(self, nc, dims, links, rmin, rmax, tmin, tmax, adjoint=False):
+        """The reference's wilson_offaxis[_adjoint]_result: {(T, size): W}."""
+        return _as_dict(self._offaxis(nc, dims, links, 1, None, rmin, rmax, tmin, tmax,
+                                      adjoint))
 
     def plaquette_time(self, nc, dims, links):
         return float(self.lib.ref_plaquette_part(nc, _dims(dims), _ptr(links), 1))

@@ -14,6 +14,8 @@
 //   get_polyakov_loop, polyakov_loop_correlator_{color_average,singlet}
 //                         lib/cpu/include/polyakov_loops.h:10-22, 83-206
 //   polyakov_average_directions            lib/cpu/src/polyakov_loops.cpp:6-40
+//   wilson_offaxis[_adjoint], wilson_offaxis[_adjoint]_result
+//                         lib/cpu/include/wilson_loops.h:313-663
 //   Data::read_data_convert / write_data   lib/cpu/include/data.h:193-205,265-338
 //
 // Link exchange layout ("row-major"): link index 4*site+mu with
@@ -323,6 +325,63 @@ int ref_polyakov_average_directions(const double *table, int D, double *dist, do
     i++;
   }
   return i;
+}
+
+// Off-axis loops. mode 0: wilson_offaxis with the given directions;
+// mode 1: wilson_offaxis_result (directions of length <= 4, merged, as the
+// map it returns). adjoint selects the _adjoint forms (su3 only: the
+// reference's su2 has no tr_adjoint). Entries go to w/t/s/n (capacity cap);
+// returns the count.
+int ref_wilson_offaxis(int nc, const int *dims, const double *links, int mode,
+                       const int *directions, int ndirections, double rmin, double rmax,
+                       int tmin, int tmax, int adjoint, double *w, int *t, double *s, int *n,
+                       int cap) {
+  set_globals(dims);
+  std::vector<std::vector<int>> dirs;
+  for (int i = 0; i < ndirections; i++)
+    dirs.push_back({directions[3 * i], directions[3 * i + 1], directions[3 * i + 2]});
+  std::vector<wilson_result> raw;
+  std::map<std::tuple<int, double>, double> merged;
+  if (nc == 2 && !adjoint) {
+    Data::LatticeData<DP, su2> c = make_conf<su2>(dims, links);
+    if (mode == 0)
+      raw = wilson_offaxis(c, dirs, rmin, rmax, tmin, tmax);
+    else
+      merged = wilson_offaxis_result(c, rmin, rmax, tmin, tmax);
+  } else if (nc == 3) {
+    Data::LatticeData<DP, su3> c = make_conf<su3>(dims, links);
+    if (mode == 0)
+      raw = adjoint ? wilson_offaxis_adjoint(c, dirs, rmin, rmax, tmin, tmax)
+                    : wilson_offaxis(c, dirs, rmin, rmax, tmin, tmax);
+    else
+      merged = adjoint ? wilson_offaxis_adjoint_result(c, rmin, rmax, tmin, tmax)
+                       : wilson_offaxis_result(c, rmin, rmax, tmin, tmax);
+  } else {
+    return -1;
+  }
+  int k = 0;
+  if (mode == 0) {
+    for (const auto &r : raw) {
+      if (k < cap) {
+        w[k] = r.wilson_loop;
+        t[k] = r.time_size;
+        s[k] = r.space_size;
+        n[k] = r.statistics_size;
+      }
+      k++;
+    }
+  } else {
+    for (const auto &kv : merged) {
+      if (k < cap) {
+        w[k] = kv.second;
+        t[k] = std::get<0>(kv.first);
+        s[k] = std::get<1>(kv.first);
+        n[k] = 0;
+      }
+      k++;
+    }
+  }
+  return k;
 }
 
 double ref_plaquette(int nc, const int *dims, const double *links) {

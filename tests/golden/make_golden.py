@@ -12,7 +12,9 @@ Also from the reference, on the same links: the adjoint W table; the
 two-configuration (GEVP) tables of (HYP+APE, HYP) (wilson_gevp_indexed and
 wilson_gevp_adjoint_indexed); the time and space plaquettes after HYP+APE;
 the Polyakov loop and both correlator tables (D_max = 2) after HYP, with the
-reference's distance averages of the tables.
+reference's distance averages of the tables; the merged off-axis loops
+(wilson_offaxis_result, and wilson_offaxis_adjoint_result for SU(3)) after
+HYP+APE for R in [1, 2], T in [1, 2].
 
 Run here (needs the reference sources and oracle/_ref):
     make -C oracle ref && python tests/golden/make_golden.py
@@ -69,6 +71,9 @@ def main() -> None:
         corr_c = ref.polyakov_correlator(nc, dims, links_hyp, d_max, False)
         avg_s = ref.polyakov_average_directions(corr_s, d_max)
         avg_c = ref.polyakov_average_directions(corr_c, d_max)
+        off = ref.wilson_offaxis_result(nc, dims, links_ape, 1.0, 2.0, 1, 2)
+        off_adj = (ref.wilson_offaxis_result(nc, dims, links_ape, 1.0, 2.0, 1, 2, True)
+                   if nc == 3 else {})
         np.savez_compressed(OUT / f"{name}.npz", links0=links0, links_hyp=links_hyp,
                             links_ape=links_ape, wilson=w, wilson_adjoint=wa,
                             plaquettes=np.array([plaq0, plaq1]), gevp=gevp,
@@ -84,7 +89,10 @@ def main() -> None:
                        "plaquette_time": plaq_t, "plaquette_space": plaq_s,
                        "polyakov_loop": poly, "polyakov_d_max": d_max,
                        "polyakov_singlet_by_distance": [[k, v] for k, v in avg_s.items()],
-                       "polyakov_color_average_by_distance": [[k, v] for k, v in avg_c.items()]}
+                       "polyakov_color_average_by_distance": [[k, v] for k, v in avg_c.items()],
+                       "offaxis_range": [1.0, 2.0, 1, 2],
+                       "offaxis": [[t, size, w] for (t, size), w in off.items()],
+                       "offaxis_adjoint": [[t, size, w] for (t, size), w in off_adj.items()]}
         print(name, "plaq", plaq0, "->", plaq1, "W[0,0]", w[0, 0])
     meta = {"generated_by": "tests/golden/make_golden.py",
             "reference_code": "oracle/_ref/libref_parity.so (lib/cpu smearing_HYP, "
@@ -93,7 +101,8 @@ def main() -> None:
                               "plaket_site_time, plaket_site_space, get_polyakov_loop, "
                               "polyakov_loop_correlator_singlet, "
                               "polyakov_loop_correlator_color_average, "
-                              "polyakov_average_directions; -O2 -fno-fast-math)",
+                              "polyakov_average_directions, wilson_offaxis_result, "
+                              "wilson_offaxis_adjoint_result; -O2 -fno-fast-math)",
             "link_layout": "4*V links, link index 4*site+mu, row-major (get_data order)",
             "cases": index}
     (OUT / "index.json").write_text(json.dumps(meta, indent=1))

@@ -278,3 +278,53 @@ def test_gevp_with_itself_and_argument_errors(nc):
             a.wilson_gevp(m, 1, 2, 1, 3)  # different precision
         with pytest.raises(GCError):
             a.polyakov_correlator(-1, True)
+
+
+@pytest.mark.parametrize("name,meta", CASES, ids=[c[0] for c in CASES])
+def test_fp64_offaxis_matches_reference_fixture(name, meta):
+    """Merged off-axis loops through the C ABI against the reference's values."""
+    g = load_golden(name)
+    nc, dims = meta["nc"], meta["dims"]
+    r0, r1, t0, t1 = meta["offaxis_range"]
+    with Lattice(dims, nc, "fp64") as lat:
+        lat.upload(g["links_ape"])
+        for adjoint, key in ((False, "offaxis"), (True, "offaxis_adjoint")):
+            want = {(int(t), float(s)): w for t, s, w in meta[key]}
+            if not want:
+                continue
+            got = lat.wilson_offaxis_result(r0, r1, t0, t1, adjoint)
+            assert set(got) == set(want)
+            for k, v in want.items():
+                assert got[k] == pytest.approx(v, rel=W_RTOL, abs=W_ATOL)
+
+
+@pytest.mark.parametrize("nc,eps", [(2, 0.3), (3, 0.25)])
+def test_offaxis_matches_oracle_seeded(port, nc, eps):
+    """Unmerged entries for several directions (multipliers up to 3, odd
+    extents, negative displacements after reflection) in both forms: FP64
+    within 1e-12, mixed within 1e-6 relative."""
+    dims = (7, 6, 8, 6)
+    links = generate_config(dims, nc, eps, 20261203, 51)
+    dirs = [[1, 0, 0], [1, 1, 0], [2, 1, 0], [1, 1, 1], [2, 2, 1]]
+    for adjoint in (False, True):
+        want = port.wilson_offaxis(nc, dims, links, dirs, 0.9, 3.1, 1, 4, adjoint)
+        for precision, rtol in (("fp64", 1e-12), ("mixed", 1e-6)):
+            with Lattice(dims, nc, precision) as lat:
+                lat.upload(links)
+                got = lat.wilson_offaxis(dirs, 0.9, 3.1, 1, 4, adjoint)
+            assert [x[1:] for x in got] == [x[1:] for x in want]
+            np.testing.assert_allclose([x[0] for x in got], [x[0] for x in want], rtol=rtol,
+                                       atol=1e-14 if precision == "fp64" else 1e-7)
+
+
+def test_offaxis_argument_errors():
+    dims = (4, 4, 4, 4)
+    with Lattice(dims, 3, "fp64") as lat:
+        lat.upload(generate_config(dims, 3, 0.25, 1, 0))
+        with pytest.raises(GCError):
+            lat.wilson_offaxis([[0, 1, 0]], 1.0, 2.0, 1, 2)  # a1 must be >= 1 and largest
+        with pytest.raises(GCError):
+            lat.wilson_offaxis([[1, 0, 0]], 1.0, 2.0, 0, 2)  # time_min >= 1
+        with pytest.raises(GCError):
+            lat.wilson_offaxis([[1, 0, 0]], 1.0, 400.0, 1, 2)  # a line over 256 links
+        assert lat.wilson_offaxis([[3, 0, 0]], 1.0, 2.0, 1, 2) == []  # no length in range

@@ -190,3 +190,51 @@ def test_polyakov_of_unit_and_abelian_configurations(port, nc):
             c = port.polyakov_correlator(nc, dims, links, 2, singlet)
             assert set(np.round(c[c != 0], 12)) == {1.0}
             assert np.count_nonzero(c) == len(visited_offsets(2))
+
+
+def _offaxis_fixture(meta, key):
+    return {(int(t), float(s)): w for t, s, w in meta[key]}
+
+
+@pytest.mark.parametrize("name,meta", CASES, ids=[c[0] for c in CASES])
+def test_port_offaxis_matches_reference_fixture(port, name, meta):
+    """Merged off-axis loops (wilson_offaxis[_adjoint]_result) of the C
+    restatement against the reference's values, 1e-12 relative."""
+    g = load_golden(name)
+    nc, dims = meta["nc"], meta["dims"]
+    r0, r1, t0, t1 = meta["offaxis_range"]
+    for adjoint, key in ((False, "offaxis"), (True, "offaxis_adjoint")):
+        want = _offaxis_fixture(meta, key)
+        if not want:
+            continue
+        got = port.wilson_offaxis_result(nc, dims, g["links_ape"], r0, r1, t0, t1, adjoint)
+        assert set(got) == set(want)
+        for k, v in want.items():
+            assert got[k] == pytest.approx(v, rel=1e-12, abs=1e-14)
+
+
+@pytest.mark.parametrize("nc", [2, 3])
+def test_port_offaxis_entries_match_reference(nc):
+    """Unmerged entries (order, sizes, orientation counts and values) of the
+    C restatement against the reference compiled here, including directions
+    with no zero component (whose identity reflection the reference counts
+    twice) and multipliers above 1."""
+    from oracle import py_oracle
+    if not py_oracle.ref_available("parity"):
+        pytest.skip("reference not compiled in this checkout (oracle/_ref)")
+    port, ref = py_oracle.port(), py_oracle.ref("parity")
+    dims = (4, 5, 4, 6)
+    links = generate_config(dims, nc, 0.3 if nc == 2 else 0.25, 17, 0)
+    dirs = [[1, 0, 0], [1, 1, 0], [2, 1, 0], [1, 1, 1], [2, 1, 1]]
+    for adjoint in ((False, True) if nc == 3 else (False,)):
+        a = port.wilson_offaxis(nc, dims, links, dirs, 0.5, 3.5, 1, 3, adjoint)
+        b = ref.wilson_offaxis(nc, dims, links, dirs, 0.5, 3.5, 1, 3, adjoint)
+        assert [x[1:] for x in a] == [x[1:] for x in b]
+        np.testing.assert_allclose([x[0] for x in a], [x[0] for x in b], rtol=1e-12, atol=1e-14)
+
+
+@pytest.mark.parametrize("nc", [2, 3])
+def test_offaxis_of_unit_configuration_is_one(port, nc):
+    dims = (4, 4, 4, 4)
+    got = port.wilson_offaxis_result(nc, dims, unit_config(dims, nc), 1.0, 2.0, 1, 2)
+    assert got and all(abs(v - 1.0) < 1e-14 for v in got.values())
