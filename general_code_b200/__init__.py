@@ -11,7 +11,7 @@ from .lattice import (GCError, Lattice, LatticeData, generate_config, job_device
                       smearing_APE, smearing_HYP, unit_config, volume, wilson_gevp_adjoint_indexed,
                       wilson_gevp_indexed, wilson_loop, wilson_loop_adjoint, wilson_offaxis,
                       wilson_offaxis_adjoint, wilson_offaxis_adjoint_result,
-                      wilson_offaxis_result)
+                      wilson_offaxis_result, wilson_spatial_3d_indexed)
 
 __all__ = ["GCError", "Lattice", "LatticeData", "generate_config", "job_device_bytes",
            "link_size", "plaket", "plaket_space", "plaket_time", "polyakov_average_directions",
@@ -20,4 +20,5 @@ __all__ = ["GCError", "Lattice", "LatticeData", "generate_config", "job_device_b
            "smearing_APE", "smearing_HYP", "unit_config", "volume",
            "wilson_gevp_adjoint_indexed", "wilson_gevp_indexed", "wilson_loop",
            "wilson_loop_adjoint", "wilson_offaxis", "wilson_offaxis_adjoint",
-           "wilson_offaxis_adjoint_result", "wilson_offaxis_result"]
+           "wilson_offaxis_adjoint_result", "wilson_offaxis_result",
+           "wilson_spatial_3d_indexed"]

@@ -64,6 +64,9 @@ SIGNATURES = {
                                    _p, _c_int, _pint]),
     "gc_wilson_offaxis_result": (_c_int, [_p, _c_dbl, _c_dbl, _c_int, _c_int, _c_int, _p,
                                           _c_int, _pint]),
+    "gc_ape_plane": (_c_int, [_p, _c_int, _c_int, _c_dbl, _c_int]),
+    "gc_wilson_spatial_3d": (_c_int, [_p, _c_int, _c_int, _c_int, _c_int, _c_dbl, _c_int,
+                                      _c_int, _c_int, _p, _c_int, _pint]),
     "gc_polyakov_correlator": (_c_int, [_p, _c_int, _c_int, _pdbl]),
     "gc_wilson_onaxis_noalloc": (_c_int, [_pint, _c_int, _c_int, ctypes.POINTER(_p), _c_int,
                                           _c_int, _c_int, _c_int, _p, _p]),
@@ -144,6 +147,12 @@ class WilsonResult(ctypes.Structure):
     """gc_wilson_result (include/gc_lattice.h)."""
     _fields_ = [("wilson_loop", ctypes.c_double), ("time_size", ctypes.c_int),
                 ("space_size", ctypes.c_double), ("statistics_size", ctypes.c_int)]
+
+
+class WilsonSpatialResult(ctypes.Structure):
+    """gc_wilson_spatial_result (include/gc_lattice.h)."""
+    _fields_ = [("smearing", ctypes.c_int), ("time_size", ctypes.c_int),
+                ("space_size", ctypes.c_int), ("wilson_loop", ctypes.c_double)]
 
 
 class GCError(RuntimeError):

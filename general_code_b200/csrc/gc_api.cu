@@ -10,6 +10,8 @@
 #include <cstdio>
 #include <cstring>
 #include <functional>
+#include <map>
+#include <tuple>
 #include <mutex>
 #include <string>
 #include <vector>
@@ -773,6 +775,145 @@ int gc_wilson_offaxis_result(gc_lattice *h, double r_min, double r_max, int time
     return rc;
   offaxis_reduce(res);
   return offaxis_out(h, res, out, capacity, count);
+}
+
+int gc_ape_plane(gc_lattice *h, int a, int b, double alpha, int steps) {
+  int rc = check_ready(h);
+  if (rc)
+    return rc;
+  if (a < 0 || a > 3 || b < 0 || b > 3 || a == b || steps < 0)
+    return fail(h, GC_ERR_ARG, "need two different directions 0..3 and steps >= 0");
+  std::lock_guard<std::mutex> lk(h->mu);
+  for (int i = 0; i < steps; i++) {
+    rc = GC_DISPATCH(h, launch_ape_plane, h->g, h->cur.f[a], h->cur.f[b], h->alt.f[a],
+                     h->alt.f[b], a, b, alpha, h->stream);
+    if (rc)
+      return launch_fail(h, rc);
+    std::swap(h->cur.f[a], h->alt.f[a]);
+    std::swap(h->cur.f[b], h->alt.f[b]);
+  }
+  return GC_OK;
+}
+
+int gc_wilson_spatial_3d(gc_lattice *h, int r_min, int r_max, int time_min, int time_max,
+                         double alpha, int smearing_start, int smearing_end, int smearing_step,
+                         gc_wilson_spatial_result *out, int capacity, int *count) {
+  int rc = check_ready(h);
+  if (rc)
+    return rc;
+  if (!count || (capacity > 0 && !out))
+    return fail(h, GC_ERR_ARG, "null argument");
+  if (r_min < 1 || r_max < r_min || time_min < 1 || time_max < time_min)
+    return fail(h, GC_ERR_ARG, "need 1 <= r_min <= r_max and 1 <= time_min <= time_max");
+  if (smearing_step < 1 || smearing_end < 0)
+    return fail(h, GC_ERR_ARG, "need smearing_step >= 1 and smearing_end >= 0");
+  const int nt = time_max - time_min + 1, nr = r_max - r_min + 1;
+  if (nt > kWilsonMaxEntries)
+    return fail(h, GC_ERR_ARG, "time range too large (at most 1024 values of T)");
+  // smearing steps measured (wilson_loops.h:1410-1419)
+  std::vector<int> measured{0};
+  for (int sm = 1; sm <= smearing_end; sm++)
+    if ((sm - smearing_start) % smearing_step == 0 && smearing_step >= smearing_start)
+      measured.push_back(sm);
+  const int nm = (int)measured.size();
+  std::lock_guard<std::mutex> lk(h->mu);
+  const size_t fb = h->field_bytes;
+  const size_t lb = ((inter_link_bytes(h->nc, h->prec) * (size_t)h->g.V + 255) / 256) * 256;
+  rc = ensure_aux(h, 4 * fb + 2 * lb);
+  if (rc)
+    return rc;
+  rc = ensure_partials(h, offaxis_partials_count(h->g, nt));
+  if (rc)
+    return rc;
+  // values[plane][measurement][r][axis][T]
+  const size_t per_plane = (size_t)nm * nr * 2 * nt;
+  rc = ensure_dev_out(h, 3 * per_plane);
+  if (rc)
+    return rc;
+  char *base = (char *)h->aux;
+  void *F[2] = {base, base + fb}, *G[2] = {base + 2 * fb, base + 3 * fb};
+  void *S[2] = {base + 4 * fb, base + 4 * fb + lb};
+  const int planes[3][2] = {{0, 1}, {0, 2}, {1, 2}};
+  for (int p = 0; p < 3; p++) {
+    const int ax[2] = {planes[p][0], planes[p][1]};
+    const int mu = 3 - ax[0] - ax[1];
+    for (int k = 0; k < 2; k++) {
+      cudaError_t e = cudaMemcpyAsync(F[k], h->cur.f[ax[k]], fb, cudaMemcpyDeviceToDevice,
+                                      h->stream);
+      if (e != cudaSuccess)
+        return cuda_fail(h, "copy of a direction field", e);
+    }
+    int mi = 0, sm = 0;
+    for (;;) {
+      if (mi < nm && measured[mi] == sm) {
+        for (int k = 0; k < 2; k++) {
+          // line of the reference's initial length (see the declaration)
+          rc = GC_DISPATCH(h, launch_line_extend, h->g, F[k], S[k], ax[k], time_min,
+                           time_min - 1, true, h->stream);
+          if (rc)
+            return launch_fail(h, rc);
+        }
+        for (int r = r_min; r <= r_max; r++) {
+          for (int k = 0; k < 2; k++) {
+            int disp[4] = {0, 0, 0, 0};
+            disp[ax[k]] = r;
+            double *o = h->dev_out + p * per_plane +
+                        (((size_t)mi * nr + (r - r_min)) * 2 + k) * nt;
+            rc = GC_DISPATCH(h, launch_line_loops, h->g, h->cur.f[mu], mu, S[k], disp,
+                             time_min, time_max, false, h->partials, o, h->stream);
+            if (rc)
+              return launch_fail(h, rc);
+          }
+          for (int k = 0; k < 2; k++) {
+            rc = GC_DISPATCH(h, launch_line_extend, h->g, F[k], S[k], ax[k], r, 1, false,
+                             h->stream);
+            if (rc)
+              return launch_fail(h, rc);
+          }
+        }
+        mi++;
+      }
+      if (sm == smearing_end)
+        break;
+      rc = GC_DISPATCH(h, launch_ape_plane, h->g, F[0], F[1], G[0], G[1], ax[0], ax[1], alpha,
+                       h->stream);
+      if (rc)
+        return launch_fail(h, rc);
+      std::swap(F[0], G[0]);
+      std::swap(F[1], G[1]);
+      sm++;
+    }
+  }
+  std::vector<double> vals(3 * per_plane);
+  cudaError_t e = cudaMemcpyAsync(vals.data(), h->dev_out, vals.size() * sizeof(double),
+                                  cudaMemcpyDeviceToHost, h->stream);
+  if (e == cudaSuccess)
+    e = cudaStreamSynchronize(h->stream);
+  if (e != cudaSuccess)
+    return cuda_fail(h, "spatial loop results", e);
+  // sums per (smearing, T, R) in the reference's order: planes, then r, t,
+  // the nu axis before the eta axis; then / 6
+  std::map<std::tuple<int, int, int>, double> acc;
+  for (int p = 0; p < 3; p++)
+    for (int mi2 = 0; mi2 < nm; mi2++)
+      for (int r = r_min; r <= r_max; r++)
+        for (int t = time_min; t <= time_max; t++)
+          for (int k = 0; k < 2; k++)
+            acc[std::make_tuple(measured[mi2], t, r)] +=
+                vals[p * per_plane + (((size_t)mi2 * nr + (r - r_min)) * 2 + k) * nt +
+                     (t - time_min)];
+  *count = (int)acc.size();
+  if (*count > capacity)
+    return fail(h, GC_ERR_ARG, "output capacity too small (*count holds the size needed)");
+  int i = 0;
+  for (const auto &kv : acc) {
+    out[i].smearing = std::get<0>(kv.first);
+    out[i].time_size = std::get<1>(kv.first);
+    out[i].space_size = std::get<2>(kv.first);
+    out[i].wilson_loop = kv.second / 6;
+    i++;
+  }
+  return GC_OK;
 }
 
 // Offsets (Dx, Dy, Dz) that polyakov_loop_correlator_{singlet,color_average}

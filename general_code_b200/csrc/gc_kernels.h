@@ -198,6 +198,24 @@ int launch_offaxis_loops(const Geom &g, const Fields4 &U, const void *S, const i
                          int tmin, int tmax, bool adjoint, double *partials, double *out_dev,
                          cudaStream_t s);
 
+// Loops of a line field S (decorated-link storage) whose end is displaced
+// by disp (disp[ax] = 0) with "time" axis ax and time links Ut:
+// out_dev[T - tmin] = mean over sites of Re Tr[L(x,T) S(x+T ax) L(x+D,T)^dag
+// S(x)^dag] / N (or the adjoint character).
+template <class Store, class CT>
+int launch_line_loops(const Geom &g, const void *Ut, int ax, const void *S, const int disp[4],
+                      int tmin, int tmax, bool adjoint, double *partials, double *out_dev,
+                      cudaStream_t s);
+// S <- (init ? F : S) * F(x + offset ax)^count for a single-direction field F.
+template <class Store, class CT>
+int launch_line_extend(const Geom &g, const void *F, void *S, int ax, int offset, int count,
+                       bool init, cudaStream_t s);
+// One two-dimensional APE step of the single-direction fields f1 (axis a)
+// and f2 (axis b) into o1, o2.
+template <class Store, class CT>
+int launch_ape_plane(const Geom &g, const void *f1, const void *f2, void *o1, void *o2, int a,
+                     int b, double alpha, cudaStream_t s);
+
 // Polyakov lines P(s) of every spatial site into `lines` (FP64 element
 // planes: 9 (SU(3)) or 2 (SU(2)) double2 planes of Vs entries), block sums of
 // Re Tr P / N into partials ((Vs + 255) / 256 of them) and, if out_dev is

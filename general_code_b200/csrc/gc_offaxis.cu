@@ -17,7 +17,7 @@
 //
 // offaxis_line_kernel: thread per site, the product of the pattern's links
 // (a negative step moves back first and multiplies by the link's adjoint)
-// into a field of V matrices. offaxis_loop_kernel: thread per site, the same
+// into a field of V matrices. line_loop_kernel: thread per site, the same
 // exact recursion as the on-axis kernel, K_0 = S(x),
 // K_T = U_t(x+(T-1)t)^dag K_{T-1} U_t(x+D+(T-1)t), value Re Tr[S(x+T t) K_T^dag],
 // with fixed-order warp / block / grid sums (deterministic).
@@ -100,11 +100,14 @@ __global__ void __launch_bounds__(256)
   IS::template store<CT>(S, V, site, A);
 }
 
-// partials[block * nt + (T - tmin)]
+// partials[block * nt + (T - tmin)]. The loop's "time" axis is ax (3 for the
+// off-axis loops, a spatial axis for the spatial loops), with its links in
+// the field Ut; d holds the displacement of the line's end as non-negative
+// residues (d[ax] = 0).
 template <class Store, class CT, bool ADJ>
 __global__ void __launch_bounds__(256)
-    offaxis_loop_kernel(const __grid_constant__ Geom g, const void *Ut, const void *S, int dx,
-                        int dy, int dz, int tmin, int tmax, double *partials) {
+    line_loop_kernel(const __grid_constant__ Geom g, const void *Ut, int ax, const void *S,
+                     int4 d, int tmin, int tmax, double *partials) {
   using M = typename Store::template M<CT>;
   using IS = typename InterStore<Store>::type;
   extern __shared__ double wacc[]; // [nwarps][nt]
@@ -117,28 +120,31 @@ __global__ void __launch_bounds__(256)
   const int site = blockIdx.x * blockDim.x + threadIdx.x;
   const bool active = site < g.V;
   const size_t V = g.V;
-  int s = 0, sD = 0, t = 0;
+  const int La = sel4(g.L, ax), sta = sel4(g.stride, ax);
+  int base = 0, baseD = 0, t = 0;
   if (active) {
     int x[4];
     site_coords(g, site, x);
-    s = site % g.Vs;
-    t = x[3];
-    const int xd = (x[0] + dx) % g.L[0], yd = (x[1] + dy) % g.L[1], zd = (x[2] + dz) % g.L[2];
-    sD = xd + g.L[0] * (yd + g.L[1] * zd);
+    const int xd[4] = {(x[0] + d.x) % g.L[0], (x[1] + d.y) % g.L[1], (x[2] + d.z) % g.L[2],
+                       (x[3] + d.w) % g.L[3]};
+    const int siteD = xd[0] + g.L[0] * (xd[1] + g.L[1] * (xd[2] + g.L[2] * xd[3]));
+    t = sel4(x, ax);
+    base = site - t * sta;
+    baseD = siteD - t * sta;
   }
   M K = active ? IS::template load<CT>(S, V, site) : unit(M());
-  int tt = t; // (t + T - 1) mod Lt
+  int tt = t; // (t + T - 1) mod La
 #pragma unroll 1
   for (int T = 1; T <= tmax; T++) {
     int tu = tt + 1;
-    tu = (tu == g.L[3]) ? 0 : tu;
+    tu = (tu == La) ? 0 : tu;
     if (active) {
-      M a = Store::template load<CT>(Ut, V, s + tt * g.Vs);
-      M b = Store::template load<CT>(Ut, V, sD + tt * g.Vs);
+      M a = Store::template load<CT>(Ut, V, base + tt * sta);
+      M b = Store::template load<CT>(Ut, V, baseD + tt * sta);
       K = mul(mul_da(a, K), b);
     }
     if (T >= tmin) {
-      double v = active ? offaxis_value<ADJ>(IS::template load<CT>(S, V, s + tu * g.Vs), K)
+      double v = active ? offaxis_value<ADJ>(IS::template load<CT>(S, V, base + tu * sta), K)
                         : 0.0;
       v = warp_sum_d(v);
       if (lane == 0)
@@ -153,6 +159,32 @@ __global__ void __launch_bounds__(256)
       sum += wacc[w * nt + e];
     partials[(size_t)blockIdx.x * nt + e] = sum;
   }
+}
+
+// S(x) <- (init ? F(x) : S(x)) * F(x + offset ax)^count, F a single-direction
+// link field along ax (the straight-line helpers of the spatial loops,
+// wilson_lines_single_direction_indexed / _prolong, wilson_loops.h:1268-1300).
+template <class Store, class CT>
+__global__ void __launch_bounds__(256)
+    line_extend_kernel(const __grid_constant__ Geom g, const void *F, void *S, int ax,
+                       int offset, int count, int init) {
+  using M = typename Store::template M<CT>;
+  using IS = typename InterStore<Store>::type;
+  const int site = blockIdx.x * blockDim.x + threadIdx.x;
+  if (site >= g.V)
+    return;
+  const size_t V = g.V;
+  int x[4];
+  site_coords(g, site, x);
+  M A = init ? Store::template load<CT>(F, V, site) : IS::template load<CT>(S, V, site);
+  if (count > 0) {
+    const int fo = site + fwd_off(g, sel4(x, ax), ax, offset);
+    const M u = Store::template load<CT>(F, V, fo);
+#pragma unroll 1
+    for (int i = 0; i < count; i++)
+      A = mul(A, u);
+  }
+  IS::template store<CT>(S, V, site, A);
 }
 
 constexpr int kOffaxisBlock = 128;
@@ -173,36 +205,64 @@ int launch_offaxis_line(const Geom &g, const Fields4 &U, const OffaxisSteps &ste
 }
 
 template <class Store, class CT>
-int launch_offaxis_loops(const Geom &g, const Fields4 &U, const void *S, const int disp[3],
-                         int tmin, int tmax, bool adjoint, double *partials, double *out_dev,
-                         cudaStream_t s) {
+int launch_line_loops(const Geom &g, const void *Ut, int ax, const void *S, const int disp[4],
+                      int tmin, int tmax, bool adjoint, double *partials, double *out_dev,
+                      cudaStream_t s) {
   const int nt = tmax - tmin + 1;
   if (nt < 1 || nt > kWilsonMaxEntries)
-    return plan_error("offaxis_loop_kernel: time range");
+    return plan_error("line_loop_kernel: time range");
+  if (ax < 0 || ax > 3 || disp[ax] != 0)
+    return plan_error("line_loop_kernel: axis");
   const int blocks = (g.V + kOffaxisBlock - 1) / kOffaxisBlock;
   const size_t smem = (size_t)(kOffaxisBlock / 32) * nt * sizeof(double);
   // displacement as non-negative residues
-  int d[3];
-  for (int i = 0; i < 3; i++)
+  int d[4];
+  for (int i = 0; i < 4; i++)
     d[i] = ((disp[i] % g.L[i]) + g.L[i]) % g.L[i];
+  const int4 d4 = make_int4(d[0], d[1], d[2], d[3]);
   if (adjoint)
-    offaxis_loop_kernel<Store, CT, true><<<blocks, kOffaxisBlock, smem, s>>>(
-        g, U.f[3], S, d[0], d[1], d[2], tmin, tmax, partials);
+    line_loop_kernel<Store, CT, true><<<blocks, kOffaxisBlock, smem, s>>>(g, Ut, ax, S, d4, tmin,
+                                                                         tmax, partials);
   else
-    offaxis_loop_kernel<Store, CT, false><<<blocks, kOffaxisBlock, smem, s>>>(
-        g, U.f[3], S, d[0], d[1], d[2], tmin, tmax, partials);
-  int rc = launch_check("offaxis_loop_kernel");
+    line_loop_kernel<Store, CT, false><<<blocks, kOffaxisBlock, smem, s>>>(g, Ut, ax, S, d4,
+                                                                          tmin, tmax, partials);
+  int rc = launch_check("line_loop_kernel");
   if (rc)
     return rc;
-  // averages over V sites (calculate_wilson_loop_offaxis divides by V); the
-  // fundamental SU(3) value is Re Tr / 3 (tr_real)
+  // averages over V sites (calculate_wilson_loop_offaxis and
+  // wilson_spatial_plane_indexed divide by V); the fundamental SU(3) value is
+  // Re Tr / 3 (tr_real, multiply_conj_tr)
   const double scale = 1.0 / ((double)g.V * ((!adjoint && Store::NC == 3) ? 3.0 : 1.0));
   return launch_reduce_rows(partials, blocks, nt, scale, out_dev, s);
+}
+
+template <class Store, class CT>
+int launch_offaxis_loops(const Geom &g, const Fields4 &U, const void *S, const int disp[3],
+                         int tmin, int tmax, bool adjoint, double *partials, double *out_dev,
+                         cudaStream_t s) {
+  const int d4[4] = {disp[0], disp[1], disp[2], 0};
+  return launch_line_loops<Store, CT>(g, U.f[3], 3, S, d4, tmin, tmax, adjoint, partials,
+                                      out_dev, s);
+}
+
+template <class Store, class CT>
+int launch_line_extend(const Geom &g, const void *F, void *S, int ax, int offset, int count,
+                       bool init, cudaStream_t s) {
+  if (ax < 0 || ax > 3 || count < 0 || offset < 0)
+    return plan_error("line_extend_kernel: arguments");
+  line_extend_kernel<Store, CT><<<(g.V + 255) / 256, 256, 0, s>>>(g, F, S, ax, offset, count,
+                                                                  init ? 1 : 0);
+  return launch_check("line_extend_kernel");
 }
 
 #define GC_INSTANTIATE_O(STORE, CT)                                                        \
   template int launch_offaxis_line<STORE, CT>(const Geom &, const Fields4 &,              \
                                               const OffaxisSteps &, void *, cudaStream_t); \
+  template int launch_line_loops<STORE, CT>(const Geom &, const void *, int, const void *, \
+                                            const int *, int, int, bool, double *,        \
+                                            double *, cudaStream_t);                      \
+  template int launch_line_extend<STORE, CT>(const Geom &, const void *, void *, int, int,  \
+                                             int, bool, cudaStream_t);                     \
   template int launch_offaxis_loops<STORE, CT>(const Geom &, const Fields4 &, const void *, \
                                                const int *, int, int, bool, double *,      \
                                                double *, cudaStream_t);

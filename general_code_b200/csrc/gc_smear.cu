@@ -297,6 +297,45 @@ __global__ void __launch_bounds__(128)
     hyp_l3_site<Store, CT>(jb.g, jb.U.f[3], jb.l2, jb.out_t, jb.a1, site);
 }
 
+// Two-dimensional APE step of two single-direction fields, links along axes
+// a (f1) and b (f2), with the staples of the (a, b) plane only
+// (smearing_APE_2d, smearing.h:223-277): per site
+//   f1'(x) = Proj[(1-alpha) f1(x) + alpha/2 (f2(x) f1(x+b) f2(x+a)^dag
+//                                    + f2(x-b)^dag f1(x-b) f2(x-b+a))]
+//   f2'(x) = Proj[(1-alpha) f2(x) + alpha/2 (f1(x) f2(x+a) f1(x+b)^dag
+//                                    + f1(x-a)^dag f2(x-a) f1(x-a+b))]
+template <class Store, class CT>
+__global__ void __launch_bounds__(128, 4)
+    ape_plane_kernel(const __grid_constant__ Geom g, const void *f1, const void *f2, void *o1,
+                     void *o2, int a, int b, double alpha) {
+  using M = typename Store::template M<CT>;
+  const int site = blockIdx.x * blockDim.x + threadIdx.x;
+  if (site >= g.V)
+    return;
+  const size_t V = g.V;
+  int x[4];
+  site_coords(g, site, x);
+  const int pa = site + step_off(g, sel4(x, a), a, +1);
+  const int pb = site + step_off(g, sel4(x, b), b, +1);
+  const int mb = site + step_off(g, sel4(x, b), b, -1);
+  const int ma = site + step_off(g, sel4(x, a), a, -1);
+  const int mb_pa = mb + step_off(g, sel4(x, a), a, +1);
+  const int ma_pb = ma + step_off(g, sel4(x, b), b, +1);
+  const CT c = CT(alpha / 2);
+  const M u1 = Store::template load<CT>(f1, V, site), u2 = Store::template load<CT>(f2, V, site);
+  // upper staples: A = f2(x+a) f1(x+b)^dag
+  const M A = mul_ad(Store::template load<CT>(f2, V, pa), Store::template load<CT>(f1, V, pb));
+  M S1 = add(scale(u1, CT(1 - alpha)), scale(mul_ad(u2, A), c));
+  M S2 = add(scale(u2, CT(1 - alpha)), scale(mul(u1, A), c));
+  // lower staples
+  const M l1 = mul_da(Store::template load<CT>(f2, V, mb), Store::template load<CT>(f1, V, mb));
+  S1 = add(S1, scale(mul(l1, Store::template load<CT>(f2, V, mb_pa)), c));
+  const M l2 = mul_da(Store::template load<CT>(f1, V, ma), Store::template load<CT>(f2, V, ma));
+  S2 = add(S2, scale(mul(l2, Store::template load<CT>(f1, V, ma_pb)), c));
+  proj_store<Store, CT>(o1, V, site, S1);
+  proj_store<Store, CT>(o2, V, site, S2);
+}
+
 } // namespace
 
 template <class Store, class CT>
@@ -349,7 +388,20 @@ int launch_hyp_batch(const HypJob *jobs, int njobs, const int blocks[3],
   return launch_check("hyp_level3_batch_kernel");
 }
 
+template <class Store, class CT>
+int launch_ape_plane(const Geom &g, const void *f1, const void *f2, void *o1, void *o2, int a,
+                     int b, double alpha, cudaStream_t s) {
+  if (a < 0 || a > 3 || b < 0 || b > 3 || a == b)
+    return plan_error("ape_plane_kernel: directions");
+  const unsigned nb = (g.V + kSmearBlock - 1) / kSmearBlock;
+  ape_plane_kernel<Store, CT><<<nb, kSmearBlock, 0, s>>>(g, f1, f2, o1, o2, a, b, alpha);
+  return launch_check("ape_plane_kernel");
+}
+
 #define GC_INSTANTIATE_SMEAR(STORE, CT)                                        \
+  template int launch_ape_plane<STORE, CT>(const Geom &, const void *,        \
+                                           const void *, void *, void *, int, \
+                                           int, double, cudaStream_t);        \
   template int launch_ape<STORE, CT>(const Geom &, const Fields4 &,           \
                                      const Fields4 &, double, cudaStream_t);  \
   template int launch_hyp<STORE, CT>(const Geom &, const Fields4 &,           \

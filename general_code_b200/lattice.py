@@ -22,7 +22,8 @@ import numpy as np
 
 from . import _lib
 from ._lib import (GC_ERR_ARG, GC_LAYOUT_EIGEN_COLMAJOR, GC_LAYOUT_ROWMAJOR, GC_PREC_FP64,
-                   GC_PREC_MIXED, GCError, WilsonResult, check, dbl_ptr, dims_arg, lib)
+                   GC_PREC_MIXED, GCError, WilsonResult, WilsonSpatialResult, check, dbl_ptr,
+                   dims_arg, lib)
 
 _PREC = {"fp64": GC_PREC_FP64, "mixed": GC_PREC_MIXED}
 _LAYOUT = {"rowmajor": GC_LAYOUT_ROWMAJOR, "eigen": GC_LAYOUT_EIGEN_COLMAJOR}
@@ -228,6 +229,33 @@ class Lattice:
             out[(t, size)] = w
         return out
 
+    def ape_plane(self, a: int, b: int, alpha: float, steps: int = 1) -> None:
+        """Two-dimensional APE steps of directions a and b in the (a, b) plane
+        (smearing_APE_2d, smearing.h:223-277), in place."""
+        self._check(lib().gc_ape_plane(self._h, int(a), int(b), float(alpha), int(steps)))
+
+    def wilson_spatial_3d(self, r_min: int, r_max: int, time_min: int, time_max: int,
+                          alpha: float, smearing_start: int, smearing_end: int,
+                          smearing_step: int) -> Dict[Tuple[int, int, int], float]:
+        """Spatial Wilson loops with two-dimensional APE smearing
+        (wilson_spatial_3d_indexed, wilson_loops.h:1384-1428):
+        {(smearing, T, R): W}."""
+        count = ctypes.c_int(0)
+        cap = 4096
+        while True:
+            out = (WilsonSpatialResult * cap)()
+            rc = lib().gc_wilson_spatial_3d(self._h, int(r_min), int(r_max), int(time_min),
+                                            int(time_max), float(alpha), int(smearing_start),
+                                            int(smearing_end), int(smearing_step),
+                                            ctypes.cast(out, ctypes.c_void_p), cap,
+                                            ctypes.byref(count))
+            if rc == GC_ERR_ARG and count.value > cap:
+                cap = count.value
+                continue
+            self._check(rc)
+            return {(r.smearing, r.time_size, r.space_size): r.wilson_loop
+                    for r in out[:count.value]}
+
     def polyakov_loop(self) -> float:
         """Mean of Re Tr P / N over spatial sites (polyakov_loops.h:24-41)."""
         out = ctypes.c_double()
@@ -387,6 +415,17 @@ def wilson_offaxis_adjoint_result(conf: LatticeData, r_min: float, r_max: float,
     with Lattice(conf.lat_dim, conf.nc) as lat:
         lat.upload(conf.array)
         return lat.wilson_offaxis_result(r_min, r_max, time_min, time_max, adjoint=True)
+
+
+def wilson_spatial_3d_indexed(conf: LatticeData, r_min: int, r_max: int, time_min: int,
+                              time_max: int, alpha: float, smearing_start: int,
+                              smearing_end: int,
+                              smearing_step: int) -> Dict[Tuple[int, int, int], float]:
+    """Spatial Wilson loops keyed (smearing, T, R) (wilson_loops.h:1384-1428)."""
+    with Lattice(conf.lat_dim, conf.nc) as lat:
+        lat.upload(conf.array)
+        return lat.wilson_spatial_3d(r_min, r_max, time_min, time_max, alpha, smearing_start,
+                                     smearing_end, smearing_step)
 
 
 def polyakov_loop(conf: LatticeData) -> float:

@@ -37,6 +37,14 @@
 //       double, double, int, int)                         wilson_loops.h:470-473, 648-651
 //   wilson_offaxis_result / wilson_offaxis_adjoint_result(const std::vector<T>&,
 //       double, double, int, int)                         basic_observables.h:34-36, 45-48
+//   wilson_spatial_3d_indexed(const LatticeData&, int, int, int, int, double,
+//       int, int, int)                                    wilson_loops.h:1384-1388
+//
+// Helpers the reference templates call internally (wilson_offaxis from
+// wilson_offaxis_result, smearing_APE_2d from wilson_spatial_3d_indexed) are
+// found by argument-dependent lookup inside those templates too; the
+// overloads below take over whole observables, and smearing_APE_2d has no
+// overload (gc_ape_plane in gc_lattice.h is its C entry point).
 #pragma once
 
 #include "gc_lattice.h"
@@ -245,6 +253,32 @@ offaxis_map(const std::vector<wilson_result> &entries) {
 }
 
 template <class MT>
+std::map<std::tuple<int, int, int>, double>
+spatial(const Data::LatticeData<DataPatternLexicographical, MT> &conf, int r_min, int r_max,
+        int time_min, int time_max, double alpha, int smearing_start, int smearing_end,
+        int smearing_step) {
+  Session<MT> s(conf.lat_dim, conf.array.data());
+  std::vector<gc_wilson_spatial_result> out(4096);
+  int count = 0;
+  for (int attempt = 0; attempt < 2; attempt++) {
+    const int rc = gc_wilson_spatial_3d(s.get(), r_min, r_max, time_min, time_max, alpha,
+                                        smearing_start, smearing_end, smearing_step,
+                                        out.data(), (int)out.size(), &count);
+    if (rc == GC_ERR_ARG && count > (int)out.size()) {
+      out.resize(count);
+      continue;
+    }
+    check(rc, s.get(), "wilson_spatial_3d_indexed");
+    break;
+  }
+  std::map<std::tuple<int, int, int>, double> m;
+  for (int i = 0; i < count; i++)
+    m[std::tuple<int, int, int>(out[i].smearing, out[i].time_size, out[i].space_size)] =
+        out[i].wilson_loop;
+  return m;
+}
+
+template <class MT>
 double polyakov(const Data::LatticeData<DataPatternLexicographical, MT> &conf) {
   Session<MT> s(conf.lat_dim, conf.array.data());
   double p = 0;
@@ -441,6 +475,21 @@ inline std::vector<double> polyakov_loop_correlator_color_average(
 GC_DROPIN_OFFAXIS(su2)
 GC_DROPIN_OFFAXIS(su3)
 #undef GC_DROPIN_OFFAXIS
+
+// Spatial Wilson loops with two-dimensional APE smearing
+// (wilson_loops.h:1384-1428), as apps/observables/wilson_loops_spatial calls
+// them (wilson_loops_spatial.cpp:117-119).
+#define GC_DROPIN_SPATIAL(MT)                                                                  \
+  inline std::map<std::tuple<int, int, int>, double> wilson_spatial_3d_indexed(                \
+      const Data::LatticeData<DataPatternLexicographical, MT> &conf, int r_min, int r_max,     \
+      int time_min, int time_max, double alpha, int smearing_start, int smearing_end,          \
+      int smearing_step) {                                                                     \
+    return gc_dropin::spatial(conf, r_min, r_max, time_min, time_max, alpha, smearing_start,   \
+                              smearing_end, smearing_step);                                    \
+  }
+GC_DROPIN_SPATIAL(su2)
+GC_DROPIN_SPATIAL(su3)
+#undef GC_DROPIN_SPATIAL
 
 // Configuration reader (data.h:265-338), as apps/smearing/smearing.cpp:188
 // calls it (qualified, Data::read_data_convert).

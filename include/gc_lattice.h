@@ -208,6 +208,41 @@ int gc_wilson_offaxis_result(gc_lattice *h, double r_min, double r_max, int time
                              int time_max, int adjoint, gc_wilson_result *out, int capacity,
                              int *count);
 
+/* One two-dimensional APE step (steps times) of the link fields of
+ * directions a and b of h, in place, with the staples of the (a, b) plane
+ * only; the other directions are unchanged.
+ * Replaces: smearing_APE_2d(conf1, conf2, data_pattern, a, b, alpha)
+ * (smearing.h:223-277) applied to h's fields of directions a and b. */
+int gc_ape_plane(gc_lattice *h, int a, int b, double alpha, int steps);
+
+/* One entry of the spatial Wilson-loop table. */
+typedef struct {
+  int smearing;       /* two-dimensional APE steps taken before the entry */
+  int time_size;      /* length along the loop's spatial "time" axis */
+  int space_size;     /* length along the smeared axis */
+  double wilson_loop;
+} gc_wilson_spatial_result;
+
+/* Spatial (three-dimensional) Wilson loops with two-dimensional APE
+ * smearing of the transverse links, as the reference computes them: for each
+ * spatial plane (nu, eta) the links of nu and eta are smeared in that plane
+ * (smearing_end steps), the loops have their "time" extent along the third
+ * spatial axis (unsmeared links) and their space extent along nu or eta
+ * (smeared links), measured before smearing and after the steps s with
+ * (s - smearing_start) % smearing_step == 0 while smearing_step >=
+ * smearing_start; every entry is the sum over the three planes and both axes
+ * / 6. The space lines follow the reference's construction step for step
+ * (wilson_lines_single_direction_indexed starts them with length time_min).
+ * Entries in (smearing, T, R) order; capacity and *count as
+ * gc_wilson_offaxis. Needs 1 <= r_min <= r_max, 1 <= time_min <= time_max,
+ * smearing_step >= 1, smearing_end >= 0.
+ * Replaces: wilson_spatial_3d_indexed(conf, r_min, r_max, time_min,
+ * time_max, alpha, smearing_start, smearing_end, smearing_step)
+ * (wilson_loops.h:1384-1428, helpers :1268-1382). */
+int gc_wilson_spatial_3d(gc_lattice *h, int r_min, int r_max, int time_min, int time_max,
+                         double alpha, int smearing_start, int smearing_end, int smearing_step,
+                         gc_wilson_spatial_result *out, int capacity, int *count);
+
 /* Average of the three spatial plaquettes per site.
  * Replaces: plaket_space(conf) (plaket.h:123-141, sites :63-81). */
 int gc_plaquette_space(gc_lattice *h, double *out);

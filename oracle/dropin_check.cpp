@@ -6,8 +6,9 @@
 // wilson_gevp_indexed, wilson_gevp_adjoint_indexed of the HYP and HYP+APE
 // configurations), plaket_time / plaket_space, the reader, and the merged
 // off-axis loops of apps/observables/wilson_loops (wilson_offaxis_result and,
-// for su3, wilson_offaxis_adjoint_result), twice on the same seeded
-// configuration:
+// for su3, wilson_offaxis_adjoint_result) and the spatial loops of
+// apps/observables/wilson_loops_spatial (wilson_spatial_3d_indexed), twice on
+// the same seeded configuration:
 //   - with unqualified calls, exactly as the app writes them, which overload
 //     resolution binds to the drop-in (GPU) functions;
 //   - with the reference templates named explicitly (CPU).
@@ -30,6 +31,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
+#include <type_traits>
 #include <unistd.h>
 
 int x_size, y_size, z_size, t_size, size1, size2;
@@ -68,6 +70,30 @@ template <class MT> double ref_polyakov(const Data::LatticeData<DP, MT> &conf) {
         sum += get_polyakov_loop(conf, dp).tr_real();
       }
   return sum / (dp.lat_dim[0] * dp.lat_dim[1] * dp.lat_dim[2]);
+}
+
+// The reference's wilson_offaxis[_adjoint]_result (wilson_loops.h:470-485,
+// 648-663) with its own steps: the templates are named with explicit
+// arguments, so the drop-in overload of wilson_offaxis cannot take over the
+// call that the result function would otherwise make by name.
+template <class MT>
+std::map<std::tuple<int, double>, double>
+ref_offaxis_result(const Data::LatticeData<DP, MT> &conf, double r_min, double r_max,
+                   int time_min, int time_max, bool adjoint) {
+  const std::vector<std::vector<int>> dirs = generate_directions(4);
+  std::vector<wilson_result> r;
+  if (adjoint) {
+    if constexpr (std::is_same<MT, su3>::value)
+      r = ::wilson_offaxis_adjoint<DP, MT>(conf, dirs, r_min - 0.1, r_max + 0.1, time_min,
+                                           time_max);
+  } else {
+    r = ::wilson_offaxis<DP, MT>(conf, dirs, r_min - 0.1, r_max + 0.1, time_min, time_max);
+  }
+  wilson_offaxis_reduce(r);
+  std::map<std::tuple<int, double>, double> m;
+  for (const auto &e : r)
+    m[std::tuple<int, double>(e.time_size, e.space_size)] = e.wilson_loop;
+  return m;
 }
 
 double max_rel(const std::map<std::tuple<int, int>, double> &a,
@@ -112,6 +138,7 @@ int run(const std::array<int, 4> &dims, int ape_steps, int rmax, int tmax) {
   double pa, pb, pta, ptb, psa, psb, la, lb;
   std::map<std::tuple<int, int>, double> wa, wb, aa, ab, ga, gb, gaa, gab;
   std::map<std::tuple<int, double>, double> oa, ob, ooa, oob;
+  std::map<std::tuple<int, int, int>, double> sa, sb;
   std::vector<double> csa, csb, cca, ccb;
   const int D = 2;
   Data::LatticeData<DP, MT> ha(dims), hb(dims); // configurations after HYP
@@ -131,6 +158,7 @@ int run(const std::array<int, 4> &dims, int ape_steps, int rmax, int tmax) {
     oa = wilson_offaxis_result(a, 1, rmax, 1, tmax);
     if (ds == 18)
       ooa = wilson_offaxis_adjoint_result(a, 1, rmax, 1, tmax);
+    sa = wilson_spatial_3d_indexed(a, 1, 2, 1, 2, 0.5, 1, 2, 1);
     pta = plaket_time(a);
     psa = plaket_space(a);
   } catch (const std::exception &e) {
@@ -178,9 +206,10 @@ int run(const std::array<int, 4> &dims, int ape_steps, int rmax, int tmax) {
   ab = ::wilson_loop_adjoint<DP, MT>(b, 1, rmax, 1, tmax);
   gb = ::wilson_gevp_indexed<DP, MT>(b, hb, 1, rmax, 1, tmax);
   gab = ::wilson_gevp_adjoint_indexed<DP, MT>(b, hb, 1, rmax, 1, tmax);
-  ob = ::wilson_offaxis_result<DP, MT>(b, 1, rmax, 1, tmax);
+  ob = ref_offaxis_result(b, 1, rmax, 1, tmax, false);
   if (ds == 18)
-    oob = ::wilson_offaxis_adjoint_result<DP, MT>(b, 1, rmax, 1, tmax);
+    oob = ref_offaxis_result(b, 1, rmax, 1, tmax, true);
+  sb = ::wilson_spatial_3d_indexed<DP, MT>(b, 1, 2, 1, 2, 0.5, 1, 2, 1);
   ptb = ref_plaquette(b, 1);
   psb = ref_plaquette(b, 2);
   double dl = 0;
@@ -212,11 +241,24 @@ int run(const std::array<int, 4> &dims, int ape_steps, int rmax, int tmax) {
       ok = ok && e <= 1e-12 * std::fabs(kv.second) + 1e-14;
     }
   }
+  double dsp = 0;
+  ok = ok && sa.size() == sb.size();
+  for (auto &kv : sb) {
+    auto it = sa.find(kv.first);
+    if (it == sa.end()) {
+      ok = false;
+      continue;
+    }
+    const double e = std::fabs(it->second - kv.second);
+    dsp = std::fmax(dsp, e / (std::fabs(kv.second) + 1e-300));
+    ok = ok && e <= 1e-12 * std::fabs(kv.second) + 1e-14;
+  }
   std::printf("links max|diff| %.3e  plaquette diff %.3e (time %.3e space %.3e)  W max rel "
               "diff %.3e  GEVP %.3e  Polyakov %.3e, correlators %.3e  reader %.3e  "
-              "off-axis %.3e (%zu entries)  entries %zu  %s\n",
+              "off-axis %.3e (%zu entries)  spatial %.3e (%zu entries)  entries %zu  %s\n",
               dl, std::fabs(pa - pb), std::fabs(pta - ptb), std::fabs(psa - psb), dw, dg,
-              std::fabs(la - lb), dc, dread, doff, ob.size(), wb.size(), ok ? "OK" : "MISMATCH");
+              std::fabs(la - lb), dc, dread, doff, ob.size(), dsp, sb.size(), wb.size(),
+              ok ? "OK" : "MISMATCH");
   return ok ? 0 : 1;
 }
 

@@ -802,6 +802,181 @@ int or_wilson_offaxis_result(int nc, const int dims[4], const double *links, dou
   return n;
 }
 
+/* ------------------------------------------------------------ spatial loops */
+/* smearing_APE_2d (smearing.h:223-277) of the single-direction fields f1
+ * (axis a) and f2 (axis b), in the reference's operation order. */
+static void ape2d(const group_t *G, const geom_t *g, double *f1, double *f2, int a, int b,
+                  double alpha) {
+  const int ds = G->ds;
+  double *o1 = (double *)malloc((size_t)g->V * ds * sizeof(double));
+  double *o2 = (double *)malloc((size_t)g->V * ds * sizeof(double));
+#pragma omp parallel for
+  for (long long x = 0; x < g->V; x++) {
+    double A[18], B[18], st[18], t[18], r[18];
+    const long long xb = shift(g, x, b, 1), xa = shift(g, x, a, 1);
+    G->mul_ad(A, f2 + xa * ds, f1 + xb * ds); /* A = f2(x+a) ^ f1(x+b) */
+    G->mul_ad(B, f2 + x * ds, A);             /* B = f2(x) ^ A */
+    G->mul(A, f1 + x * ds, A);                /* A = f1(x) * A */
+    const long long xmb = shift(g, x, b, -1), xmb_pa = shift(g, xmb, a, 1);
+    G->mul_da(st, f2 + xmb * ds, f1 + xmb * ds); /* staple = f2(x-b) % f1(x-b) */
+    G->mul(t, st, f2 + xmb_pa * ds);
+    for (int k = 0; k < ds; k++)
+      r[k] = (1 - alpha) * f1[x * ds + k] + (alpha / 2) * (B[k] + t[k]);
+    G->proj(r);
+    memcpy(o1 + x * ds, r, ds * sizeof(double));
+    const long long xma = shift(g, x, a, -1), xma_pb = shift(g, xma, b, 1);
+    G->mul_da(B, f1 + xma * ds, f2 + xma * ds); /* B = f1(x-a) % f2(x-a) */
+    G->mul(t, B, f1 + xma_pb * ds);
+    for (int k = 0; k < ds; k++)
+      r[k] = (1 - alpha) * f2[x * ds + k] + (alpha / 2) * (A[k] + t[k]);
+    G->proj(r);
+    memcpy(o2 + x * ds, r, ds * sizeof(double));
+  }
+  memcpy(f1, o1, (size_t)g->V * ds * sizeof(double));
+  memcpy(f2, o2, (size_t)g->V * ds * sizeof(double));
+  free(o1);
+  free(o2);
+}
+
+/* smearing_APE_2d applied to the direction fields a, b of a configuration */
+int or_ape_plane(int nc, const int dims[4], double *links, int a, int b, double alpha,
+                 int steps) {
+  const group_t *G = group_of(nc);
+  if (!G || a < 0 || a > 3 || b < 0 || b > 3 || a == b)
+    return -1;
+  geom_t g;
+  geom_init(&g, dims);
+  const int ds = G->ds;
+  double *f1 = (double *)malloc((size_t)g.V * ds * sizeof(double));
+  double *f2 = (double *)malloc((size_t)g.V * ds * sizeof(double));
+  for (long long x = 0; x < g.V; x++) {
+    memcpy(f1 + x * ds, links + (4 * x + a) * ds, ds * sizeof(double));
+    memcpy(f2 + x * ds, links + (4 * x + b) * ds, ds * sizeof(double));
+  }
+  for (int i = 0; i < steps; i++)
+    ape2d(G, &g, f1, f2, a, b, alpha);
+  for (long long x = 0; x < g.V; x++) {
+    memcpy(links + (4 * x + a) * ds, f1 + x * ds, ds * sizeof(double));
+    memcpy(links + (4 * x + b) * ds, f2 + x * ds, ds * sizeof(double));
+  }
+  free(f1);
+  free(f2);
+  return 0;
+}
+
+/* wilson_lines_single_direction_prolong (wilson_loops.h:1268-1287):
+ * S(x) <- S(x) F(x + length mu) */
+static void sd_prolong(const group_t *G, const geom_t *g, const double *F, double *S,
+                       int length, int mu) {
+  const int ds = G->ds;
+#pragma omp parallel for
+  for (long long x = 0; x < g->V; x++)
+    G->mul(S + x * ds, S + x * ds, F + shift(g, x, mu, length) * ds);
+}
+
+/* wilson_spatial_plane_indexed (wilson_loops.h:1303-1334): mean over x of
+ * Re Tr[Q(x) S(x + lm mu) Q(x + ln nu)^dag S(x)^dag] / N */
+static double spatial_plane(int nc, const group_t *G, const geom_t *g, const double *Q,
+                            const double *S, int mu, int nu, int lm, int ln) {
+  const int ds = G->ds;
+  double result = 0;
+#pragma omp parallel for reduction(+ : result)
+  for (long long x = 0; x < g->V; x++) {
+    double w[18];
+    G->mul(w, Q + x * ds, S + shift(g, x, mu, lm) * ds);
+    G->mul_ad(w, w, Q + shift(g, x, nu, ln) * ds);
+    result += (nc == 3) ? su3_conj_tr(w, S + x * ds) : su2_conj_tr(w, S + x * ds);
+  }
+  return result / g->V;
+}
+
+/* wilson_spatial_3d_indexed (wilson_loops.h:1384-1428) with its helpers,
+ * step for step (space lines start with length time_min, see
+ * wilson_lines_single_direction_indexed :1289-1301). Entries (smearing, T, R,
+ * W) in (smearing, T, R) order; returns the count or -1. */
+int or_wilson_spatial_3d(int nc, const int dims[4], const double *links, int rmin, int rmax,
+                         int tmin, int tmax, double alpha, int sm_start, int sm_end,
+                         int sm_step, int *out_s, int *out_t, int *out_r, double *out_w,
+                         int cap) {
+  const group_t *G = group_of(nc);
+  if (!G || rmin < 1 || rmax < rmin || tmin < 1 || tmax < tmin || sm_step < 1 || sm_end < 0)
+    return -1;
+  geom_t g;
+  geom_init(&g, dims);
+  const int ds = G->ds, nt = tmax - tmin + 1, nr = rmax - rmin + 1;
+  int *meas = (int *)malloc((sm_end + 1) * sizeof(int));
+  int nm = 0;
+  meas[nm++] = 0;
+  for (int sm = 1; sm <= sm_end; sm++)
+    if ((sm - sm_start) % sm_step == 0 && sm_step >= sm_start)
+      meas[nm++] = sm;
+  double *acc = (double *)calloc((size_t)nm * nt * nr, sizeof(double)); /* [m][t][r] */
+  const size_t fsz = (size_t)g.V * ds * sizeof(double);
+  double *F1 = (double *)malloc(fsz), *F2 = (double *)malloc(fsz);
+  double *S1 = (double *)malloc(fsz), *S2 = (double *)malloc(fsz);
+  const int planes[3][2] = {{0, 1}, {0, 2}, {1, 2}};
+  for (int p = 0; p < 3; p++) {
+    const int nu = planes[p][0], eta = planes[p][1], mu = 3 - nu - eta;
+    for (long long x = 0; x < g.V; x++) {
+      memcpy(F1 + x * ds, links + (4 * x + nu) * ds, ds * sizeof(double));
+      memcpy(F2 + x * ds, links + (4 * x + eta) * ds, ds * sizeof(double));
+    }
+    /* quark lines along mu, lengths tmin..tmax */
+    double **Q = (double **)malloc(nt * sizeof(double *));
+    Q[0] = lines_indexed(G, &g, links, tmin, mu);
+    for (int t = tmin + 1; t <= tmax; t++) {
+      Q[t - tmin] = (double *)malloc(fsz);
+      memcpy(Q[t - tmin], Q[t - tmin - 1], fsz);
+      prolong(G, &g, links, Q[t - tmin], t - 1, mu);
+    }
+    int mi = 0;
+    for (int sm = 0; sm <= sm_end; sm++) {
+      if (sm > 0)
+        ape2d(G, &g, F1, F2, nu, eta, alpha);
+      if (mi >= nm || meas[mi] != sm)
+        continue;
+      memcpy(S1, F1, fsz);
+      memcpy(S2, F2, fsz);
+      for (int i = 1; i < tmin; i++) {
+        sd_prolong(G, &g, F1, S1, tmin, nu);
+        sd_prolong(G, &g, F2, S2, tmin, eta);
+      }
+      for (int r = rmin; r <= rmax; r++) {
+        for (int t = tmin; t <= tmax; t++) {
+          double *a = acc + ((size_t)mi * nt + (t - tmin)) * nr + (r - rmin);
+          *a += spatial_plane(nc, G, &g, Q[t - tmin], S1, mu, nu, t, r);
+          *a += spatial_plane(nc, G, &g, Q[t - tmin], S2, mu, eta, t, r);
+        }
+        sd_prolong(G, &g, F1, S1, r, nu);
+        sd_prolong(G, &g, F2, S2, r, eta);
+      }
+      mi++;
+    }
+    for (int i = 0; i < nt; i++)
+      free(Q[i]);
+    free(Q);
+  }
+  int n = 0;
+  for (int m = 0; m < nm; m++)
+    for (int t = tmin; t <= tmax; t++)
+      for (int r = rmin; r <= rmax; r++) {
+        if (n < cap) {
+          out_s[n] = meas[m];
+          out_t[n] = t;
+          out_r[n] = r;
+          out_w[n] = acc[((size_t)m * nt + (t - tmin)) * nr + (r - rmin)] / 6;
+        }
+        n++;
+      }
+  free(F1);
+  free(F2);
+  free(S1);
+  free(S2);
+  free(acc);
+  free(meas);
+  return n;
+}
+
 /* ------------------------------------------------------------ plaquette */
 /* which = 0: all six planes / 6 (plaket_site, plaket.h:24-42);
  * 1: (mu, t) planes / 3 (plaket_site_time, :44-61);

@@ -43,6 +43,14 @@ int or_wilson_offaxis(int nc, const int dims[4], const double *links, const int 
 int or_wilson_offaxis_result(int nc, const int dims[4], const double *links, double r_min,
                              double r_max, int time_min, int time_max, int adjoint,
                              or_wilson_result *out, int capacity);
+/* smearing_APE_2d of the direction fields a, b (in place). */
+int or_ape_plane(int nc, const int dims[4], double *links, int a, int b, double alpha,
+                 int steps);
+/* wilson_spatial_3d_indexed: entries (smearing, T, R, W); returns the count. */
+int or_wilson_spatial_3d(int nc, const int dims[4], const double *links, int rmin, int rmax,
+                         int tmin, int tmax, double alpha, int sm_start, int sm_end,
+                         int sm_step, int *out_s, int *out_t, int *out_r, double *out_w,
+                         int cap);
 double or_plaquette(int nc, const int dims[4], const double *links);
 double or_plaquette_time(int nc, const int dims[4], const double *links);
 double or_plaquette_space(int nc, const int dims[4], const double *links);

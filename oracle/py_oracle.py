@@ -77,6 +77,28 @@ class _Checker:
     def plaquette(self, nc, dims, links):
         return float(self._fn("plaquette")(nc, _dims(dims), _ptr(links)))
 
+    def ape_plane(self, nc, dims, links, a, b, alpha, steps=1):
+        """smearing_APE_2d on the direction fields a, b, in place."""
+        fn = self._fn("ape_plane")
+        fn.restype = _c_int
+        fn.argtypes = [_c_int, _pint, _pdbl, _c_int, _c_int, _c_dbl, _c_int]
+        assert fn(nc, _dims(dims), _ptr(links), a, b, alpha, steps) == 0
+
+    def wilson_spatial_3d(self, nc, dims, links, rmin, rmax, tmin, tmax, alpha, sm_start,
+                          sm_end, sm_step, capacity=100000):
+        """wilson_spatial_3d_indexed: {(smearing, T, R): W}."""
+        fn = self._fn("wilson_spatial_3d")
+        fn.restype = _c_int
+        fn.argtypes = [_c_int, _pint, _pdbl, _c_int, _c_int, _c_int, _c_int, _c_dbl, _c_int,
+                       _c_int, _c_int, _pint, _pint, _pint, _pdbl, _c_int]
+        s_, t_, r_ = (np.zeros(capacity, dtype=np.int32) for _ in range(3))
+        w = np.zeros(capacity)
+        n = fn(nc, _dims(dims), _ptr(links), rmin, rmax, tmin, tmax, alpha, sm_start, sm_end,
+               sm_step, s_.ctypes.data_as(_pint), t_.ctypes.data_as(_pint),
+               r_.ctypes.data_as(_pint), _ptr(w), capacity)
+        assert 0 <= n <= capacity
+        return {(int(s_[i]), int(t_[i]), int(r_[i])): float(w[i]) for i in range(n)}
+
     def _setup_observables(self):
         p = self.prefix
         sig = {

@@ -16,6 +16,8 @@
 //   polyakov_average_directions            lib/cpu/src/polyakov_loops.cpp:6-40
 //   wilson_offaxis[_adjoint], wilson_offaxis[_adjoint]_result
 //                         lib/cpu/include/wilson_loops.h:313-663
+//   smearing_APE_2d       lib/cpu/include/smearing.h:223-277
+//   wilson_spatial_3d_indexed              lib/cpu/include/wilson_loops.h:1384-1428
 //   Data::read_data_convert / write_data   lib/cpu/include/data.h:193-205,265-338
 //
 // Link exchange layout ("row-major"): link index 4*site+mu with
@@ -179,6 +181,22 @@ int read_conf(const int *dims, const char *path, const char *format,
   Data::LatticeData<DP, MT> conf({dims[0], dims[1], dims[2], dims[3]});
   Data::read_data_convert(conf, std::string(path), std::string(format),
                           bytes_skip, std::string(precision), convert != 0);
+  export_conf(conf, links);
+  return 0;
+}
+
+template <class MT>
+int ape_plane(const int *dims, double *links, int a, int b, double alpha, int steps) {
+  Data::LatticeData<DP, MT> conf = make_conf<MT>(dims, links);
+  DP dp(conf.lat_dim);
+  std::vector<MT> f1 = get_data_single_direction(conf, a);
+  std::vector<MT> f2 = get_data_single_direction(conf, b);
+  for (int i = 0; i < steps; i++)
+    smearing_APE_2d(f1, f2, dp, a, b, alpha);
+  for (size_t x = 0; x < f1.size(); x++) {
+    conf.array[4 * x + a] = f1[x];
+    conf.array[4 * x + b] = f2[x];
+  }
   export_conf(conf, links);
   return 0;
 }
@@ -380,6 +398,45 @@ int ref_wilson_offaxis(int nc, const int *dims, const double *links, int mode,
       }
       k++;
     }
+  }
+  return k;
+}
+
+// smearing_APE_2d on the direction fields a, b of a configuration (in place)
+int ref_ape_plane(int nc, const int *dims, double *links, int a, int b, double alpha,
+                  int steps) {
+  set_globals(dims);
+  if (nc == 2)
+    return ape_plane<su2>(dims, links, a, b, alpha, steps);
+  if (nc == 3)
+    return ape_plane<su3>(dims, links, a, b, alpha, steps);
+  return -1;
+}
+
+// wilson_spatial_3d_indexed: entries (smearing, T, R, W) in map order
+int ref_wilson_spatial_3d(int nc, const int *dims, const double *links, int rmin, int rmax,
+                          int tmin, int tmax, double alpha, int sm_start, int sm_end,
+                          int sm_step, int *out_s, int *out_t, int *out_r, double *out_w,
+                          int cap) {
+  set_globals(dims);
+  std::map<std::tuple<int, int, int>, double> m;
+  if (nc == 2)
+    m = wilson_spatial_3d_indexed(make_conf<su2>(dims, links), rmin, rmax, tmin, tmax, alpha,
+                                  sm_start, sm_end, sm_step);
+  else if (nc == 3)
+    m = wilson_spatial_3d_indexed(make_conf<su3>(dims, links), rmin, rmax, tmin, tmax, alpha,
+                                  sm_start, sm_end, sm_step);
+  else
+    return -1;
+  int k = 0;
+  for (const auto &kv : m) {
+    if (k < cap) {
+      out_s[k] = std::get<0>(kv.first);
+      out_t[k] = std::get<1>(kv.first);
+      out_r[k] = std::get<2>(kv.first);
+      out_w[k] = kv.second;
+    }
+    k++;
   }
   return k;
 }

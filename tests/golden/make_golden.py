@@ -14,7 +14,9 @@ wilson_gevp_adjoint_indexed); the time and space plaquettes after HYP+APE;
 the Polyakov loop and both correlator tables (D_max = 2) after HYP, with the
 reference's distance averages of the tables; the merged off-axis loops
 (wilson_offaxis_result, and wilson_offaxis_adjoint_result for SU(3)) after
-HYP+APE for R in [1, 2], T in [1, 2].
+HYP+APE for R in [1, 2], T in [1, 2]; two smearing_APE_2d steps of the
+(x, z) links after HYP; the spatial loops (wilson_spatial_3d_indexed) after
+HYP for R, T in [1, 2], alpha 0.5, smearing 1..3 measured every step.
 
 Run here (needs the reference sources and oracle/_ref):
     make -C oracle ref && python tests/golden/make_golden.py
@@ -71,6 +73,9 @@ def main() -> None:
         corr_c = ref.polyakov_correlator(nc, dims, links_hyp, d_max, False)
         avg_s = ref.polyakov_average_directions(corr_s, d_max)
         avg_c = ref.polyakov_average_directions(corr_c, d_max)
+        links_plane = links_hyp.copy()
+        ref.ape_plane(nc, dims, links_plane, 0, 2, 0.5, 2)
+        spatial = ref.wilson_spatial_3d(nc, dims, links_hyp, 1, 2, 1, 2, 0.5, 1, 3, 1)
         off = ref.wilson_offaxis_result(nc, dims, links_ape, 1.0, 2.0, 1, 2)
         off_adj = (ref.wilson_offaxis_result(nc, dims, links_ape, 1.0, 2.0, 1, 2, True)
                    if nc == 3 else {})
@@ -79,7 +84,7 @@ def main() -> None:
                             plaquettes=np.array([plaq0, plaq1]), gevp=gevp,
                             gevp_adjoint=gevp_adj, plaquettes_time_space=np.array([plaq_t, plaq_s]),
                             polyakov_loop=np.array([poly]), polyakov_singlet=corr_s,
-                            polyakov_color_average=corr_c)
+                            polyakov_color_average=corr_c, links_ape_plane=links_plane)
         index[name] = {"nc": nc, "dims": list(dims), "eps": eps, "seed": seed,
                        "config_index": cfg, "hyp_alpha": [a1, a2, a3], "ape_steps": n_ape,
                        "ape_alpha": alpha, "r_min": r0, "r_max": r1, "time_min": t0,
@@ -92,7 +97,10 @@ def main() -> None:
                        "polyakov_color_average_by_distance": [[k, v] for k, v in avg_c.items()],
                        "offaxis_range": [1.0, 2.0, 1, 2],
                        "offaxis": [[t, size, w] for (t, size), w in off.items()],
-                       "offaxis_adjoint": [[t, size, w] for (t, size), w in off_adj.items()]}
+                       "offaxis_adjoint": [[t, size, w] for (t, size), w in off_adj.items()],
+                       "ape_plane": [0, 2, 0.5, 2],
+                       "spatial_args": [1, 2, 1, 2, 0.5, 1, 3, 1],
+                       "spatial": [[sm, t, r, w] for (sm, t, r), w in spatial.items()]}
         print(name, "plaq", plaq0, "->", plaq1, "W[0,0]", w[0, 0])
     meta = {"generated_by": "tests/golden/make_golden.py",
             "reference_code": "oracle/_ref/libref_parity.so (lib/cpu smearing_HYP, "
@@ -102,7 +110,8 @@ def main() -> None:
                               "polyakov_loop_correlator_singlet, "
                               "polyakov_loop_correlator_color_average, "
                               "polyakov_average_directions, wilson_offaxis_result, "
-                              "wilson_offaxis_adjoint_result; -O2 -fno-fast-math)",
+                              "wilson_offaxis_adjoint_result, smearing_APE_2d, "
+                              "wilson_spatial_3d_indexed; -O2 -fno-fast-math)",
             "link_layout": "4*V links, link index 4*site+mu, row-major (get_data order)",
             "cases": index}
     (OUT / "index.json").write_text(json.dumps(meta, indent=1))

@@ -328,3 +328,39 @@ def test_offaxis_argument_errors():
         with pytest.raises(GCError):
             lat.wilson_offaxis([[1, 0, 0]], 1.0, 400.0, 1, 2)  # a line over 256 links
         assert lat.wilson_offaxis([[3, 0, 0]], 1.0, 2.0, 1, 2) == []  # no length in range
+
+
+@pytest.mark.parametrize("name,meta", CASES, ids=[c[0] for c in CASES])
+def test_fp64_spatial_loops_match_reference_fixture(name, meta):
+    """gc_ape_plane against the reference's smearing_APE_2d links, and the
+    spatial loop table against wilson_spatial_3d_indexed."""
+    g = load_golden(name)
+    nc, dims = meta["nc"], meta["dims"]
+    a, b, alpha, steps = meta["ape_plane"]
+    with Lattice(dims, nc, "fp64") as lat:
+        lat.upload(g["links_hyp"])
+        got = lat.wilson_spatial_3d(*meta["spatial_args"])
+        lat.ape_plane(a, b, alpha, steps)
+        assert max_abs(lat.download(), g["links_ape_plane"]) <= LINK_ATOL
+    want = {(s, t, r): w for s, t, r, w in meta["spatial"]}
+    assert set(got) == set(want)
+    for k, v in want.items():
+        assert got[k] == pytest.approx(v, rel=W_RTOL, abs=W_ATOL)
+
+
+@pytest.mark.parametrize("nc,eps", [(2, 0.3), (3, 0.25)])
+def test_spatial_loops_match_oracle_seeded(port, nc, eps):
+    """Larger, unequal lattice and the quirky ranges (r_min != time_min,
+    measurement every second step) in both forms: FP64 within 1e-12, mixed
+    within 1e-6 relative."""
+    dims = (6, 8, 7, 5)
+    links = generate_config(dims, nc, eps, 20261203, 61)
+    for args in ((1, 3, 1, 3, 0.5, 1, 4, 1), (2, 4, 1, 2, 0.45, 0, 4, 2)):
+        want = port.wilson_spatial_3d(nc, dims, links, *args)
+        for precision, rtol, atol in (("fp64", 1e-12, 1e-14), ("mixed", 1e-6, 1e-7)):
+            with Lattice(dims, nc, precision) as lat:
+                lat.upload(links)
+                got = lat.wilson_spatial_3d(*args)
+            assert set(got) == set(want)
+            for k, v in want.items():
+                assert got[k] == pytest.approx(v, rel=rtol, abs=atol)

@@ -238,3 +238,39 @@ def test_offaxis_of_unit_configuration_is_one(port, nc):
     dims = (4, 4, 4, 4)
     got = port.wilson_offaxis_result(nc, dims, unit_config(dims, nc), 1.0, 2.0, 1, 2)
     assert got and all(abs(v - 1.0) < 1e-14 for v in got.values())
+
+
+@pytest.mark.parametrize("name,meta", CASES, ids=[c[0] for c in CASES])
+def test_port_spatial_loops_match_reference_fixture(port, name, meta):
+    """smearing_APE_2d (bit for bit) and wilson_spatial_3d_indexed of the C
+    restatement against the reference's values."""
+    g = load_golden(name)
+    nc, dims = meta["nc"], meta["dims"]
+    a, b, alpha, steps = meta["ape_plane"]
+    links = g["links_hyp"].copy()
+    port.ape_plane(nc, dims, links, a, b, alpha, steps)
+    assert max_abs(links, g["links_ape_plane"]) <= 1e-13
+    got = port.wilson_spatial_3d(nc, dims, g["links_hyp"], *meta["spatial_args"])
+    want = {(s, t, r): w for s, t, r, w in meta["spatial"]}
+    assert set(got) == set(want)
+    for k, v in want.items():
+        assert got[k] == pytest.approx(v, rel=1e-12, abs=1e-14)
+
+
+@pytest.mark.parametrize("nc", [2, 3])
+def test_port_spatial_loops_match_reference_quirky_ranges(nc):
+    """Ranges where the reference's space lines start with length time_min
+    (r_min != time_min), a start above the step (only smearing 0 measured)
+    and steps of 2."""
+    from oracle import py_oracle
+    if not py_oracle.ref_available("parity"):
+        pytest.skip("reference not compiled in this checkout (oracle/_ref)")
+    port, ref = py_oracle.port(), py_oracle.ref("parity")
+    dims = (4, 5, 4, 6)
+    links = generate_config(dims, nc, 0.3 if nc == 2 else 0.25, 23, 0)
+    for args in ((1, 2, 2, 3, 0.5, 0, 4, 2), (2, 3, 1, 2, 0.4, 2, 3, 1), (1, 3, 1, 3, 0.5, 1, 2, 1)):
+        a = port.wilson_spatial_3d(nc, dims, links, *args)
+        b = ref.wilson_spatial_3d(nc, dims, links, *args)
+        assert set(a) == set(b)
+        for k, v in b.items():
+            assert a[k] == pytest.approx(v, rel=1e-12, abs=1e-14)
