@@ -50,6 +50,13 @@ SIGNATURES = {
     "gc_upload": (_c_int, [_p, _pdbl, _c_int]),
     "gc_download": (_c_int, [_p, _pdbl, _c_int]),
     "gc_copy_links": (_c_int, [_p, _p]),
+    "gc_upload_slices": (_c_int, [_p, _c_int, _c_int, _pdbl, _c_int]),
+    "gc_slice_bytes": (ctypes.c_longlong, [_p, _c_int]),
+    "gc_pack_slices": (_c_int, [_p, _c_int, _c_int, _p]),
+    "gc_unpack_slices": (_c_int, [_p, _c_int, _c_int, _p]),
+    "gc_copy_slices": (_c_int, [_p, _c_int, _p, _c_int, _c_int]),
+    "gc_wilson_onaxis_tslab": (_c_int, [_p, _c_int, _c_int, _c_int, _c_int, _c_int, _c_int,
+                                        _pdbl]),
     "gc_ape": (_c_int, [_p, _c_dbl, _c_int]),
     "gc_hyp": (_c_int, [_p, _c_dbl, _c_dbl, _c_dbl, _c_int]),
     "gc_wilson_onaxis": (_c_int, [_p, _c_int, _c_int, _c_int, _c_int, _pdbl]),

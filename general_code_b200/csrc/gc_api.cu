@@ -8,6 +8,7 @@
 #include <array>
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <functional>
 #include <map>
@@ -452,6 +453,164 @@ int gc_copy_links(gc_lattice *dst, gc_lattice *src) {
   return GC_OK;
 }
 
+// ---------------------------------------------------------------- t-slices
+// A run of time slices [t0, t0 + nt) is, in every plane of every direction's
+// field, one contiguous range of nt * Vs 16-byte elements (t varies slowest
+// over the sites): a slice copy is one 2-D copy per direction, with the
+// plane stride as the pitch.
+
+static size_t slice_planes(const gc_lattice *h) { return bytes_per_link(h->nc, h->prec) / 16; }
+
+static int check_slices(gc_lattice *h, int t0, int nt) {
+  if (!h)
+    return fail(nullptr, GC_ERR_ARG, "null handle");
+  if (t0 < 0 || nt < 0 || t0 + nt > h->g.L[3])
+    return fail(h, GC_ERR_ARG, "time slices outside the lattice");
+  return GC_OK;
+}
+
+// Copies nt slices of every direction between two SoA field sets; dst_t0 /
+// src_t0 are the first slices, dst_pitch / src_pitch the plane strides in
+// bytes (a packed buffer has pitch nt * Vs * 16).
+static cudaError_t copy_slice_planes(const gc_lattice *h, void *const dst[4], size_t dst_pitch,
+                                     int dst_t0, const void *const src[4], size_t src_pitch,
+                                     int src_t0, int nt, cudaMemcpyKind kind, cudaStream_t s) {
+  const size_t vs = (size_t)h->g.Vs;
+  const size_t width = (size_t)nt * vs * 16;
+  for (int d = 0; d < 4 && width; d++) {
+    cudaError_t e = cudaMemcpy2DAsync(
+        static_cast<unsigned char *>(dst[d]) + (size_t)dst_t0 * vs * 16, dst_pitch,
+        static_cast<const unsigned char *>(src[d]) + (size_t)src_t0 * vs * 16, src_pitch,
+        width, slice_planes(h), kind, s);
+    if (e != cudaSuccess)
+      return e;
+  }
+  return cudaSuccess;
+}
+
+long long gc_slice_bytes(const gc_lattice *h, int nt) {
+  if (!h || nt < 0)
+    return -1;
+  return 4LL * (long long)bytes_per_link(h->nc, h->prec) * h->g.Vs * nt;
+}
+
+int gc_upload_slices(gc_lattice *h, int t0, int nt, const double *host, int layout) {
+  int rc = check_slices(h, t0, nt);
+  if (rc)
+    return rc;
+  if (!host)
+    return fail(h, GC_ERR_ARG, "null argument");
+  if (layout != GC_LAYOUT_ROWMAJOR && layout != GC_LAYOUT_EIGEN_COLMAJOR)
+    return fail(h, GC_ERR_ARG, "unknown layout");
+  std::lock_guard<std::mutex> lk(h->mu);
+  rc = ensure_staging(h);
+  if (rc)
+    return rc;
+  const size_t sites = (size_t)nt * h->g.Vs;
+  const size_t bytes = (h->nc == 3 ? 18 : 4) * sizeof(double) * 4 * sites;
+  if (bytes) {
+    cudaError_t e = cudaMemcpyAsync(h->staging, host, bytes, cudaMemcpyHostToDevice, h->stream);
+    if (e != cudaSuccess)
+      return cuda_fail(h, "cudaMemcpyAsync(upload slices)", e);
+  }
+  rc = launch_aos_to_soa(h->g, h->nc, h->prec, layout, h->staging, h->cur, h->stream,
+                         t0 * h->g.Vs, (int)sites);
+  if (rc)
+    return launch_fail(h, rc);
+  h->has_links = true;
+  return GC_OK;
+}
+
+int gc_pack_slices(gc_lattice *h, int t0, int nt, void *dev_buf) {
+  int rc = check_ready(h);
+  if (rc)
+    return rc;
+  rc = check_slices(h, t0, nt);
+  if (rc)
+    return rc;
+  if (!dev_buf)
+    return fail(h, GC_ERR_ARG, "null buffer");
+  std::lock_guard<std::mutex> lk(h->mu);
+  const size_t per_dir = slice_planes(h) * (size_t)nt * h->g.Vs * 16;
+  void *dst[4];
+  for (int d = 0; d < 4; d++)
+    dst[d] = static_cast<unsigned char *>(dev_buf) + d * per_dir;
+  cudaError_t e = copy_slice_planes(h, dst, (size_t)nt * h->g.Vs * 16, 0, h->cur.f,
+                                    16 * (size_t)h->g.V, t0, nt, cudaMemcpyDeviceToDevice,
+                                    h->stream);
+  if (e != cudaSuccess)
+    return cuda_fail(h, "cudaMemcpy2DAsync(pack slices)", e);
+  return GC_OK;
+}
+
+int gc_unpack_slices(gc_lattice *h, int t0, int nt, const void *dev_buf) {
+  int rc = check_slices(h, t0, nt);
+  if (rc)
+    return rc;
+  if (!dev_buf)
+    return fail(h, GC_ERR_ARG, "null buffer");
+  std::lock_guard<std::mutex> lk(h->mu);
+  const size_t per_dir = slice_planes(h) * (size_t)nt * h->g.Vs * 16;
+  const void *src[4];
+  for (int d = 0; d < 4; d++)
+    src[d] = static_cast<const unsigned char *>(dev_buf) + d * per_dir;
+  cudaError_t e = copy_slice_planes(h, h->cur.f, 16 * (size_t)h->g.V, t0, src,
+                                    (size_t)nt * h->g.Vs * 16, 0, nt,
+                                    cudaMemcpyDeviceToDevice, h->stream);
+  if (e != cudaSuccess)
+    return cuda_fail(h, "cudaMemcpy2DAsync(unpack slices)", e);
+  h->has_links = true;
+  return GC_OK;
+}
+
+int gc_copy_slices(gc_lattice *dst, int dst_t0, gc_lattice *src, int src_t0, int nt) {
+  if (!dst || !src)
+    return fail(dst, GC_ERR_ARG, "null handle");
+  int rc = check_ready(src);
+  if (rc)
+    return fail(dst, rc, std::string("source: ") + src->err);
+  bool same = dst->nc == src->nc && dst->prec == src->prec;
+  for (int d = 0; d < 3; d++)
+    same = same && dst->g.L[d] == src->g.L[d];
+  if (!same)
+    return fail(dst, GC_ERR_ARG,
+                "gc_copy_slices: handles differ in spatial extents, group or precision");
+  rc = check_slices(dst, dst_t0, nt);
+  if (rc)
+    return rc;
+  if (src_t0 < 0 || src_t0 + nt > src->g.L[3])
+    return fail(dst, GC_ERR_ARG, "source time slices outside the lattice");
+  if (dst == src) {
+    if (nt && dst_t0 != src_t0 && std::abs(dst_t0 - src_t0) < nt)
+      return fail(dst, GC_ERR_ARG, "overlapping slice ranges in one lattice");
+  }
+  std::unique_lock<std::mutex> lk1, lk2;
+  if (dst != src) {
+    gc_lattice *a = std::less<gc_lattice *>()(dst, src) ? dst : src;
+    gc_lattice *b = a == dst ? src : dst;
+    lk1 = std::unique_lock<std::mutex>(a->mu);
+    lk2 = std::unique_lock<std::mutex>(b->mu);
+  } else {
+    lk1 = std::unique_lock<std::mutex>(dst->mu);
+  }
+  if (src->stream != dst->stream) {
+    cudaEvent_t ev;
+    cudaError_t e = cudaEventCreateWithFlags(&ev, cudaEventDisableTiming);
+    if (e != cudaSuccess)
+      return cuda_fail(dst, "cudaEventCreate", e);
+    cudaEventRecord(ev, src->stream);
+    cudaStreamWaitEvent(dst->stream, ev, 0);
+    cudaEventDestroy(ev);
+  }
+  cudaError_t e = copy_slice_planes(dst, dst->cur.f, 16 * (size_t)dst->g.V, dst_t0, src->cur.f,
+                                    16 * (size_t)src->g.V, src_t0, nt,
+                                    cudaMemcpyDeviceToDevice, dst->stream);
+  if (e != cudaSuccess)
+    return cuda_fail(dst, "cudaMemcpy2DAsync(copy slices)", e);
+  dst->has_links = true;
+  return GC_OK;
+}
+
 int gc_ape(gc_lattice *h, double alpha, int steps) {
   int rc = check_ready(h);
   if (rc)
@@ -504,7 +663,8 @@ int gc_hyp(gc_lattice *h, double a1, double a2, double a3, int steps) {
 // W(R,T) of h, or with `second` the GEVP loops of the pair (h, second):
 // h's time lines, space lines of both (wilson_gevp_indexed).
 static int wilson_impl(gc_lattice *h, int rmin, int rmax, int tmin, int tmax,
-                       double *out, bool adjoint, gc_lattice *second = nullptr) {
+                       double *out, bool adjoint, gc_lattice *second = nullptr,
+                       int tstarts = 0) {
   int rc = check_ready(h);
   if (rc)
     return rc;
@@ -564,7 +724,7 @@ static int wilson_impl(gc_lattice *h, int rmin, int rmax, int tmin, int tmax,
     const int r1 = std::min(rmax, r0 + rchunk - 1);
     const int ncr = r1 - r0 + 1;
     rc = GC_DISPATCH(h, launch_wilson, h->g, h->cur, r0, r1, tmin, tmax,
-                     h->partials, chunk_out, h->stream, adjoint, u2);
+                     h->partials, chunk_out, h->stream, adjoint, u2, tstarts);
     if (rc)
       return launch_fail(h, rc);
     // chunk_out[(T-tmin)*ncr + (R-r0)] -> dev_out[(T-tmin)*nr + (R-rmin)]
@@ -593,6 +753,13 @@ int gc_wilson_onaxis(gc_lattice *h, int rmin, int rmax, int tmin, int tmax,
 int gc_wilson_adjoint_onaxis(gc_lattice *h, int rmin, int rmax, int tmin, int tmax,
                              double *out) {
   return wilson_impl(h, rmin, rmax, tmin, tmax, out, true);
+}
+
+int gc_wilson_onaxis_tslab(gc_lattice *h, int t_starts, int rmin, int rmax, int tmin,
+                           int tmax, int adjoint, double *out) {
+  if (h && (t_starts < 1 || t_starts > h->g.L[3]))
+    return fail(h, GC_ERR_ARG, "t_starts must be in [1, Lt]");
+  return wilson_impl(h, rmin, rmax, tmin, tmax, out, adjoint != 0, nullptr, t_starts);
 }
 
 int gc_wilson_gevp_onaxis(gc_lattice *h1, gc_lattice *h2, int rmin, int rmax, int tmin,

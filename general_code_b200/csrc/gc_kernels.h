@@ -130,10 +130,14 @@ WilsonPlan wilson_plan(const Geom &g, int nr, int nt, int nc, int ct_bytes, int 
 // adjoint: the adjoint-representation loop |Tr W|^2 - 1 instead of Re Tr W/N.
 // second: a second configuration of the same lattice for the GEVP loops
 // (wilson_gevp_indexed): its space lines pair with U's, time lines from U.
+// tstarts > 0: only loops whose lower edge lies on the slices [0, tstarts)
+// are counted, and the result is their average (a t-slab whose forward halo
+// occupies the slices above).
 template <class Store, class CT>
 int launch_wilson(const Geom &g, const Fields4 &U, int rmin, int rmax,
                   int tmin, int tmax, double *partials, double *out_dev,
-                  cudaStream_t s, bool adjoint = false, const Fields4 *second = nullptr);
+                  cudaStream_t s, bool adjoint = false, const Fields4 *second = nullptr,
+                  int tstarts = 0);
 
 // An explicit block shape (rows must divide Lt, at most 256 threads).
 WilsonPlan wilson_plan_shape(const Geom &g, int nr, int nt, int nc, int ct_bytes, int rows,
@@ -230,8 +234,11 @@ int launch_polyakov_correlator(const Geom &g, int nc, const double2 *lines, cons
 size_t wilson_partials_count(const Geom &g, int nr, int nt, int nc, int sets = 3);
 
 // Host AoS (uploaded raw to a device staging buffer) <-> device SoA fields.
+// The upload converts the sites [site0, site0 + nsites) (all of them when
+// nsites < 0); the staging buffer holds exactly those sites' links.
 int launch_aos_to_soa(const Geom &g, int nc, int prec, int layout,
-                      const double *staging, const Fields4 &U, cudaStream_t s);
+                      const double *staging, const Fields4 &U, cudaStream_t s,
+                      int site0 = 0, int nsites = -1);
 int launch_soa_to_aos(const Geom &g, int nc, int prec, int layout,
                       const Fields4 &U, double *staging, cudaStream_t s);
 

@@ -1,7 +1,10 @@
 // Conversion between the reference's host link layout (array of structures,
 // link index 4*site+mu; data.h:78-112, indexing.h:111-123) and the device
 // structure-of-arrays fields. The host array is copied verbatim into a device
-// staging buffer first; one thread then converts one link.
+// staging buffer first; one thread then converts one link. The host-to-device
+// direction takes a window of sites [site0, site0 + nsites): the staging
+// buffer holds just those sites' links (a run of time slices of a larger
+// lattice, whose sites are contiguous because t varies slowest).
 #include "gc_internal.cuh"
 #include "gc_kernels.h"
 
@@ -16,11 +19,11 @@ __device__ __forceinline__ int su3_off(int layout, int i, int j) {
 
 template <class Store>
 __global__ void aos_to_soa_su3(Geom g, int layout, const double *__restrict__ in,
-                               Fields4 U) {
+                               Fields4 U, int site0, int nsites) {
   const long long l = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (l >= 4LL * g.V)
+  if (l >= 4LL * nsites)
     return;
-  const int site = (int)(l >> 2), mu = (int)(l & 3);
+  const int site = site0 + (int)(l >> 2), mu = (int)(l & 3);
   const double *p = in + l * 18;
   SU3<double> m;
 #pragma unroll
@@ -53,11 +56,12 @@ __global__ void soa_to_aos_su3(Geom g, int layout, Fields4 U,
 }
 
 template <class Store>
-__global__ void aos_to_soa_su2(Geom g, const double *__restrict__ in, Fields4 U) {
+__global__ void aos_to_soa_su2(Geom g, const double *__restrict__ in, Fields4 U, int site0,
+                               int nsites) {
   const long long l = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (l >= 4LL * g.V)
+  if (l >= 4LL * nsites)
     return;
-  const int site = (int)(l >> 2), mu = (int)(l & 3);
+  const int site = site0 + (int)(l >> 2), mu = (int)(l & 3);
   const double2 a = reinterpret_cast<const double2 *>(in)[2 * l];
   const double2 b = reinterpret_cast<const double2 *>(in)[2 * l + 1];
   Store::template store<double>(U.f[mu], g.V, site,
@@ -78,20 +82,27 @@ __global__ void soa_to_aos_su2(Geom g, Fields4 U, double *__restrict__ out) {
 } // namespace
 
 int launch_aos_to_soa(const Geom &g, int nc, int prec, int layout,
-                      const double *staging, const Fields4 &U, cudaStream_t s) {
-  const long long n = 4LL * g.V;
+                      const double *staging, const Fields4 &U, cudaStream_t s, int site0,
+                      int nsites) {
+  if (nsites < 0)
+    nsites = g.V - site0;
+  if (site0 < 0 || nsites < 0 || site0 + nsites > g.V)
+    return plan_error("aos_to_soa: site window outside the lattice");
+  if (nsites == 0)
+    return GC_OK;
+  const long long n = 4LL * nsites;
   const int blk = 256;
   const unsigned grid = (unsigned)((n + blk - 1) / blk);
   if (nc == 3) {
     if (prec == 0)
-      aos_to_soa_su3<StoreF64SU3><<<grid, blk, 0, s>>>(g, layout, staging, U);
+      aos_to_soa_su3<StoreF64SU3><<<grid, blk, 0, s>>>(g, layout, staging, U, site0, nsites);
     else
-      aos_to_soa_su3<StoreF32SU3><<<grid, blk, 0, s>>>(g, layout, staging, U);
+      aos_to_soa_su3<StoreF32SU3><<<grid, blk, 0, s>>>(g, layout, staging, U, site0, nsites);
   } else {
     if (prec == 0)
-      aos_to_soa_su2<StoreF64SU2><<<grid, blk, 0, s>>>(g, staging, U);
+      aos_to_soa_su2<StoreF64SU2><<<grid, blk, 0, s>>>(g, staging, U, site0, nsites);
     else
-      aos_to_soa_su2<StoreF32SU2><<<grid, blk, 0, s>>>(g, staging, U);
+      aos_to_soa_su2<StoreF32SU2><<<grid, blk, 0, s>>>(g, staging, U, site0, nsites);
   }
   return launch_check("aos_to_soa");
 }

@@ -228,7 +228,8 @@ template <class Store, class CT, bool ADJ = false, bool GEVP = false>
 __device__ __forceinline__ void wilson_block(const Geom &g, const Fields4 &U, const Fields4 &U2,
                                              int rmin, int rmax, int tmin, int tmax, int cols,
                                              int rows, int colblock, int nu,
-                                             double *part, unsigned char *smem_raw) {
+                                             double *part, unsigned char *smem_raw,
+                                             int tstarts) {
   constexpr int LANES = wilson_lanes(Store::NC, sizeof(CT));
   using LL = LaneLoad<Store, CT, LANES>;
   using M = typename LL::M;
@@ -313,18 +314,23 @@ __device__ __forceinline__ void wilson_block(const Geom &g, const Fields4 &U, co
 #pragma unroll 1
         for (int k = 0; k < kt; k++) {
           const int t0 = row + k * rows;
-          M K = active ? CS::load(sbot, nslots, t0 * units + u) : unit(M());
+          // loops start on the slices [0, tstarts) only (all of them unless
+          // the lattice is a t-slab with its forward halo)
+          const bool counted = active && t0 < tstarts;
+          if (!__any_sync(0xffffffffu, counted))
+            continue; // warp-uniform
+          M K = counted ? CS::load(sbot, nslots, t0 * units + u) : unit(M());
           int tt = t0; // (t0 + T - 1) mod Lt
 #pragma unroll 1
           for (int T = 1; T <= tmax; T++) {
             int tu = tt + 1; // (t0 + T) mod Lt
             tu = (tu == Lt) ? 0 : tu;
-            if (active) {
+            if (counted) {
               const int i = tt * units + u;
               K = mul(mul_da(CS::load(ucol, nslots, i), K), CS::load(ncol, nslots, i));
             }
             if (T >= tmin) {
-              double term = active
+              double term = counted
                   ? loop_value<ADJ>(CS::load(stop, nslots, tu * units + u), K, lane1)
                   : 0.0;
               term = warp_sum(term);
@@ -352,12 +358,12 @@ template <class Store, class CT, bool ADJ, bool GEVP>
 __global__ void __launch_bounds__(256)
     wilson_kernel(const __grid_constant__ Geom g, const __grid_constant__ Fields4 U,
                   const __grid_constant__ Fields4 U2, int rmin, int rmax, int tmin, int tmax,
-                  int cols, int rows, double *partials) {
+                  int cols, int rows, double *partials, int tstarts) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const size_t blk = (size_t)blockIdx.y * gridDim.x + blockIdx.x;
   const int ne = (rmax - rmin + 1) * (tmax - tmin + 1);
   wilson_block<Store, CT, ADJ, GEVP>(g, U, U2, rmin, rmax, tmin, tmax, cols, rows, blockIdx.x,
-                                     blockIdx.y, partials + blk * ne, smem_raw);
+                                     blockIdx.y, partials + blk * ne, smem_raw, tstarts);
 }
 
 // Several lattices in one launch. A block finds its lattice by binary search
@@ -386,7 +392,7 @@ __global__ void __launch_bounds__(256)
   wilson_block<Store, CT, false>(jb.g, jb.U, jb.U, jb.rmin, jb.rmax, jb.tmin, jb.tmax, jb.cols,
                                  jb.rows, colblock, nu,
                                  jb.partials + ((size_t)nu * colblocks + colblock) * ne,
-                                 smem_raw);
+                                 smem_raw, jb.g.L[3]);
 }
 
 // Fixed-order reduction of several lattices' partials; block = (lattice,
@@ -570,8 +576,11 @@ int plaquette_partials_count(const Geom &g) { return 2 * ((g.V + 255) / 256); }
 
 template <class Store, class CT, bool ADJ, bool GEVP>
 int launch_wilson_mode(const Geom &g, const Fields4 &U, const Fields4 &U2, int rmin, int rmax,
-                       int tmin, int tmax, double *partials, double *out_dev, cudaStream_t s) {
+                       int tmin, int tmax, double *partials, double *out_dev, cudaStream_t s,
+                       int tstarts) {
   const int nr = rmax - rmin + 1, nt = tmax - tmin + 1;
+  if (tstarts <= 0 || tstarts > g.L[3])
+    tstarts = g.L[3];
   WilsonPlan p = wilson_plan(g, nr, nt, Store::NC, (int)sizeof(CT), GEVP ? 4 : 3);
   if (!p.fits || nr * nt > kWilsonMaxEntries)
     return plan_error("wilson_kernel: time extent or (R,T) range too large for "
@@ -580,12 +589,14 @@ int launch_wilson_mode(const Geom &g, const Fields4 &U, const Fields4 &U2, int r
   if (rc)
     return rc;
   wilson_kernel<Store, CT, ADJ, GEVP><<<dim3(p.blocks / 3, 3), p.threads, p.smem, s>>>(
-      g, U, U2, rmin, rmax, tmin, tmax, p.cols_per_block, p.rows, partials);
+      g, U, U2, rmin, rmax, tmin, tmax, p.cols_per_block, p.rows, partials, tstarts);
   rc = launch_check("wilson_kernel");
   if (rc)
     return rc;
+  // average over the loops counted (all V sites, or the tstarts slices);
   // GEVP counts every loop twice (the / (6 V) of wilson_loops.h:910, 954)
-  const double scale = wilson_scale(g.V, Store::NC, ADJ) / (GEVP ? 2.0 : 1.0);
+  const double scale =
+      wilson_scale((long long)g.Vs * tstarts, Store::NC, ADJ) / (GEVP ? 2.0 : 1.0);
   reduce_partials_kernel<<<nr * nt, 256, 0, s>>>(partials, p.blocks, nr * nt, nr, nt, scale,
                                                  out_dev);
   return launch_check("reduce_partials_kernel");
@@ -594,16 +605,16 @@ int launch_wilson_mode(const Geom &g, const Fields4 &U, const Fields4 &U2, int r
 template <class Store, class CT>
 int launch_wilson(const Geom &g, const Fields4 &U, int rmin, int rmax,
                   int tmin, int tmax, double *partials, double *out_dev,
-                  cudaStream_t s, bool adjoint, const Fields4 *second) {
+                  cudaStream_t s, bool adjoint, const Fields4 *second, int tstarts) {
   if (second)
-    return adjoint ? launch_wilson_mode<Store, CT, true, true>(g, U, *second, rmin, rmax, tmin,
-                                                               tmax, partials, out_dev, s)
-                   : launch_wilson_mode<Store, CT, false, true>(g, U, *second, rmin, rmax,
-                                                                tmin, tmax, partials, out_dev, s);
+    return adjoint ? launch_wilson_mode<Store, CT, true, true>(
+                         g, U, *second, rmin, rmax, tmin, tmax, partials, out_dev, s, tstarts)
+                   : launch_wilson_mode<Store, CT, false, true>(
+                         g, U, *second, rmin, rmax, tmin, tmax, partials, out_dev, s, tstarts);
   return adjoint ? launch_wilson_mode<Store, CT, true, false>(g, U, U, rmin, rmax, tmin, tmax,
-                                                              partials, out_dev, s)
+                                                              partials, out_dev, s, tstarts)
                  : launch_wilson_mode<Store, CT, false, false>(g, U, U, rmin, rmax, tmin, tmax,
-                                                               partials, out_dev, s);
+                                                               partials, out_dev, s, tstarts);
 }
 
 // out_dev[0] = spatial-plane average (plaket_space), out_dev[1] = (mu, t)
@@ -650,7 +661,7 @@ int launch_wilson_plan(const Geom &g, const Fields4 &U, int rmin, int rmax, int 
   if (rc)
     return rc;
   wilson_kernel<Store, CT, false, false><<<dim3(p.blocks / 3, 3), p.threads, p.smem, s>>>(
-      g, U, U, rmin, rmax, tmin, tmax, p.cols_per_block, p.rows, partials);
+      g, U, U, rmin, rmax, tmin, tmax, p.cols_per_block, p.rows, partials, g.L[3]);
   rc = launch_check("wilson_kernel");
   if (rc)
     return rc;
@@ -712,7 +723,8 @@ int launch_reduce_batch(const RJob *jobs, int njobs, int entries, cudaStream_t s
 #define GC_INSTANTIATE_W(STORE, CT)                                            \
   template int launch_wilson<STORE, CT>(const Geom &, const Fields4 &, int,   \
                                         int, int, int, double *, double *,    \
-                                        cudaStream_t, bool, const Fields4 *); \
+                                        cudaStream_t, bool, const Fields4 *,  \
+                                        int);                                 \
   template int launch_plaquette<STORE, CT>(const Geom &, const Fields4 &,     \
                                            double *, double *, cudaStream_t);  \
   template int launch_wilson_batch<STORE, CT>(const WJob *, int, int, int,     \

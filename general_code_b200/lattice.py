@@ -141,6 +141,51 @@ class Lattice:
         """Device-to-device copy of other's links (same shape and precision)."""
         self._check(lib().gc_copy_links(self._h, other.handle))
 
+    # --- time slices (t-slab decomposition; see general_code_b200.tslab)
+    def upload_slices(self, t0: int, links: np.ndarray, layout: str = "rowmajor") -> None:
+        """Uploads host links of whole time slices (4 links per site, the
+        reference's layout, t slowest) into the slices starting at t0."""
+        a = np.ascontiguousarray(links, dtype=np.float64)
+        per_slice = 4 * self.dims[0] * self.dims[1] * self.dims[2] * link_size(self.nc)
+        if a.size % per_slice:
+            raise ValueError("link array is not a whole number of time slices")
+        self._check(lib().gc_upload_slices(self._h, int(t0), a.size // per_slice, dbl_ptr(a),
+                                           _LAYOUT[layout]))
+        if a is not links:
+            self.synchronize()
+
+    def slice_bytes(self, nt: int) -> int:
+        """Bytes of nt packed time slices in this lattice's device form."""
+        n = lib().gc_slice_bytes(self._h, int(nt))
+        if n < 0:
+            raise GCError(GC_ERR_ARG, "bad slice count")
+        return int(n)
+
+    def pack_slices(self, t0: int, nt: int, dev_ptr: int) -> None:
+        """Packs the slices [t0, t0+nt) into the device buffer at dev_ptr."""
+        self._check(lib().gc_pack_slices(self._h, int(t0), int(nt), ctypes.c_void_p(dev_ptr)))
+
+    def unpack_slices(self, t0: int, nt: int, dev_ptr: int) -> None:
+        """Fills the slices [t0, t0+nt) from the packed device buffer at dev_ptr."""
+        self._check(lib().gc_unpack_slices(self._h, int(t0), int(nt),
+                                           ctypes.c_void_p(dev_ptr)))
+
+    def copy_slices_from(self, dst_t0: int, other: "Lattice", src_t0: int, nt: int) -> None:
+        """Device copy of other's slices [src_t0, src_t0+nt) to [dst_t0, dst_t0+nt)."""
+        self._check(lib().gc_copy_slices(self._h, int(dst_t0), other.handle, int(src_t0),
+                                         int(nt)))
+
+    def wilson_loop_tslab(self, t_starts: int, r_min: int, r_max: int, time_min: int,
+                          time_max: int, adjoint: bool = False) -> np.ndarray:
+        """W table averaged over the loops whose lower edge lies on the slices
+        [0, t_starts) (a t-slab with its forward halo above); same layout as
+        wilson_loop."""
+        out = np.empty((time_max - time_min + 1, r_max - r_min + 1), dtype=np.float64)
+        self._check(lib().gc_wilson_onaxis_tslab(self._h, int(t_starts), int(r_min), int(r_max),
+                                                 int(time_min), int(time_max), int(bool(adjoint)),
+                                                 dbl_ptr(out)))
+        return out
+
     def generate(self, eps: float, seed: int, index: int = 0, gauge: bool = True) -> None:
         self._check(lib().gc_generate(self._h, float(eps), int(seed) & 0xffffffff,
                                       int(index) & 0xffffffff, int(bool(gauge))))

@@ -98,6 +98,49 @@ int gc_download(gc_lattice *h, double *host_links, int layout);
  * copy-assignment of LatticeData (data.h:78-93), e.g. `smeared = conf`. */
 int gc_copy_links(gc_lattice *dst, gc_lattice *src);
 
+/* ---- time slices (t-slab decomposition of one lattice over several GPUs).
+ * The reference has no domain decomposition (it runs one lattice on the
+ * OpenMP threads of one node); these entry points are the pieces a
+ * decomposition over time slabs needs: a slab lattice of Lt_slab slices is
+ * filled from the slices of a larger lattice, smeared, its smeared slices
+ * exchanged with the neighbouring slabs, and its Wilson loops counted from
+ * its own slices only (gc_wilson_onaxis_tslab). Slices are whole time
+ * slices t = const of all four directions (sites with t varying slowest, as
+ * in the reference's lexicographic order, indexing.h:71-126). */
+
+/* Uploads nt time slices of host links (layout GC_LAYOUT_*) into the slices
+ * [t0, t0 + nt) of the lattice: host_links holds the 4 * nt * Lx*Ly*Lz links
+ * of those slices, i.e. the run of a larger lattice's host array starting at
+ * its slice (link index 4*site+mu, site of the first slice = 0). */
+int gc_upload_slices(gc_lattice *h, int t0, int nt, const double *host_links, int layout);
+
+/* Bytes of nt time slices of all four directions in the handle's device
+ * form (the size of a gc_pack_slices buffer); -1 for a bad argument. */
+long long gc_slice_bytes(const gc_lattice *h, int nt);
+
+/* Packs the device links of the slices [t0, t0 + nt) into the device buffer
+ * dev_buf (gc_slice_bytes(h, nt) bytes, 16-byte aligned), queued on the
+ * handle's stream; gc_unpack_slices is the inverse. The packed form is the
+ * handle's own (FP64 or mixed), for an exchange between handles of the same
+ * spatial extents, group and precision (e.g. over NCCL). */
+int gc_pack_slices(gc_lattice *h, int t0, int nt, void *dev_buf);
+int gc_unpack_slices(gc_lattice *h, int t0, int nt, const void *dev_buf);
+
+/* Device-to-device copy of the slices [src_t0, src_t0 + nt) of src into the
+ * slices [dst_t0, dst_t0 + nt) of dst (same Lx, Ly, Lz, group and precision;
+ * Lt may differ), queued on dst's stream after src's queued work. */
+int gc_copy_slices(gc_lattice *dst, int dst_t0, gc_lattice *src, int src_t0, int nt);
+
+/* On-axis Wilson loops (adjoint != 0: the adjoint representation) counted
+ * only from the lower-edge slices t in [0, t_starts), averaged over those
+ * loops (3 * Lx*Ly*Lz * t_starts of them); the slices above hold the forward
+ * halo of a t-slab, at least time_max slices deep so no loop wraps. The
+ * global average over slabs is sum_slab W_slab * t_starts / Lt. Same output
+ * layout as gc_wilson_onaxis. With t_starts = Lt it is gc_wilson_onaxis
+ * (wilson_loops.h:1047-1074). */
+int gc_wilson_onaxis_tslab(gc_lattice *h, int t_starts, int r_min, int r_max, int time_min,
+                           int time_max, int adjoint, double *out);
+
 /* One or more APE steps on the spatial links (temporal links unchanged):
  * U'_i = Proj[(1-alpha) U_i + alpha/4 sum_{j != i, j < 3} staples].
  * Replaces: smearing_APE(conf, alpha) (smearing.h:115-161), called steps
