@@ -10,7 +10,12 @@ the headline metric is quoted on). Metric: smeared+measured sites/s.
            from a resident copy (device-to-device) and runs the job; inputs are
            in HBM when the timed region starts.
   e2e    : the same job through the public C ABI with HOST buffers: pinned
-           host links -> gc_upload, gc_hyp, gc_ape, gc_wilson_onaxis -> host.
+           host links -> gc_upload, gc_hyp, gc_ape, gc_wilson_onaxis -> host,
+           for a stream of K configurations through two handles on two CUDA
+           streams (job i+1's upload overlaps job i's smearing and
+           measurement); every job's upload and result read lie inside the
+           timed region. `e2e.serial_value` is the same with one handle, each
+           job's upload, compute and result read one after the other.
 Both forms are timed on the same configuration (--form both, the default):
 the headline is the mixed form (FP32 links, FP64 projection and sums); the
 FP64 form is reported under "forms", with the largest relative difference of
@@ -338,7 +343,7 @@ def run_reference(args, wl, rank):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--form", choices=["both", "fp64", "mixed"], default="both")
@@ -427,6 +432,37 @@ def main():
                                e2.elapsed_time(e3)))
             return w
 
+        stream2 = torch.cuda.Stream()
+        work2 = Lattice(dims, nc, form)
+        work2.set_stream(stream2.cuda_stream)
+        pair = ((work, stream), (work2, stream2))
+
+        def e2e_pipelined(k, record):
+            # two handles: job i+1's upload (pinned host -> device, on the
+            # other handle's stream) is issued before job i's result is read,
+            # so the copy engine overlaps job i's kernels; the other handle is
+            # idle then (its previous job's result has been read)
+            e0 = ev()
+            stream2.wait_event(e0)
+            pair[0][0].upload(host)
+            w = None
+            for i in range(k):
+                lat, s = pair[i % 2]
+                with torch.cuda.stream(s):
+                    flush_buf.fill_(1.0)
+                lat.hyp(*wl["hyp"], 1)
+                lat.ape(wl["alpha"], wl["ape"])
+                if i + 1 < k:
+                    pair[(i + 1) % 2][0].upload(host)
+                w = lat.wilson_loop(r0, r1, t0, t1)
+            last = pair[(k - 1) % 2][1]
+            e1 = torch.cuda.Event(enable_timing=True)
+            e1.record(last)
+            last.synchronize()
+            if record is not None:
+                record.append(e0.elapsed_time(e1))
+            return w
+
         def e2e_step(record):
             flush()
             e0 = ev()
@@ -455,17 +491,27 @@ def main():
             w_e2e = e2e_step(rec_e2e)
         barrier()
         assert np.array_equal(w, w_e2e), "device and end-to-end runs disagree"
+        e2e_pipelined(max(2, args.warmup), None)
+        barrier()
+        rec_pipe = []
+        w_pipe = e2e_pipelined(args.steps, rec_pipe)
+        barrier()
+        assert np.array_equal(w, w_pipe), "device and pipelined end-to-end runs disagree"
         pristine.close()
         work.close()
+        work2.close()
         total_ms = max_over_ranks(sum(r[0] for r in rec))
-        total_e2e_ms = max_over_ranks(sum(rec_e2e))
+        total_e2e_ms = max_over_ranks(sum(rec_pipe))
+        total_serial_ms = max_over_ranks(sum(rec_e2e))
         return {"w": w, "total_ms": total_ms, "total_e2e_ms": total_e2e_ms,
+                "total_serial_ms": total_serial_ms,
                 "hyp_ms": sum(r[1] for r in rec) / args.steps,
                 "ape_ms": sum(r[2] for r in rec) / args.steps,
                 "w_ms": sum(r[3] for r in rec) / args.steps,
-                # our kernels per timed step: HYP 3 + APE n + W 2; e2e adds the
-                # layout conversion
-                "launches": args.steps * (3 + wl["ape"] + 2) * 2 + args.steps}
+                # our kernels per timed step: HYP 3 + APE n + W 2, in the
+                # device-resident, serial and pipelined end-to-end runs; the
+                # two end-to-end runs add the layout conversion
+                "launches": args.steps * (3 + wl["ape"] + 2) * 3 + 2 * args.steps}
 
     forms = ["mixed", "fp64"] if args.form == "both" else [args.form]
     sampler = ClockSampler(local_rank)
@@ -495,6 +541,7 @@ def main():
         return {
             "value": world * V * args.steps / (r["total_ms"] * 1e-3),
             "e2e_value": world * V * args.steps / (r["total_e2e_ms"] * 1e-3),
+            "e2e_serial": world * V * args.steps / (r["total_serial_ms"] * 1e-3),
             "ms_per_step": r["total_ms"] / args.steps,
             "phases_ms": {"hyp": r["hyp_ms"], "ape_total": r["ape_ms"],
                           "ape_per_step": r["ape_ms"] / wl["ape"], "wilson": r["w_ms"]},
@@ -531,7 +578,9 @@ def main():
         "roofline": hs["roofline"],
         "e2e": {"value": hs["e2e_value"], "unit": "sites/s",
                 "h2d_bytes_per_step": int(host.nbytes),
-                "d2h_bytes_per_step": int(hr["w"].nbytes)},
+                "d2h_bytes_per_step": int(hr["w"].nbytes),
+                "mode": "two handles on two streams: job i+1's upload overlaps job i",
+                "serial_value": hs["e2e_serial"]},
         "gpu_launches": sum(results[f]["launches"] for f in forms),
         "clocks": clocks,
     }
@@ -540,6 +589,7 @@ def main():
         line["mixed_vs_fp64"] = {"max_rel_err_W": float(np.max(np.abs(wm - wd) / np.abs(wd))),
                                  "tolerance": 1e-6}
         line["forms"] = {f: {"value": sums[f]["value"], "e2e": sums[f]["e2e_value"],
+                             "e2e_serial": sums[f]["e2e_serial"],
                              "ms_per_step": sums[f]["ms_per_step"],
                              "phases_ms": sums[f]["phases_ms"],
                              "roofline": sums[f]["roofline"]} for f in forms}

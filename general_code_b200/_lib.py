@@ -120,7 +120,7 @@ class ServerOpts(ctypes.Structure):
     _fields_ = [("slots", ctypes.c_int), ("precision", ctypes.c_int),
                 ("memory_budget", ctypes.c_longlong), ("queue_capacity", ctypes.c_int),
                 ("free_bytes", FREE_BYTES_FN), ("free_bytes_ctx", ctypes.c_void_p),
-                ("simulate_us", ctypes.c_int)]
+                ("simulate_us", ctypes.c_int), ("reserve_bytes", ctypes.c_longlong)]
 
 
 class ServerMetrics(ctypes.Structure):

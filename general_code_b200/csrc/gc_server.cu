@@ -88,6 +88,22 @@ struct gc_server {
 
 namespace {
 
+// Bytes the requests' pool holds but no request uses: free for the next
+// request although the device's free memory does not count them.
+long long pool_slack(const gc_server *s) {
+  if (s->opts.simulate_us > 0)
+    return 0;
+  cudaMemPool_t pool;
+  if (cudaDeviceGetDefaultMemPool(&pool, s->device) != cudaSuccess)
+    return 0;
+  unsigned long long reserved = 0, used = 0;
+  if (cudaMemPoolGetAttribute(pool, cudaMemPoolAttrReservedMemCurrent, &reserved) !=
+          cudaSuccess ||
+      cudaMemPoolGetAttribute(pool, cudaMemPoolAttrUsedMemCurrent, &used) != cudaSuccess)
+    return 0;
+  return reserved > used ? (long long)(reserved - used) : 0;
+}
+
 int run_request(gc_server *s, cudaStream_t st, Request &r) {
   if (s->opts.simulate_us > 0) {
     std::this_thread::sleep_for(std::chrono::microseconds(s->opts.simulate_us));
@@ -139,7 +155,7 @@ void worker(gc_server *s, int slot) {
         // budget alone, so the queue cannot stall.
         bool fits = s->in_use + head.bytes <= s->budget;
         if (fits && s->opts.free_bytes && s->inflight > 0)
-          fits = head.bytes <= s->opts.free_bytes(s->opts.free_bytes_ctx);
+          fits = head.bytes <= s->opts.free_bytes(s->opts.free_bytes_ctx) + pool_slack(s);
         if (fits) {
           id = s->pending.front();
           s->pending.pop_front();
@@ -226,6 +242,25 @@ int gc_server_create(const gc_server_opts *opts, gc_server **out) {
                           : opts->simulate_us > 0 ? (1LL << 40)
                                                   : default_free_bytes(nullptr);
   s->budget = opts->memory_budget > 0 ? opts->memory_budget : (long long)(0.9 * (double)avail);
+  if (opts->simulate_us <= 0 && !s->streams.empty()) {
+    // Grow the pool once, now: a pool that grows while requests run maps new
+    // device memory, and the mapping holds up every stream on the device
+    // (measured: all requests in flight stalled together for ~250 ms, most
+    // after another program had freed tens of GB). Freed back at once, the
+    // reserve stays in the pool (release threshold above) and requests
+    // suballocate from it.
+    const long long reserve =
+        opts->reserve_bytes == 0 ? std::min(s->budget, 16LL << 30) : opts->reserve_bytes;
+    if (reserve > 0) {
+      void *p = nullptr;
+      if (cudaMallocAsync(&p, (size_t)reserve, s->streams[0]) == cudaSuccess) {
+        cudaFreeAsync(p, s->streams[0]);
+        cudaStreamSynchronize(s->streams[0]);
+      } else {
+        cudaGetLastError(); // no reserve: requests grow the pool as before
+      }
+    }
+  }
   for (int i = 0; i < opts->slots; i++)
     s->workers.emplace_back(worker, s, i);
   *out = s;

@@ -19,12 +19,13 @@ from .lattice import _LAYOUT, _PREC
 class Server:
     def __init__(self, slots: int = 8, precision: str = "mixed", memory_budget: int = 0,
                  queue_capacity: int = 0, free_bytes: Optional[Callable[[], int]] = None,
-                 simulate_us: int = 0):
+                 simulate_us: int = 0, reserve_bytes: int = 0):
         self.precision = precision
         self._cb = FREE_BYTES_FN(lambda _ctx: int(free_bytes())) if free_bytes else FREE_BYTES_FN()
         opts = ServerOpts(slots=slots, precision=_PREC[precision], memory_budget=memory_budget,
                           queue_capacity=queue_capacity, free_bytes=self._cb,
-                          free_bytes_ctx=None, simulate_us=simulate_us)
+                          free_bytes_ctx=None, simulate_us=simulate_us,
+                          reserve_bytes=reserve_bytes)
         self._h = ctypes.c_void_p()
         check(lib().gc_server_create(ctypes.byref(opts), ctypes.byref(self._h)))
         self._keep: Dict[int, tuple] = {}  # host arrays and jobs of open requests

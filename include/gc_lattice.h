@@ -429,6 +429,11 @@ typedef struct {
   void *free_bytes_ctx;
   int simulate_us;           /* > 0: no GPU work, each request sleeps this many
                                 microseconds (tests of the admission logic) */
+  long long reserve_bytes;   /* device memory the requests' stream-ordered pool
+                                takes at creation and keeps, so that running
+                                requests allocate without mapping new memory
+                                (a mapping stalls every stream on the device);
+                                0: min(budget, 16 GiB); < 0: none */
 } gc_server_opts;
 
 typedef struct {
