@@ -54,14 +54,34 @@ template <class Store> struct SplitProj {
   static constexpr bool value = Store::NC == 3 && (Store::kBytes == 48 || Store::kBytes == 72);
 };
 
-template <class Store, class CT, class M>
+// NORM (APE): the FP32 iteration starts from S scaled to sum_ij |S_ij|^2 = 3
+// (mean squared singular value 1). A Newton-Schulz step and the determinant
+// phase fix commute with a positive real factor, so a converging iteration
+// ends at the same SU(3) matrix; it gets there in fewer steps (APE sums of a
+// smeared field are close to a multiple of a unitary matrix: about one FP32
+// step instead of one to two). HYP's level-1 and level-2 sums, which need
+// not converge, keep the reference's trajectory (NORM false).
+template <class Store, class CT, bool NORM = false, class M>
 __device__ __forceinline__ void proj_store(void *out, size_t V, int site,
                                            const M &S) {
   using MD = typename Store::template M<double>;
   if constexpr (SplitProj<Store>::value) {
     using MF = typename Store::template M<float>;
     int n;
-    const MF f = ns_until(convert(S, (MF *)nullptr), 2e-5f, 5, &n);
+    MF a = convert(S, (MF *)nullptr);
+    if constexpr (NORM) {
+      float f2 = 0.f;
+#pragma unroll
+      for (int i = 0; i < 3; i++)
+#pragma unroll
+        for (int j = 0; j < 3; j++) {
+          f2 = fmaf(a.e[i][j].re, a.e[i][j].re, f2);
+          f2 = fmaf(a.e[i][j].im, a.e[i][j].im, f2);
+        }
+      if (f2 > 0.f)
+        a = scale(a, rsqrtf(f2 * (1.f / 3.f)));
+    }
+    const MF f = ns_until(a, 2e-5f, 5, &n);
     Store::template store<double>(out, V, site, ns_step(convert(f, (MD *)nullptr)));
   } else {
     MD d = convert(S, (MD *)nullptr);
@@ -107,7 +127,7 @@ __device__ __forceinline__ void ape_site(const Geom &g, const Fields4 &in,
     add_staples<Store, CT>(S, in.f[mu], in.f[nu], V, site, n.pnu, n.pmu,
                            n.mnu, n.mnu_pmu, c);
   }
-  proj_store<Store, CT>(out.f[mu], V, site, S);
+  proj_store<Store, CT, true>(out.f[mu], V, site, S);
 }
 
 // Level-1 decorated links. Field index f:
