@@ -1,0 +1,93 @@
+"""Parity at the benchmark's full sizes (GPU).
+
+* The SU(3) 24^4 job (HYP x1 + APE x20, W for R,T = 1..12) and the SU(2)
+  16^4 job (HYP x1 + APE x10, R,T = 1..8) on the GPU against the reference's
+  own CPU path on the same configuration (the oracle restatement when the
+  reference library is not built): FP64 within 1e-12 relative, mixed within
+  1e-6.
+* SU(3) 32^4 (HYP x1 + APE x40, R,T = 1..16), too large for a CPU check in a
+  test: the mixed form within 1e-6 of the FP64 form, smeared links in SU(3)
+  to FP32 precision.
+* Gauge invariance at 24^4: the same configuration with and without a random
+  gauge transformation gives the same smeared W(R,T) table.
+"""
+from __future__ import annotations
+
+import os
+
+import numpy as np
+import pytest
+
+from conftest import su3_matrices
+from general_code_b200 import Lattice, generate_config
+from oracle import py_oracle
+
+pytestmark = pytest.mark.gpu
+SEED = 20261203
+HYP = (1.0, 0.75, 0.6)
+
+
+def _job(lat, links, ape, rt):
+    lat.upload(links)
+    lat.hyp(*HYP, 1)
+    lat.ape(0.5, ape)
+    return lat.wilson_loop(1, rt, 1, rt)
+
+
+def _cpu_job(nc, dims, links, ape, rt):
+    """W table of the reference's CPU path (its library built from the
+    reference sources), else the oracle restatement, on a copy of links."""
+    a = links.copy()
+    if py_oracle.ref_available("parity"):
+        r = py_oracle.ref("parity")
+        r.set_threads(os.cpu_count() or 1)
+        w, _ = r.job(nc, dims, a, 1, *HYP, ape, 0.5, 1, rt, 1, rt)
+        return w
+    p = py_oracle.port()
+    p.set_threads(os.cpu_count() or 1)
+    p.hyp(nc, dims, a, *HYP, 1)
+    p.ape(nc, dims, a, 0.5, ape)
+    return p.wilson(nc, dims, a, 1, rt, 1, rt)
+
+
+@pytest.mark.parametrize("nc,dims,eps,ape,rt", [
+    (3, (24, 24, 24, 24), 0.25, 20, 12),
+    (2, (16, 16, 16, 16), 0.3, 10, 8),
+])
+def test_full_size_job_matches_reference_cpu_path(nc, dims, eps, ape, rt):
+    links = generate_config(dims, nc, eps, SEED, 0)
+    want = _cpu_job(nc, dims, links, ape, rt)
+    with Lattice(dims, nc, "fp64") as lat:
+        w64 = _job(lat, links, ape, rt)
+    with Lattice(dims, nc, "mixed") as lat:
+        w32 = _job(lat, links, ape, rt)
+    np.testing.assert_allclose(w64, want, rtol=1e-12, atol=1e-14)
+    assert np.max(np.abs(w32 - want) / np.abs(want)) <= 1e-6
+
+
+def test_su3_32_mixed_within_1e6_of_fp64_and_links_in_su3():
+    nc, dims, ape, rt = 3, (32, 32, 32, 32), 40, 16
+    links = generate_config(dims, nc, 0.25, SEED, 0)
+    with Lattice(dims, nc, "fp64") as lat:
+        w64 = _job(lat, links, ape, rt)
+    with Lattice(dims, nc, "mixed") as lat:
+        w32 = _job(lat, links, ape, rt)
+        m = su3_matrices(lat.download())
+    assert np.max(np.abs(w32 - w64) / np.abs(w64)) <= 1e-6
+    # every smeared link (APE'd spatial, HYP'd temporal) unitary with det 1 to
+    # FP32 precision
+    uu = np.einsum("nij,nkj->nik", m, m.conj())
+    assert np.max(np.abs(uu - np.eye(3))) <= 2e-6
+    assert np.max(np.abs(np.linalg.det(m) - 1)) <= 2e-6
+
+
+@pytest.mark.parametrize("form,rtol", [("fp64", 1e-11), ("mixed", 1e-6)])
+def test_w_is_gauge_invariant_at_full_size(form, rtol):
+    nc, dims, ape, rt = 3, (24, 24, 24, 24), 20, 12
+    plain = generate_config(dims, nc, 0.25, SEED, 0, gauge=False)
+    rotated = generate_config(dims, nc, 0.25, SEED, 0, gauge=True)
+    assert np.max(np.abs(plain - rotated)) > 0.1  # the transformation is not trivial
+    with Lattice(dims, nc, form) as lat:
+        w0 = _job(lat, plain, ape, rt)
+        w1 = _job(lat, rotated, ape, rt)
+    np.testing.assert_allclose(w1, w0, rtol=rtol, atol=1e-14)
