@@ -34,16 +34,22 @@ template <class T> struct cx {
   T re, im;
 };
 
+// Every product-sum below is an explicit fused multiply-add chain: left to
+// the compiler, `a*b + c*d` may be contracted into either fma(a, b, c*d) or
+// fma(c, d, a*b) depending on the surrounding code, so the same function
+// inlined into two kernels could round differently. Written out, one
+// function rounds one way everywhere (the batch, serving and single-lattice
+// paths give bitwise equal results).
 template <class T> GC_HD cx<T> cmul(cx<T> a, cx<T> b) {
-  return {a.re * b.re - a.im * b.im, a.re * b.im + a.im * b.re};
+  return {GC_FMA(-a.im, b.im, a.re * b.re), GC_FMA(a.im, b.re, a.re * b.im)};
 }
 // conj(a) * b
 template <class T> GC_HD cx<T> cmulc(cx<T> a, cx<T> b) {
-  return {a.re * b.re + a.im * b.im, a.re * b.im - a.im * b.re};
+  return {GC_FMA(a.im, b.im, a.re * b.re), GC_FMA(-a.im, b.re, a.re * b.im)};
 }
 // a * conj(b)
 template <class T> GC_HD cx<T> cmul_c(cx<T> a, cx<T> b) {
-  return {a.re * b.re + a.im * b.im, a.im * b.re - a.re * b.im};
+  return {GC_FMA(a.im, b.im, a.re * b.re), GC_FMA(-a.re, b.im, a.im * b.re)};
 }
 template <class T> GC_HD cx<T> cadd(cx<T> a, cx<T> b) {
   return {a.re + b.re, a.im + b.im};
@@ -60,23 +66,27 @@ template <class T> struct SU2 {
 
 template <class T> GC_HD SU2<T> unit(SU2<T>) { return {T(1), T(0), T(0), T(0)}; }
 
+// sum of four products p0 + s1 p1 + s2 p2 + s3 p3 as one fused chain
+template <class T> GC_HD T dot4(T x0, T y0, T x1, T y1, T x2, T y2, T x3, T y3) {
+  return GC_FMA(x3, y3, GC_FMA(x2, y2, GC_FMA(x1, y1, x0 * y0)));
+}
 template <class T> GC_HD SU2<T> mul(const SU2<T> &A, const SU2<T> &B) {
-  return {A.a0 * B.a0 - A.a1 * B.a1 - A.a2 * B.a2 - A.a3 * B.a3,
-          A.a0 * B.a1 + B.a0 * A.a1 + A.a3 * B.a2 - A.a2 * B.a3,
-          A.a0 * B.a2 + B.a0 * A.a2 + A.a1 * B.a3 - A.a3 * B.a1,
-          A.a0 * B.a3 + B.a0 * A.a3 + A.a2 * B.a1 - A.a1 * B.a2};
+  return {dot4(A.a0, B.a0, -A.a1, B.a1, -A.a2, B.a2, -A.a3, B.a3),
+          dot4(A.a0, B.a1, B.a0, A.a1, A.a3, B.a2, -A.a2, B.a3),
+          dot4(A.a0, B.a2, B.a0, A.a2, A.a1, B.a3, -A.a3, B.a1),
+          dot4(A.a0, B.a3, B.a0, A.a3, A.a2, B.a1, -A.a1, B.a2)};
 }
 template <class T> GC_HD SU2<T> mul_ad(const SU2<T> &A, const SU2<T> &B) {
-  return {A.a0 * B.a0 + A.a1 * B.a1 + A.a2 * B.a2 + A.a3 * B.a3,
-          -A.a0 * B.a1 + B.a0 * A.a1 - A.a3 * B.a2 + A.a2 * B.a3,
-          -A.a0 * B.a2 + B.a0 * A.a2 - A.a1 * B.a3 + A.a3 * B.a1,
-          -A.a0 * B.a3 + B.a0 * A.a3 - A.a2 * B.a1 + A.a1 * B.a2};
+  return {dot4(A.a0, B.a0, A.a1, B.a1, A.a2, B.a2, A.a3, B.a3),
+          dot4(-A.a0, B.a1, B.a0, A.a1, -A.a3, B.a2, A.a2, B.a3),
+          dot4(-A.a0, B.a2, B.a0, A.a2, -A.a1, B.a3, A.a3, B.a1),
+          dot4(-A.a0, B.a3, B.a0, A.a3, -A.a2, B.a1, A.a1, B.a2)};
 }
 template <class T> GC_HD SU2<T> mul_da(const SU2<T> &A, const SU2<T> &B) {
-  return {A.a0 * B.a0 + A.a1 * B.a1 + A.a2 * B.a2 + A.a3 * B.a3,
-          A.a0 * B.a1 - B.a0 * A.a1 - A.a3 * B.a2 + A.a2 * B.a3,
-          A.a0 * B.a2 - B.a0 * A.a2 - A.a1 * B.a3 + A.a3 * B.a1,
-          A.a0 * B.a3 - B.a0 * A.a3 - A.a2 * B.a1 + A.a1 * B.a2};
+  return {dot4(A.a0, B.a0, A.a1, B.a1, A.a2, B.a2, A.a3, B.a3),
+          dot4(A.a0, B.a1, -B.a0, A.a1, -A.a3, B.a2, A.a2, B.a3),
+          dot4(A.a0, B.a2, -B.a0, A.a2, -A.a1, B.a3, A.a3, B.a1),
+          dot4(A.a0, B.a3, -B.a0, A.a3, -A.a2, B.a1, A.a1, B.a2)};
 }
 template <class T> GC_HD SU2<T> scale(const SU2<T> &A, T s) {
   return {A.a0 * s, A.a1 * s, A.a2 * s, A.a3 * s};
@@ -85,14 +95,14 @@ template <class T> GC_HD SU2<T> add(const SU2<T> &A, const SU2<T> &B) {
   return {A.a0 + B.a0, A.a1 + B.a1, A.a2 + B.a2, A.a3 + B.a3};
 }
 template <class T> GC_HD T conj_tr(const SU2<T> &A, const SU2<T> &B) {
-  return A.a0 * B.a0 + A.a1 * B.a1 + A.a2 * B.a2 + A.a3 * B.a3;
+  return dot4(A.a0, B.a0, A.a1, B.a1, A.a2, B.a2, A.a3, B.a3);
 }
 template <class T> GC_HD T tr_real(const SU2<T> &A) { return A.a0; }
 template <class T> GC_HD SU2<T> adjoint(const SU2<T> &A) {
   return {A.a0, -A.a1, -A.a2, -A.a3};
 }
 template <class T> GC_HD SU2<T> proj(const SU2<T> &A) {
-  T rho = sqrt(A.a0 * A.a0 + A.a1 * A.a1 + A.a2 * A.a2 + A.a3 * A.a3);
+  T rho = sqrt(dot4(A.a0, A.a0, A.a1, A.a1, A.a2, A.a2, A.a3, A.a3));
   return {A.a0 / rho, A.a1 / rho, A.a2 / rho, A.a3 / rho};
 }
 
@@ -216,7 +226,7 @@ template <class T> GC_HD T conj_tr(const SU3<T> &A, const SU3<T> &B) {
   for (int i = 0; i < 3; i++)
 #pragma unroll
     for (int j = 0; j < 3; j++)
-      s += A.e[i][j].re * B.e[i][j].re + A.e[i][j].im * B.e[i][j].im;
+      s = GC_FMA(A.e[i][j].im, B.e[i][j].im, GC_FMA(A.e[i][j].re, B.e[i][j].re, s));
   return s / T(3);
 }
 template <class T> GC_HD T tr_real(const SU3<T> &A) {
@@ -309,7 +319,7 @@ template <class T> GC_HD SU3<T> ns_finish(const SU3<T> &A, const cx<T> H[3][3]) 
     }
   cx<T> dt = det(B);
   const T third = T(1) / T(3);
-  cx<T> c = {T(1) - third * (dt.re - T(1)), -third * dt.im};
+  cx<T> c = {GC_FMA(-third, dt.re - T(1), T(1)), -third * dt.im};
 #pragma unroll
   for (int i = 0; i < 3; i++)
 #pragma unroll

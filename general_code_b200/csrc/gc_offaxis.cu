@@ -49,12 +49,12 @@ template <bool ADJ, class T> __device__ __forceinline__ double offaxis_value(con
     re += double(GC_FMA(x.re, y.re, x.im * y.im));
     im += double(GC_FMA(x.im, y.re, -(x.re * y.im)));
   }
-  return ADJ ? re * re + im * im - 1.0 : re;
+  return ADJ ? fma(re, re, fma(im, im, -1.0)) : re;
 }
 template <bool ADJ, class T> __device__ __forceinline__ double offaxis_value(const SU2<T> &a,
                                                                             const SU2<T> &b) {
-  const double d = double(a.a0) * b.a0 + double(a.a1) * b.a1 + double(a.a2) * b.a2 +
-                   double(a.a3) * b.a3;
+  const double d = dot4(double(a.a0), double(b.a0), double(a.a1), double(b.a1),
+                        double(a.a2), double(b.a2), double(a.a3), double(b.a3));
   return ADJ ? 4.0 * d * d - 1.0 : d;
 }
 

@@ -126,7 +126,7 @@ __global__ void __launch_bounds__(256)
       acc += conj_tr(a, b);
     } else {
       const double2 p = norm_trace(a), q = norm_trace(b);
-      acc += p.x * q.x + p.y * q.y; // Re(p conj(q))
+      acc += fma(p.y, q.y, p.x * q.x); // Re(p conj(q))
     }
   }
   const double sum = block_sum(acc, sh);

@@ -152,7 +152,7 @@ __device__ __forceinline__ double loop_value(const SU3<T> &a, const SU3<T> &b, b
     im = GC_FMA(-a.e[k / 3][k % 3].re, b.e[k / 3][k % 3].im, im);
   }
   const double r = double(re), i = double(im);
-  return r * r + i * i - 1.0;
+  return fma(r, r, fma(i, i, -1.0));
 }
 template <bool ADJ, class T>
 __device__ __forceinline__ double loop_value(const SU2<T> &a, const SU2<T> &b, bool) {
@@ -189,11 +189,11 @@ __device__ __forceinline__ double loop_value(const SU3<f2> &a, const SU3<f2> &b,
     im = fma(-a.e[k / 3][k % 3].re, b.e[k / 3][k % 3].im, im);
   }
   const double r0 = double(re.v.x), i0 = double(im.v.x);
-  const double v0 = r0 * r0 + i0 * i0 - 1.0;
+  const double v0 = fma(r0, r0, fma(i0, i0, -1.0));
   if (!lane1)
     return v0;
   const double r1 = double(re.v.y), i1 = double(im.v.y);
-  return v0 + (r1 * r1 + i1 * i1 - 1.0);
+  return v0 + fma(r1, r1, fma(i1, i1, -1.0));
 }
 
 // Matrix of `lanes` adjacent sites from a link field (lane 1 = site s1).
