@@ -87,6 +87,7 @@ SIGNATURES = {
     "gc_generate": (_c_int, [_p, _c_dbl, _c_uint, _c_uint, _c_int]),
     "gc_generate_host": (_c_int, [_pint, _c_int, _c_dbl, _c_uint, _c_uint, _c_int, _pdbl]),
     "gc_job_device_bytes": (ctypes.c_longlong, [_pint, _c_int, _c_int, _c_int, _c_int]),
+    "gc_fma_peak": (_c_int, [_c_int, _pdbl]),
 }
 
 class GcJob(ctypes.Structure):

@@ -57,6 +57,14 @@ def generate_config(dims: Sequence[int], nc: int, eps: float, seed: int,
     return out
 
 
+def fma_peak(precision: str = "mixed") -> float:
+    """Measured vector FMA throughput of the current device, TFLOP/s (packed
+    FP32x2 for "mixed", FP64 for "fp64")."""
+    out = ctypes.c_double()
+    check(lib().gc_fma_peak(_PREC[precision], ctypes.byref(out)))
+    return float(out.value)
+
+
 def unit_config(dims: Sequence[int], nc: int) -> np.ndarray:
     n = 4 * volume(dims)
     a = np.zeros((n, link_size(nc)), dtype=np.float64)

@@ -468,6 +468,14 @@ int gc_server_destroy(gc_server *s);
 long long gc_job_device_bytes(const int dims[4], int nc, int precision,
                               int r_max, int time_max);
 
+/* Measured vector FMA throughput of the current device in TFLOP/s: packed
+ * FP32x2 fused multiply-adds (precision GC_PREC_MIXED) or FP64 ones
+ * (GC_PREC_FP64) on every SM, best of three timed launches. The compute
+ * roofline denominator of the smearing and Wilson-loop kernels, which are
+ * bound by the FP32 or FP64 pipe rather than by HBM. No reference
+ * counterpart. */
+int gc_fma_peak(int precision, double *tflops);
+
 #ifdef __cplusplus
 }
 #endif

@@ -364,3 +364,13 @@ def test_spatial_loops_match_oracle_seeded(port, nc, eps):
             assert set(got) == set(want)
             for k, v in want.items():
                 assert got[k] == pytest.approx(v, rel=rtol, abs=atol)
+
+
+def test_fma_peak_is_plausible():
+    """The measured FMA throughput behind the compute roofline: packed FP32
+    near 148 SMs x 128 lanes x 2 flops x clock, FP64 about half of it."""
+    from general_code_b200 import fma_peak
+    f32, f64 = fma_peak("mixed"), fma_peak("fp64")
+    assert 30.0 < f32 < 80.0, f32
+    assert 15.0 < f64 < 40.0, f64
+    assert 1.5 < f32 / f64 < 2.5
