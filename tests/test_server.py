@@ -140,3 +140,24 @@ def test_server_request_matches_oracle(port):
     with Server(slots=2, precision="fp64") as s:
         w = s.wait(s.submit(j, links), timeout=120)
     np.testing.assert_allclose(w, w_ref, rtol=1e-12, atol=1e-14)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("reserve", [-1, 64 << 20, 0])
+def test_pool_reserve_keeps_results_and_admission(reserve):
+    """The server's stream-ordered pool reserved at creation (default),
+    a small reserve the requests outgrow, or none: the same results, and a
+    free-memory provider that reports only the device's free memory still
+    admits requests (the pool's idle reserve counts as free)."""
+    import torch
+    inputs = [generate_config(j.dims, j.nc, 0.3 if j.nc == 2 else 0.25, 12, k)
+              for k, j in enumerate(MIX[:6])]
+    alone = [_single(j, inputs[k], "mixed") for k, j in enumerate(MIX[:6])]
+    free = lambda: int(torch.cuda.mem_get_info()[0])
+    with Server(slots=3, precision="mixed", reserve_bytes=reserve, free_bytes=free) as s:
+        ids = [s.submit(j, inputs[k]) for k, j in enumerate(MIX[:6])]
+        got = [s.wait(i, timeout=120) for i in ids]
+        st = s.stats()
+    for k in range(6):
+        assert np.array_equal(got[k], alone[k]), k
+    assert st["completed"] == 6
