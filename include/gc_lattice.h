@@ -430,10 +430,14 @@ typedef struct {
   int simulate_us;           /* > 0: no GPU work, each request sleeps this many
                                 microseconds (tests of the admission logic) */
   long long reserve_bytes;   /* device memory the requests' stream-ordered pool
-                                takes at creation and keeps, so that running
-                                requests allocate without mapping new memory
-                                (a mapping stalls every stream on the device);
-                                0: min(budget, 16 GiB); < 0: none */
+                                (the device's default pool) takes at creation
+                                and keeps, so that running requests allocate
+                                without mapping new memory (a mapping stalls
+                                every stream on the device); 0: min(budget,
+                                16 GiB); < 0: none. With a free-memory provider,
+                                the pool's reserved but unused bytes count as
+                                free for admission (other users of the default
+                                pool share them) */
 } gc_server_opts;
 
 typedef struct {
@@ -470,10 +474,11 @@ long long gc_job_device_bytes(const int dims[4], int nc, int precision,
 
 /* Measured vector FMA throughput of the current device in TFLOP/s: packed
  * FP32x2 fused multiply-adds (precision GC_PREC_MIXED) or FP64 ones
- * (GC_PREC_FP64) on every SM, best of three timed launches. The compute
- * roofline denominator of the smearing and Wilson-loop kernels, which are
- * bound by the FP32 or FP64 pipe rather than by HBM. No reference
- * counterpart. */
+ * (GC_PREC_FP64) on every SM, best of three timed launches on the legacy
+ * default stream (so it waits for, and is not overlapped by, other work on
+ * the device). The compute roofline denominator of the smearing and
+ * Wilson-loop kernels, which are bound by the FP32 or FP64 pipe rather than
+ * by HBM. No reference counterpart. */
 int gc_fma_peak(int precision, double *tflops);
 
 #ifdef __cplusplus
