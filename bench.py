@@ -316,6 +316,156 @@ def bench_serving(duration_s: float, rate: float = 200.0, slots: int = 8):
             "checked_requests": len(sample)}
 
 
+OBS_DIMS_GPU, OBS_DIMS_CPU = (24, 24, 24, 24), (12, 12, 12, 12)
+
+
+def _observable_calls(rt=6):
+    """(name, GPU call on a Lattice (second lattice for GEVP), reference CPU
+    call on (nc, dims, links, links2)) for each observable of the widened
+    rows, all with the same ranges (R, T <= 6, D_max = 6) so that per-site
+    rates compare."""
+    return [
+        ("wilson_loop_adjoint R,T<=6",
+         lambda a, b: a.wilson_loop_adjoint(1, rt, 1, rt),
+         lambda r, nc, d, x, y: r.wilson_adjoint(nc, d, x.copy(), 1, rt, 1, rt)),
+        ("wilson_gevp R,T<=6",
+         lambda a, b: a.wilson_gevp(b, 1, rt, 1, rt),
+         lambda r, nc, d, x, y: r.wilson_gevp(nc, d, x, y, 1, rt, 1, rt)),
+        ("polyakov_loop",
+         lambda a, b: a.polyakov_loop(),
+         lambda r, nc, d, x, y: r.polyakov_loop(nc, d, x)),
+        ("polyakov_correlator singlet D<=6",
+         lambda a, b: a.polyakov_correlator(rt, True),
+         lambda r, nc, d, x, y: r.polyakov_correlator(nc, d, x, rt, True)),
+        ("plaket_time",
+         lambda a, b: a.plaquette_time(),
+         lambda r, nc, d, x, y: r.plaquette_time(nc, d, x)),
+        ("wilson_offaxis_result r<=6, T<=6",
+         lambda a, b: a.wilson_offaxis_result(1.0, float(rt), 1, rt),
+         lambda r, nc, d, x, y: r.wilson_offaxis_result(nc, d, x, 1.0, float(rt), 1, rt)),
+        ("smearing_APE_2d x10",
+         lambda a, b: a.ape_plane(0, 1, 0.5, 10),
+         lambda r, nc, d, x, y: r.ape_plane(nc, d, x.copy(), 0, 1, 0.5, 10)),
+        ("wilson_spatial_3d R,T<=6, APE2d 1..10/3",
+         lambda a, b: a.wilson_spatial_3d(1, rt, 1, rt, 0.5, 1, 10, 3),
+         lambda r, nc, d, x, y: r.wilson_spatial_3d(nc, d, x.copy(), 1, rt, 1, rt, 0.5, 1, 10,
+                                                    3)),
+    ]
+
+
+def cpu_reference_observables():
+    """The reference's own CPU implementation of each observable (oracle/_ref,
+    the reference's flags, all host threads) on a bounded sample: SU(3) 12^4.
+    Returns {name: sites/s} and the thread count, or None without the
+    library."""
+    sys.path.insert(0, str(ROOT))
+    from oracle import py_oracle
+    if not py_oracle.ref_available("timed"):
+        return None, 0
+    from general_code_b200 import generate_config
+    ref = py_oracle.ref("timed")
+    cores = os.cpu_count() or 1
+    ref.set_threads(cores)
+    d = OBS_DIMS_CPU
+    x = generate_config(d, 3, 0.25, SEED, 0)
+    y = generate_config(d, 3, 0.25, SEED, 1)
+    V = int(np.prod(d))
+    out = {}
+    for name, _, cpu in _observable_calls():
+        t0 = time.perf_counter()
+        cpu(ref, 3, d, x, y)
+        out[name] = V / (time.perf_counter() - t0)
+    return out, cores
+
+
+def bench_observables(steps: int):
+    """The observables beside the on-axis loops, on the GPU: SU(3) 24^4 in both
+    forms, each call timed with CUDA events on the lattice's stream (mean of
+    `steps` calls after one untimed), next to the reference's CPU path on a
+    bounded SU(3) 12^4 sample with the same ranges. Also the configuration
+    reader on a 24^4 lexicographical file and the t-slab decomposition
+    emulated on one GPU (all slabs one after another) against one lattice."""
+    import tempfile
+
+    import torch
+    from general_code_b200 import Lattice, generate_config
+    from general_code_b200.tslab import emulate
+    d = OBS_DIMS_GPU
+    V = int(np.prod(d))
+    x = generate_config(d, 3, 0.25, SEED, 0)
+    y = generate_config(d, 3, 0.25, SEED, 1)
+    cpu, cores = cpu_reference_observables()
+    res = {}
+    for form in ("mixed", "fp64"):
+        s = torch.cuda.Stream()
+        with Lattice(d, 3, form) as a, Lattice(d, 3, form) as b:
+            for lat in (a, b):
+                lat.set_stream(s.cuda_stream)
+            a.upload(x)
+            b.upload(y)
+            for name, gpu, _ in _observable_calls():
+                gpu(a, b)
+                a.upload(x)
+                ms = []
+                for _ in range(max(1, steps)):
+                    e0, e1 = (torch.cuda.Event(enable_timing=True) for _ in range(2))
+                    e0.record(s)
+                    gpu(a, b)
+                    e1.record(s)
+                    s.synchronize()
+                    ms.append(e0.elapsed_time(e1))
+                    a.upload(x)  # the smearing calls change the links
+                m = sum(ms) / len(ms)
+                r = res.setdefault(name, {})
+                r[f"{form}_ms"] = m
+                r[f"{form}_sites_per_s"] = V / (m * 1e-3)
+    for name in res:
+        if cpu:
+            res[name]["reference_cpu_sites_per_s"] = cpu[name]
+            res[name]["fp64_vs_reference"] = res[name]["fp64_sites_per_s"] / cpu[name]
+    # configuration reader: 24^4 SU(3) lexicographical doubles, file -> device
+    rd = {}
+    with tempfile.TemporaryDirectory() as tmp:
+        path = os.path.join(tmp, "conf.lex")
+        with Lattice(d, 3, "fp64") as a:
+            a.upload(x)
+            a.write(path)
+            nbytes = os.path.getsize(path)
+            for form in ("fp64", "mixed"):
+                with Lattice(d, 3, form) as c:
+                    c.read(path)
+                    c.synchronize()
+                    t0 = time.perf_counter()
+                    for _ in range(max(1, steps)):
+                        c.read(path)
+                        c.synchronize()
+                    dt = (time.perf_counter() - t0) / max(1, steps)
+                rd[form] = {"ms": dt * 1e3, "file_GB_per_s": nbytes / dt / 1e9}
+        if cpu is not None:
+            from oracle import py_oracle
+            ref = py_oracle.ref("timed")
+            t0 = time.perf_counter()
+            ref.read(3, d, path, "lexicographical", 0, "double", False)
+            dt = time.perf_counter() - t0
+            rd["reference_cpu"] = {"ms": dt * 1e3, "file_GB_per_s": nbytes / dt / 1e9}
+    rd["file_bytes"] = nbytes
+    # t-slab decomposition emulated on one GPU: the headline job as 1 and 2 slabs
+    job = dict(precision="mixed", hyp=(1.0, 0.75, 0.6), hyp_steps=1, ape_alpha=0.5,
+               ape_steps=20, r_min=1, r_max=12, time_min=1, time_max=12)
+    ts = {}
+    for k in (1, 2):
+        emulate(x, d, 3, k, **job)
+        t0 = time.perf_counter()
+        emulate(x, d, 3, k, **job)
+        ts[f"slabs_{k}_ms"] = (time.perf_counter() - t0) * 1e3
+    return {"workload": "SU(3) 24^4 on the GPU (both forms), the reference's CPU path on "
+                        "SU(3) 12^4 with the same ranges",
+            "reference_cpu_threads": cores, "unit": "sites/s", "observables": res,
+            "reader_lexicographical_double": rd,
+            "tslab_emulated_one_gpu": dict(ts, note="wall time incl. lattice allocation; "
+                                                    "slabs run one after another on one GPU")}
+
+
 def run_reference(args, wl, rank):
     if rank != 0:
         return 0
@@ -349,8 +499,9 @@ def main():
     ap.add_argument("--form", choices=["both", "fp64", "mixed"], default="both")
     ap.add_argument("--workload", choices=sorted(WORKLOADS), default="su3_24")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--sections", default="batch,serving",
-                    help="extra single-GPU measurements: batch, serving (comma list, or none)")
+    ap.add_argument("--sections", default="batch,serving,observables",
+                    help="extra single-GPU measurements: batch, serving, observables "
+                         "(comma list, or none)")
     ap.add_argument("--serving-seconds", type=float, default=10.0)
     args = ap.parse_args()
     if args.warmup < 3:
@@ -603,6 +754,8 @@ def main():
         line["batch"] = bench_batch(args.steps)
     if world == 1 and "serving" in sections:
         line["serving"] = bench_serving(args.serving_seconds)
+    if world == 1 and "observables" in sections:
+        line["observables"] = bench_observables(min(args.steps, 5))
     if world == 1 and not args.no_cpu_baseline:
         v, info = cpu_baseline(wl, args.workload, host)
         line["cpu_baseline"] = {"value": v, "unit": "sites/s", "cores": info["cores"],
