@@ -5,6 +5,7 @@
 #include "gc_internal.cuh"
 #include "gc_kernels.h"
 
+#include <algorithm>
 #include <array>
 #include <cmath>
 #include <cstdio>
@@ -72,6 +73,8 @@ struct gc_lattice {
   size_t dev_out_cap = 0;   // doubles
   void *aux = nullptr;      // Polyakov lines and offset tables
   size_t aux_cap = 0;       // bytes
+  unsigned char *io_buf[2] = {nullptr, nullptr}; // pinned file chunks (reader, writer)
+  cudaEvent_t io_ev[2] = {nullptr, nullptr};     // last copy out of / into each chunk
   cudaStream_t own_stream = nullptr;
   cudaStream_t stream = nullptr;
   bool stream_ordered = false; // device memory from cudaMallocAsync on `stream`
@@ -205,6 +208,25 @@ int ensure_aux(gc_lattice *h, size_t bytes) {
     return cuda_fail(h, "cudaMalloc(Polyakov scratch)", e);
   }
   h->aux_cap = bytes;
+  return GC_OK;
+}
+
+// Two pinned host chunks for configuration files: the reader fills one from
+// the file while the other is copied to the device, the writer writes one to
+// the file while the next is copied from the device (no pinning of a whole
+// configuration per call, which costs more than reading it).
+constexpr size_t kIoChunk = 16u << 20;
+
+int ensure_io(gc_lattice *h) {
+  for (int i = 0; i < 2; i++) {
+    if (h->io_buf[i])
+      continue;
+    cudaError_t e = cudaMallocHost(reinterpret_cast<void **>(&h->io_buf[i]), kIoChunk);
+    if (e == cudaSuccess)
+      e = cudaEventCreateWithFlags(&h->io_ev[i], cudaEventDisableTiming);
+    if (e != cudaSuccess)
+      return cuda_fail(h, "cudaMallocHost(file chunks)", e);
+  }
   return GC_OK;
 }
 
@@ -346,6 +368,14 @@ int gc_lattice_destroy(gc_lattice *h) {
     dev_free(h, h->partials);
     dev_free(h, h->dev_out);
     dev_free(h, h->aux);
+    for (int i = 0; i < 2; i++) {
+      if (h->io_ev[i])
+        cudaEventSynchronize(h->io_ev[i]);
+      if (h->io_buf[i])
+        cudaFreeHost(h->io_buf[i]);
+      if (h->io_ev[i])
+        cudaEventDestroy(h->io_ev[i]);
+    }
     if (h->own_stream)
       cudaStreamDestroy(h->own_stream);
   }
@@ -1186,29 +1216,41 @@ int gc_read_config(gc_lattice *h, const char *path, const char *format,
     return fail(h, rc, err);
   std::lock_guard<std::mutex> lk(h->mu);
   rc = ensure_staging(h);
+  if (!rc)
+    rc = ensure_io(h);
   if (rc)
     return rc;
-  unsigned char *buf = nullptr;
-  cudaError_t e = cudaMallocHost(&buf, (size_t)length);
-  if (e != cudaSuccess)
-    return cuda_fail(h, "cudaMallocHost(read buffer)", e);
+  // chunk k of the file goes through pinned buffer k % 2: its read waits only
+  // for the copy of chunk k - 2 out of the same buffer
   FILE *f = std::fopen(path, "rb");
-  bool ok = f && std::fseek(f, (long)offset, SEEK_SET) == 0 &&
-            std::fread(buf, 1, (size_t)length, f) == (size_t)length;
+  bool ok = f && std::fseek(f, (long)offset, SEEK_SET) == 0;
+  cudaError_t e = cudaSuccess;
+  unsigned char *dst = reinterpret_cast<unsigned char *>(h->staging);
+  for (size_t done = 0, k = 0; ok && e == cudaSuccess && done < (size_t)length; k ^= 1) {
+    const size_t n = std::min(kIoChunk, (size_t)length - done);
+    e = cudaEventSynchronize(h->io_ev[k]);
+    if (e != cudaSuccess)
+      break;
+    ok = std::fread(h->io_buf[k], 1, n, f) == n;
+    if (!ok)
+      break;
+    e = cudaMemcpyAsync(dst + done, h->io_buf[k], n, cudaMemcpyHostToDevice, h->stream);
+    if (e == cudaSuccess)
+      e = cudaEventRecord(h->io_ev[k], h->stream);
+    done += n;
+  }
   if (f)
     std::fclose(f);
-  if (!ok) {
-    cudaFreeHost(buf);
-    return fail(h, GC_ERR_IO, std::string("read failed: ") + path);
-  }
-  e = cudaMemcpyAsync(h->staging, buf, (size_t)length, cudaMemcpyHostToDevice, h->stream);
-  if (e == cudaSuccess) {
+  if (e == cudaSuccess && ok) {
     rc = gc::launch_file_to_soa(h->g, h->nc, h->prec, format, precision, convert != 0,
                                 reinterpret_cast<const unsigned char *>(h->staging), h->cur,
                                 h->stream);
     e = cudaStreamSynchronize(h->stream);
+  } else {
+    cudaStreamSynchronize(h->stream); // the chunks in flight finish before a retry reuses them
   }
-  cudaFreeHost(buf);
+  if (!ok)
+    return fail(h, GC_ERR_IO, std::string("read failed: ") + path);
   if (rc)
     return launch_fail(h, rc);
   if (e != cudaSuccess)
@@ -1223,22 +1265,47 @@ int gc_write_config(gc_lattice *h, const char *path) {
     return rc;
   if (!path)
     return fail(h, GC_ERR_ARG, "null path");
-  const size_t n = (size_t)(h->nc == 3 ? 18 : 4) * 4 * (size_t)h->g.V;
-  double *buf = nullptr;
-  cudaError_t e = cudaMallocHost(&buf, n * sizeof(double));
-  if (e != cudaSuccess)
-    return cuda_fail(h, "cudaMallocHost(write buffer)", e);
-  rc = gc_download(h, buf, GC_LAYOUT_ROWMAJOR);
-  if (rc == GC_OK) {
-    FILE *f = std::fopen(path, "wb");
-    bool ok = f && std::fwrite(buf, sizeof(double), n, f) == n;
-    if (f)
-      ok = (std::fclose(f) == 0) && ok;
-    if (!ok)
-      rc = fail(h, GC_ERR_IO, std::string("write failed: ") + path);
+  const size_t bytes = (size_t)(h->nc == 3 ? 18 : 4) * 4 * (size_t)h->g.V * sizeof(double);
+  std::lock_guard<std::mutex> lk(h->mu);
+  rc = ensure_staging(h);
+  if (!rc)
+    rc = ensure_io(h);
+  if (rc)
+    return rc;
+  rc = launch_soa_to_aos(h->g, h->nc, h->prec, GC_LAYOUT_ROWMAJOR, h->cur, h->staging,
+                         h->stream);
+  if (rc)
+    return launch_fail(h, rc);
+  // chunk k is copied into buffer k % 2 while chunk k - 1 is written out
+  const unsigned char *src = reinterpret_cast<const unsigned char *>(h->staging);
+  const size_t nchunks = (bytes + kIoChunk - 1) / kIoChunk;
+  auto issue = [&](size_t k) {
+    const size_t off = k * kIoChunk, n = std::min(kIoChunk, bytes - off);
+    cudaError_t e = cudaMemcpyAsync(h->io_buf[k & 1], src + off, n, cudaMemcpyDeviceToHost,
+                                    h->stream);
+    return e == cudaSuccess ? cudaEventRecord(h->io_ev[k & 1], h->stream) : e;
+  };
+  FILE *f = std::fopen(path, "wb");
+  bool ok = f != nullptr;
+  cudaError_t e = ok && nchunks ? issue(0) : cudaSuccess;
+  for (size_t k = 0; ok && e == cudaSuccess && k < nchunks; k++) {
+    if (k + 1 < nchunks)
+      e = issue(k + 1);
+    if (e == cudaSuccess)
+      e = cudaEventSynchronize(h->io_ev[k & 1]);
+    if (e != cudaSuccess)
+      break;
+    const size_t n = std::min(kIoChunk, bytes - k * kIoChunk);
+    ok = std::fwrite(h->io_buf[k & 1], 1, n, f) == n;
   }
-  cudaFreeHost(buf);
-  return rc;
+  cudaStreamSynchronize(h->stream);
+  if (f)
+    ok = (std::fclose(f) == 0) && ok;
+  if (e != cudaSuccess)
+    return cuda_fail(h, "write_config", e);
+  if (!ok)
+    return fail(h, GC_ERR_IO, std::string("write failed: ") + path);
+  return GC_OK;
 }
 
 int gc_generate_host(const int dims[4], int nc, double eps, unsigned int seed,
