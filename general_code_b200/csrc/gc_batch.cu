@@ -266,49 +266,74 @@ int build_schedule(gc_batch *b) {
         b->launches.push_back(L);
       }
     }
-    // W and the reductions
+    // W and the reductions. Jobs are launched in occupancy classes (threads
+    // per block, blocks that fit on an SM by shared memory): a launch runs at
+    // the widest shape and largest shared memory of its jobs, and one launch
+    // over all jobs would hold every block to the occupancy of the largest
+    // one (a 24^3x48 job's ~93 KB per block halves the resident blocks of
+    // every other job's W). A block's work depends only on its own job's
+    // shape, so the results do not depend on the grouping.
     {
-      std::vector<WJob> t;
-      std::vector<RJob> r;
-      int blocks = 0, entries = 0, threads = 32;
-      size_t smem = 0;
       const int ct = prec == GC_PREC_FP64 ? 8 : 4;
+      std::map<std::pair<int, int>, std::vector<int>> classes; // (threads, blocks/SM) -> jobs
       for (int i : ids) {
         JobState &j = b->jobs[i];
         if (j.nr <= 0)
           continue;
         WJob w;
         w.g = j.g;
-        w.U = cur[i];
         w.rmin = j.desc.r_min;
         w.rmax = j.desc.r_max;
         w.tmin = j.desc.time_min;
         w.tmax = j.desc.time_max;
         w.cols = j.cols;
         w.rows = j.rows;
-        w.partials = j.partials;
-        w.block_start = blocks;
-        w.blocks = j.w_blocks;
-        blocks += j.w_blocks;
-        threads = std::max(threads, wilson_threads(j.cols, j.rows, wilson_lanes(nc, ct)));
-        t.push_back(w);
-        RJob q;
-        q.partials = j.partials;
-        q.nblocks = j.w_blocks;
-        q.nr = j.nr;
-        q.nt = j.nt;
-        q.scale = wilson_scale(j.g.V, j.desc.nc, false);
-        q.out = j.out_dev;
-        q.entry_start = entries;
-        entries += j.nr * j.nt;
-        r.push_back(q);
+        const int th = wilson_threads(j.cols, j.rows, wilson_lanes(nc, ct));
+        const size_t sm = wilson_job_smem(w, nc, ct, th);
+        const int per_sm = (int)std::max<size_t>(1, (227u * 1024u) / std::max<size_t>(sm, 1));
+        classes[{th, std::min(per_sm, 2048 / th)}].push_back(i);
       }
-      for (const WJob &w : t)
-        smem = std::max(smem, wilson_job_smem(w, nc, ct, threads));
-      if (!t.empty()) {
+      std::vector<RJob> r;
+      int entries = 0;
+      for (const auto &kv : classes) {
+        std::vector<WJob> t;
+        int blocks = 0, threads = 32;
+        size_t smem = 0;
+        for (int i : kv.second) {
+          JobState &j = b->jobs[i];
+          WJob w;
+          w.g = j.g;
+          w.U = cur[i];
+          w.rmin = j.desc.r_min;
+          w.rmax = j.desc.r_max;
+          w.tmin = j.desc.time_min;
+          w.tmax = j.desc.time_max;
+          w.cols = j.cols;
+          w.rows = j.rows;
+          w.partials = j.partials;
+          w.block_start = blocks;
+          w.blocks = j.w_blocks;
+          blocks += j.w_blocks;
+          threads = std::max(threads, wilson_threads(j.cols, j.rows, wilson_lanes(nc, ct)));
+          t.push_back(w);
+          RJob q;
+          q.partials = j.partials;
+          q.nblocks = j.w_blocks;
+          q.nr = j.nr;
+          q.nt = j.nt;
+          q.scale = wilson_scale(j.g.V, j.desc.nc, false);
+          q.out = j.out_dev;
+          q.entry_start = entries;
+          entries += j.nr * j.nt;
+          r.push_back(q);
+        }
+        for (const WJob &w : t)
+          smem = std::max(smem, wilson_job_smem(w, nc, ct, threads));
         // blocks[1]: threads per block (the widest job shape of the launch)
         Launch L{Launch::W, cls, push_table(arena, t), (int)t.size(), {blocks, threads, 0}, smem};
         b->launches.push_back(L);
+      }
+      if (!r.empty()) {
         Launch R{Launch::REDUCE, cls, push_table(arena, r), (int)r.size(), {entries, 0, 0}, 0};
         b->launches.push_back(R);
       }
