@@ -463,7 +463,7 @@ int tune_job(gc_batch *b, JobState &j, double *scratch, cudaStream_t s, int *row
   const int Lt = j.g.L[3];
   float best = 1e30f;
   int br = j.rows, bc = j.cols;
-  for (int rows = 1; rows <= 32 && rows <= Lt; rows++) {
+  for (int rows = 1; rows <= 64 && rows <= Lt; rows++) {
     if (Lt % rows || rows < std::min(4, Lt))
       continue;
     for (int threads : {128, 256}) {

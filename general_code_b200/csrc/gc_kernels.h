@@ -82,7 +82,7 @@ size_t wilson_job_smem(const WJob &j, int nc, int ct_bytes, int threads);
 // ((tmax-tmin+1)*(rmax-rmin+1) doubles, index (T-tmin)*nR + (R-rmin)).
 struct WilsonPlan {
   int cols_per_block; // spatial columns per block
-  int rows;           // threads per column (a divisor of Lt, <= 32)
+  int rows;           // threads per column (a divisor of Lt, <= 64)
   int threads;        // ceil(cols_per_block / lanes) * rows, whole warps
   int blocks;         // ceil(Vs / cols_per_block) * 3
   size_t smem;        // dynamic shared memory bytes
@@ -120,8 +120,9 @@ __host__ __device__ inline int wilson_threads(int cols, int rows, int lanes) {
 // At most this many (R,T) entries per launch (callers split R into chunks).
 constexpr int kWilsonMaxEntries = 1024;
 // Shared-memory budget for the column storage of one block (bytes), sized
-// so that two blocks fit on an SM with their per-warp accumulators.
-constexpr size_t kWilsonColumnBudget = 96 * 1024;
+// so that two blocks fit on an SM with their per-warp accumulators (a
+// 256-thread block with 12 x 12 (R,T) entries: 2 x (104 + 9) KB).
+constexpr size_t kWilsonColumnBudget = 104 * 1024;
 
 // sets: shared column sets of the block (3; 4 for the two-configuration
 // GEVP loops).

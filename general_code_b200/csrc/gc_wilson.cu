@@ -538,18 +538,21 @@ int largest_divisor_upto(int n, int cap) {
 } // namespace
 
 // The block shape depends only on Lt, the group and the compute type, never
-// on the R/T ranges. A block has about 128 threads (rows = the largest divisor
-// of Lt up to 32, each thread carrying `lanes` columns); columns are limited
-// so that the shared column storage fits kWilsonColumnBudget. The FP64 plan
-// has the fewest columns per block and so the most blocks: callers that size
-// per-block partials before the compute type is known use it.
+// on the R/T ranges. rows = the largest divisor of Lt up to 64 threads per
+// column (each thread carrying `lanes` columns, so one start slice per thread
+// when Lt <= 64): about 128 threads per block, 256 when rows > 32. A thread
+// walking several starts would need that many times the shared memory per
+// thread, and shared memory is what bounds the resident warps. Columns are
+// limited so that the shared column storage fits kWilsonColumnBudget. The
+// FP64 plan has the fewest columns per block and so the most blocks: callers
+// that size per-block partials before the compute type is known use it.
 WilsonPlan wilson_plan(const Geom &g, int nr, int nt, int nc, int ct_bytes, int sets) {
   WilsonPlan p;
   const int Lt = g.L[3];
   const int ncomp = (nc == 3) ? 18 : 4;
   const int lanes = wilson_lanes(nc, ct_bytes);
-  p.rows = largest_divisor_upto(Lt, 32);
-  p.cols_per_block = lanes * (128 / p.rows);
+  p.rows = largest_divisor_upto(Lt, 64);
+  p.cols_per_block = lanes * ((p.rows > 32 ? 256 : 128) / p.rows);
   if (p.cols_per_block < 1)
     p.cols_per_block = 1;
   const size_t col_bytes = (size_t)sets * ncomp * Lt * ct_bytes;

@@ -52,6 +52,9 @@ def test_fp64_matches_reference_fixture(name, meta):
     # 7 warps x 25 (R,T) entries: an odd number of FP64 accumulators in the W
     # kernel's shared memory ahead of its 16-byte column arrays
     (3, (10, 10, 10, 10), 0.25, (1.0, 0.75, 0.6), 2, (1, 5, 1, 5)),
+    # time extents above 32: one start slice per thread, 256-thread W blocks
+    (3, (4, 4, 4, 48), 0.25, (1.0, 0.75, 0.6), 2, (1, 2, 1, 20)),
+    (2, (4, 3, 5, 40), 0.3, (1.0, 0.75, 0.6), 2, (1, 2, 2, 17)),
 ])
 def test_fp64_matches_oracle_seeded(port, nc, dims, eps, hyp, n_ape, rng):
     links = generate_config(dims, nc, eps, 20261203, 7)
@@ -374,3 +377,18 @@ def test_fma_peak_is_plausible():
     assert 30.0 < f32 < 80.0, f32
     assert 15.0 < f64 < 40.0, f64
     assert 1.5 < f32 / f64 < 2.5
+
+
+@pytest.mark.parametrize("dims", [(6, 6, 6, 48), (5, 4, 6, 36)])
+def test_mixed_long_time_extent_within_1e6(dims):
+    """W blocks with more than 32 threads per column (Lt = 48, 36) in the
+    mixed form against the FP64 form."""
+    links = generate_config(dims, 3, 0.25, 20261203, 11)
+    out = {}
+    for form in ("fp64", "mixed"):
+        with Lattice(dims, 3, form) as lat:
+            lat.upload(links)
+            lat.hyp(1.0, 0.75, 0.6, 1)
+            lat.ape(0.5, 4)
+            out[form] = lat.wilson_loop(1, 3, 1, 16)
+    assert np.max(np.abs(out["mixed"] - out["fp64"]) / np.abs(out["fp64"])) <= 1e-6
