@@ -895,21 +895,38 @@ static int offaxis_impl(gc_lattice *h, const std::vector<std::array<int, 3>> &di
   rc = ensure_aux(h, line_bytes);
   if (rc)
     return rc;
-  rc = ensure_partials(h, offaxis_partials_count(h->g, nt));
+  // Lines go in chunks that share one partials buffer, [block][line][T], and
+  // one reduction launch (a reduction per line cost as much as a tenth of
+  // the line's time); a chunk's partials stay within 32 MB.
+  const size_t per_line = (size_t)offaxis_partials_count(h->g, nt);
+  const size_t chunk =
+      std::max<size_t>(1, std::min(plan.lines.size(), ((size_t)4 << 20) / per_line));
+  rc = ensure_partials(h, per_line * chunk);
   if (rc)
     return rc;
   rc = ensure_dev_out(h, plan.lines.size() * (size_t)nt);
   if (rc)
     return rc;
-  for (size_t i = 0; i < plan.lines.size(); i++) {
-    OffaxisSteps steps;
-    steps.n = (int)plan.lines[i].pattern.size();
-    for (int k = 0; k < steps.n; k++)
-      steps.s[k] = (signed char)plan.lines[i].pattern[k];
-    rc = GC_DISPATCH(h, launch_offaxis_line, h->g, h->cur, steps, h->aux, h->stream);
-    if (!rc)
-      rc = GC_DISPATCH(h, launch_offaxis_loops, h->g, h->cur, h->aux, plan.lines[i].disp, tmin,
-                       tmax, adjoint, h->partials, h->dev_out + i * nt, h->stream);
+  const int blocks = (int)(per_line / nt);
+  for (size_t c0 = 0; c0 < plan.lines.size(); c0 += chunk) {
+    const size_t n = std::min(chunk, plan.lines.size() - c0);
+    for (size_t k = 0; k < n; k++) {
+      const OffaxisLine &line = plan.lines[c0 + k];
+      OffaxisSteps steps;
+      steps.n = (int)line.pattern.size();
+      for (int q = 0; q < steps.n; q++)
+        steps.s[q] = (signed char)line.pattern[q];
+      rc = GC_DISPATCH(h, launch_offaxis_line, h->g, h->cur, steps, h->aux, h->stream);
+      if (!rc)
+        rc = GC_DISPATCH(h, launch_offaxis_loops, h->g, h->cur, h->aux, line.disp, tmin, tmax,
+                         adjoint, h->partials + k * nt, (double *)nullptr, h->stream,
+                         (int)(n * nt));
+      if (rc)
+        return launch_fail(h, rc);
+    }
+    rc = launch_reduce_rows(h->partials, blocks, (int)(n * nt),
+                            line_loop_scale(h->g, h->nc, adjoint), h->dev_out + c0 * nt,
+                            h->stream);
     if (rc)
       return launch_fail(h, rc);
   }
@@ -1019,7 +1036,11 @@ int gc_wilson_spatial_3d(gc_lattice *h, int r_min, int r_max, int time_min, int 
   rc = ensure_aux(h, 4 * fb + 2 * lb);
   if (rc)
     return rc;
-  rc = ensure_partials(h, offaxis_partials_count(h->g, nt));
+  // the 2 nr lines of one (plane, measurement) share a partials buffer,
+  // [block][(r, axis)][T], and one reduction launch when it stays within 32 MB
+  const size_t per_line = (size_t)offaxis_partials_count(h->g, nt);
+  const bool shared_reduce = per_line * 2 * nr <= ((size_t)4 << 20);
+  rc = ensure_partials(h, shared_reduce ? per_line * 2 * nr : per_line);
   if (rc)
     return rc;
   // values[plane][measurement][r][axis][T]
@@ -1050,14 +1071,19 @@ int gc_wilson_spatial_3d(gc_lattice *h, int r_min, int r_max, int time_min, int 
           if (rc)
             return launch_fail(h, rc);
         }
+        double *plane_out = h->dev_out + p * per_plane + (size_t)mi * nr * 2 * nt;
         for (int r = r_min; r <= r_max; r++) {
           for (int k = 0; k < 2; k++) {
             int disp[4] = {0, 0, 0, 0};
             disp[ax[k]] = r;
-            double *o = h->dev_out + p * per_plane +
-                        (((size_t)mi * nr + (r - r_min)) * 2 + k) * nt;
-            rc = GC_DISPATCH(h, launch_line_loops, h->g, h->cur.f[mu], mu, S[k], disp,
-                             time_min, time_max, false, h->partials, o, h->stream);
+            const size_t q = (size_t)(r - r_min) * 2 + k;
+            rc = shared_reduce
+                     ? GC_DISPATCH(h, launch_line_loops, h->g, h->cur.f[mu], mu, S[k], disp,
+                                   time_min, time_max, false, h->partials + q * nt,
+                                   (double *)nullptr, h->stream, 2 * nr * nt)
+                     : GC_DISPATCH(h, launch_line_loops, h->g, h->cur.f[mu], mu, S[k], disp,
+                                   time_min, time_max, false, h->partials,
+                                   plane_out + q * nt, h->stream, 0);
             if (rc)
               return launch_fail(h, rc);
           }
@@ -1067,6 +1093,12 @@ int gc_wilson_spatial_3d(gc_lattice *h, int r_min, int r_max, int time_min, int 
             if (rc)
               return launch_fail(h, rc);
           }
+        }
+        if (shared_reduce) {
+          rc = launch_reduce_rows(h->partials, (int)(per_line / nt), 2 * nr * nt,
+                                  line_loop_scale(h->g, h->nc, false), plane_out, h->stream);
+          if (rc)
+            return launch_fail(h, rc);
         }
         mi++;
       }

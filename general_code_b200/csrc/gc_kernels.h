@@ -198,10 +198,17 @@ template <class Store, class CT>
 int launch_offaxis_line(const Geom &g, const Fields4 &U, const OffaxisSteps &steps, void *S,
                         cudaStream_t s);
 // out_dev[T - tmin] = the loop average for the line S with displacement disp.
+// out_dev == nullptr: only the per-block partial sums, at
+// partials[block * pstride + (T - tmin)] (pstride >= tmax - tmin + 1), for
+// one reduction over several lines (launch_reduce_rows with
+// line_loop_scale).
 template <class Store, class CT>
 int launch_offaxis_loops(const Geom &g, const Fields4 &U, const void *S, const int disp[3],
                          int tmin, int tmax, bool adjoint, double *partials, double *out_dev,
-                         cudaStream_t s);
+                         cudaStream_t s, int pstride = 0);
+// Scale of the summed partials of the line loops (1/V, and 1/N for the
+// fundamental SU(3) trace).
+double line_loop_scale(const Geom &g, int nc, bool adjoint);
 
 // Loops of a line field S (decorated-link storage) whose end is displaced
 // by disp (disp[ax] = 0) with "time" axis ax and time links Ut:
@@ -210,7 +217,7 @@ int launch_offaxis_loops(const Geom &g, const Fields4 &U, const void *S, const i
 template <class Store, class CT>
 int launch_line_loops(const Geom &g, const void *Ut, int ax, const void *S, const int disp[4],
                       int tmin, int tmax, bool adjoint, double *partials, double *out_dev,
-                      cudaStream_t s);
+                      cudaStream_t s, int pstride = 0);
 // S <- (init ? F : S) * F(x + offset ax)^count for a single-direction field F.
 template <class Store, class CT>
 int launch_line_extend(const Geom &g, const void *F, void *S, int ax, int offset, int count,

@@ -107,7 +107,7 @@ __global__ void __launch_bounds__(256)
 template <class Store, class CT, bool ADJ>
 __global__ void __launch_bounds__(256)
     line_loop_kernel(const __grid_constant__ Geom g, const void *Ut, int ax, const void *S,
-                     int4 d, int tmin, int tmax, double *partials) {
+                     int4 d, int tmin, int tmax, double *partials, int pstride) {
   using M = typename Store::template M<CT>;
   using IS = typename InterStore<Store>::type;
   extern __shared__ double wacc[]; // [nwarps][nt]
@@ -157,7 +157,7 @@ __global__ void __launch_bounds__(256)
     double sum = 0.0;
     for (int w = 0; w < nwarps; w++)
       sum += wacc[w * nt + e];
-    partials[(size_t)blockIdx.x * nt + e] = sum;
+    partials[(size_t)blockIdx.x * pstride + e] = sum;
   }
 }
 
@@ -204,10 +204,17 @@ int launch_offaxis_line(const Geom &g, const Fields4 &U, const OffaxisSteps &ste
   return launch_check("offaxis_line_kernel");
 }
 
+double line_loop_scale(const Geom &g, int nc, bool adjoint) {
+  // averages over V sites (calculate_wilson_loop_offaxis and
+  // wilson_spatial_plane_indexed divide by V); the fundamental SU(3) value is
+  // Re Tr / 3 (tr_real, multiply_conj_tr)
+  return 1.0 / ((double)g.V * ((!adjoint && nc == 3) ? 3.0 : 1.0));
+}
+
 template <class Store, class CT>
 int launch_line_loops(const Geom &g, const void *Ut, int ax, const void *S, const int disp[4],
                       int tmin, int tmax, bool adjoint, double *partials, double *out_dev,
-                      cudaStream_t s) {
+                      cudaStream_t s, int pstride) {
   const int nt = tmax - tmin + 1;
   if (nt < 1 || nt > kWilsonMaxEntries)
     return plan_error("line_loop_kernel: time range");
@@ -220,29 +227,28 @@ int launch_line_loops(const Geom &g, const void *Ut, int ax, const void *S, cons
   for (int i = 0; i < 4; i++)
     d[i] = ((disp[i] % g.L[i]) + g.L[i]) % g.L[i];
   const int4 d4 = make_int4(d[0], d[1], d[2], d[3]);
+  if (pstride < nt)
+    pstride = nt;
   if (adjoint)
-    line_loop_kernel<Store, CT, true><<<blocks, kOffaxisBlock, smem, s>>>(g, Ut, ax, S, d4, tmin,
-                                                                         tmax, partials);
+    line_loop_kernel<Store, CT, true><<<blocks, kOffaxisBlock, smem, s>>>(
+        g, Ut, ax, S, d4, tmin, tmax, partials, pstride);
   else
-    line_loop_kernel<Store, CT, false><<<blocks, kOffaxisBlock, smem, s>>>(g, Ut, ax, S, d4,
-                                                                          tmin, tmax, partials);
+    line_loop_kernel<Store, CT, false><<<blocks, kOffaxisBlock, smem, s>>>(
+        g, Ut, ax, S, d4, tmin, tmax, partials, pstride);
   int rc = launch_check("line_loop_kernel");
-  if (rc)
+  if (rc || !out_dev)
     return rc;
-  // averages over V sites (calculate_wilson_loop_offaxis and
-  // wilson_spatial_plane_indexed divide by V); the fundamental SU(3) value is
-  // Re Tr / 3 (tr_real, multiply_conj_tr)
-  const double scale = 1.0 / ((double)g.V * ((!adjoint && Store::NC == 3) ? 3.0 : 1.0));
-  return launch_reduce_rows(partials, blocks, nt, scale, out_dev, s);
+  return launch_reduce_rows(partials, blocks, nt, line_loop_scale(g, Store::NC, adjoint),
+                            out_dev, s);
 }
 
 template <class Store, class CT>
 int launch_offaxis_loops(const Geom &g, const Fields4 &U, const void *S, const int disp[3],
                          int tmin, int tmax, bool adjoint, double *partials, double *out_dev,
-                         cudaStream_t s) {
+                         cudaStream_t s, int pstride) {
   const int d4[4] = {disp[0], disp[1], disp[2], 0};
   return launch_line_loops<Store, CT>(g, U.f[3], 3, S, d4, tmin, tmax, adjoint, partials,
-                                      out_dev, s);
+                                      out_dev, s, pstride);
 }
 
 template <class Store, class CT>
@@ -260,12 +266,12 @@ int launch_line_extend(const Geom &g, const void *F, void *S, int ax, int offset
                                               const OffaxisSteps &, void *, cudaStream_t); \
   template int launch_line_loops<STORE, CT>(const Geom &, const void *, int, const void *, \
                                             const int *, int, int, bool, double *,        \
-                                            double *, cudaStream_t);                      \
+                                            double *, cudaStream_t, int);                 \
   template int launch_line_extend<STORE, CT>(const Geom &, const void *, void *, int, int,  \
                                              int, bool, cudaStream_t);                     \
   template int launch_offaxis_loops<STORE, CT>(const Geom &, const Fields4 &, const void *, \
                                                const int *, int, int, bool, double *,      \
-                                               double *, cudaStream_t);
+                                               double *, cudaStream_t, int);
 
 GC_INSTANTIATE_O(StoreF64SU3, double)
 GC_INSTANTIATE_O(StoreF64SU2, double)
