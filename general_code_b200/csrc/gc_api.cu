@@ -890,15 +890,30 @@ static int offaxis_impl(gc_lattice *h, const std::vector<std::array<int, 3>> &di
   if (plan.lines.empty())
     return GC_OK;
   std::lock_guard<std::mutex> lk(h->mu);
-  const size_t line_bytes =
-      ((inter_link_bytes(h->nc, h->prec) * (size_t)h->g.V + 255) / 256) * 256;
-  rc = ensure_aux(h, line_bytes);
+  // the lines as a device table (steps and end displacement as residues)
+  std::vector<OffaxisLineDesc> table(plan.lines.size());
+  for (size_t i = 0; i < table.size(); i++) {
+    const OffaxisLine &line = plan.lines[i];
+    OffaxisLineDesc &d = table[i];
+    std::memset(&d, 0, sizeof d);
+    d.n = (int)line.pattern.size();
+    for (int k = 0; k < 3; k++)
+      d.d[k] = ((line.disp[k] % h->g.L[k]) + h->g.L[k]) % h->g.L[k];
+    for (int q = 0; q < d.n; q++)
+      d.s[q] = (signed char)line.pattern[q];
+  }
+  rc = ensure_aux(h, table.size() * sizeof(OffaxisLineDesc));
   if (rc)
     return rc;
-  // Lines go in chunks that share one partials buffer, [block][line][T], and
-  // one reduction launch (a reduction per line cost as much as a tenth of
-  // the line's time); a chunk's partials stay within 32 MB.
-  const size_t per_line = (size_t)offaxis_partials_count(h->g, nt);
+  // (from pageable memory: returns once the table is staged, so `table` may go)
+  cudaError_t ce = cudaMemcpyAsync(h->aux, table.data(), table.size() * sizeof(OffaxisLineDesc),
+                                   cudaMemcpyHostToDevice, h->stream);
+  if (ce != cudaSuccess)
+    return cuda_fail(h, "cudaMemcpyAsync(off-axis lines)", ce);
+  // Lines go in chunks whose partials, [block][line][T], stay within 32 MB,
+  // one fused launch and one reduction per chunk.
+  const int blocks = offaxis_fused_blocks(h->g, h->nc, h->prec == GC_PREC_FP64 ? 8 : 4);
+  const size_t per_line = (size_t)blocks * nt;
   const size_t chunk =
       std::max<size_t>(1, std::min(plan.lines.size(), ((size_t)4 << 20) / per_line));
   rc = ensure_partials(h, per_line * chunk);
@@ -907,26 +922,15 @@ static int offaxis_impl(gc_lattice *h, const std::vector<std::array<int, 3>> &di
   rc = ensure_dev_out(h, plan.lines.size() * (size_t)nt);
   if (rc)
     return rc;
-  const int blocks = (int)(per_line / nt);
+  const OffaxisLineDesc *dev_lines = static_cast<const OffaxisLineDesc *>(h->aux);
   for (size_t c0 = 0; c0 < plan.lines.size(); c0 += chunk) {
-    const size_t n = std::min(chunk, plan.lines.size() - c0);
-    for (size_t k = 0; k < n; k++) {
-      const OffaxisLine &line = plan.lines[c0 + k];
-      OffaxisSteps steps;
-      steps.n = (int)line.pattern.size();
-      for (int q = 0; q < steps.n; q++)
-        steps.s[q] = (signed char)line.pattern[q];
-      rc = GC_DISPATCH(h, launch_offaxis_line, h->g, h->cur, steps, h->aux, h->stream);
-      if (!rc)
-        rc = GC_DISPATCH(h, launch_offaxis_loops, h->g, h->cur, h->aux, line.disp, tmin, tmax,
-                         adjoint, h->partials + k * nt, (double *)nullptr, h->stream,
-                         (int)(n * nt));
-      if (rc)
-        return launch_fail(h, rc);
-    }
-    rc = launch_reduce_rows(h->partials, blocks, (int)(n * nt),
-                            line_loop_scale(h->g, h->nc, adjoint), h->dev_out + c0 * nt,
-                            h->stream);
+    const int n = (int)std::min(chunk, plan.lines.size() - c0);
+    int b = 0;
+    rc = GC_DISPATCH(h, launch_offaxis_fused, h->g, h->cur, dev_lines + c0, n, tmin, tmax,
+                     adjoint, h->partials, &b, h->stream);
+    if (!rc)
+      rc = launch_reduce_rows(h->partials, b, n * nt, line_loop_scale(h->g, h->nc, adjoint),
+                              h->dev_out + c0 * nt, h->stream);
     if (rc)
       return launch_fail(h, rc);
   }

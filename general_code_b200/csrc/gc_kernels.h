@@ -1,6 +1,10 @@
 // Host-side declarations of the kernel launchers (implemented in the .cu files).
 #pragma once
 
+#include <mutex>
+#include <set>
+#include <utility>
+
 #include "../../include/gc_lattice.h"
 #include "gc_internal.cuh"
 
@@ -166,15 +170,19 @@ int launch_reduce_rows(const double *partials, int blocks, int n, double scale,
 
 // ------------------------------------------------------------ off-axis loops
 constexpr int kOffaxisMaxSteps = 256;
-// A space line's links, in order: +a steps forward along axis a-1 (1..3), -a
-// steps back and takes the link's adjoint.
-struct OffaxisSteps {
-  signed char s[kOffaxisMaxSteps];
-  int n;
-};
+// A space line's links, in order (OffaxisLine::pattern, OffaxisLineDesc::s):
+// +a steps forward along axis a-1 (1..3), -a steps back and takes the
+// link's adjoint.
 struct OffaxisLine {
   std::vector<int> pattern;
   int disp[3];
+};
+// Device table entry of one line for the fused kernel: its steps and the
+// displacement of its end as non-negative residues.
+struct OffaxisLineDesc {
+  int n;
+  int d[3];
+  signed char s[kOffaxisMaxSteps];
 };
 // The lines of one (direction, length multiplier), in the order whose
 // values are averaged.
@@ -192,23 +200,21 @@ OffaxisPlan offaxis_plan(const std::vector<std::array<int, 3>> &directions, doub
                          double r_max);
 void offaxis_reduce(std::vector<gc_wilson_result> &results);
 int offaxis_partials_count(const Geom &g, int nt);
-// The space line of `steps` from every site into S (V matrices in the
-// decorated-link storage of Store).
-template <class Store, class CT>
-int launch_offaxis_line(const Geom &g, const Fields4 &U, const OffaxisSteps &steps, void *S,
-                        cudaStream_t s);
-// out_dev[T - tmin] = the loop average for the line S with displacement disp.
-// out_dev == nullptr: only the per-block partial sums, at
-// partials[block * pstride + (T - tmin)] (pstride >= tmax - tmin + 1), for
-// one reduction over several lines (launch_reduce_rows with
-// line_loop_scale).
-template <class Store, class CT>
-int launch_offaxis_loops(const Geom &g, const Fields4 &U, const void *S, const int disp[3],
-                         int tmin, int tmax, bool adjoint, double *partials, double *out_dev,
-                         cudaStream_t s, int pstride = 0);
 // Scale of the summed partials of the line loops (1/V, and 1/N for the
 // fundamental SU(3) trace).
 double line_loop_scale(const Geom &g, int nc, bool adjoint);
+// Off-axis loops of nlines lines (device table `lines`) in one launch: a
+// block owns a few spatial columns over all t and a group of lines; the
+// line products, the columns' time links and the displaced columns' time
+// links sit in shared memory and the T walk reads only those. Per-block
+// partial sums at partials[(block * nlines + line) * nt + (T - tmin)];
+// returns the number of blocks (rows of partials) in *blocks.
+template <class Store, class CT>
+int launch_offaxis_fused(const Geom &g, const Fields4 &U, const OffaxisLineDesc *lines,
+                         int nlines, int tmin, int tmax, bool adjoint, double *partials,
+                         int *blocks, cudaStream_t s);
+// Column blocks of the fused launch (rows of its partials) for a lattice.
+int offaxis_fused_blocks(const Geom &g, int nc, int ct_bytes);
 
 // Loops of a line field S (decorated-link storage) whose end is displaced
 // by disp (disp[ax] = 0) with "time" axis ax and time links Ut:
@@ -249,5 +255,36 @@ int launch_aos_to_soa(const Geom &g, int nc, int prec, int layout,
                       int site0 = 0, int nsites = -1);
 int launch_soa_to_aos(const Geom &g, int nc, int prec, int layout,
                       const Fields4 &U, double *staging, cudaStream_t s);
+
+// Lets `kernel` use up to the device's opt-in shared memory per block. Set
+// once per (kernel, device) rather than before every launch: concurrent
+// request threads would otherwise call cudaFuncSetAttribute on every W
+// launch. The attribute only raises the allowed maximum; each launch still
+// asks for the shared memory it needs.
+template <class K> inline int allow_large_smem(K *kernel, size_t smem, bool capturing = false) {
+  if (smem <= 48 * 1024)
+    return GC_OK;
+  static std::mutex mu;
+  static std::set<std::pair<const void *, int>> done;
+  int dev = 0;
+  cudaGetDevice(&dev);
+  std::lock_guard<std::mutex> lk(mu);
+  if (done.count({(const void *)kernel, dev}))
+    return GC_OK;
+  // (while a stream is captured the attribute set by an earlier eager launch
+  // of the same schedule stays in force)
+  if (capturing)
+    return GC_OK;
+  int optin = 0;
+  cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+  if ((size_t)optin < smem)
+    return plan_error("kernel: shared memory above the device's limit");
+  if (cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, optin) !=
+      cudaSuccess)
+    return launch_check("shared-memory attribute");
+  done.insert({(const void *)kernel, dev});
+  return GC_OK;
+}
+
 
 } // namespace gc

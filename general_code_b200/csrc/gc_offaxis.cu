@@ -15,12 +15,16 @@
 //     Re Tr[ L(x,T) S(x+T t) L(x+D,T)^dag S(x)^dag ] / N   (or |Tr|^2 - 1),
 // averaged over all sites x.
 //
-// offaxis_line_kernel: thread per site, the product of the pattern's links
-// (a negative step moves back first and multiplies by the link's adjoint)
-// into a field of V matrices. line_loop_kernel: thread per site, the same
-// exact recursion as the on-axis kernel, K_0 = S(x),
+// offaxis_fused_kernel: a block owns a few spatial columns over all t and a
+// group of lines. Per line, a thread per (column, t) forms the product of
+// the pattern's links (a negative step moves back first and multiplies by
+// the link's adjoint) into shared memory, beside the columns' own time links
+// (loaded once per block) and the displaced columns' time links; then the
+// same exact recursion as the on-axis kernel, K_0 = S(x),
 // K_T = U_t(x+(T-1)t)^dag K_{T-1} U_t(x+D+(T-1)t), value Re Tr[S(x+T t) K_T^dag],
-// with fixed-order warp / block / grid sums (deterministic).
+// reads only shared memory. line_loop_kernel is that recursion over a line
+// field in global memory, thread per site, for the spatial loops (any
+// "time" axis). Fixed-order warp / block / grid sums (deterministic).
 #include "gc_internal.cuh"
 #include "gc_kernels.h"
 
@@ -56,48 +60,6 @@ template <bool ADJ, class T> __device__ __forceinline__ double offaxis_value(con
   const double d = dot4(double(a.a0), double(b.a0), double(a.a1), double(b.a1),
                         double(a.a2), double(b.a2), double(a.a3), double(b.a3));
   return ADJ ? 4.0 * d * d - 1.0 : d;
-}
-
-template <class Store, class CT>
-__global__ void __launch_bounds__(256)
-    offaxis_line_kernel(const __grid_constant__ Geom g, const __grid_constant__ Fields4 U,
-                        const __grid_constant__ OffaxisSteps steps, void *S) {
-  using M = typename Store::template M<CT>;
-  using IS = typename InterStore<Store>::type;
-  const int site = blockIdx.x * blockDim.x + threadIdx.x;
-  if (site >= g.V)
-    return;
-  const size_t V = g.V;
-  int x[4];
-  site_coords(g, site, x);
-  int cur = site;
-  M A = unit(M());
-#pragma unroll 1
-  for (int i = 0; i < steps.n; i++) {
-    const int e = steps.s[i];
-    const int mu = (e > 0 ? e : -e) - 1;
-    const int L = sel4(g.L, mu), st = sel4(g.stride, mu);
-    int c = mu == 0 ? x[0] : (mu == 1 ? x[1] : x[2]);
-    M u;
-    if (e > 0) {
-      u = Store::template load<CT>(U.f[mu], V, cur);
-      cur += (c == L - 1) ? -(L - 1) * st : st;
-      c = (c == L - 1) ? 0 : c + 1;
-    } else {
-      cur += (c == 0) ? (L - 1) * st : -st;
-      c = (c == 0) ? L - 1 : c - 1;
-      u = adjoint(Store::template load<CT>(U.f[mu], V, cur));
-    }
-    if (mu == 0)
-      x[0] = c;
-    else if (mu == 1)
-      x[1] = c;
-    else
-      x[2] = c;
-    // the first factor is taken as it is (identity times a link is exact)
-    A = (i == 0) ? u : mul(A, u);
-  }
-  IS::template store<CT>(S, V, site, A);
 }
 
 // partials[block * nt + (T - tmin)]. The loop's "time" axis is ax (3 for the
@@ -189,19 +151,230 @@ __global__ void __launch_bounds__(256)
 
 constexpr int kOffaxisBlock = 128;
 
+// Matrices in shared memory as planes of reals, [real][slot], so that
+// consecutive threads (consecutive slots) touch consecutive words.
+template <class T>
+__device__ __forceinline__ void sm_store(T *a, int nslots, int i, const SU3<T> &m) {
+#pragma unroll
+  for (int k = 0; k < 9; k++) {
+    a[(2 * k) * nslots + i] = m.e[k / 3][k % 3].re;
+    a[(2 * k + 1) * nslots + i] = m.e[k / 3][k % 3].im;
+  }
+}
+template <class T> __device__ __forceinline__ SU3<T> sm_load(const T *a, int nslots, int i) {
+  SU3<T> m;
+#pragma unroll
+  for (int k = 0; k < 9; k++)
+    m.e[k / 3][k % 3] = {a[(2 * k) * nslots + i], a[(2 * k + 1) * nslots + i]};
+  return m;
+}
+template <class T>
+__device__ __forceinline__ void sm_store(T *a, int nslots, int i, const SU2<T> &m) {
+  a[i] = m.a0;
+  a[nslots + i] = m.a1;
+  a[2 * nslots + i] = m.a2;
+  a[3 * nslots + i] = m.a3;
+}
+template <class T> __device__ __forceinline__ SU2<T> sm_load(const T *a, int nslots, int i,
+                                                             SU2<T> *) {
+  return {a[i], a[nslots + i], a[2 * nslots + i], a[3 * nslots + i]};
+}
+template <class T> __device__ __forceinline__ SU3<T> sm_load(const T *a, int nslots, int i,
+                                                             SU3<T> *) {
+  return sm_load(a, nslots, i);
+}
+
+// Lines per block of the fused kernel (the block loads its columns' time
+// links once for these).
+constexpr int kOffaxisLinesPerBlock = 8;
+
+// Block shape of the fused kernel: rows threads per column (one start slice
+// each up to Lt = 64), cols columns, about 128 threads (256 when rows > 32),
+// shared memory (three sets of Lt x cols matrices) at most ~100 KB.
+struct FusedShape {
+  int rows, cols, threads;
+  size_t smem;
+};
+FusedShape fused_shape(const Geom &g, int nc, int ct_bytes, int nt) {
+  FusedShape f;
+  const int Lt = g.L[3];
+  f.rows = 1;
+  for (int d = 64; d >= 1; d--)
+    if (d <= Lt && Lt % d == 0) {
+      f.rows = d;
+      break;
+    }
+  f.cols = std::max(1, (f.rows > 32 ? 256 : 128) / f.rows);
+  const size_t nreal = nc == 3 ? 18 : 4;
+  auto smem_of = [&](int cols, int threads) {
+    return ((size_t)(threads / 32) * nt + 1) / 2 * 2 * sizeof(double) +
+           3 * nreal * (size_t)Lt * cols * ct_bytes;
+  };
+  for (;;) {
+    f.threads = (f.cols * f.rows + 31) / 32 * 32;
+    f.smem = smem_of(f.cols, f.threads);
+    if (f.cols == 1 || f.smem <= 100 * 1024)
+      break;
+    f.cols--;
+  }
+  return f;
+}
+
+// Off-axis loops, fused (see launch_offaxis_fused): line products walked
+// from each (column, t), then the T walk of line_loop_kernel with every
+// operand in shared memory.
+template <class Store, class CT, bool ADJ>
+__global__ void __launch_bounds__(256)
+    offaxis_fused_kernel(const __grid_constant__ Geom g, const __grid_constant__ Fields4 U,
+                         const OffaxisLineDesc *__restrict__ lines, int nlines, int tmin,
+                         int tmax, int cols, int rows, double *partials) {
+  using M = typename Store::template M<CT>;
+  constexpr int NREAL = Store::NC == 3 ? 18 : 4;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int Lt = g.L[3];
+  const int nt = tmax - tmin + 1;
+  const int nslots = Lt * cols;
+  const int nwarps = blockDim.x >> 5;
+  double *wacc = reinterpret_cast<double *>(smem_raw); // [nwarps][nt]
+  CT *ucol = reinterpret_cast<CT *>(wacc + ((nwarps * nt + 1) & ~1));
+  CT *ncol = ucol + NREAL * nslots;
+  CT *scol = ncol + NREAL * nslots;
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int c = tid % cols, row = tid / cols;
+  const int s = blockIdx.x * cols + c;
+  const bool active = row < rows && s < g.Vs;
+  const int kt = Lt / rows;
+  const size_t V = g.V;
+  const int xs0 = s % g.L[0], xs1 = (s / g.L[0]) % g.L[1], xs2 = s / (g.L[0] * g.L[1]);
+  if (active) {
+#pragma unroll 1
+    for (int k = 0; k < kt; k++) {
+      const int t = row + k * rows;
+      sm_store(ucol, nslots, t * cols + c, Store::template load<CT>(U.f[3], V, s + t * g.Vs));
+    }
+  }
+  const int l0 = blockIdx.y * kOffaxisLinesPerBlock;
+  const int l1 = min(nlines, l0 + kOffaxisLinesPerBlock);
+#pragma unroll 1
+  for (int l = l0; l < l1; l++) {
+    const OffaxisLineDesc *L = lines + l;
+    const int n = __ldg(&L->n);
+    for (int i = tid; i < nwarps * nt; i += blockDim.x)
+      wacc[i] = 0.0;
+    if (active) {
+      const int sd = (xs0 + __ldg(&L->d[0])) % g.L[0] +
+                     g.L[0] * ((xs1 + __ldg(&L->d[1])) % g.L[1] +
+                               g.L[1] * ((xs2 + __ldg(&L->d[2])) % g.L[2]));
+#pragma unroll 1
+      for (int k = 0; k < kt; k++) {
+        const int t = row + k * rows;
+        const int i = t * cols + c;
+        sm_store(ncol, nslots, i, Store::template load<CT>(U.f[3], V, sd + t * g.Vs));
+        // the line from (s, t): steps along the spatial axes, periodic
+        int x0 = xs0, x1 = xs1, x2 = xs2;
+        int cur = s + t * g.Vs;
+        M A = unit(M());
+#pragma unroll 1
+        for (int q = 0; q < n; q++) {
+          const int e = __ldg(&L->s[q]);
+          const int mu = (e > 0 ? e : -e) - 1;
+          const int Lm = sel4(g.L, mu), st = sel4(g.stride, mu);
+          int cm = mu == 0 ? x0 : (mu == 1 ? x1 : x2);
+          M u;
+          if (e > 0) {
+            u = Store::template load<CT>(U.f[mu], V, cur);
+            cur += (cm == Lm - 1) ? -(Lm - 1) * st : st;
+            cm = (cm == Lm - 1) ? 0 : cm + 1;
+          } else {
+            cur += (cm == 0) ? (Lm - 1) * st : -st;
+            cm = (cm == 0) ? Lm - 1 : cm - 1;
+            u = adjoint(Store::template load<CT>(U.f[mu], V, cur));
+          }
+          if (mu == 0)
+            x0 = cm;
+          else if (mu == 1)
+            x1 = cm;
+          else
+            x2 = cm;
+          // the first factor is taken as it is (identity times a link is exact)
+          A = (q == 0) ? u : mul(A, u);
+        }
+        sm_store(scol, nslots, i, A);
+      }
+    }
+    __syncthreads();
+#pragma unroll 1
+    for (int k = 0; k < kt; k++) {
+      const int t0 = row + k * rows;
+      M K = active ? sm_load(scol, nslots, t0 * cols + c, (M *)nullptr) : unit(M());
+      int tt = t0; // (t0 + T - 1) mod Lt
+#pragma unroll 1
+      for (int T = 1; T <= tmax; T++) {
+        int tu = tt + 1;
+        tu = (tu == Lt) ? 0 : tu;
+        if (active) {
+          const int i = tt * cols + c;
+          K = mul(mul_da(sm_load(ucol, nslots, i, (M *)nullptr), K),
+                  sm_load(ncol, nslots, i, (M *)nullptr));
+        }
+        if (T >= tmin) {
+          double v = active ? offaxis_value<ADJ>(
+                                  sm_load(scol, nslots, tu * cols + c, (M *)nullptr), K)
+                            : 0.0;
+          v = warp_sum_d(v);
+          if (lane == 0)
+            wacc[warp * nt + (T - tmin)] += v;
+        }
+        tt = tu;
+      }
+    }
+    __syncthreads();
+    for (int e = tid; e < nt; e += blockDim.x) {
+      double sum = 0.0;
+      for (int w = 0; w < nwarps; w++)
+        sum += wacc[w * nt + e];
+      partials[((size_t)blockIdx.x * nlines + l) * nt + e] = sum;
+    }
+    __syncthreads();
+  }
+}
+
 } // namespace
 
 int offaxis_partials_count(const Geom &g, int nt) {
   return ((g.V + kOffaxisBlock - 1) / kOffaxisBlock) * nt;
 }
 
+int offaxis_fused_blocks(const Geom &g, int nc, int ct_bytes) {
+  const FusedShape f = fused_shape(g, nc, ct_bytes, 1);
+  return (g.Vs + f.cols - 1) / f.cols;
+}
+
 template <class Store, class CT>
-int launch_offaxis_line(const Geom &g, const Fields4 &U, const OffaxisSteps &steps, void *S,
-                        cudaStream_t s) {
-  if (steps.n < 1 || steps.n > kOffaxisMaxSteps)
-    return plan_error("offaxis_line_kernel: pattern length");
-  offaxis_line_kernel<Store, CT><<<(g.V + 255) / 256, 256, 0, s>>>(g, U, steps, S);
-  return launch_check("offaxis_line_kernel");
+int launch_offaxis_fused(const Geom &g, const Fields4 &U, const OffaxisLineDesc *lines,
+                         int nlines, int tmin, int tmax, bool adjoint, double *partials,
+                         int *blocks, cudaStream_t s) {
+  const int nt = tmax - tmin + 1;
+  if (nt < 1 || nt > kWilsonMaxEntries || nlines < 1)
+    return plan_error("offaxis_fused_kernel: time range or line count");
+  const FusedShape f = fused_shape(g, Store::NC, (int)sizeof(CT), nt);
+  if (f.smem > 227 * 1024)
+    return plan_error("offaxis_fused_kernel: time extent too large for shared memory");
+  const int colblocks = (g.Vs + f.cols - 1) / f.cols;
+  const dim3 grid(colblocks, (nlines + kOffaxisLinesPerBlock - 1) / kOffaxisLinesPerBlock);
+  int rc = adjoint ? allow_large_smem(offaxis_fused_kernel<Store, CT, true>, f.smem)
+                   : allow_large_smem(offaxis_fused_kernel<Store, CT, false>, f.smem);
+  if (rc)
+    return rc;
+  if (adjoint)
+    offaxis_fused_kernel<Store, CT, true><<<grid, f.threads, f.smem, s>>>(
+        g, U, lines, nlines, tmin, tmax, f.cols, f.rows, partials);
+  else
+    offaxis_fused_kernel<Store, CT, false><<<grid, f.threads, f.smem, s>>>(
+        g, U, lines, nlines, tmin, tmax, f.cols, f.rows, partials);
+  if (blocks)
+    *blocks = colblocks;
+  return launch_check("offaxis_fused_kernel");
 }
 
 double line_loop_scale(const Geom &g, int nc, bool adjoint) {
@@ -243,15 +416,6 @@ int launch_line_loops(const Geom &g, const void *Ut, int ax, const void *S, cons
 }
 
 template <class Store, class CT>
-int launch_offaxis_loops(const Geom &g, const Fields4 &U, const void *S, const int disp[3],
-                         int tmin, int tmax, bool adjoint, double *partials, double *out_dev,
-                         cudaStream_t s, int pstride) {
-  const int d4[4] = {disp[0], disp[1], disp[2], 0};
-  return launch_line_loops<Store, CT>(g, U.f[3], 3, S, d4, tmin, tmax, adjoint, partials,
-                                      out_dev, s, pstride);
-}
-
-template <class Store, class CT>
 int launch_line_extend(const Geom &g, const void *F, void *S, int ax, int offset, int count,
                        bool init, cudaStream_t s) {
   if (ax < 0 || ax > 3 || count < 0 || offset < 0)
@@ -262,16 +426,14 @@ int launch_line_extend(const Geom &g, const void *F, void *S, int ax, int offset
 }
 
 #define GC_INSTANTIATE_O(STORE, CT)                                                        \
-  template int launch_offaxis_line<STORE, CT>(const Geom &, const Fields4 &,              \
-                                              const OffaxisSteps &, void *, cudaStream_t); \
   template int launch_line_loops<STORE, CT>(const Geom &, const void *, int, const void *, \
                                             const int *, int, int, bool, double *,        \
                                             double *, cudaStream_t, int);                 \
   template int launch_line_extend<STORE, CT>(const Geom &, const void *, void *, int, int,  \
                                              int, bool, cudaStream_t);                     \
-  template int launch_offaxis_loops<STORE, CT>(const Geom &, const Fields4 &, const void *, \
-                                               const int *, int, int, bool, double *,      \
-                                               double *, cudaStream_t, int);
+  template int launch_offaxis_fused<STORE, CT>(const Geom &, const Fields4 &,              \
+                                               const OffaxisLineDesc *, int, int, int,     \
+                                               bool, double *, int *, cudaStream_t);
 
 GC_INSTANTIATE_O(StoreF64SU3, double)
 GC_INSTANTIATE_O(StoreF64SU2, double)

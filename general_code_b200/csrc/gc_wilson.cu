@@ -498,36 +498,6 @@ __global__ void __launch_bounds__(256)
   }
 }
 
-// Lets `kernel` use up to the device's opt-in shared memory per block. Set
-// once per (kernel, device) rather than before every launch: concurrent
-// request threads would otherwise call cudaFuncSetAttribute on every W
-// launch. The attribute only raises the allowed maximum; each launch still
-// asks for the shared memory it needs.
-template <class K> int allow_large_smem(K *kernel, size_t smem, bool capturing = false) {
-  if (smem <= 48 * 1024)
-    return GC_OK;
-  static std::mutex mu;
-  static std::set<std::pair<const void *, int>> done;
-  int dev = 0;
-  cudaGetDevice(&dev);
-  std::lock_guard<std::mutex> lk(mu);
-  if (done.count({(const void *)kernel, dev}))
-    return GC_OK;
-  // (while a stream is captured the attribute set by an earlier eager launch
-  // of the same schedule stays in force)
-  if (capturing)
-    return GC_OK;
-  int optin = 0;
-  cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
-  if ((size_t)optin < smem)
-    return plan_error("W kernel: shared memory above the device's limit");
-  if (cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, optin) !=
-      cudaSuccess)
-    return launch_check("wilson kernel shared-memory attribute");
-  done.insert({(const void *)kernel, dev});
-  return GC_OK;
-}
-
 int largest_divisor_upto(int n, int cap) {
   for (int d = cap < n ? cap : n; d > 1; d--)
     if (n % d == 0)
