@@ -184,6 +184,38 @@ template <class T> __device__ __forceinline__ SU3<T> sm_load(const T *a, int nsl
   return sm_load(a, nslots, i);
 }
 
+// One step of a space line from the site `cur` with spatial coordinates
+// (x0, x1, x2): e = +a moves forward along axis a-1 and returns the link it
+// crossed, e = -a moves back and returns the adjoint of the link it crossed.
+template <class Store, class CT>
+__device__ __forceinline__ typename Store::template M<CT>
+step_link(const Geom &g, const Fields4 &U, int e, int &x0, int &x1, int &x2, int &cur) {
+  using M = typename Store::template M<CT>;
+  const size_t V = g.V;
+  const int mu = (e > 0 ? e : -e) - 1;
+  const int Lm = sel4(g.L, mu), st = sel4(g.stride, mu);
+  int cm = mu == 0 ? x0 : (mu == 1 ? x1 : x2);
+  // (a select, not U.f[mu]: an indexed parameter array goes to the stack)
+  const void *f = mu == 0 ? U.f[0] : (mu == 1 ? U.f[1] : U.f[2]);
+  M u;
+  if (e > 0) {
+    u = Store::template load<CT>(f, V, cur);
+    cur += (cm == Lm - 1) ? -(Lm - 1) * st : st;
+    cm = (cm == Lm - 1) ? 0 : cm + 1;
+  } else {
+    cur += (cm == 0) ? (Lm - 1) * st : -st;
+    cm = (cm == 0) ? Lm - 1 : cm - 1;
+    u = adjoint(Store::template load<CT>(f, V, cur));
+  }
+  if (mu == 0)
+    x0 = cm;
+  else if (mu == 1)
+    x1 = cm;
+  else
+    x2 = cm;
+  return u;
+}
+
 // Lines per block of the fused kernel (the block loads its columns' time
 // links once for these).
 constexpr int kOffaxisLinesPerBlock = 8;
@@ -270,34 +302,20 @@ __global__ void __launch_bounds__(256)
         const int t = row + k * rows;
         const int i = t * cols + c;
         sm_store(ncol, nslots, i, Store::template load<CT>(U.f[3], V, sd + t * g.Vs));
-        // the line from (s, t): steps along the spatial axes, periodic
+        // the line from (s, t): steps along the spatial axes, periodic. The
+        // link of step q+1 is loaded before step q's product (its address
+        // needs only the step pattern), so the load's latency overlaps it.
         int x0 = xs0, x1 = xs1, x2 = xs2;
         int cur = s + t * g.Vs;
-        M A = unit(M());
+        // the first factor is taken as it is (identity times a link is exact)
+        M A = step_link<Store, CT>(g, U, __ldg(&L->s[0]), x0, x1, x2, cur);
+        M u = (n > 1) ? step_link<Store, CT>(g, U, __ldg(&L->s[1]), x0, x1, x2, cur) : A;
 #pragma unroll 1
-        for (int q = 0; q < n; q++) {
-          const int e = __ldg(&L->s[q]);
-          const int mu = (e > 0 ? e : -e) - 1;
-          const int Lm = sel4(g.L, mu), st = sel4(g.stride, mu);
-          int cm = mu == 0 ? x0 : (mu == 1 ? x1 : x2);
-          M u;
-          if (e > 0) {
-            u = Store::template load<CT>(U.f[mu], V, cur);
-            cur += (cm == Lm - 1) ? -(Lm - 1) * st : st;
-            cm = (cm == Lm - 1) ? 0 : cm + 1;
-          } else {
-            cur += (cm == 0) ? (Lm - 1) * st : -st;
-            cm = (cm == 0) ? Lm - 1 : cm - 1;
-            u = adjoint(Store::template load<CT>(U.f[mu], V, cur));
-          }
-          if (mu == 0)
-            x0 = cm;
-          else if (mu == 1)
-            x1 = cm;
-          else
-            x2 = cm;
-          // the first factor is taken as it is (identity times a link is exact)
-          A = (q == 0) ? u : mul(A, u);
+        for (int q = 1; q < n; q++) {
+          const M cu = u;
+          if (q + 1 < n)
+            u = step_link<Store, CT>(g, U, __ldg(&L->s[q + 1]), x0, x1, x2, cur);
+          A = mul(A, cu);
         }
         sm_store(scol, nslots, i, A);
       }
