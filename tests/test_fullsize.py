@@ -91,3 +91,23 @@ def test_w_is_gauge_invariant_at_full_size(form, rtol):
         w0 = _job(lat, plain, ape, rt)
         w1 = _job(lat, rotated, ape, rt)
     np.testing.assert_allclose(w1, w0, rtol=rtol, atol=1e-14)
+
+
+def test_offaxis_full_size_translation_and_mixed():
+    """Off-axis loops on SU(3) 24^4 (r <= 6, T <= 6: 678 lines in three
+    launches of the fused kernel): the same table for the configuration
+    translated by (3, 0, 0, 5) (FP64, 1e-12), and the mixed form within 1e-6
+    of FP64."""
+    nc, dims = 3, (24, 24, 24, 24)
+    links = generate_config(dims, nc, 0.25, SEED, 2)
+    moved = np.roll(links.reshape(dims[3], dims[2], dims[1], dims[0], 4, 18), (5, 3),
+                    axis=(0, 3)).reshape(links.shape)
+    res = {}
+    for key, form, x in (("a", "fp64", links), ("b", "fp64", moved), ("m", "mixed", links)):
+        with Lattice(dims, nc, form) as lat:
+            lat.upload(np.ascontiguousarray(x))
+            res[key] = lat.wilson_offaxis_result(1.0, 6.0, 1, 6)
+    assert res["a"].keys() == res["b"].keys() == res["m"].keys() and len(res["a"]) > 100
+    for k, v in res["a"].items():
+        assert res["b"][k] == pytest.approx(v, rel=1e-12, abs=1e-14)
+        assert abs(res["m"][k] - v) <= 1e-6 * abs(v) + 1e-9

@@ -301,12 +301,13 @@ def test_fp64_offaxis_matches_reference_fixture(name, meta):
                 assert got[k] == pytest.approx(v, rel=W_RTOL, abs=W_ATOL)
 
 
-@pytest.mark.parametrize("nc,eps", [(2, 0.3), (3, 0.25)])
-def test_offaxis_matches_oracle_seeded(port, nc, eps):
+@pytest.mark.parametrize("nc,eps,dims", [(2, 0.3, (7, 6, 8, 6)), (3, 0.25, (7, 6, 8, 6)),
+                                         (3, 0.25, (4, 3, 5, 40))])
+def test_offaxis_matches_oracle_seeded(port, nc, eps, dims):
     """Unmerged entries for several directions (multipliers up to 3, odd
-    extents, negative displacements after reflection) in both forms: FP64
-    within 1e-12, mixed within 1e-6 relative."""
-    dims = (7, 6, 8, 6)
+    extents, negative displacements after reflection; Lt = 40: 40 threads
+    per column in the fused kernel) in both forms: FP64 within 1e-12, mixed
+    within 1e-6 relative."""
     links = generate_config(dims, nc, eps, 20261203, 51)
     dirs = [[1, 0, 0], [1, 1, 0], [2, 1, 0], [1, 1, 1], [2, 2, 1]]
     for adjoint in (False, True):
