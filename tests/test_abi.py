@@ -55,6 +55,22 @@ def test_null_handle_is_an_error_not_a_crash():
     assert lib().gc_lattice_destroy(None) == _lib.GC_OK
 
 
+def test_slice_and_probe_entry_points_validate_arguments():
+    """The t-slab slice entry points, the slab W and the FMA probe reject
+    null handles and bad arguments before any device call."""
+    l = lib()
+    out = (ctypes.c_double * 4)()
+    host = (ctypes.c_double * 4)()
+    assert l.gc_upload_slices(None, 0, 1, host, 0) == _lib.GC_ERR_ARG
+    assert l.gc_slice_bytes(None, 1) == -1
+    assert l.gc_pack_slices(None, 0, 1, ctypes.c_void_p(16)) == _lib.GC_ERR_ARG
+    assert l.gc_unpack_slices(None, 0, 1, ctypes.c_void_p(16)) == _lib.GC_ERR_ARG
+    assert l.gc_copy_slices(None, 0, None, 0, 1) == _lib.GC_ERR_ARG
+    assert l.gc_wilson_onaxis_tslab(None, 1, 1, 1, 1, 1, 0, out) == _lib.GC_ERR_ARG
+    assert l.gc_fma_peak(7, out) == _lib.GC_ERR_ARG
+    assert l.gc_fma_peak(0, None) == _lib.GC_ERR_ARG
+
+
 def _has_gpu():
     h = ctypes.c_void_p()
     rc = lib().gc_lattice_create(dims_arg((2, 2, 2, 2)), 2, 0, ctypes.byref(h))
