@@ -246,6 +246,7 @@ int launch_polyakov_lines(const Geom &g, const Fields4 &U, double2 *lines, doubl
 int launch_polyakov_correlator(const Geom &g, int nc, const double2 *lines, const int4 *offsets,
                                int noffsets, bool singlet, double *out_dev, cudaStream_t s);
 size_t wilson_partials_count(const Geom &g, int nr, int nt, int nc, int sets = 3);
+int wilson_max_blocks(const Geom &g, int nc, int sets = 3);
 
 // Host AoS (uploaded raw to a device staging buffer) <-> device SoA fields.
 // The upload converts the sites [site0, site0 + nsites) (all of them when

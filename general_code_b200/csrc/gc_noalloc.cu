@@ -130,7 +130,7 @@ extern "C" int gc_wilson_onaxis_noalloc(const int dims[4], int nc, int precision
   g.V = (int)V;
   g.Vs = dims[0] * dims[1] * dims[2];
 
-  const size_t blocks = (size_t)wilson_plan(g, 1, nt, nc, 8).blocks;
+  const size_t blocks = (size_t)wilson_max_blocks(g, nc);
   const size_t per_r = blocks * nt + nt;
   const size_t fit = kNoAllocScratchDoubles / per_r;
   if (fit < 1) {

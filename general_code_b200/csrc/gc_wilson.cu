@@ -26,6 +26,7 @@
 #include "gc_kernels.h"
 #include "gc_pair.cuh"
 
+#include <algorithm>
 #include <mutex>
 #include <set>
 #include <type_traits>
@@ -508,14 +509,15 @@ int largest_divisor_upto(int n, int cap) {
 } // namespace
 
 // The block shape depends only on Lt, the group and the compute type, never
-// on the R/T ranges. rows = the largest divisor of Lt up to 64 threads per
-// column (each thread carrying `lanes` columns, so one start slice per thread
-// when Lt <= 64): about 128 threads per block, 256 when rows > 32. A thread
-// walking several starts would need that many times the shared memory per
-// thread, and shared memory is what bounds the resident warps. Columns are
-// limited so that the shared column storage fits kWilsonColumnBudget. The
-// FP64 plan has the fewest columns per block and so the most blocks: callers
-// that size per-block partials before the compute type is known use it.
+// on the R/T ranges (callers size the partial sums before they know the
+// ranges of later launches). rows = the largest divisor of Lt up to 64
+// threads per column, so one start slice per thread up to Lt = 64 (a thread
+// walking several starts needs that many times the shared memory per
+// thread); each thread carries `lanes` columns; about 128 threads per block,
+// 256 when rows > 32. Columns are limited so that the column storage fits
+// kWilsonColumnBudget. (Choosing the columns instead for the most resident
+// threads per SM -- smaller blocks at Lt = 16 and 32 -- measured slower:
+// 32^4 W 9.06 -> 9.60 ms mixed, 18.2 -> 19.1 ms FP64.)
 WilsonPlan wilson_plan(const Geom &g, int nr, int nt, int nc, int ct_bytes, int sets) {
   WilsonPlan p;
   const int Lt = g.L[3];
@@ -541,8 +543,15 @@ WilsonPlan wilson_plan(const Geom &g, int nr, int nt, int nc, int ct_bytes, int 
   return p;
 }
 
+// Blocks of the W plan for either compute type, whichever has more: the
+// size of per-block partial sums a handle needs before its form is known.
+int wilson_max_blocks(const Geom &g, int nc, int sets) {
+  return std::max(wilson_plan(g, 1, 1, nc, 4, sets).blocks,
+                  wilson_plan(g, 1, 1, nc, 8, sets).blocks);
+}
+
 size_t wilson_partials_count(const Geom &g, int nr, int nt, int nc, int sets) {
-  return (size_t)wilson_plan(g, nr, nt, nc, 8, sets).blocks * nr * nt;
+  return (size_t)wilson_max_blocks(g, nc, sets) * nr * nt;
 }
 
 int plaquette_partials_count(const Geom &g) { return 2 * ((g.V + 255) / 256); }
