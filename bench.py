@@ -466,6 +466,91 @@ def bench_observables(steps: int):
                                                     "slabs run one after another on one GPU")}
 
 
+def run_tslab(args, wl, rank, world, dist):
+    """One lattice (the workload's) split into time slabs over the ranks:
+    strong scaling. Each step smears and measures from the rank's resident raw
+    slices (value) or from the pinned host configuration (e2e), with the
+    forward-halo exchange and the all-reduce of the W table inside; CUDA
+    events on the current stream, max over ranks. The mixed form."""
+    import torch
+    from general_code_b200 import generate_config, link_size
+    from general_code_b200.tslab import TSlabJob
+
+    nc, dims = wl["nc"], wl["dims"]
+    V = int(np.prod(dims))
+    host_t = torch.empty((4 * V, link_size(nc)), dtype=torch.float64, pin_memory=True)
+    host = host_t.numpy()
+    generate_config(dims, nc, wl["eps"], SEED, 0, out=host)  # the same lattice on every rank
+    flush_buf = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device="cuda")
+    form = "fp64" if args.form == "fp64" else "mixed"
+
+    def barrier():
+        torch.cuda.synchronize()
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    def timed(job, steps, from_host):
+        ms, w = 0.0, None
+        for _ in range(steps):
+            with torch.cuda.stream(job.stream):
+                flush_buf.fill_(1.0)
+            e0, e1 = (torch.cuda.Event(enable_timing=True) for _ in range(2))
+            e0.record(job.stream)
+            w = job.run(host if from_host else None)
+            e1.record(job.stream)
+            torch.cuda.synchronize()
+            ms += e0.elapsed_time(e1)
+        return ms, w
+
+    def max_over_ranks(x):
+        if dist is None:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    with TSlabJob(dims, nc, precision=form, hyp=wl["hyp"], hyp_steps=1, ape_alpha=wl["alpha"],
+                  ape_steps=wl["ape"], r_min=wl["r"][0], r_max=wl["r"][1],
+                  time_min=wl["t"][0], time_max=wl["t"][1]) as job:
+        job.load(host)
+        timed(job, args.warmup, False)
+        barrier()
+        ms, w = timed(job, args.steps, False)
+        barrier()
+        timed(job, args.warmup, True)
+        barrier()
+        ms_e2e, w_e2e = timed(job, args.steps, True)
+        barrier()
+        slab = job.plan.bounds[rank][1]
+        runs = job.plan.upload_runs(rank)
+    h2d = sum(k for _, _, k in runs) * 4 * (V // dims[3]) * link_size(nc) * 8
+    assert np.array_equal(w, w_e2e), "resident and end-to-end runs disagree"
+    ms, ms_e2e = max_over_ranks(ms), max_over_ranks(ms_e2e)
+    if rank == 0:
+        print(json.dumps({
+            "metric": "smeared+measured sites/s", "value": V * args.steps / (ms * 1e-3),
+            "unit": "sites/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "strong",
+            "vs_baseline": None, "dtype": "f64" if form == "fp64" else "f32/f64",
+            "data": "synthetic",
+            "config": {"workload": args.workload, "form": form, "lattice": list(dims),
+                       "decomposition": f"{world} time slabs (rank 0: {slab} slices)",
+                       "l2": "flushed (256 MiB write) before every timed step",
+                       "parallelism": f"tslab x{world}"},
+            "e2e": {"value": V * args.steps / (ms_e2e * 1e-3), "unit": "sites/s",
+                    "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": int(w.nbytes)},
+            # per step: HYP 3 + APE n + W 2 kernels; e2e adds a layout conversion
+            # per uploaded run of slices
+            "gpu_launches": args.steps * (2 * (3 + wl["ape"] + 2) + len(runs)),
+            "roofline": None,
+            "note": "the headline run (--decomp replicas) carries the roofline and CPU baseline"}),
+            flush=True)
+    if dist is not None:
+        dist.destroy_process_group()
+    return 0
+
+
 def run_reference(args, wl, rank):
     if rank != 0:
         return 0
@@ -503,6 +588,9 @@ def main():
                     help="extra single-GPU measurements: batch, serving, observables "
                          "(comma list, or none)")
     ap.add_argument("--serving-seconds", type=float, default=10.0)
+    ap.add_argument("--decomp", choices=["replicas", "tslab"], default="replicas",
+                    help="replicas: one configuration per rank (weak scaling); tslab: one "
+                         "lattice split into time slabs over the ranks (strong scaling)")
     args = ap.parse_args()
     if args.warmup < 3:
         ap.error("--warmup must be >= 3")
@@ -524,6 +612,9 @@ def main():
                                 device_id=torch.device("cuda", local_rank))
 
     from general_code_b200 import Lattice, generate_config, link_size
+
+    if args.decomp == "tslab":
+        return run_tslab(args, wl, rank, world, dist)
 
     nc, dims = wl["nc"], wl["dims"]
     V = int(np.prod(dims))

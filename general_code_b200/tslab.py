@@ -43,8 +43,8 @@ import numpy as np
 
 from .lattice import Lattice, link_size, volume
 
-__all__ = ["slab_bounds", "SlabPlan", "Run", "exchange_forward_halo", "smear_measure",
-           "emulate"]
+__all__ = ["slab_bounds", "SlabPlan", "Run", "exchange_forward_halo", "TSlabJob",
+           "smear_measure", "emulate"]
 
 
 def slab_bounds(lt: int, world: int) -> List[Tuple[int, int]]:
@@ -237,6 +237,109 @@ def _check_args(dims, nc, host, hyp, hyp_steps):
     return dims, (hyp_steps if hyp is not None else 0)
 
 
+class TSlabJob:
+    """One lattice's smear-and-measure job split into time slabs over the
+    ranks of `group` (the default process group; a single process when
+    torch.distributed is not initialised), with this rank's slab lattices
+    kept between runs: `load` keeps the rank's raw slices resident, `run`
+    smears and measures them (from the resident copy, or from a host array
+    it uploads first) and returns the global W table on every rank. Every
+    rank must call `run` the same number of times (each holds one batch of
+    point-to-point operations and one all-reduce). The lattices, the
+    exchange and the all-reduce run on the job's own CUDA stream
+    (`self.stream`, a torch stream: record timing events there)."""
+
+    def __init__(self, dims: Sequence[int], nc: int, *, precision: str = "mixed",
+                 hyp: Optional[Tuple[float, float, float]] = (1.0, 1.0, 0.5),
+                 hyp_steps: int = 1, ape_alpha: float = 0.5, ape_steps: int = 0,
+                 r_min: int = 1, r_max: int = 1, time_min: int = 1, time_max: int = 1,
+                 group=None):
+        import torch
+        import torch.distributed as dist
+
+        self.dims = tuple(int(d) for d in dims)
+        if len(self.dims) != 4:
+            raise ValueError("dims must have four extents")
+        self.nc, self.precision, self.group = nc, precision, group
+        self.hyp, self.ape_alpha, self.ape_steps = hyp, ape_alpha, ape_steps
+        self.ranges = (int(r_min), int(r_max), int(time_min), int(time_max))
+        self.distributed = dist.is_available() and dist.is_initialized()
+        self.world = dist.get_world_size(group) if self.distributed else 1
+        self.rank = dist.get_rank(group) if self.distributed else 0
+        self.plan = SlabPlan(self.dims, self.world, int(time_max),
+                             hyp_steps if hyp is not None else 0)
+        self.device = torch.device("cuda", torch.cuda.current_device())
+        self.stream = torch.cuda.Stream(self.device)
+        stream = self.stream.cuda_stream
+        self._lats = []
+        try:
+            for d in (self.plan.smear_dims(self.rank), self.plan.smear_dims(self.rank),
+                      self.plan.measure_dims(self.rank)):
+                lat = Lattice(d, nc, precision)
+                self._lats.append(lat)
+                lat.set_stream(stream)
+        except Exception:
+            self.close()
+            raise
+        self.pristine, self.smear, self.meas = self._lats
+        self._loaded = False
+
+    def _upload(self, lat: Lattice, host: np.ndarray) -> None:
+        if host.size != 4 * volume(self.dims) * link_size(self.nc):
+            raise ValueError("link array has the wrong size for this lattice")
+        for g0, l0, k in self.plan.upload_runs(self.rank):
+            lat.upload_slices(l0, _slices(host, self.dims, self.nc, g0, k))
+
+    def load(self, host: np.ndarray) -> None:
+        """Keeps this rank's raw slices (and the HYP halo above) resident."""
+        self._upload(self.pristine, host)
+        self._loaded = True
+
+    def run(self, host: Optional[np.ndarray] = None) -> np.ndarray:
+        """Smears and measures: from `host` (uploaded first) or the copy
+        `load` keeps. Returns the global table [T - time_min, R - r_min]."""
+        import torch
+        import torch.distributed as dist
+
+        if host is not None:
+            self._upload(self.smear, host)
+        elif self._loaded:
+            self.smear.copy_from(self.pristine)
+        else:
+            raise RuntimeError("TSlabJob.run without links: call load() or pass host")
+        plan, rank = self.plan, self.rank
+        if self.hyp is not None and plan.hyp_steps:
+            self.smear.hyp(*self.hyp, plan.hyp_steps)
+        if self.ape_steps:
+            self.smear.ape(self.ape_alpha, self.ape_steps)
+        n = plan.bounds[rank][1]
+        with torch.cuda.stream(self.stream):
+            self.meas.copy_slices_from(0, self.smear, 0, n)
+            if self.distributed and self.world > 1:
+                exchange_forward_halo(plan, rank, self.smear, self.meas, self.device,
+                                      self.group)
+            else:
+                for x in plan.forward_halo(rank):
+                    self.meas.copy_slices_from(x.dst_t0, self.smear, x.src_t0, x.n)
+            w = self.meas.wilson_loop_tslab(n, *self.ranges)
+            if self.distributed and self.world > 1:
+                t = torch.from_numpy(w * n).to(self.device)
+                dist.all_reduce(t, group=self.group)
+                return t.cpu().numpy() / self.dims[3]
+        return w * n / self.dims[3]
+
+    def close(self) -> None:
+        for lat in getattr(self, "_lats", []):
+            lat.close()
+        self._lats = []
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+
 def smear_measure(host: np.ndarray, dims: Sequence[int], nc: int, *, precision: str = "mixed",
                   hyp: Optional[Tuple[float, float, float]] = (1.0, 1.0, 0.5),
                   hyp_steps: int = 1, ape_alpha: float = 0.5, ape_steps: int = 0,
@@ -250,38 +353,11 @@ def smear_measure(host: np.ndarray, dims: Sequence[int], nc: int, *, precision: 
     configuration in the reference's row-major layout; a rank reads only its
     slices and the hyp_steps above them. Every rank must call it (it holds
     one batch of point-to-point operations and one all-reduce)."""
-    import torch
-    import torch.distributed as dist
-
-    dims, hsteps = _check_args(dims, nc, host, hyp, hyp_steps)
-    distributed = dist.is_available() and dist.is_initialized()
-    world = dist.get_world_size(group) if distributed else 1
-    rank = dist.get_rank(group) if distributed else 0
-    plan = SlabPlan(dims, world, int(time_max), hsteps)
-    device = torch.device("cuda", torch.cuda.current_device())
-    stream = torch.cuda.current_stream(device).cuda_stream
-    smear = _smear(plan, rank, host, nc, precision, hyp, ape_alpha, ape_steps, stream)
-    try:
-        meas = Lattice(plan.measure_dims(rank), nc, precision)
-        try:
-            meas.set_stream(stream)
-            n = plan.bounds[rank][1]
-            meas.copy_slices_from(0, smear, 0, n)
-            if distributed and world > 1:
-                exchange_forward_halo(plan, rank, smear, meas, device, group)
-            else:
-                for x in plan.forward_halo(rank):
-                    meas.copy_slices_from(x.dst_t0, smear, x.src_t0, x.n)
-            w = meas.wilson_loop_tslab(n, r_min, r_max, time_min, time_max)
-        finally:
-            meas.close()
-    finally:
-        smear.close()
-    if distributed and world > 1:
-        t = torch.from_numpy(w * n).to(device)
-        dist.all_reduce(t, group=group)
-        return t.cpu().numpy() / dims[3]
-    return w * n / dims[3]
+    dims, _ = _check_args(dims, nc, host, hyp, hyp_steps)
+    with TSlabJob(dims, nc, precision=precision, hyp=hyp, hyp_steps=hyp_steps,
+                  ape_alpha=ape_alpha, ape_steps=ape_steps, r_min=r_min, r_max=r_max,
+                  time_min=time_min, time_max=time_max, group=group) as job:
+        return job.run(host)
 
 
 def emulate(host: np.ndarray, dims: Sequence[int], nc: int, slabs: int, *,

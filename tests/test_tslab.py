@@ -291,3 +291,30 @@ def test_smear_measure_single_process_matches_fixture_job(port):
     w = smear_measure(links, dims, nc, precision="fp64", hyp=(1.0, 0.75, 0.6), ape_steps=2,
                       r_min=1, r_max=3, time_min=1, time_max=4)
     np.testing.assert_allclose(w, want, rtol=1e-12, atol=1e-14)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("form", ["fp64", "mixed"])
+def test_tslab_job_reuses_its_lattices(form):
+    """TSlabJob in one process: runs from the resident slices and from the
+    host array agree bitwise, repeated runs are identical, and the table is
+    the one-lattice job's within 1e-12."""
+    from general_code_b200 import Lattice
+    from general_code_b200.tslab import TSlabJob
+    nc, dims = 3, (6, 6, 6, 10)
+    links = generate_config(dims, nc, 0.25, 20261203, 12)
+    with Lattice(dims, nc, form) as lat:
+        lat.upload(links)
+        lat.hyp(1.0, 0.75, 0.6, 1)
+        lat.ape(0.5, 3)
+        ref = lat.wilson_loop(1, 3, 1, 5)
+    with TSlabJob(dims, nc, precision=form, hyp=(1.0, 0.75, 0.6), ape_steps=3, r_min=1,
+                  r_max=3, time_min=1, time_max=5) as job:
+        with pytest.raises(RuntimeError):
+            job.run()
+        job.load(links)
+        a = job.run()
+        b = job.run()
+        c = job.run(links)
+    assert np.array_equal(a, b) and np.array_equal(a, c)
+    np.testing.assert_allclose(a, ref, rtol=1e-12, atol=1e-15)
