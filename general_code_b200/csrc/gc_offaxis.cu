@@ -151,37 +151,50 @@ __global__ void __launch_bounds__(256)
 
 constexpr int kOffaxisBlock = 128;
 
-// Matrices in shared memory as planes of reals, [real][slot], so that
-// consecutive threads (consecutive slots) touch consecutive words.
+// Matrices in shared memory as planes of complex entries (float2 / double2),
+// [entry][slot], so that consecutive threads (consecutive slots) touch
+// consecutive words and a matrix is 9 (SU(2): 2) vector loads.
+template <class T> struct Vec2;
+template <> struct Vec2<float> {
+  using type = float2;
+};
+template <> struct Vec2<double> {
+  using type = double2;
+};
+
 template <class T>
 __device__ __forceinline__ void sm_store(T *a, int nslots, int i, const SU3<T> &m) {
-#pragma unroll
-  for (int k = 0; k < 9; k++) {
-    a[(2 * k) * nslots + i] = m.e[k / 3][k % 3].re;
-    a[(2 * k + 1) * nslots + i] = m.e[k / 3][k % 3].im;
-  }
-}
-template <class T> __device__ __forceinline__ SU3<T> sm_load(const T *a, int nslots, int i) {
-  SU3<T> m;
+  using V = typename Vec2<T>::type;
+  V *p = reinterpret_cast<V *>(a) + i;
 #pragma unroll
   for (int k = 0; k < 9; k++)
-    m.e[k / 3][k % 3] = {a[(2 * k) * nslots + i], a[(2 * k + 1) * nslots + i]};
+    p[k * nslots] = V{m.e[k / 3][k % 3].re, m.e[k / 3][k % 3].im};
+}
+template <class T> __device__ __forceinline__ SU3<T> sm_load(const T *a, int nslots, int i,
+                                                             SU3<T> *) {
+  using V = typename Vec2<T>::type;
+  const V *p = reinterpret_cast<const V *>(a) + i;
+  SU3<T> m;
+#pragma unroll
+  for (int k = 0; k < 9; k++) {
+    const V v = p[k * nslots];
+    m.e[k / 3][k % 3] = {v.x, v.y};
+  }
   return m;
 }
 template <class T>
 __device__ __forceinline__ void sm_store(T *a, int nslots, int i, const SU2<T> &m) {
-  a[i] = m.a0;
-  a[nslots + i] = m.a1;
-  a[2 * nslots + i] = m.a2;
-  a[3 * nslots + i] = m.a3;
+  using V = typename Vec2<T>::type;
+  V *p = reinterpret_cast<V *>(a) + i;
+  p[0] = V{m.a0, m.a1};
+  p[nslots] = V{m.a2, m.a3};
 }
 template <class T> __device__ __forceinline__ SU2<T> sm_load(const T *a, int nslots, int i,
                                                              SU2<T> *) {
-  return {a[i], a[nslots + i], a[2 * nslots + i], a[3 * nslots + i]};
-}
-template <class T> __device__ __forceinline__ SU3<T> sm_load(const T *a, int nslots, int i,
-                                                             SU3<T> *) {
-  return sm_load(a, nslots, i);
+  using V = typename Vec2<T>::type;
+  const V *p = reinterpret_cast<const V *>(a) + i;
+  const V u = p[0], v = p[nslots];
+  return {u.x, u.y, v.x, v.y};
 }
 
 // One step of a space line from the site `cur` with spatial coordinates
