@@ -833,8 +833,10 @@ def main():
     }
     if len(forms) > 1:
         wm, wd = results["mixed"]["w"], results["fp64"]["w"]
-        line["mixed_vs_fp64"] = {"max_rel_err_W": float(np.max(np.abs(wm - wd) / np.abs(wd))),
-                                 "tolerance": 1e-6}
+        rel = np.abs(wm - wd) / np.abs(wd)
+        line["mixed_vs_fp64"] = {"max_rel_err_W": float(np.max(rel)), "tolerance": 1e-6,
+                                 # per W(R,T): rows T = t_min.., columns R = r_min..
+                                 "rel_err_W": [[float(f"{v:.3g}") for v in row] for row in rel]}
         line["forms"] = {f: {"value": sums[f]["value"], "e2e": sums[f]["e2e_value"],
                              "e2e_serial": sums[f]["e2e_serial"],
                              "ms_per_step": sums[f]["ms_per_step"],
