@@ -3,8 +3,8 @@
 
 One step = one smear-and-measure job on one synthetic configuration:
 HYP x1 (alpha 1, 0.75, 0.6) + APE x n (alpha 0.5) + the on-axis W(R,T) table.
-Default workload: SU(3) 24^4, 1 HYP + 20 APE, R,T = 1..12 (the configuration
-the headline metric is quoted on). Metric: smeared+measured sites/s.
+Default workload: SU(3) 32^4, 1 HYP + 40 APE, R,T = 1..16, the largest
+single-GPU configuration of the metric. Metric: smeared+measured sites/s.
 
   value  : device-resident throughput. Each step restores the unsmeared links
            from a resident copy (device-to-device) and runs the job; inputs are
@@ -17,16 +17,23 @@ the headline metric is quoted on). Metric: smeared+measured sites/s.
            timed region. `e2e.serial_value` is the same with one handle, each
            job's upload, compute and result read one after the other.
 Both forms are timed on the same configuration (--form both, the default):
-the headline is the mixed form (FP32 links, FP64 projection and sums); the
-FP64 form is reported under "forms", with the largest relative difference of
-the two W(R,T) tables (the mixed form's error against FP64).
+the headline is the mixed form (FP32 links, FP64 sums); the FP64 form is
+reported under "forms", with the largest relative difference of the two
+W(R,T) tables (the mixed form's error against FP64).
 Between timed steps the L2 cache is flushed by writing a 256 MiB buffer.
 Timing: CUDA events on the stream the kernels run on, max over ranks.
+Sections (default on, 1 GPU): "su2" times SU(2) 16^4 (HYP + APE x10, R,T <= 8)
+and SU(2) 48^4 (HYP + APE x10, R,T <= 24, 680 MB of FP64 links) the same way,
+with each kernel family's HBM and FP-pipe fractions; "batch", "serving" and
+"observables" time the other forms and observables.
 
 --gpus N (under torchrun): every rank runs the job on its own configuration
 (config index = rank); no data-path collective; weak scaling.
 --impl reference: the reference's own CPU implementation (oracle/_ref, compiled
-from the reference sources) on the host cores, rank 0 only.
+from the reference sources) on the host cores, rank 0 only, on a bounded
+sample of the same job (one phase per step: HYP, one APE step, the W table;
+the job time is the phases' mean times with the APE step counted n times).
+The input comes from oracle/libgen.so, so that arm loads no product library.
 """
 from __future__ import annotations
 
@@ -46,18 +53,35 @@ ROOT = Path(__file__).resolve().parent
 sys.path.insert(0, str(ROOT))
 
 WORKLOADS = {
-    # SU(3) 24^4, 1 HYP + 20 APE, W R,T=1..12 (headline configuration)
+    # SU(3) 32^4, 1 HYP + 40 APE, W R,T=1..16 (the headline: the largest
+    # single-GPU configuration)
+    "su3_32": dict(nc=3, dims=(32, 32, 32, 32), eps=0.25, hyp=(1.0, 0.75, 0.6), ape=40,
+                   alpha=0.5, r=(1, 16), t=(1, 16)),
+    # SU(3) 24^4, 1 HYP + 20 APE, W R,T=1..12 (FP64 vs mixed comparison case)
     "su3_24": dict(nc=3, dims=(24, 24, 24, 24), eps=0.25, hyp=(1.0, 0.75, 0.6), ape=20,
                    alpha=0.5, r=(1, 12), t=(1, 12)),
     # SU(2) 16^4, 1 HYP + 10 APE, W R,T=1..8 (the reference's CPU-sized case)
     "su2_16": dict(nc=2, dims=(16, 16, 16, 16), eps=0.3, hyp=(1.0, 0.75, 0.6), ape=10,
                    alpha=0.5, r=(1, 8), t=(1, 8)),
-    # SU(3) 32^4, 1 HYP + 40 APE, W R,T=1..16 (HBM scaling case)
-    "su3_32": dict(nc=3, dims=(32, 32, 32, 32), eps=0.25, hyp=(1.0, 0.75, 0.6), ape=40,
-                   alpha=0.5, r=(1, 16), t=(1, 16)),
+    # SU(2) 48^4, 1 HYP + 10 APE, W R,T=1..24: SU(2) at a size where the
+    # memory-bound kernels are HBM-bound rather than launch-bound
+    "su2_48": dict(nc=2, dims=(48, 48, 48, 48), eps=0.3, hyp=(1.0, 0.75, 0.6), ape=10,
+                   alpha=0.5, r=(1, 24), t=(1, 24)),
 }
+DEFAULT_WORKLOAD = "su3_32"
 SEED = 20261203
 L2_FLUSH_BYTES = 256 << 20
+L2_NOTE = ("GPU arm: L2 flushed (256 MiB write) before every timed step; "
+           "CPU arm: host caches, no flush")
+
+
+def config_dict(name, wl, world):
+    """The workload's description; the same dict in both arms."""
+    return {"workload": name, "lattice": list(wl["dims"]), "group": f"SU({wl['nc']})",
+            "hyp_steps": 1, "hyp_alpha": list(wl["hyp"]), "ape_steps": wl["ape"],
+            "ape_alpha": wl["alpha"], "r_range": list(wl["r"]), "t_range": list(wl["t"]),
+            "sites": int(np.prod(wl["dims"])), "l2": L2_NOTE,
+            "parallelism": f"replicas x{world}"}
 
 
 def link_bytes(nc, form):
@@ -156,42 +180,79 @@ def load_traffic():
     return {}
 
 
-def cpu_baseline(wl, workload, host_links, steps=1, warmup=0):
-    """The reference's own CPU path (oracle/_ref, -Ofast -fopenmp, all host
-    threads) on the same configuration; the C restatement when the reference
-    was not compiled. Returns (sites/s, detail)."""
+def reference_checker():
+    """The reference's own CPU path (oracle/_ref/libref_timed.so: -Ofast
+    -fopenmp, all host threads), else the C restatement. Returns (checker,
+    kind, threads)."""
     from oracle import py_oracle
+    threads = os.cpu_count() or 1
     if py_oracle.ref_available("timed"):
-        chk, kind = py_oracle.ref("timed"), "reference"
-        threads = os.cpu_count() or 1
+        chk = py_oracle.ref("timed")
         chk.set_threads(threads)
-        cores = chk.num_threads()
-    else:
-        chk, kind = py_oracle.port(), "port"
-        cores = os.cpu_count() or 1
-        chk.set_threads(cores)
+        return chk, "reference", chk.num_threads()
+    chk = py_oracle.port()
+    chk.set_threads(threads)
+    return chk, "port", threads
+
+
+PHASES = ("hyp", "ape", "wilson")
+
+
+def cpu_sample(wl, workload, host_links, steps, warmup=0):
+    """A bounded sample of the job on the host cores: step i runs one phase,
+    PHASES[i % 3] (the HYP step on the input links, one APE step on the
+    HYP-smeared links, the W(R,T) table on the HYP+APE-smeared links); the
+    job time is mean(HYP) + n_APE * mean(APE) + mean(W). Returns (sites/s,
+    detail)."""
+    chk, kind, cores = reference_checker()
     nc, dims = wl["nc"], wl["dims"]
     V = int(np.prod(dims))
-    times = []
+    r0, r1 = wl["r"]
+    t0, t1 = wl["t"]
+    # inputs of the three phases (untimed)
+    hyp_in = host_links
+    ape_in = host_links.copy()
+    chk.hyp(nc, dims, ape_in, *wl["hyp"], 1)
+    w_in = ape_in.copy()
+    chk.ape(nc, dims, w_in, wl["alpha"], 1)
+    times = {p: [] for p in PHASES}
+    busy = 0.0
     for i in range(warmup + steps):
-        links = host_links.copy()
-        t0 = time.perf_counter()
-        if kind == "reference":
-            chk.job(nc, dims, links, 1, *wl["hyp"], wl["ape"], wl["alpha"],
-                    wl["r"][0], wl["r"][1], wl["t"][0], wl["t"][1])
-        else:
+        phase = PHASES[i % 3]
+        src = {"hyp": hyp_in, "ape": ape_in, "wilson": w_in}[phase]
+        links = src.copy() if phase != "wilson" else src
+        t = time.perf_counter()
+        if phase == "hyp":
             chk.hyp(nc, dims, links, *wl["hyp"], 1)
-            chk.ape(nc, dims, links, wl["alpha"], wl["ape"])
-            chk.wilson(nc, dims, links, wl["r"][0], wl["r"][1], wl["t"][0], wl["t"][1])
-        dt = time.perf_counter() - t0
+        elif phase == "ape":
+            chk.ape(nc, dims, links, wl["alpha"], 1)
+        else:
+            chk.wilson(nc, dims, links, r0, r1, t0, t1)
+        dt = time.perf_counter() - t
+        busy += dt
         if i >= warmup:
-            times.append(dt)
-    total = sum(times)
-    sample = (f"{steps} full job(s) on {workload}: HYP x1 + APE x{wl['ape']} + W "
-              f"R={wl['r'][0]}..{wl['r'][1]} T={wl['t'][0]}..{wl['t'][1]}, FP64, "
-              f"{total:.1f} s of CPU time")
-    return V * steps / total, {"cores": cores, "kind": kind, "sample": sample,
-                               "seconds": total}
+            times[phase].append(dt)
+    for p in PHASES:  # every phase measured at least once
+        if not times[p]:
+            links = {"hyp": hyp_in, "ape": ape_in, "wilson": w_in}[p].copy()
+            t = time.perf_counter()
+            if p == "hyp":
+                chk.hyp(nc, dims, links, *wl["hyp"], 1)
+            elif p == "ape":
+                chk.ape(nc, dims, links, wl["alpha"], 1)
+            else:
+                chk.wilson(nc, dims, links, r0, r1, t0, t1)
+            dt = time.perf_counter() - t
+            busy += dt
+            times[p].append(dt)
+    mean = {p: sum(v) / len(v) for p, v in times.items()}
+    job_s = mean["hyp"] + wl["ape"] * mean["ape"] + mean["wilson"]
+    sample = (f"{workload}, FP64: one phase per step in rotation (HYP x1; APE x1, counted "
+              f"x{wl['ape']}; W R={r0}..{r1} T={t0}..{t1}), "
+              f"{sum(len(v) for v in times.values())} timed phases, {busy:.1f} s of CPU "
+              f"time; job = {job_s:.2f} s")
+    return V / job_s, {"cores": cores, "kind": kind, "sample": sample, "job_seconds": job_s,
+                       "phase_seconds": mean}
 
 
 def bench_batch(steps: int):
@@ -554,25 +615,259 @@ def run_tslab(args, wl, rank, world, dist):
 def run_reference(args, wl, rank):
     if rank != 0:
         return 0
-    from general_code_b200 import generate_config
-    host = generate_config(wl["dims"], wl["nc"], wl["eps"], SEED, 0)
-    value, info = cpu_baseline(wl, args.workload, host, steps=args.steps, warmup=args.warmup)
-    V = int(np.prod(wl["dims"]))
+    from oracle import py_oracle
+    host = py_oracle.generator().generate(wl["dims"], wl["nc"], wl["eps"], SEED, 0)
+    value, info = cpu_sample(wl, args.workload, host, steps=args.steps, warmup=args.warmup)
     line = {
         "impl": "reference", "metric": "smeared+measured sites/s", "value": value,
         "unit": "sites/s", "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
-        "ms_per_step": 1000.0 * info["seconds"] / args.steps, "higher_is_better": True,
+        "ms_per_step": 1000.0 * info["job_seconds"], "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": args.workload, "lattice": list(wl["dims"]),
-                   "group": f"SU({wl['nc']})", "hyp_steps": 1, "ape_steps": wl["ape"],
-                   "r_range": list(wl["r"]), "t_range": list(wl["t"]), "sites": V},
+        "form": "fp64 (the reference's only form)",
+        "config": config_dict(args.workload, wl, args.gpus),
         "cpu_baseline": {"value": value, "unit": "sites/s", "cores": info["cores"],
                          "kind": info["kind"], "sample": info["sample"]},
+        "phase_seconds": info["phase_seconds"],
         "e2e": {"value": value, "unit": "sites/s", "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
     return 0
+
+
+class Runner:
+    """Times smear-and-measure jobs on this rank's GPU."""
+
+    def __init__(self, rank, world, dist):
+        import torch
+        self.torch = torch
+        self.rank, self.world, self.dist = rank, world, dist
+        self.stream = torch.cuda.Stream()
+        self.flush_buf = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device="cuda")
+
+    def flush(self, stream=None):
+        with self.torch.cuda.stream(stream or self.stream):
+            self.flush_buf.fill_(1.0)
+
+    def ev(self, stream=None):
+        e = self.torch.cuda.Event(enable_timing=True)
+        e.record(stream or self.stream)
+        return e
+
+    def barrier(self):
+        self.torch.cuda.synchronize()
+        if self.dist is not None:
+            self.dist.barrier()
+        self.torch.cuda.synchronize()
+
+    def max_over_ranks(self, x):
+        if self.dist is None:
+            return x
+        t = self.torch.tensor([x], dtype=self.torch.float64, device="cuda")
+        self.dist.all_reduce(t, op=self.dist.ReduceOp.MAX)
+        return float(t.item())
+
+    def measure(self, wl, host, form, steps, warmup):
+        """One form of the job: device-resident steps, serial end-to-end steps,
+        then pipelined end-to-end steps (two handles)."""
+        torch = self.torch
+        from general_code_b200 import Lattice
+        nc, dims = wl["nc"], wl["dims"]
+        r0, r1 = wl["r"]
+        t0, t1 = wl["t"]
+        stream = self.stream
+        pristine = Lattice(dims, nc, form)
+        work = Lattice(dims, nc, form)
+        for lat in (pristine, work):
+            lat.set_stream(stream.cuda_stream)
+        pristine.upload(host)
+        pristine.synchronize()
+
+        def device_step(record):
+            self.flush()
+            e0 = self.ev()
+            work.copy_from(pristine)
+            work.hyp(*wl["hyp"], 1)
+            e1 = self.ev()
+            work.ape(wl["alpha"], wl["ape"])
+            e2 = self.ev()
+            w = work.wilson_loop(r0, r1, t0, t1)
+            e3 = self.ev()
+            stream.synchronize()
+            if record is not None:
+                record.append((e0.elapsed_time(e3), e0.elapsed_time(e1), e1.elapsed_time(e2),
+                               e2.elapsed_time(e3)))
+            return w
+
+        stream2 = torch.cuda.Stream()
+        work2 = Lattice(dims, nc, form)
+        work2.set_stream(stream2.cuda_stream)
+        pair = ((work, stream), (work2, stream2))
+
+        def e2e_pipelined(k, record):
+            # two handles: job i+1's upload (pinned host -> device, on the
+            # other handle's stream) is issued before job i's result is read,
+            # so the copy engine overlaps job i's kernels; the other handle is
+            # idle then (its previous job's result has been read)
+            e0 = self.ev()
+            stream2.wait_event(e0)
+            pair[0][0].upload(host)
+            w = None
+            for i in range(k):
+                lat, s = pair[i % 2]
+                self.flush(s)
+                lat.hyp(*wl["hyp"], 1)
+                lat.ape(wl["alpha"], wl["ape"])
+                if i + 1 < k:
+                    pair[(i + 1) % 2][0].upload(host)
+                w = lat.wilson_loop(r0, r1, t0, t1)
+            last = pair[(k - 1) % 2][1]
+            e1 = torch.cuda.Event(enable_timing=True)
+            e1.record(last)
+            last.synchronize()
+            if record is not None:
+                record.append(e0.elapsed_time(e1))
+            return w
+
+        def e2e_step(record):
+            self.flush()
+            e0 = self.ev()
+            work.upload(host)
+            work.hyp(*wl["hyp"], 1)
+            work.ape(wl["alpha"], wl["ape"])
+            w = work.wilson_loop(r0, r1, t0, t1)
+            e1 = self.ev()
+            stream.synchronize()
+            if record is not None:
+                record.append(e0.elapsed_time(e1))
+            return w
+
+        for _ in range(warmup):
+            device_step(None)
+        self.barrier()
+        rec = []
+        for _ in range(steps):
+            w = device_step(rec)
+        self.barrier()
+        for _ in range(warmup):
+            e2e_step(None)
+        self.barrier()
+        rec_e2e = []
+        for _ in range(steps):
+            w_e2e = e2e_step(rec_e2e)
+        self.barrier()
+        assert np.array_equal(w, w_e2e), "device and end-to-end runs disagree"
+        e2e_pipelined(max(2, warmup), None)
+        self.barrier()
+        rec_pipe = []
+        w_pipe = e2e_pipelined(steps, rec_pipe)
+        self.barrier()
+        assert np.array_equal(w, w_pipe), "device and pipelined end-to-end runs disagree"
+        pristine.close()
+        work.close()
+        work2.close()
+        from general_code_b200 import launches_per_job
+        per_job = launches_per_job(nc, wl["ape"])
+        return {"w": w,
+                "total_ms": self.max_over_ranks(sum(r[0] for r in rec)),
+                "total_e2e_ms": self.max_over_ranks(sum(rec_pipe)),
+                "total_serial_ms": self.max_over_ranks(sum(rec_e2e)),
+                "hyp_ms": sum(r[1] for r in rec) / steps,
+                "ape_ms": sum(r[2] for r in rec) / steps,
+                "w_ms": sum(r[3] for r in rec) / steps,
+                # our kernels per timed step in the device-resident, serial and
+                # pipelined end-to-end runs; the two end-to-end runs add one
+                # layout conversion per upload
+                "launches": steps * per_job * 3 + 2 * steps}
+
+
+def summarize(wl, name, form, r, steps, world, peak, peak_kind, fp_peak, traffic):
+    """Throughput, phase times and per-kernel-family rooflines of one form."""
+    V = int(np.prod(wl["dims"]))
+    alg = algorithmic(wl, form)
+    per_launch = {"hyp": r["hyp_ms"], "ape": r["ape_ms"] / wl["ape"], "wilson": r["w_ms"]}
+    totals = {"hyp": r["hyp_ms"], "ape": r["ape_ms"], "wilson": r["w_ms"]}
+    pipe = "fp64" if form == "fp64" else "fp32"
+    kernels = {}
+    for k, ms in per_launch.items():
+        gbs = alg[k]["bytes"] * V / (ms * 1e-3) / 1e9
+        tf = alg[k]["flops"] * V / (ms * 1e-3) / 1e12
+        tr = traffic.get(f"{k}:{name}:{form}")
+        kernels[k] = {"ms_per_launch": ms, "share_of_step": totals[k] / sum(totals.values()),
+                      "alg_bytes_per_launch": alg[k]["bytes"] * V,
+                      "hbm_gbs": gbs, "hbm_frac": gbs / peak,
+                      "traffic_per_launch": (tr["dram_bytes_per_site"] * V if tr else None),
+                      "fp_flops_per_launch": alg[k]["flops"] * V, "fp_tflops": tf,
+                      "fp_pipe": pipe, "fp_frac": tf / fp_peak[pipe]}
+    dom = max(totals, key=totals.get)
+    kd = kernels[dom]
+    return {
+        "value": world * V * steps / (r["total_ms"] * 1e-3),
+        "e2e_value": world * V * steps / (r["total_e2e_ms"] * 1e-3),
+        "e2e_serial": world * V * steps / (r["total_serial_ms"] * 1e-3),
+        "ms_per_step": r["total_ms"] / steps,
+        "phases_ms": {"hyp": r["hyp_ms"], "ape_total": r["ape_ms"],
+                      "ape_per_step": r["ape_ms"] / wl["ape"], "wilson": r["w_ms"]},
+        "kernels": kernels,
+        "roofline": {"bound": "hbm", "kernel": dom, "achieved": kd["hbm_gbs"], "peak": peak,
+                     "peak_kind": peak_kind, "unit": "GB/s", "frac": kd["hbm_frac"],
+                     "traffic": kd["traffic_per_launch"],
+                     "alg_bytes_per_launch": kd["alg_bytes_per_launch"],
+                     # the SU(3) kernels are bound by the vector FP pipes, not
+                     # HBM: algorithmic FLOPs over the pipe the form computes
+                     # in, against that pipe's FMA throughput measured in this run
+                     "compute": {"pipe": pipe, "achieved_tflops": kd["fp_tflops"],
+                                 "peak_tflops": fp_peak[pipe],
+                                 "peak_kind": "measured in-run (gc_fma_peak)",
+                                 "frac": kd["fp_frac"]}},
+    }
+
+
+def run_workload(runner, name, wl, forms, steps, warmup, peak, peak_kind, fp_peak, traffic):
+    """Both forms of one workload; returns (per-form summaries, results)."""
+    import torch
+    from general_code_b200 import generate_config, link_size
+    V = int(np.prod(wl["dims"]))
+    host_t = torch.empty((4 * V, link_size(wl["nc"])), dtype=torch.float64, pin_memory=True)
+    host = host_t.numpy()
+    generate_config(wl["dims"], wl["nc"], wl["eps"], SEED, runner.rank, out=host)
+    results = {f: runner.measure(wl, host, f, steps, warmup) for f in forms}
+    sums = {f: summarize(wl, name, f, results[f], steps, runner.world, peak, peak_kind,
+                         fp_peak, traffic) for f in forms}
+    return sums, results, host
+
+
+def form_errors(results):
+    wm, wd = results["mixed"]["w"], results["fp64"]["w"]
+    rel = np.abs(wm - wd) / np.abs(wd)
+    return {"max_rel_err_W": float(np.max(rel)), "tolerance": 1e-6,
+            # per W(R,T): rows T = t_min.., columns R = r_min..
+            "rel_err_W": [[float(f"{v:.3g}") for v in row] for row in rel]}
+
+
+def bench_su2(runner, steps, warmup, peak, peak_kind, fp_peak, traffic, cpu=True):
+    """SU(2) 16^4 (the reference's CPU-sized case) and SU(2) 48^4, both forms,
+    device-resident and end to end, with per-kernel HBM and FP fractions and
+    the reference's CPU path on a bounded sample."""
+    out = {}
+    for name in ("su2_16", "su2_48"):
+        wl = WORKLOADS[name]
+        sums, results, host = run_workload(runner, name, wl, ["mixed", "fp64"], steps, warmup,
+                                           peak, peak_kind, fp_peak, traffic)
+        sec = {"config": config_dict(name, wl, 1),
+               "value": sums["mixed"]["value"], "unit": "sites/s",
+               "forms": {f: {"value": v["value"], "e2e": v["e2e_value"],
+                             "e2e_serial": v["e2e_serial"], "ms_per_step": v["ms_per_step"],
+                             "phases_ms": v["phases_ms"], "kernels": v["kernels"]}
+                         for f, v in sums.items()},
+               "mixed_vs_fp64_max_rel_err_W": form_errors(results)["max_rel_err_W"],
+               "h2d_bytes_per_step": int(host.nbytes)}
+        if cpu:
+            v, info = cpu_sample(wl, name, host, steps=3)
+            sec["cpu_baseline"] = {"value": v, "unit": "sites/s", "cores": info["cores"],
+                                   "kind": info["kind"], "sample": info["sample"]}
+        out[name] = sec
+    return out
 
 
 def main():
@@ -582,10 +877,10 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--form", choices=["both", "fp64", "mixed"], default="both")
-    ap.add_argument("--workload", choices=sorted(WORKLOADS), default="su3_24")
+    ap.add_argument("--workload", choices=sorted(WORKLOADS), default=DEFAULT_WORKLOAD)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--sections", default="batch,serving,observables",
-                    help="extra single-GPU measurements: batch, serving, observables "
+    ap.add_argument("--sections", default="su2,batch,serving,observables",
+                    help="extra single-GPU measurements: su2, batch, serving, observables "
                          "(comma list, or none)")
     ap.add_argument("--serving-seconds", type=float, default=10.0)
     ap.add_argument("--decomp", choices=["replicas", "tslab"], default="replicas",
@@ -611,154 +906,20 @@ def main():
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
                                 device_id=torch.device("cuda", local_rank))
 
-    from general_code_b200 import Lattice, generate_config, link_size
-
     if args.decomp == "tslab":
         return run_tslab(args, wl, rank, world, dist)
 
+    from general_code_b200 import fma_peak
     nc, dims = wl["nc"], wl["dims"]
-    V = int(np.prod(dims))
-    r0, r1 = wl["r"]
-    t0, t1 = wl["t"]
-    stream = torch.cuda.Stream()
-    # pinned host input (the job's input for the end-to-end measurement)
-    host_t = torch.empty((4 * V, link_size(nc)), dtype=torch.float64, pin_memory=True)
-    host = host_t.numpy()
-    generate_config(dims, nc, wl["eps"], SEED, rank, out=host)
-    flush_buf = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device="cuda")
-
-    def flush():
-        with torch.cuda.stream(stream):
-            flush_buf.fill_(1.0)
-
-    def ev():
-        e = torch.cuda.Event(enable_timing=True)
-        e.record(stream)
-        return e
-
-    def barrier():
-        torch.cuda.synchronize()
-        if dist is not None:
-            dist.barrier()
-        torch.cuda.synchronize()
-
-    def max_over_ranks(x):
-        if dist is None:
-            return x
-        t = torch.tensor([x], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
-
-    def measure(form):
-        """Times the job in one form: device-resident steps, then end-to-end steps."""
-        pristine = Lattice(dims, nc, form)
-        work = Lattice(dims, nc, form)
-        for lat in (pristine, work):
-            lat.set_stream(stream.cuda_stream)
-        pristine.upload(host)
-        pristine.synchronize()
-
-        def device_step(record):
-            flush()
-            e0 = ev()
-            work.copy_from(pristine)
-            work.hyp(*wl["hyp"], 1)
-            e1 = ev()
-            work.ape(wl["alpha"], wl["ape"])
-            e2 = ev()
-            w = work.wilson_loop(r0, r1, t0, t1)
-            e3 = ev()
-            stream.synchronize()
-            if record is not None:
-                record.append((e0.elapsed_time(e3), e0.elapsed_time(e1), e1.elapsed_time(e2),
-                               e2.elapsed_time(e3)))
-            return w
-
-        stream2 = torch.cuda.Stream()
-        work2 = Lattice(dims, nc, form)
-        work2.set_stream(stream2.cuda_stream)
-        pair = ((work, stream), (work2, stream2))
-
-        def e2e_pipelined(k, record):
-            # two handles: job i+1's upload (pinned host -> device, on the
-            # other handle's stream) is issued before job i's result is read,
-            # so the copy engine overlaps job i's kernels; the other handle is
-            # idle then (its previous job's result has been read)
-            e0 = ev()
-            stream2.wait_event(e0)
-            pair[0][0].upload(host)
-            w = None
-            for i in range(k):
-                lat, s = pair[i % 2]
-                with torch.cuda.stream(s):
-                    flush_buf.fill_(1.0)
-                lat.hyp(*wl["hyp"], 1)
-                lat.ape(wl["alpha"], wl["ape"])
-                if i + 1 < k:
-                    pair[(i + 1) % 2][0].upload(host)
-                w = lat.wilson_loop(r0, r1, t0, t1)
-            last = pair[(k - 1) % 2][1]
-            e1 = torch.cuda.Event(enable_timing=True)
-            e1.record(last)
-            last.synchronize()
-            if record is not None:
-                record.append(e0.elapsed_time(e1))
-            return w
-
-        def e2e_step(record):
-            flush()
-            e0 = ev()
-            work.upload(host)
-            work.hyp(*wl["hyp"], 1)
-            work.ape(wl["alpha"], wl["ape"])
-            w = work.wilson_loop(r0, r1, t0, t1)
-            e1 = ev()
-            stream.synchronize()
-            if record is not None:
-                record.append(e0.elapsed_time(e1))
-            return w
-
-        for _ in range(args.warmup):
-            device_step(None)
-        barrier()
-        rec = []
-        for _ in range(args.steps):
-            w = device_step(rec)
-        barrier()
-        for _ in range(args.warmup):
-            e2e_step(None)
-        barrier()
-        rec_e2e = []
-        for _ in range(args.steps):
-            w_e2e = e2e_step(rec_e2e)
-        barrier()
-        assert np.array_equal(w, w_e2e), "device and end-to-end runs disagree"
-        e2e_pipelined(max(2, args.warmup), None)
-        barrier()
-        rec_pipe = []
-        w_pipe = e2e_pipelined(args.steps, rec_pipe)
-        barrier()
-        assert np.array_equal(w, w_pipe), "device and pipelined end-to-end runs disagree"
-        pristine.close()
-        work.close()
-        work2.close()
-        total_ms = max_over_ranks(sum(r[0] for r in rec))
-        total_e2e_ms = max_over_ranks(sum(rec_pipe))
-        total_serial_ms = max_over_ranks(sum(rec_e2e))
-        return {"w": w, "total_ms": total_ms, "total_e2e_ms": total_e2e_ms,
-                "total_serial_ms": total_serial_ms,
-                "hyp_ms": sum(r[1] for r in rec) / args.steps,
-                "ape_ms": sum(r[2] for r in rec) / args.steps,
-                "w_ms": sum(r[3] for r in rec) / args.steps,
-                # our kernels per timed step: HYP 3 + APE n + W 2, in the
-                # device-resident, serial and pipelined end-to-end runs; the
-                # two end-to-end runs add the layout conversion
-                "launches": args.steps * (3 + wl["ape"] + 2) * 3 + 2 * args.steps}
-
+    runner = Runner(rank, world, dist)
+    peak, peak_kind = load_peaks()
+    traffic = load_traffic()
+    fp_peak = {"fp32": fma_peak("mixed"), "fp64": fma_peak("fp64")}
     forms = ["mixed", "fp64"] if args.form == "both" else [args.form]
     sampler = ClockSampler(local_rank)
     sampler.start()
-    results = {f: measure(f) for f in forms}
+    sums, results, host = run_workload(runner, args.workload, wl, forms, args.steps,
+                                       args.warmup, peak, peak_kind, fp_peak, traffic)
     clocks = sampler.stop()
 
     if rank != 0:
@@ -767,82 +928,38 @@ def main():
         return 0
 
     head = forms[0]
-    hr = results[head]
-    peak, peak_kind = load_peaks()
-    traffic = load_traffic()
-
-    def summary(form, r):
-        alg = algorithmic(wl, form)
-        per_launch = {"hyp": r["hyp_ms"], "ape": r["ape_ms"] / wl["ape"], "wilson": r["w_ms"]}
-        totals = {"hyp": r["hyp_ms"], "ape": r["ape_ms"], "wilson": r["w_ms"]}
-        dom = max(totals, key=totals.get)
-        ms = per_launch[dom]
-        achieved = alg[dom]["bytes"] * V / (ms * 1e-3) / 1e9
-        tr = traffic.get(f"{dom}:{args.workload}:{form}")
-        pipe = "fp64" if form == "fp64" else "fp32"
-        return {
-            "value": world * V * args.steps / (r["total_ms"] * 1e-3),
-            "e2e_value": world * V * args.steps / (r["total_e2e_ms"] * 1e-3),
-            "e2e_serial": world * V * args.steps / (r["total_serial_ms"] * 1e-3),
-            "ms_per_step": r["total_ms"] / args.steps,
-            "phases_ms": {"hyp": r["hyp_ms"], "ape_total": r["ape_ms"],
-                          "ape_per_step": r["ape_ms"] / wl["ape"], "wilson": r["w_ms"]},
-            "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak,
-                         "peak_kind": peak_kind, "unit": "GB/s", "frac": achieved / peak,
-                         "traffic": (tr["dram_bytes_per_site"] * V if tr else None),
-                         "alg_bytes_per_launch": alg[dom]["bytes"] * V,
-                         "fp_flops_per_launch": alg[dom]["flops"] * V,
-                         "fp_tflops": alg[dom]["flops"] * V / (ms * 1e-3) / 1e12,
-                         # the kernels are bound by the vector FP pipes, not HBM:
-                         # algorithmic FLOPs over the pipe the form computes in,
-                         # against that pipe's FMA throughput measured in this run
-                         "compute": {"pipe": pipe,
-                                     "achieved_tflops": alg[dom]["flops"] * V / (ms * 1e-3) / 1e12,
-                                     "peak_tflops": fp_peak[pipe],
-                                     "peak_kind": "measured in-run (gc_fma_peak)",
-                                     "nominal_peak_tflops": FP_PEAK_TFLOPS[pipe],
-                                     "frac": alg[dom]["flops"] * V / (ms * 1e-3) / 1e12
-                                     / fp_peak[pipe]}},
-        }
-
-    from general_code_b200 import fma_peak
-    fp_peak = {"fp32": fma_peak("mixed"), "fp64": fma_peak("fp64")}
-    sums = {f: summary(f, results[f]) for f in forms}
     hs = sums[head]
     line = {
         "metric": "smeared+measured sites/s", "value": hs["value"], "unit": "sites/s",
         "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": hs["ms_per_step"], "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64" if head == "fp64" else "f32/f64",
-        "data": "synthetic",
-        "config": {"workload": args.workload, "form": head, "lattice": list(dims),
-                   "group": f"SU({nc})", "hyp_steps": 1, "hyp_alpha": list(wl["hyp"]),
-                   "ape_steps": wl["ape"], "ape_alpha": wl["alpha"], "r_range": [r0, r1],
-                   "t_range": [t0, t1], "sites": V,
-                   "l2": "flushed (256 MiB write) before every timed step",
-                   "parallelism": f"replicas x{world}"},
+        "data": "synthetic", "form": head,
+        "config": config_dict(args.workload, wl, world),
         "phases_ms": hs["phases_ms"],
         "roofline": hs["roofline"],
+        "kernels": hs["kernels"],
         "e2e": {"value": hs["e2e_value"], "unit": "sites/s",
                 "h2d_bytes_per_step": int(host.nbytes),
-                "d2h_bytes_per_step": int(hr["w"].nbytes),
+                "d2h_bytes_per_step": int(results[head]["w"].nbytes),
                 "mode": "two handles on two streams: job i+1's upload overlaps job i",
                 "serial_value": hs["e2e_serial"]},
         "gpu_launches": sum(results[f]["launches"] for f in forms),
         "clocks": clocks,
+        "fp_peak_tflops_measured": fp_peak,
     }
     if len(forms) > 1:
-        wm, wd = results["mixed"]["w"], results["fp64"]["w"]
-        rel = np.abs(wm - wd) / np.abs(wd)
-        line["mixed_vs_fp64"] = {"max_rel_err_W": float(np.max(rel)), "tolerance": 1e-6,
-                                 # per W(R,T): rows T = t_min.., columns R = r_min..
-                                 "rel_err_W": [[float(f"{v:.3g}") for v in row] for row in rel]}
+        line["mixed_vs_fp64"] = form_errors(results)
         line["forms"] = {f: {"value": sums[f]["value"], "e2e": sums[f]["e2e_value"],
                              "e2e_serial": sums[f]["e2e_serial"],
                              "ms_per_step": sums[f]["ms_per_step"],
                              "phases_ms": sums[f]["phases_ms"],
-                             "roofline": sums[f]["roofline"]} for f in forms}
+                             "roofline": sums[f]["roofline"],
+                             "kernels": sums[f]["kernels"]} for f in forms}
     sections = [x for x in args.sections.split(",") if x and x != "none"]
+    if world == 1 and "su2" in sections:
+        line["su2"] = bench_su2(runner, min(args.steps, 10), args.warmup, peak, peak_kind,
+                                fp_peak, traffic, cpu=not args.no_cpu_baseline)
     if world == 1 and "batch" in sections:
         line["batch"] = bench_batch(args.steps)
     if world == 1 and "serving" in sections:
@@ -850,7 +967,7 @@ def main():
     if world == 1 and "observables" in sections:
         line["observables"] = bench_observables(min(args.steps, 5))
     if world == 1 and not args.no_cpu_baseline:
-        v, info = cpu_baseline(wl, args.workload, host)
+        v, info = cpu_sample(wl, args.workload, host, steps=3)
         line["cpu_baseline"] = {"value": v, "unit": "sites/s", "cores": info["cores"],
                                 "kind": info["kind"], "sample": info["sample"]}
     print(json.dumps(line), flush=True)

@@ -5,6 +5,7 @@ The compute path is libgc_b200.so (hand-written CUDA kernels behind the C ABI
 in include/gc_lattice.h); this package is a thin ctypes host layer over it.
 """
 from .lattice import (GCError, Lattice, LatticeData, fma_peak, generate_config, job_device_bytes,
+                      launches_per_job,
                       link_size, plaket, plaket_space, plaket_time, polyakov_average_directions,
                       polyakov_loop, polyakov_loop_correlator_color_average,
                       polyakov_loop_correlator_singlet, probe_config, read_data_convert,
@@ -14,6 +15,7 @@ from .lattice import (GCError, Lattice, LatticeData, fma_peak, generate_config, 
                       wilson_offaxis_result, wilson_spatial_3d_indexed)
 
 __all__ = ["GCError", "Lattice", "LatticeData", "fma_peak", "generate_config", "job_device_bytes",
+           "launches_per_job",
            "link_size", "plaket", "plaket_space", "plaket_time", "polyakov_average_directions",
            "polyakov_loop", "polyakov_loop_correlator_color_average",
            "polyakov_loop_correlator_singlet", "probe_config", "read_data_convert",

@@ -12,16 +12,25 @@
 // library's module is loaded. No cudaMalloc, cudaFree, cudaMallocHost or
 // allocating library routine is called on this path.
 //
-// Size: 16 MiB (2,097,152 doubles) on every GPU that loads the library, held
-// until the process exits. One value of R needs blocks*nT + nT doubles, where
-// blocks = 3 * ceil(Lx*Ly*Lz / columns_per_block); larger R ranges are done in
-// chunks of R. A lattice for which even one R does not fit is rejected with
-// GC_ERR_ARG (SU(3) 24^4 with T up to 12 needs 49,800 doubles per R).
+// Size: 16 MiB (2,097,152 doubles) per GPU, held until the process exits.
+// The array belongs to the library's device module, and the CUDA runtime
+// loads modules lazily: the 16 MiB are taken on a device when the module is
+// loaded there, which is the first call of this entry point on that device
+// (its cudaGetSymbolAddress), unless another entry point of the library ran
+// on that device before. A caller whose allocator claims the device budget
+// should therefore make one call before the allocator takes its share; if the
+// device has no room left then, the call fails with GC_ERR_NOMEM. One value
+// of R needs blocks*nT + nT doubles, where blocks = 3 * ceil(Lx*Ly*Lz /
+// columns_per_block); larger R ranges are done in chunks of R. A lattice for
+// which even one R does not fit is rejected with GC_ERR_ARG (SU(3) 24^4 with T
+// up to 12 needs 49,800 doubles per R).
 //
-// Set-up: the first call on a device looks up the array's device address
-// with cudaGetSymbolAddress (the host-side name of a __device__ array is not
-// a device address) while that device is current, and keeps it for later
-// calls; make that first call before any stream capture.
+// Set-up: every call looks up the array's device address with
+// cudaGetSymbolAddress while the caller's device is current (the host-side
+// name of a __device__ array is not a device address), so the address stays
+// right after cudaDeviceReset re-creates the context. The first call for each
+// group and precision on a device also raises the W kernel's shared-memory
+// limit (cudaFuncSetAttribute): make that first call outside stream capture.
 //
 // Sharing: all calls in the process use the same array and it keeps the last
 // call's contents. Every element a call reads was written earlier in the same
@@ -54,10 +63,11 @@ static __device__ __align__(256) double g_wilson_scratch[kNoAllocScratchDoubles]
 namespace {
 
 std::mutex g_setup_mu;
-double *g_scratch_addr[kMaxDevices] = {};
+bool g_checked[kMaxDevices] = {};
 
-// Device address of g_wilson_scratch on the current device (looked up once per
-// device, with that device current).
+// Device address of g_wilson_scratch on the current device. The address is
+// looked up on every call (a host-side table lookup once the module is
+// loaded), so a context re-created by cudaDeviceReset gets its own address.
 int scratch_for_current_device(double **out) {
   int dev = 0;
   cudaError_t e = cudaGetDevice(&dev);
@@ -66,24 +76,31 @@ int scratch_for_current_device(double **out) {
                             std::string("cudaGetDevice: ") + cudaGetErrorString(e));
   if (dev < 0 || dev >= kMaxDevices)
     return gc::record_error(GC_ERR_NODEVICE, "device ordinal out of range");
-  std::lock_guard<std::mutex> lk(g_setup_mu);
-  if (!g_scratch_addr[dev]) {
-    int major = 0;
-    e = cudaDeviceGetAttribute(&major, cudaDevAttrComputeCapabilityMajor, dev);
-    if (e != cudaSuccess)
-      return gc::record_error(GC_ERR_NODEVICE,
-                              std::string("no CUDA device: ") + cudaGetErrorString(e));
-    if (major != 10)
-      return gc::record_error(GC_ERR_NODEVICE,
-                              "device is not sm_100 (this library is built for sm_100a only)");
-    void *p = nullptr;
-    e = cudaGetSymbolAddress(&p, g_wilson_scratch);
-    if (e != cudaSuccess || p == nullptr)
-      return gc::record_error(GC_ERR_CUDA, std::string("cudaGetSymbolAddress: ") +
-                                               cudaGetErrorString(e));
-    g_scratch_addr[dev] = static_cast<double *>(p);
+  {
+    std::lock_guard<std::mutex> lk(g_setup_mu);
+    if (!g_checked[dev]) {
+      int major = 0;
+      e = cudaDeviceGetAttribute(&major, cudaDevAttrComputeCapabilityMajor, dev);
+      if (e != cudaSuccess)
+        return gc::record_error(GC_ERR_NODEVICE,
+                                std::string("no CUDA device: ") + cudaGetErrorString(e));
+      if (major != 10)
+        return gc::record_error(GC_ERR_NODEVICE,
+                                "device is not sm_100 (this library is built for sm_100a only)");
+      g_checked[dev] = true;
+    }
   }
-  *out = g_scratch_addr[dev];
+  void *p = nullptr;
+  e = cudaGetSymbolAddress(&p, g_wilson_scratch);
+  if (e == cudaErrorMemoryAllocation)
+    return gc::record_error(GC_ERR_NOMEM,
+                            "gc_wilson_onaxis_noalloc: loading the library's device module "
+                            "needs 16 MiB of free device memory for the fixed scratch array; "
+                            "make the first call before the device memory is claimed");
+  if (e != cudaSuccess || p == nullptr)
+    return gc::record_error(GC_ERR_CUDA,
+                            std::string("cudaGetSymbolAddress: ") + cudaGetErrorString(e));
+  *out = static_cast<double *>(p);
   return GC_OK;
 }
 

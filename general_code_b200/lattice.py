@@ -57,6 +57,20 @@ def generate_config(dims: Sequence[int], nc: int, eps: float, seed: int,
     return out
 
 
+# Kernels one call launches: gc_hyp per step, gc_ape per step, and
+# gc_wilson_onaxis (the W kernel and its fixed-order reduction) for the
+# ranges the benchmark uses.
+HYP_LAUNCHES_PER_STEP = 3
+APE_LAUNCHES_PER_STEP = 1
+WILSON_LAUNCHES = 2
+
+
+def launches_per_job(nc: int, ape_steps: int, hyp_steps: int = 1) -> int:
+    """Our kernel launches in one smear-and-measure job (HYP, APE, W)."""
+    return (hyp_steps * HYP_LAUNCHES_PER_STEP + ape_steps * APE_LAUNCHES_PER_STEP
+            + WILSON_LAUNCHES)
+
+
 def fma_peak(precision: str = "mixed") -> float:
     """Measured vector FMA throughput of the current device, TFLOP/s (packed
     FP32x2 for "mixed", FP64 for "fp64")."""

@@ -203,11 +203,17 @@ int gc_wilson_gevp_adjoint_onaxis(gc_lattice *h1, gc_lattice *h2, int r_min, int
  * gc_wilson_onaxis fills `out`. The work is queued on cuda_stream (a
  * cudaStream_t as void*, NULL = default stream) and the call returns without
  * waiting. Working memory is a fixed 16 MiB array in the library's static
- * device memory, held by every GPU that loads the library until exit; a
- * lattice for which one value of R does not fit in it is rejected with
- * GC_ERR_ARG. The first call on a device looks up that array's device address
- * and must come before any stream capture. All calls share the array: calls
- * whose work overlaps on the GPU race and must be serialised by the caller.
+ * device memory. The CUDA runtime loads the library's device module lazily,
+ * so the 16 MiB are taken on a device at the first call there (if no other
+ * entry point of the library ran on it before) and held until exit: make one
+ * call before an allocator that owns the device budget claims it; without
+ * room for the array the call fails with GC_ERR_NOMEM. A lattice for which
+ * one value of R does not fit in the array is rejected with GC_ERR_ARG. Every
+ * call looks up the array's device address with the caller's device current
+ * (so cudaDeviceReset does not leave a stale address behind); the first call
+ * for each group and precision on a device also sets a kernel attribute, so
+ * make it outside stream capture. All calls share the array: calls whose
+ * work overlaps on the GPU race and must be serialised by the caller.
  * Errors: gc_last_error(NULL). */
 int gc_wilson_onaxis_noalloc(const int dims[4], int nc, int precision,
                              const void *const fields[4], int r_min, int r_max,

@@ -4,6 +4,9 @@
   ref("parity")     -> oracle/_ref/libref_parity.so (the reference's own code,
                        -O2, no fast-math), if it was built here
   ref("timed")      -> oracle/_ref/libref_timed.so (reference flags -Ofast)
+  generator()       -> oracle/libgen.so (the seeded configuration generator,
+                       built from its source for the checkers, so that they
+                       make their input without loading the product library)
 
 All take/return host link arrays of shape (4V, 4|18) in the row-major layout.
 Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg use this.
@@ -17,6 +20,7 @@ import numpy as np
 
 HERE = Path(__file__).resolve().parent
 PORT_LIB = HERE / "liboracle.so"
+GEN_LIB = HERE / "libgen.so"
 REF_LIBS = {"parity": HERE / "_ref" / "libref_parity.so",
             "timed": HERE / "_ref" / "libref_timed.so"}
 
@@ -293,8 +297,42 @@ class Ref(_Checker):
                                                   str(path).encode()) == 0
 
 
+class Generator:
+    """Seeded synthetic configurations (the generator of gc_generate_host:
+    Philox-4x32-10 keyed by (seed, config index), eps-scaled exp(iH) links and
+    a Haar gauge transformation); host array (4V, 4|18), row-major."""
+
+    def __init__(self, path: Path = GEN_LIB):
+        self.lib = ctypes.CDLL(str(path))
+        self.lib.og_generate_host.restype = _c_int
+        self.lib.og_generate_host.argtypes = [_pint, _c_int, _c_dbl, ctypes.c_uint,
+                                              ctypes.c_uint, _c_int, _pdbl]
+
+    def generate(self, dims, nc, eps, seed, index=0, gauge=True, out=None):
+        n = 4
+        for d in dims:
+            n *= int(d)
+        if out is None:
+            out = np.empty((n, 4 if nc == 2 else 18), dtype=np.float64)
+        assert out.shape == (n, 4 if nc == 2 else 18)
+        assert self.lib.og_generate_host(_dims(dims), nc, float(eps), int(seed) & 0xffffffff,
+                                         int(index) & 0xffffffff, int(bool(gauge)),
+                                         _ptr(out)) == 0
+        return out
+
+
 _port = None
+_gen = None
 _refs = {}
+
+
+def generator() -> Generator:
+    global _gen
+    if _gen is None:
+        if not GEN_LIB.exists():
+            raise ImportError(f"{GEN_LIB} missing: run `make -C oracle gen`")
+        _gen = Generator()
+    return _gen
 
 
 def port() -> Port:

@@ -5,9 +5,12 @@
   own CPU path on the same configuration (the oracle restatement when the
   reference library is not built): FP64 within 1e-12 relative, mixed within
   1e-6.
-* SU(3) 32^4 (HYP x1 + APE x40, R,T = 1..16), too large for a CPU check in a
-  test: the mixed form within 1e-6 of the FP64 form, smeared links in SU(3)
-  to FP32 precision.
+* SU(3) 32^4 (HYP x1 + APE x40, R,T = 1..16) and SU(2) 48^4 (HYP x1 + APE
+  x10, R,T = 1..24), too slow for the CPU inside a test: against the W tables
+  the reference's CPU path computed once on the same seeded configurations
+  (tests/golden/fullsize.json, made by tests/golden/make_golden_fullsize.py
+  from the reference compiled from its sources): FP64 within 1e-12 relative,
+  mixed within 1e-6; the smeared links in SU(3) to FP32 precision.
 * Gauge invariance at 24^4: the same configuration with and without a random
   gauge transformation gives the same smeared W(R,T) table.
 """
@@ -65,20 +68,49 @@ def test_full_size_job_matches_reference_cpu_path(nc, dims, eps, ape, rt):
     assert np.max(np.abs(w32 - want) / np.abs(want)) <= 1e-6
 
 
-def test_su3_32_mixed_within_1e6_of_fp64_and_links_in_su3():
-    nc, dims, ape, rt = 3, (32, 32, 32, 32), 40, 16
-    links = generate_config(dims, nc, 0.25, SEED, 0)
-    with Lattice(dims, nc, "fp64") as lat:
-        w64 = _job(lat, links, ape, rt)
-    with Lattice(dims, nc, "mixed") as lat:
-        w32 = _job(lat, links, ape, rt)
-        m = su3_matrices(lat.download())
-    assert np.max(np.abs(w32 - w64) / np.abs(w64)) <= 1e-6
-    # every smeared link (APE'd spatial, HYP'd temporal) unitary with det 1 to
-    # FP32 precision
-    uu = np.einsum("nij,nkj->nik", m, m.conj())
-    assert np.max(np.abs(uu - np.eye(3))) <= 2e-6
-    assert np.max(np.abs(np.linalg.det(m) - 1)) <= 2e-6
+def _golden(name):
+    import json
+    from pathlib import Path
+    p = Path(__file__).resolve().parent / "golden" / "fullsize.json"
+    cases = json.loads(p.read_text())["cases"]
+    if name not in cases:
+        pytest.skip(f"no {name} table in tests/golden/fullsize.json")
+    return cases[name]
+
+
+def _sha(links):
+    import hashlib
+    return hashlib.sha256(np.ascontiguousarray(links).tobytes()).hexdigest()
+
+
+@pytest.mark.parametrize("name", ["su3_32", "su2_48"])
+def test_large_job_matches_reference_table(name):
+    c = _golden(name)
+    nc, dims = c["nc"], tuple(c["dims"])
+    links = generate_config(dims, nc, c["eps"], c["seed"], c["config_index"])
+    assert _sha(links) == c["input_sha256"], "the generator no longer gives the fixture's input"
+    rng = (c["r_min"], c["r_max"], c["time_min"], c["time_max"])
+    want = np.array(c["wilson"])
+    res = {}
+    for form in ("fp64", "mixed"):
+        with Lattice(dims, nc, form) as lat:
+            lat.upload(links)
+            lat.hyp(*c["hyp_alpha"], c["hyp_steps"])
+            lat.ape(c["ape_alpha"], c["ape_steps"])
+            res[form] = lat.wilson_loop(*rng)
+            if form == "fp64":
+                res["plaq"] = lat.plaquette()
+            elif nc == 3:
+                m = su3_matrices(lat.download())
+    np.testing.assert_allclose(res["fp64"], want, rtol=1e-12, atol=1e-14)
+    assert res["plaq"] == pytest.approx(c["plaquette_out"], rel=1e-12)
+    assert np.max(np.abs(res["mixed"] - want) / np.abs(want)) <= 1e-6
+    if nc == 3:
+        # every smeared link (APE'd spatial, HYP'd temporal) unitary with det 1
+        # to FP32 precision
+        uu = np.einsum("nij,nkj->nik", m, m.conj())
+        assert np.max(np.abs(uu - np.eye(3))) <= 2e-6
+        assert np.max(np.abs(np.linalg.det(m) - 1)) <= 2e-6
 
 
 @pytest.mark.parametrize("form,rtol", [("fp64", 1e-11), ("mixed", 1e-6)])

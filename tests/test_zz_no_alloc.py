@@ -74,11 +74,22 @@ def test_noalloc_matches_handle_entry_point_twice(nc, dims, precision, rng):
         expect = lat.wilson_loop(*rng)
     fields = device_fields(links, nc, precision, V)
     shape = (rng[3] - rng[2] + 1, rng[1] - rng[0] + 1)
-    for _ in range(2):
-        out = torch.full(shape, float("nan"), dtype=torch.float64, device="cuda")
+    # both output buffers exist before the first call, so that nothing else
+    # allocates device memory between the two calls
+    outs = [torch.full(shape, float("nan"), dtype=torch.float64, device="cuda")
+            for _ in range(2)]
+    torch.cuda.synchronize()
+    free_after_first = None
+    for k, out in enumerate(outs):
         rc = call_noalloc(dims, nc, precision, fields, rng, out)
         assert rc == _lib.GC_OK, lib().gc_last_error(None)
         torch.cuda.synchronize()
+        if k == 0:
+            free_after_first = torch.cuda.mem_get_info()[0]
+        else:
+            # the second call took no device memory
+            assert torch.cuda.mem_get_info()[0] >= free_after_first
+    for out in outs:
         np.testing.assert_allclose(out.cpu().numpy(), expect, rtol=1e-12, atol=1e-14)
 
 
