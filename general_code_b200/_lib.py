@@ -29,6 +29,9 @@ GC_ERR_BUSY = 8
 GC_PREC_FP64 = 0
 GC_PREC_MIXED = 1
 GC_LAYOUT_ROWMAJOR = 0
+GC_WILSON_AUTO = 0
+GC_WILSON_EXACT = 1
+GC_WILSON_GAUGE = 2
 GC_LAYOUT_EIGEN_COLMAJOR = 1
 
 ERROR_NAMES = {
@@ -61,6 +64,8 @@ SIGNATURES = {
     "gc_hyp": (_c_int, [_p, _c_dbl, _c_dbl, _c_dbl, _c_int]),
     "gc_wilson_onaxis": (_c_int, [_p, _c_int, _c_int, _c_int, _c_int, _pdbl]),
     "gc_wilson_adjoint_onaxis": (_c_int, [_p, _c_int, _c_int, _c_int, _c_int, _pdbl]),
+    "gc_set_wilson_method": (_c_int, [_p, _c_int]),
+    "gc_wilson_method_used": (_c_int, [_p, _pint]),
     "gc_plaquette": (_c_int, [_p, _pdbl]),
     "gc_plaquette_space": (_c_int, [_p, _pdbl]),
     "gc_plaquette_time": (_c_int, [_p, _pdbl]),

@@ -79,6 +79,9 @@ struct gc_lattice {
   cudaStream_t stream = nullptr;
   bool stream_ordered = false; // device memory from cudaMallocAsync on `stream`
   bool has_links = false;
+  int *flag_dev = nullptr;    // device word: temporal links failed the unitarity check
+  int wilson_method = GC_WILSON_AUTO;
+  int wilson_used = 0;        // GC_WILSON_EXACT or GC_WILSON_GAUGE, last W call
   std::string err;
   std::mutex mu;
 };
@@ -368,6 +371,7 @@ int gc_lattice_destroy(gc_lattice *h) {
     dev_free(h, h->partials);
     dev_free(h, h->dev_out);
     dev_free(h, h->aux);
+    dev_free(h, h->flag_dev);
     for (int i = 0; i < 2; i++) {
       if (h->io_ev[i])
         cudaEventSynchronize(h->io_ev[i]);
@@ -690,6 +694,50 @@ int gc_hyp(gc_lattice *h, double a1, double a2, double a3, int steps) {
   return GC_OK;
 }
 
+// Prepares the temporal-gauge form of W: the gauge time lines of both cuts
+// and the transformed spatial links, in the HYP decorated-link scratch (which
+// holds them: per site at most 2 x 144 + 6 x 144 bytes against 15 x 144 for
+// FP64 SU(3)), and the device's unitarity check of the temporal links, which
+// the host reads (one synchronisation). *use stays true when the check
+// passed.
+static int gauge_prepare(gc_lattice *h, Fields4 *UA, Fields4 *UB, bool *use) {
+  int rc = ensure_hyp(h);
+  if (rc)
+    return rc;
+  if (!h->flag_dev) {
+    cudaError_t e = dev_alloc(h, (void **)&h->flag_dev, 256);
+    if (e != cudaSuccess) {
+      h->flag_dev = nullptr;
+      return cuda_fail(h, "cudaMalloc(flag)", e);
+    }
+  }
+  const size_t lb = wilson_gauge_line_bytes(h->g, h->nc);
+  if (2 * lb + 6 * h->field_bytes > 15 * hyp_field_bytes(h)) {
+    *use = false;
+    return GC_OK;
+  }
+  char *base = (char *)h->hyp;
+  void *GA = base, *GB = base + lb;
+  for (int d = 0; d < 3; d++) {
+    UA->f[d] = base + 2 * lb + d * h->field_bytes;
+    UB->f[d] = base + 2 * lb + (3 + d) * h->field_bytes;
+  }
+  UA->f[3] = UB->f[3] = nullptr;
+  rc = GC_DISPATCH(h, launch_wilson_gauge_prep, h->g, h->cur, GA, GB, *UA, *UB, h->flag_dev,
+                   h->stream);
+  if (rc)
+    return launch_fail(h, rc);
+  int flag = 1;
+  cudaError_t e = cudaMemcpyAsync(&flag, h->flag_dev, sizeof(int), cudaMemcpyDeviceToHost,
+                                  h->stream);
+  if (e == cudaSuccess)
+    e = cudaStreamSynchronize(h->stream);
+  if (e != cudaSuccess)
+    return cuda_fail(h, "unitarity check", e);
+  *use = flag == 0;
+  return GC_OK;
+}
+
 // W(R,T) of h, or with `second` the GEVP loops of the pair (h, second):
 // h's time lines, space lines of both (wilson_gevp_indexed).
 static int wilson_impl(gc_lattice *h, int rmin, int rmax, int tmin, int tmax,
@@ -750,11 +798,36 @@ static int wilson_impl(gc_lattice *h, int rmin, int rmax, int tmin, int tmax,
   if (rc)
     return rc;
   double *chunk_out = h->dev_out + (size_t)nr * nt;
+  // The temporal-gauge form (gc_wilson_gauge.cu) for one configuration's
+  // on-axis or adjoint loops over the whole lattice with T <= Lt/2; it runs
+  // only after the device has checked that the temporal links are unitary to
+  // the form's tolerance, and the exact recursion otherwise.
+  const int ct_bytes = h->prec == GC_PREC_FP64 ? 8 : 4;
+  bool gauge = h->wilson_method == GC_WILSON_AUTO && !second &&
+               (tstarts <= 0 || tstarts == h->g.L[3]) &&
+               wilson_gauge_applies(h->g, tmax, nt, h->nc, ct_bytes);
+  Fields4 UA{}, UB{};
+  if (gauge) {
+    rc = gauge_prepare(h, &UA, &UB, &gauge);
+    if (rc)
+      return rc;
+  }
+  if (gauge) {
+    const WilsonPlan gp = wilson_gauge_plan(h->g, nt, h->nc, ct_bytes);
+    rc = ensure_partials(h, (size_t)gp.blocks * std::min(rchunk, nr) * nt);
+    if (rc)
+      return rc;
+  }
+  h->wilson_used = gauge ? GC_WILSON_GAUGE : GC_WILSON_EXACT;
   for (int r0 = rmin; r0 <= rmax; r0 += rchunk) {
     const int r1 = std::min(rmax, r0 + rchunk - 1);
     const int ncr = r1 - r0 + 1;
-    rc = GC_DISPATCH(h, launch_wilson, h->g, h->cur, r0, r1, tmin, tmax,
-                     h->partials, chunk_out, h->stream, adjoint, u2, tstarts);
+    if (gauge)
+      rc = GC_DISPATCH(h, launch_wilson_gauge, h->g, UA, UB, r0, r1, tmin, tmax, adjoint,
+                       h->partials, chunk_out, h->stream);
+    else
+      rc = GC_DISPATCH(h, launch_wilson, h->g, h->cur, r0, r1, tmin, tmax,
+                       h->partials, chunk_out, h->stream, adjoint, u2, tstarts);
     if (rc)
       return launch_fail(h, rc);
     // chunk_out[(T-tmin)*ncr + (R-r0)] -> dev_out[(T-tmin)*nr + (R-rmin)]
@@ -790,6 +863,24 @@ int gc_wilson_onaxis_tslab(gc_lattice *h, int t_starts, int rmin, int rmax, int 
   if (h && (t_starts < 1 || t_starts > h->g.L[3]))
     return fail(h, GC_ERR_ARG, "t_starts must be in [1, Lt]");
   return wilson_impl(h, rmin, rmax, tmin, tmax, out, adjoint != 0, nullptr, t_starts);
+}
+
+int gc_set_wilson_method(gc_lattice *h, int method) {
+  if (!h)
+    return fail(nullptr, GC_ERR_ARG, "null handle");
+  if (method != GC_WILSON_AUTO && method != GC_WILSON_EXACT)
+    return fail(h, GC_ERR_ARG, "method must be GC_WILSON_AUTO or GC_WILSON_EXACT");
+  std::lock_guard<std::mutex> lk(h->mu);
+  h->wilson_method = method;
+  return GC_OK;
+}
+
+int gc_wilson_method_used(gc_lattice *h, int *method) {
+  if (!h || !method)
+    return fail(h, GC_ERR_ARG, "null argument");
+  std::lock_guard<std::mutex> lk(h->mu);
+  *method = h->wilson_used;
+  return GC_OK;
 }
 
 int gc_wilson_gevp_onaxis(gc_lattice *h1, gc_lattice *h2, int rmin, int rmax, int tmin,

@@ -144,6 +144,30 @@ int launch_wilson(const Geom &g, const Fields4 &U, int rmin, int rmax,
                   cudaStream_t s, bool adjoint = false, const Fields4 *second = nullptr,
                   int tstarts = 0);
 
+// W(R,T) in the temporal gauge (gc_wilson_gauge.cu): applies to one
+// configuration's loops over the whole lattice with T <= Lt/2 when the block
+// shape fits; exact to rounding when the temporal links are unitary.
+WilsonPlan wilson_gauge_plan(const Geom &g, int nt, int nc, int ct_bytes);
+bool wilson_gauge_applies(const Geom &g, int tmax, int nt, int nc, int ct_bytes);
+// Largest unitarity defect max |U U^dag - 1| of a temporal link for which the
+// form is used (FP64: ct_bytes 8; mixed: 4).
+double wilson_gauge_tolerance(int ct_bytes);
+// Bytes of one field of gauge time lines (FP64 matrices, 256-byte aligned).
+size_t wilson_gauge_line_bytes(const Geom &g, int nc);
+// Gauge time lines GA, GB (cuts at slices 0 and Lt/2) and the transformed
+// spatial links UA.f[0..2], UB.f[0..2] (the link storage format); *flag (a
+// device int) is set to 1 when a temporal link's defect exceeds the
+// tolerance, else left 0.
+template <class Store, class CT>
+int launch_wilson_gauge_prep(const Geom &g, const Fields4 &U, void *GA, void *GB,
+                             const Fields4 &UA, const Fields4 &UB, int *flag, cudaStream_t s);
+// The W table from the transformed links (partials: blocks of
+// wilson_gauge_plan x nr x nt doubles), reduced into out_dev.
+template <class Store, class CT>
+int launch_wilson_gauge(const Geom &g, const Fields4 &UA, const Fields4 &UB, int rmin,
+                        int rmax, int tmin, int tmax, bool adjoint, double *partials,
+                        double *out_dev, cudaStream_t s);
+
 // An explicit block shape (rows must divide Lt, at most 256 threads).
 WilsonPlan wilson_plan_shape(const Geom &g, int nr, int nt, int nc, int ct_bytes, int rows,
                              int cols);
@@ -165,6 +189,11 @@ int launch_reduce_sum(const double *partials, int n, double scale, double *out_d
 
 // out_dev[e] = scale * (fixed-order sum over blocks b of partials[b * n + e]),
 // e < n.
+// out_dev[(T-tmin)*nr + (R-rmin)] = scale * (fixed-order sum over blocks b of
+// partials[b * nr * nt + (R-rmin) * nt + (T-tmin)]).
+int launch_reduce_wilson(const double *partials, int blocks, int nr, int nt, double scale,
+                         double *out_dev, cudaStream_t s);
+
 int launch_reduce_rows(const double *partials, int blocks, int n, double scale,
                        double *out_dev, cudaStream_t s);
 

@@ -1,0 +1,347 @@
+// On-axis Wilson loops W(R,T) in the temporal gauge (sm_100a).
+//
+// Reference: wilson_loop (wilson_loops.h:1047-1074) averages, over x and the
+// spatial directions nu, the loop
+//     Re Tr[S(x,R) L(x+R nu,T) S(x+T t,R)^dag L(x,T)^dag] / N
+// with time lines L(x,T) = U_t(x) U_t(x+t) ... U_t(x+(T-1)t) and space lines
+// S(x,R) = U_nu(x) ... U_nu(x+(R-1)nu).
+//
+// The loop is gauge invariant. With G_c(s,t) the time line of spatial site s
+// from a cut slice c up to slice t (G_c(s,c) = 1, G_c(s,t+1) = G_c(s,t)
+// U_t(s,t) walking forward from c), a time line that does not pass the cut
+// is L(s;t0,T) = G_c(s,t0)^dag G_c(s,t0+T) when the temporal links are
+// unitary, and the loop becomes
+//     Re Tr[S'(x,R) S'(x+T t,R)^dag] / N,
+//     S'(s,t,R) = G_c(s,t) S(s,t,R) G_c(s+R nu,t)^dag
+//               = U'_nu(s,t) ... U'_nu(s+(R-1)nu,t),
+//     U'_nu(s,t) = G_c(s,t) U_nu(s,t) G_c(s+nu,t)^dag.
+// Two cuts cover every loop with T <= h = floor(Lt/2): cut A at slice 0 for
+// loops starting on slices t0 < h (they end at t0+T <= 2h-1 <= Lt-1), cut B
+// at slice h for loops starting on t0 >= h (t0-h+T <= Lt-1). A loop then
+// costs one 9-element trace instead of two matrix products (the T walk of
+// the exact recursion in gc_wilson.cu), and each space line one product per
+// R and cut.
+//
+// The identity needs unitary temporal links. The lines kernel measures the
+// largest unitarity defect max |U_t U_t^dag - 1| of the lattice's temporal
+// links and raises a flag above the form's tolerance (FP64: 1e-14, a few
+// roundings; mixed: 1e-6, FP32 rounding of the 12-real links is 2.6e-7);
+// the host then runs the exact recursion instead. With defect d per link a
+// loop differs from the reference's product of links by at most about
+// 2 T d (the two time lines), well inside the parity tolerances at these d.
+//
+// Kernels:
+//   gauge_lines_kernel      thread per spatial site: G_A(s,t), G_B(s,t) for
+//                           all t (FP64, stored as FP64 fields), the defect
+//   gauge_transform_kernel  thread per (site, spatial nu): U'_nu for both
+//                           cuts, computed in FP64, stored in the lattice's
+//                           link format
+//   wilson_gauge_kernel     block = `cols` columns (s, nu) over all t: the
+//                           transformed space lines of both cuts in shared
+//                           memory, extended by one link per R; a thread per
+//                           (column unit, start slice) adds the traces of its
+//                           loops for every T into a per-thread slot; a
+//                           fixed-order sum over the block's threads gives
+//                           one partial per (block, R, T), and the fixed-order
+//                           tree over blocks of gc_wilson.cu finishes.
+#include "gc_internal.cuh"
+#include "gc_kernels.h"
+#include "gc_pair.cuh"
+#include "gc_wcol.cuh"
+
+#include <algorithm>
+
+namespace gc {
+
+namespace {
+
+template <int NC> struct F64Store;
+template <> struct F64Store<3> {
+  using type = StoreF64SU3;
+};
+template <> struct F64Store<2> {
+  using type = StoreF64SU2;
+};
+
+// max_ij |(U U^dag - 1)_ij|
+__device__ __forceinline__ double unitarity_defect(const SU3<double> &u) {
+  double d = 0.0;
+#pragma unroll
+  for (int i = 0; i < 3; i++)
+#pragma unroll
+    for (int j = i; j < 3; j++) {
+      double re = 0.0, im = 0.0;
+#pragma unroll
+      for (int k = 0; k < 3; k++) {
+        re = fma(u.e[i][k].re, u.e[j][k].re, re);
+        re = fma(u.e[i][k].im, u.e[j][k].im, re);
+        im = fma(u.e[i][k].im, u.e[j][k].re, im);
+        im = fma(-u.e[i][k].re, u.e[j][k].im, im);
+      }
+      if (i == j)
+        re -= 1.0;
+      d = fmax(d, fmax(fabs(re), fabs(im)));
+    }
+  return d;
+}
+// SU(2) quaternion a0 + i a.sigma: U U^dag = |a|^2 1
+__device__ __forceinline__ double unitarity_defect(const SU2<double> &u) {
+  return fabs(dot4(u.a0, u.a0, u.a1, u.a1, u.a2, u.a2, u.a3, u.a3) - 1.0);
+}
+
+template <class Store>
+__global__ void __launch_bounds__(128)
+    gauge_lines_kernel(const __grid_constant__ Geom g, const void *Ut, void *GA, void *GB,
+                       int h, double tol, int *flag) {
+  using GS = typename F64Store<Store::NC>::type;
+  using MD = typename Store::template M<double>;
+  const int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= g.Vs)
+    return;
+  const size_t V = g.V;
+  const int Lt = g.L[3];
+  double dmax = 0.0;
+  // cut A: G_A(s,0) = 1, G_A(s,t+1) = G_A(s,t) U_t(s,t)
+  MD G = unit(MD());
+#pragma unroll 1
+  for (int t = 0; t < Lt; t++) {
+    GS::template store<double>(GA, V, s + t * g.Vs, G);
+    const MD u = Store::template load<double>(Ut, V, s + t * g.Vs);
+    dmax = fmax(dmax, unitarity_defect(u));
+    if (t + 1 < Lt)
+      G = mul(G, u);
+  }
+  // cut B: G_B(s,h) = 1, forward through Lt-1 and around to h-1
+  G = unit(MD());
+  int t = h;
+#pragma unroll 1
+  for (int k = 0; k < Lt; k++) {
+    GS::template store<double>(GB, V, s + t * g.Vs, G);
+    if (k + 1 < Lt)
+      G = mul(G, Store::template load<double>(Ut, V, s + t * g.Vs));
+    t = (t + 1 == Lt) ? 0 : t + 1;
+  }
+  if (!(dmax <= tol)) // (a NaN link counts as not unitary)
+    *flag = 1;
+}
+
+// U'_nu(x) = G(x) U_nu(x) G(x + nu)^dag for both cuts; thread per (site, nu).
+template <class Store>
+__global__ void __launch_bounds__(128)
+    gauge_transform_kernel(const __grid_constant__ Geom g, const __grid_constant__ Fields4 U,
+                           const void *GA, const void *GB, const __grid_constant__ Fields4 UA,
+                           const __grid_constant__ Fields4 UB) {
+  using GS = typename F64Store<Store::NC>::type;
+  using MD = typename Store::template M<double>;
+  const int site = blockIdx.x * blockDim.x + threadIdx.x;
+  if (site >= g.V)
+    return;
+  const int nu = blockIdx.y;
+  int x[4];
+  site_coords(g, site, x);
+  const int sn = site + step_off(g, sel4(x, nu), nu, +1);
+  const size_t V = g.V;
+  const MD u = Store::template load<double>(U.f[nu], V, site);
+  Store::template store<double>(
+      UA.f[nu], V, site,
+      mul_ad(mul(GS::template load<double>(GA, V, site), u),
+             GS::template load<double>(GA, V, sn)));
+  Store::template store<double>(
+      UB.f[nu], V, site,
+      mul_ad(mul(GS::template load<double>(GB, V, site), u),
+             GS::template load<double>(GB, V, sn)));
+}
+
+// Shared memory of one block: per-thread loop sums red[nt][threads] (FP64),
+// then the space lines of cut A and of cut B, one slot per (t, column unit).
+template <class Store, class CT, bool ADJ>
+__global__ void __launch_bounds__(256)
+    wilson_gauge_kernel(const __grid_constant__ Geom g, const __grid_constant__ Fields4 UA,
+                        const __grid_constant__ Fields4 UB, int rmin, int rmax, int tmin,
+                        int tmax, int cols, int rows, double *partials) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  constexpr int LANES = wilson_lanes(Store::NC, sizeof(CT));
+  using LL = LaneLoad<Store, CT, LANES>;
+  using M = typename LL::M;
+  using CS = ColSet<M>;
+  const int Lt = g.L[3], h = Lt / 2;
+  const int nt = tmax - tmin + 1;
+  const int nthreads = blockDim.x;
+  const int cs = wilson_col_stride(cols, LANES);
+  const int units = cs / LANES;
+  const int nslots = Lt * units;
+  double *red = reinterpret_cast<double *>(smem_raw); // [nt][nthreads]
+  unsigned char *sa = reinterpret_cast<unsigned char *>(red + (size_t)nt * nthreads);
+  unsigned char *sb = sa + (size_t)CS::kBytes * nslots;
+
+  const int tid = threadIdx.x;
+  const int warp = tid >> 5, lane = tid & 31, nwarps = nthreads >> 5;
+  const int u = tid % units;
+  const int row = tid / units;
+  const int colblock = blockIdx.x, nu = blockIdx.y;
+  const int s0 = colblock * cols + LANES * u;
+  const bool active = (row < rows) && (s0 < g.Vs);
+  const bool lane1 = LANES == 2 && active && (LANES * u + 1 < cols) && (s0 + 1 < g.Vs);
+  const int s1 = lane1 ? s0 + 1 : s0;
+  const int kt = Lt / rows;
+  const int Ln = sel4(g.L, nu), stn = sel4(g.stride, nu);
+  const int xn0 = (s0 / stn) % Ln, xn1 = (s1 / stn) % Ln;
+  const size_t V = g.V;
+  const int ne = (rmax - rmin + 1) * nt;
+  double *part = partials + ((size_t)blockIdx.y * gridDim.x + blockIdx.x) * ne;
+
+#pragma unroll 1
+  for (int R = 1; R <= rmax; R++) {
+    // extend the space lines of both cuts by the link at x + (R-1) nu
+    if (active) {
+      const int l0 = s0 + ((xn0 + R - 1) % Ln - xn0) * stn;
+      const int l1 = s1 + ((xn1 + R - 1) % Ln - xn1) * stn;
+#pragma unroll 1
+      for (int k = 0; k < kt; k++) {
+        const int t = row + k * rows;
+        const int i = t * units + u;
+        const M la = LL::load(UA.f[nu], V, l0 + t * g.Vs, l1 + t * g.Vs);
+        CS::store(sa, nslots, i, (R == 1) ? la : mul(CS::load(sa, nslots, i), la));
+        const M lb = LL::load(UB.f[nu], V, l0 + t * g.Vs, l1 + t * g.Vs);
+        CS::store(sb, nslots, i, (R == 1) ? lb : mul(CS::load(sb, nslots, i), lb));
+      }
+    }
+    __syncthreads();
+    if (R >= rmin) {
+#pragma unroll 1
+      for (int k = 0; k < kt; k++) {
+        const int t0 = row + k * rows;
+        // the cut this start slice's loops use
+        const unsigned char *set = (t0 < h) ? sa : sb;
+        const M a = active ? CS::load(set, nslots, t0 * units + u) : unit(M());
+        int tt = t0 + tmin;
+        tt = (tt >= Lt) ? tt - Lt : tt;
+#pragma unroll 1
+        for (int T = 0; T < nt; T++) {
+          const double v =
+              active ? loop_value<ADJ>(a, CS::load(set, nslots, tt * units + u), lane1) : 0.0;
+          double *r = red + (size_t)T * nthreads + tid;
+          *r = (k == 0) ? v : *r + v;
+          tt = (tt + 1 == Lt) ? 0 : tt + 1;
+        }
+      }
+      __syncthreads();
+      // fixed-order sum over the block's threads: warp w takes T = w, w +
+      // nwarps, ...; each lane sums a strided subset, then a warp tree
+#pragma unroll 1
+      for (int T = warp; T < nt; T += nwarps) {
+        double v = 0.0;
+        for (int i = lane; i < nthreads; i += 32)
+          v += red[(size_t)T * nthreads + i];
+        v = warp_sum(v);
+        if (lane == 0)
+          part[(R - rmin) * nt + T] = v;
+      }
+    }
+    __syncthreads();
+  }
+}
+
+int largest_divisor_upto_g(int n, int cap) {
+  for (int d = cap < n ? cap : n; d > 1; d--)
+    if (n % d == 0)
+      return d;
+  return 1;
+}
+
+} // namespace
+
+// Block shape: every start slice of a column has a thread (rows = Lt up to
+// 64; beyond, the largest divisor of Lt up to 64 with Lt/rows slices each),
+// and about 128 threads per block.
+WilsonPlan wilson_gauge_plan(const Geom &g, int nt, int nc, int ct_bytes) {
+  WilsonPlan p{};
+  const int Lt = g.L[3];
+  const int ncomp = (nc == 3) ? 18 : 4;
+  const int lanes = wilson_lanes(nc, ct_bytes);
+  p.rows = largest_divisor_upto_g(Lt, 64);
+  const int units = std::max(1, 128 / p.rows);
+  p.cols_per_block = units * lanes;
+  p.threads = wilson_threads(p.cols_per_block, p.rows, lanes);
+  p.blocks = ((g.Vs + p.cols_per_block - 1) / p.cols_per_block) * 3;
+  const size_t sets = 2 * (size_t)ncomp * Lt * wilson_col_stride(p.cols_per_block, lanes) *
+                      ct_bytes;
+  p.smem = (size_t)nt * p.threads * sizeof(double) + sets;
+  p.fits = p.threads <= 256 && p.smem <= 200 * 1024;
+  return p;
+}
+
+bool wilson_gauge_applies(const Geom &g, int tmax, int nt, int nc, int ct_bytes) {
+  if (tmax > g.L[3] / 2 || g.L[3] < 2)
+    return false;
+  return wilson_gauge_plan(g, nt, nc, ct_bytes).fits;
+}
+
+double wilson_gauge_tolerance(int ct_bytes) { return ct_bytes == 8 ? 1e-14 : 1e-6; }
+
+size_t wilson_gauge_line_bytes(const Geom &g, int nc) {
+  return ((size_t)(nc == 3 ? 144 : 32) * (size_t)g.V + 255) / 256 * 256;
+}
+
+template <class Store, class CT>
+int launch_wilson_gauge_prep(const Geom &g, const Fields4 &U, void *GA, void *GB,
+                             const Fields4 &UA, const Fields4 &UB, int *flag,
+                             cudaStream_t s) {
+  cudaError_t e = cudaMemsetAsync(flag, 0, sizeof(int), s);
+  if (e != cudaSuccess)
+    return launch_check("gauge flag reset");
+  gauge_lines_kernel<Store><<<(g.Vs + 127) / 128, 128, 0, s>>>(
+      g, U.f[3], GA, GB, g.L[3] / 2, wilson_gauge_tolerance((int)sizeof(CT)), flag);
+  int rc = launch_check("gauge_lines_kernel");
+  if (rc)
+    return rc;
+  gauge_transform_kernel<Store><<<dim3((g.V + 127) / 128, 3), 128, 0, s>>>(g, U, GA, GB, UA,
+                                                                          UB);
+  return launch_check("gauge_transform_kernel");
+}
+
+template <class Store, class CT>
+int launch_wilson_gauge(const Geom &g, const Fields4 &UA, const Fields4 &UB, int rmin,
+                        int rmax, int tmin, int tmax, bool adjoint, double *partials,
+                        double *out_dev, cudaStream_t s) {
+  const int nr = rmax - rmin + 1, nt = tmax - tmin + 1;
+  if (tmax > g.L[3] / 2)
+    return plan_error("wilson_gauge_kernel: time_max above Lt/2");
+  const WilsonPlan p = wilson_gauge_plan(g, nt, Store::NC, (int)sizeof(CT));
+  if (!p.fits || nr * nt > kWilsonMaxEntries)
+    return plan_error("wilson_gauge_kernel: block shape does not fit");
+  int rc;
+  if (adjoint) {
+    rc = allow_large_smem(wilson_gauge_kernel<Store, CT, true>, p.smem);
+    if (rc)
+      return rc;
+    wilson_gauge_kernel<Store, CT, true><<<dim3(p.blocks / 3, 3), p.threads, p.smem, s>>>(
+        g, UA, UB, rmin, rmax, tmin, tmax, p.cols_per_block, p.rows, partials);
+  } else {
+    rc = allow_large_smem(wilson_gauge_kernel<Store, CT, false>, p.smem);
+    if (rc)
+      return rc;
+    wilson_gauge_kernel<Store, CT, false><<<dim3(p.blocks / 3, 3), p.threads, p.smem, s>>>(
+        g, UA, UB, rmin, rmax, tmin, tmax, p.cols_per_block, p.rows, partials);
+  }
+  rc = launch_check("wilson_gauge_kernel");
+  if (rc)
+    return rc;
+  return launch_reduce_wilson(partials, p.blocks, nr, nt, wilson_scale(g.V, Store::NC, adjoint),
+                              out_dev, s);
+}
+
+#define GC_INSTANTIATE_WG(STORE, CT)                                                        \
+  template int launch_wilson_gauge_prep<STORE, CT>(const Geom &, const Fields4 &, void *,   \
+                                                   void *, const Fields4 &, const Fields4 &, \
+                                                   int *, cudaStream_t);                    \
+  template int launch_wilson_gauge<STORE, CT>(const Geom &, const Fields4 &, const Fields4 &, \
+                                              int, int, int, int, bool, double *, double *,  \
+                                              cudaStream_t);
+
+GC_INSTANTIATE_WG(StoreF64SU3, double)
+GC_INSTANTIATE_WG(StoreF64SU2, double)
+GC_INSTANTIATE_WG(StoreF32SU3, float)
+GC_INSTANTIATE_WG(StoreF32SU2, float)
+
+} // namespace gc

@@ -234,6 +234,19 @@ class Lattice:
                                                    int(time_min), int(time_max), dbl_ptr(out)))
         return out
 
+    def set_wilson_method(self, method: str) -> None:
+        """"auto" (the temporal-gauge form where it applies, after a device
+        check of the temporal links' unitarity; else the exact product) or
+        "exact" (always the exact product of links)."""
+        m = {"auto": _lib.GC_WILSON_AUTO, "exact": _lib.GC_WILSON_EXACT}[method]
+        self._check(lib().gc_set_wilson_method(self._h, m))
+
+    def wilson_method_used(self) -> str:
+        """Method of the last on-axis W call: "exact", "gauge" or "" (none yet)."""
+        m = ctypes.c_int()
+        self._check(lib().gc_wilson_method_used(self._h, ctypes.byref(m)))
+        return {_lib.GC_WILSON_EXACT: "exact", _lib.GC_WILSON_GAUGE: "gauge"}.get(m.value, "")
+
     def plaquette(self) -> float:
         out = ctypes.c_double()
         self._check(lib().gc_plaquette(self._h, ctypes.byref(out)))

@@ -49,6 +49,11 @@ extern "C" {
 #define GC_PREC_MIXED 1    /* FP32 links (SU(3): 12 reals, third row rebuilt),
                               FP64 projection and FP64 trace accumulation     */
 
+/* Methods of the on-axis Wilson loops (gc_set_wilson_method). */
+#define GC_WILSON_AUTO 0   /* temporal gauge where it applies, else exact     */
+#define GC_WILSON_EXACT 1  /* always the exact product of links               */
+#define GC_WILSON_GAUGE 2  /* (reported by gc_wilson_method_used)             */
+
 #define GC_LAYOUT_ROWMAJOR 0
 #define GC_LAYOUT_EIGEN_COLMAJOR 1
 
@@ -159,6 +164,12 @@ int gc_hyp(gc_lattice *h, double alpha1, double alpha2, double alpha3,
  * out (host) receives (time_max-time_min+1)*(r_max-r_min+1) doubles:
  * out[(T-time_min)*(r_max-r_min+1) + (R-r_min)] = W(R,T), i.e. the entries of
  * the reference's std::map keyed (T,R), in the map's iteration order.
+ * Two methods give the same table: the exact product of links (walked in T
+ * for every corner), and, for T <= Lt/2 when the temporal links are unitary
+ * (checked on the device for every call: defect max |U U^dag - 1| at most
+ * 1e-14 in FP64, 1e-6 in the mixed form), the same loops in the temporal
+ * gauge (one trace per loop instead of two matrix products); see
+ * gc_set_wilson_method.
  * Replaces: wilson_loop(conf, r_min, r_max, time_min, time_max)
  * (wilson_loops.h:1047-1074) and the legacy vector overload
  * (basic_observables.h:108-111). */
@@ -172,6 +183,15 @@ int gc_wilson_onaxis(gc_lattice *h, int r_min, int r_max, int time_min,
  * (wilson_loops.h:1173-1200, plane sums :793-861). */
 int gc_wilson_adjoint_onaxis(gc_lattice *h, int r_min, int r_max, int time_min,
                              int time_max, double *out);
+
+/* Selects the method of gc_wilson_onaxis and gc_wilson_adjoint_onaxis on this
+ * handle: GC_WILSON_AUTO (default) or GC_WILSON_EXACT. No counterpart in the
+ * reference (which has one method, the exact product). */
+int gc_set_wilson_method(gc_lattice *h, int method);
+
+/* The method the last on-axis W call of the handle ran: GC_WILSON_EXACT or
+ * GC_WILSON_GAUGE (0 before the first call). */
+int gc_wilson_method_used(gc_lattice *h, int *method);
 
 /* On-axis Wilson loops between two configurations of the same lattice (for
  * a generalised eigenvalue problem over smearing levels): time lines from
