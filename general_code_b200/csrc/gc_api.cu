@@ -697,9 +697,8 @@ int gc_hyp(gc_lattice *h, double a1, double a2, double a3, int steps) {
 // Prepares the temporal-gauge form of W: the gauge time lines of both cuts
 // and the transformed spatial links, in the HYP decorated-link scratch (which
 // holds them: per site at most 2 x 144 + 6 x 144 bytes against 15 x 144 for
-// FP64 SU(3)), and the device's unitarity check of the temporal links, which
-// the host reads (one synchronisation). *use stays true when the check
-// passed.
+// FP64 SU(3)), and the device's unitarity check of the temporal links into
+// h->flag_dev. *use is cleared when the scratch cannot hold them.
 static int gauge_prepare(gc_lattice *h, Fields4 *UA, Fields4 *UB, bool *use) {
   int rc = ensure_hyp(h);
   if (rc)
@@ -727,14 +726,6 @@ static int gauge_prepare(gc_lattice *h, Fields4 *UA, Fields4 *UB, bool *use) {
                    h->stream);
   if (rc)
     return launch_fail(h, rc);
-  int flag = 1;
-  cudaError_t e = cudaMemcpyAsync(&flag, h->flag_dev, sizeof(int), cudaMemcpyDeviceToHost,
-                                  h->stream);
-  if (e == cudaSuccess)
-    e = cudaStreamSynchronize(h->stream);
-  if (e != cudaSuccess)
-    return cuda_fail(h, "unitarity check", e);
-  *use = flag == 0;
   return GC_OK;
 }
 
@@ -813,18 +804,18 @@ static int wilson_impl(gc_lattice *h, int rmin, int rmax, int tmin, int tmax,
       return rc;
   }
   if (gauge) {
-    const WilsonPlan gp = wilson_gauge_plan(h->g, nt, h->nc, ct_bytes);
-    rc = ensure_partials(h, (size_t)gp.blocks * std::min(rchunk, nr) * nt);
+    rc = ensure_partials(h, wilson_auto_partials_count(h->g, std::min(rchunk, nr), nt, h->nc));
     if (rc)
       return rc;
   }
-  h->wilson_used = gauge ? GC_WILSON_GAUGE : GC_WILSON_EXACT;
+  // (the method the device chose is read back only when asked for)
+  h->wilson_used = gauge ? -1 : GC_WILSON_EXACT;
   for (int r0 = rmin; r0 <= rmax; r0 += rchunk) {
     const int r1 = std::min(rmax, r0 + rchunk - 1);
     const int ncr = r1 - r0 + 1;
     if (gauge)
-      rc = GC_DISPATCH(h, launch_wilson_gauge, h->g, UA, UB, r0, r1, tmin, tmax, adjoint,
-                       h->partials, chunk_out, h->stream);
+      rc = GC_DISPATCH(h, launch_wilson_auto, h->g, h->cur, UA, UB, r0, r1, tmin, tmax,
+                       adjoint, h->flag_dev, h->partials, chunk_out, h->stream);
     else
       rc = GC_DISPATCH(h, launch_wilson, h->g, h->cur, r0, r1, tmin, tmax,
                        h->partials, chunk_out, h->stream, adjoint, u2, tstarts);
@@ -879,6 +870,16 @@ int gc_wilson_method_used(gc_lattice *h, int *method) {
   if (!h || !method)
     return fail(h, GC_ERR_ARG, "null argument");
   std::lock_guard<std::mutex> lk(h->mu);
+  if (h->wilson_used == -1) { // chosen on the device: read the flag
+    int flag = 1;
+    cudaError_t e = cudaMemcpyAsync(&flag, h->flag_dev, sizeof(int), cudaMemcpyDeviceToHost,
+                                    h->stream);
+    if (e == cudaSuccess)
+      e = cudaStreamSynchronize(h->stream);
+    if (e != cudaSuccess)
+      return cuda_fail(h, "gc_wilson_method_used", e);
+    h->wilson_used = flag ? GC_WILSON_EXACT : GC_WILSON_GAUGE;
+  }
   *method = h->wilson_used;
   return GC_OK;
 }

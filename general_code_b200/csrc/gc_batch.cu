@@ -8,10 +8,17 @@
 //   (round k covers the jobs with more than k steps) -> W -> reductions ->
 //   one copy of all W tables to pinned host memory,
 // with SU(2) and SU(3) jobs as two classes on two streams that run
-// concurrently. Each phase is ONE launch over all jobs of a class: blocks
-// find their job in a per-launch job table (tables built on the host at plan
-// time and kept in device memory). The first gc_batch_run captures the whole
-// schedule into a CUDA graph; every run after that is one graph launch.
+// concurrently. Each smearing phase is ONE launch over all jobs of a class:
+// blocks find their job in a per-launch job table (tables built on the host
+// at plan time and kept in device memory). The W phase runs each job's loops
+// in the temporal gauge where that applies (T <= Lt/2, the job has HYP
+// scratch to hold the transformed links): the job's unitarity check, gauge
+// lines and transformed links, then both W kernels gated on the check (the
+// exact product computes only when the check failed) and the reduction, the
+// jobs spread over kWStreams side streams per class so that the small jobs'
+// launches overlap; other jobs share multi-job exact W launches. The first
+// gc_batch_run captures the whole schedule into a CUDA graph; every run after
+// that is one graph launch.
 //
 // gc_batch_autotune times the candidate W block shapes (threads per column
 // x columns per block) for each distinct (time extent, group, R/T range) in
@@ -42,7 +49,14 @@ namespace {
 
 using namespace gc;
 
+#define GC_DISPATCH_NC(NC, PREC, FN, ...)                                      \
+  ((NC) == 3 ? ((PREC) == GC_PREC_FP64 ? FN<StoreF64SU3, double>(__VA_ARGS__)  \
+                                       : FN<StoreF32SU3, float>(__VA_ARGS__))  \
+             : ((PREC) == GC_PREC_FP64 ? FN<StoreF64SU2, double>(__VA_ARGS__)  \
+                                       : FN<StoreF32SU2, float>(__VA_ARGS__)))
+
 constexpr int kBlock = 128; // smearing kernels' block size
+constexpr int kWStreams = 8; // side streams of each class's per-job W launches
 
 size_t link_bytes(int nc, int prec) {
   if (nc == 3)
@@ -89,12 +103,18 @@ struct JobState {
   int nr = 0, nt = 0;
   int rows = 0, cols = 0; // W block shape
   int w_blocks = 0;
+  bool gauge = false;     // W in the temporal gauge (per-job launches)
+  int gunits = 0;         // its block shape (column units; 0 = default)
+  Fields4 wU{};           // the job's links when its W runs
+  int *flag = nullptr;    // the job's unitarity flag (device)
+  void *GA = nullptr, *GB = nullptr; // gauge lines (in the HYP scratch)
+  Fields4 UA{}, UB{};     // transformed spatial links (in the HYP scratch)
   bool has_input = false;
 };
 
 // One launch of the schedule.
 struct Launch {
-  enum Kind { COPY, HYP, APE, W, REDUCE } kind;
+  enum Kind { COPY, HYP, APE, W, REDUCE, WAUTO } kind;
   int cls;            // 0: SU(2), 1: SU(3)
   size_t table_off;   // byte offset of the job table in the descriptor arena
   int njobs;
@@ -121,6 +141,11 @@ struct gc_batch {
   bool planned = false;        // tables + launches built
   cudaStream_t main = nullptr, side = nullptr;
   cudaEvent_t fork = nullptr, join = nullptr;
+  cudaStream_t wstream[2][kWStreams] = {}; // per class: per-job W launches
+  cudaEvent_t wfork[2] = {}, wjoin[2][kWStreams] = {};
+  int *status = nullptr;       // device: [0] a multi-job W launch could not run a job
+  int *status_host = nullptr;  // pinned mirror, copied with the results
+  int *flags = nullptr;        // device: one unitarity flag per job
   cudaEvent_t done = nullptr;  // recorded after each run's result copy
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t exec = nullptr;
@@ -276,9 +301,22 @@ int build_schedule(gc_batch *b) {
     {
       const int ct = prec == GC_PREC_FP64 ? 8 : 4;
       std::map<std::pair<int, int>, std::vector<int>> classes; // (threads, blocks/SM) -> jobs
+      // per-job temporal-gauge W, largest lattices first
+      std::vector<int> gids;
+      for (int i : ids)
+        if (b->jobs[i].gauge) {
+          b->jobs[i].wU = cur[i];
+          gids.push_back(i);
+        }
+      std::stable_sort(gids.begin(), gids.end(),
+                       [&](int x, int y) { return b->jobs[x].g.V > b->jobs[y].g.V; });
+      for (int i : gids) {
+        Launch L{Launch::WAUTO, cls, 0, i, {0, 0, 0}, 0};
+        b->launches.push_back(L);
+      }
       for (int i : ids) {
         JobState &j = b->jobs[i];
-        if (j.nr <= 0)
+        if (j.nr <= 0 || j.gauge)
           continue;
         WJob w;
         w.g = j.g;
@@ -311,6 +349,7 @@ int build_schedule(gc_batch *b) {
           w.cols = j.cols;
           w.rows = j.rows;
           w.partials = j.partials;
+          w.status = b->status;
           w.block_start = blocks;
           w.blocks = j.w_blocks;
           blocks += j.w_blocks;
@@ -356,14 +395,53 @@ int build_schedule(gc_batch *b) {
   return GC_OK;
 }
 
+// The per-job gauge-form W launches of a class, spread over the class's
+// side streams (forked from and joined back into s).
+template <class Store, class CT>
+int enqueue_wauto(gc_batch *b, int cls, const std::vector<int> &jobs, cudaStream_t s) {
+  if (jobs.empty())
+    return GC_OK;
+  cudaEventRecord(b->wfork[cls], s);
+  const int ns = std::min<int>(kWStreams, (int)jobs.size());
+  for (int k = 0; k < ns; k++)
+    cudaStreamWaitEvent(b->wstream[cls][k], b->wfork[cls], 0);
+  for (size_t m = 0; m < jobs.size(); m++) {
+    JobState &j = b->jobs[jobs[m]];
+    cudaStream_t ws = b->wstream[cls][m % ns];
+    int rc = launch_wilson_gauge_prep<Store, CT>(j.g, j.wU, j.GA, j.GB, j.UA, j.UB, j.flag, ws);
+    if (rc)
+      return rc;
+    rc = launch_wilson_auto<Store, CT>(j.g, j.wU, j.UA, j.UB, j.desc.r_min, j.desc.r_max,
+                                       j.desc.time_min, j.desc.time_max, false, j.flag,
+                                       j.partials, j.out_dev, ws, j.gunits);
+    if (rc)
+      return rc;
+  }
+  for (int k = 0; k < ns; k++) {
+    cudaEventRecord(b->wjoin[cls][k], b->wstream[cls][k]);
+    cudaStreamWaitEvent(s, b->wjoin[cls][k], 0);
+  }
+  return GC_OK;
+}
+
 template <class Store, class CT>
 int enqueue_class(gc_batch *b, int cls, cudaStream_t s) {
+  std::vector<int> wauto;
+  for (const Launch &L : b->launches)
+    if (L.cls == cls && L.kind == Launch::WAUTO)
+      wauto.push_back(L.njobs);
+  bool wauto_done = false;
   for (const Launch &L : b->launches) {
     if (L.cls != cls)
       continue;
     const unsigned char *tab = b->desc + L.table_off;
     int rc = GC_OK;
     switch (L.kind) {
+    case Launch::WAUTO:
+      if (!wauto_done)
+        rc = enqueue_wauto<Store, CT>(b, cls, wauto, s);
+      wauto_done = true;
+      break;
     case Launch::COPY:
       copy_batch_kernel<<<L.blocks[0], 256, 0, s>>>((const CopyJob *)tab, L.njobs);
       rc = launch_check("copy_batch_kernel");
@@ -399,6 +477,7 @@ int enqueue_class_any(gc_batch *b, int cls, cudaStream_t s) {
 // The whole run on `s`: SU(3) jobs on s, SU(2) jobs on the side stream,
 // joined before the result copy.
 int enqueue_run(gc_batch *b, cudaStream_t s) {
+  cudaMemsetAsync(b->status, 0, sizeof(int), s);
   cudaEventRecord(b->fork, s);
   cudaStreamWaitEvent(b->side, b->fork, 0);
   int rc = enqueue_class_any(b, 1, s);
@@ -411,6 +490,8 @@ int enqueue_run(gc_batch *b, cudaStream_t s) {
   cudaStreamWaitEvent(s, b->join, 0);
   cudaError_t e = cudaMemcpyAsync(b->outs_host, b->outs, b->outs_count * sizeof(double),
                                   cudaMemcpyDeviceToHost, s);
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(b->status_host, b->status, sizeof(int), cudaMemcpyDeviceToHost, s);
   if (e != cudaSuccess)
     return cfail(b, "cudaMemcpyAsync(batch results)", e);
   return GC_OK;
@@ -496,13 +577,21 @@ int tune_job(gc_batch *b, JobState &j, double *scratch, cudaStream_t s, int *row
   return GC_OK;
 }
 
+// W partial sums of a job: its multi-job exact launch's blocks, or for the
+// gauge form whichever of the two gated kernels has more blocks.
+size_t partials_doubles(const JobState &j) {
+  if (j.gauge)
+    return wilson_auto_partials_count(j.g, j.nr, j.nt, j.desc.nc, j.gunits);
+  return (size_t)j.w_blocks * j.nr * j.nt;
+}
+
 int alloc_partials(gc_batch *b) {
   if (b->partials)
     cudaFree(b->partials);
   b->partials = nullptr;
   size_t total = 0;
   for (JobState &j : b->jobs)
-    total += align256((size_t)j.w_blocks * j.nr * j.nt * sizeof(double));
+    total += align256(partials_doubles(j) * sizeof(double));
   if (total == 0)
     return GC_OK;
   cudaError_t e = cudaMalloc(&b->partials, total);
@@ -511,7 +600,7 @@ int alloc_partials(gc_batch *b) {
   size_t off = 0;
   for (JobState &j : b->jobs) {
     j.partials = (double *)((char *)b->partials + off);
-    off += align256((size_t)j.w_blocks * j.nr * j.nt * sizeof(double));
+    off += align256(partials_doubles(j) * sizeof(double));
   }
   return GC_OK;
 }
@@ -629,11 +718,41 @@ int gc_batch_create(const gc_job *jobs, int njobs, int precision, gc_batch **out
             cudaEventCreateWithFlags(&b->fork, cudaEventDisableTiming) == cudaSuccess &&
             cudaEventCreateWithFlags(&b->join, cudaEventDisableTiming) == cudaSuccess &&
             cudaEventCreateWithFlags(&b->done, cudaEventDisableTiming) == cudaSuccess;
+  for (int c = 0; c < 2 && ok; c++) {
+    ok = cudaEventCreateWithFlags(&b->wfork[c], cudaEventDisableTiming) == cudaSuccess;
+    for (int k = 0; k < kWStreams && ok; k++)
+      ok = cudaStreamCreateWithFlags(&b->wstream[c][k], cudaStreamNonBlocking) == cudaSuccess &&
+           cudaEventCreateWithFlags(&b->wjoin[c][k], cudaEventDisableTiming) == cudaSuccess;
+  }
+  if (ok)
+    ok = cudaMalloc(&b->flags, 256 * ((njobs + 63) / 64)) == cudaSuccess &&
+         cudaMalloc(&b->status, 256) == cudaSuccess &&
+         cudaMallocHost(&b->status_host, sizeof(int)) == cudaSuccess;
+  if (ok)
+    *b->status_host = 0;
   b->staging_bytes = staging;
   size_t o = 0;
-  for (JobState &j : b->jobs) {
+  const int ct_bytes = precision == GC_PREC_FP64 ? 8 : 4;
+  for (int i = 0; i < njobs; i++) {
+    JobState &j = b->jobs[i];
     j.out_dev = b->outs + o;
     o += (size_t)j.nr * j.nt;
+    // the temporal-gauge W: its lines and transformed links go into the HYP
+    // decorated-link scratch (a job without HYP steps has none)
+    const size_t lb = wilson_gauge_line_bytes(j.g, j.desc.nc);
+    j.gauge = ok && j.nr > 0 && j.desc.hyp_steps > 0 &&
+              wilson_gauge_applies(j.g, j.desc.time_max, j.nt, j.desc.nc, ct_bytes) &&
+              2 * lb + 6 * j.field_bytes <= 15 * j.hyp_bytes;
+    if (j.gauge) {
+      char *base = (char *)j.hyp[0];
+      j.GA = base;
+      j.GB = base + lb;
+      for (int d = 0; d < 3; d++) {
+        j.UA.f[d] = base + 2 * lb + d * j.field_bytes;
+        j.UB.f[d] = base + 2 * lb + (3 + d) * j.field_bytes;
+      }
+      j.flag = b->flags + i;
+    }
   }
   if (ok)
     ok = alloc_partials(b) == GC_OK;
@@ -661,6 +780,22 @@ int gc_batch_destroy(gc_batch *b) {
   cudaFree(b->outs);
   cudaFree(b->staging);
   cudaFree(b->desc);
+  cudaFree(b->flags);
+  cudaFree(b->status);
+  if (b->status_host)
+    cudaFreeHost(b->status_host);
+  for (int c = 0; c < 2; c++) {
+    for (int k = 0; k < kWStreams; k++) {
+      if (b->wstream[c][k]) {
+        cudaStreamSynchronize(b->wstream[c][k]);
+        cudaStreamDestroy(b->wstream[c][k]);
+      }
+      if (b->wjoin[c][k])
+        cudaEventDestroy(b->wjoin[c][k]);
+    }
+    if (b->wfork[c])
+      cudaEventDestroy(b->wfork[c]);
+  }
   if (b->outs_host)
     cudaFreeHost(b->outs_host);
   if (b->fork)
@@ -739,10 +874,53 @@ int gc_batch_autotune(gc_batch *b) {
     return cfail(b, "cudaMalloc(autotune scratch)", e);
   // one tuning per distinct (Lt, nc, nr, nt, Vs)
   std::map<std::tuple<int, int, int, int, int>, std::pair<int, int>> cache;
+  std::map<std::tuple<int, int, int, int, int>, int> gcache;
   int rc = GC_OK;
   for (JobState &j : b->jobs) {
     if (j.nr <= 0)
       continue;
+    if (j.gauge) {
+      // the gauge-form W kernel's columns per block, timed on the job's input
+      auto key = std::make_tuple(j.g.L[3], j.desc.nc, j.nr, j.nt, j.g.Vs);
+      auto it = gcache.find(key);
+      if (it != gcache.end()) {
+        j.gunits = it->second;
+        continue;
+      }
+      Fields4 U;
+      for (int d = 0; d < 4; d++)
+        U.f[d] = j.input[d];
+      rc = GC_DISPATCH_NC(j.desc.nc, b->prec, launch_wilson_gauge_prep, j.g, U, j.GA, j.GB,
+                          j.UA, j.UB, j.flag, b->main);
+      if (rc)
+        break;
+      float best = 1e30f;
+      int bu = 0;
+      const WilsonPlan dp = wilson_gauge_plan(j.g, j.nt, j.desc.nc,
+                                              b->prec == GC_PREC_FP64 ? 8 : 4);
+      for (int units = 1; units * dp.rows <= 256; units *= 2) {
+        float ms = 0;
+        rc = GC_DISPATCH_NC(j.desc.nc, b->prec, time_wilson_gauge, j.g, j.UA, j.UB,
+                            j.desc.r_min, j.desc.r_max, j.desc.time_min, j.desc.time_max,
+                            units, scratch, b->main, &ms);
+        if (rc == GC_ERR_ARG) {
+          cudaGetLastError();
+          rc = GC_OK;
+          continue;
+        }
+        if (rc)
+          break;
+        if (ms < best) {
+          best = ms;
+          bu = units;
+        }
+      }
+      if (rc)
+        break;
+      j.gunits = bu;
+      gcache[key] = bu;
+      continue;
+    }
     auto key = std::make_tuple(j.g.L[3], j.desc.nc, j.nr, j.nt, j.g.Vs);
     auto it = cache.find(key);
     int rows, cols;
@@ -824,6 +1002,9 @@ int gc_batch_synchronize(gc_batch *b) {
   cudaError_t e = cudaEventSynchronize(b->done);
   if (e != cudaSuccess)
     return cfail(b, "batch synchronize", e);
+  if (*b->status_host)
+    return bfail(b, GC_ERR_STATE, "batch run: a multi-job W launch had fewer threads per "
+                                  "block than a job's shape needs; its results are invalid");
   return GC_OK;
 }
 
@@ -833,6 +1014,9 @@ int gc_batch_wilson(gc_batch *b, int job, double *out) {
   cudaError_t e = cudaEventSynchronize(b->done);
   if (e != cudaSuccess)
     return cfail(b, "gc_batch_wilson", e);
+  if (*b->status_host)
+    return bfail(b, GC_ERR_STATE, "gc_batch_wilson: a multi-job W launch had fewer threads "
+                                  "per block than a job's shape needs");
   const JobState &j = b->jobs[job];
   const size_t off = (size_t)(j.out_dev - b->outs);
   std::memcpy(out, b->outs_host + off, (size_t)j.nr * j.nt * sizeof(double));
@@ -880,8 +1064,10 @@ int gc_batch_info(const gc_batch *b, long long *device_bytes, int *graph_nodes,
     *graph_nodes = b->graph_nodes;
   if (launches) {
     int n = 0;
+    // HYP: three levels; per-job gauge W: lines, transform, the two gated
+    // W kernels, the reduction
     for (const Launch &L : b->launches)
-      n += (L.kind == Launch::HYP) ? 3 : 1;
+      n += (L.kind == Launch::HYP) ? 3 : (L.kind == Launch::WAUTO) ? 5 : 1;
     *launches = n;
   }
   return GC_OK;

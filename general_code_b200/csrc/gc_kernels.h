@@ -66,6 +66,7 @@ struct WJob {
   double *partials;     // this lattice's per-block partials
   int block_start;      // first block (blocks = colblocks * 3, nu fastest)
   int blocks;
+  int *status;          // set to 1 when the launch cannot run this lattice's shape
 };
 struct RJob {           // fixed-order reduction of one lattice's partials
   const double *partials;
@@ -147,7 +148,8 @@ int launch_wilson(const Geom &g, const Fields4 &U, int rmin, int rmax,
 // W(R,T) in the temporal gauge (gc_wilson_gauge.cu): applies to one
 // configuration's loops over the whole lattice with T <= Lt/2 when the block
 // shape fits; exact to rounding when the temporal links are unitary.
-WilsonPlan wilson_gauge_plan(const Geom &g, int nt, int nc, int ct_bytes);
+// units: column units (threads per time row) per block; 0 = about 128 threads.
+WilsonPlan wilson_gauge_plan(const Geom &g, int nt, int nc, int ct_bytes, int units = 0);
 bool wilson_gauge_applies(const Geom &g, int tmax, int nt, int nc, int ct_bytes);
 // Largest unitarity defect max |U U^dag - 1| of a temporal link for which the
 // form is used (FP64: ct_bytes 8; mixed: 4).
@@ -167,6 +169,28 @@ template <class Store, class CT>
 int launch_wilson_gauge(const Geom &g, const Fields4 &UA, const Fields4 &UB, int rmin,
                         int rmax, int tmin, int tmax, bool adjoint, double *partials,
                         double *out_dev, cudaStream_t s);
+
+// Both methods with the choice made on the device: the exact W kernel runs
+// (and the gauge one returns at once) when *flag != 0, else the other way
+// round; the fixed-order reduction then sums the partials of the method that
+// ran. No host synchronisation (usable inside stream capture once each
+// kernel's shared-memory attribute has been set by an earlier launch).
+// partials: wilson_auto_partials_count doubles.
+template <class Store, class CT>
+int launch_wilson_auto(const Geom &g, const Fields4 &U, const Fields4 &UA, const Fields4 &UB,
+                       int rmin, int rmax, int tmin, int tmax, bool adjoint, const int *flag,
+                       double *partials, double *out_dev, cudaStream_t s, int units = 0);
+size_t wilson_auto_partials_count(const Geom &g, int nr, int nt, int nc, int units = 0);
+template <class Store, class CT>
+int time_wilson_gauge(const Geom &g, const Fields4 &UA, const Fields4 &UB, int rmin, int rmax,
+                      int tmin, int tmax, int units, double *partials, cudaStream_t s,
+                      float *ms);
+// The exact W kernel, gated on *gate != 0, without the reduction; *blocks
+// receives the number of blocks (rows of partials).
+template <class Store, class CT>
+int launch_wilson_exact_gated(const Geom &g, const Fields4 &U, int rmin, int rmax, int tmin,
+                              int tmax, bool adjoint, const int *gate, double *partials,
+                              int *blocks, cudaStream_t s);
 
 // An explicit block shape (rows must divide Lt, at most 256 threads).
 WilsonPlan wilson_plan_shape(const Geom &g, int nr, int nt, int nc, int ct_bytes, int rows,

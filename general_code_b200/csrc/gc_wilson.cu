@@ -185,7 +185,12 @@ template <class Store, class CT, bool ADJ, bool GEVP>
 __global__ void __launch_bounds__(256)
     wilson_kernel(const __grid_constant__ Geom g, const __grid_constant__ Fields4 U,
                   const __grid_constant__ Fields4 U2, int rmin, int rmax, int tmin, int tmax,
-                  int cols, int rows, double *partials, int tstarts) {
+                  int cols, int rows, double *partials, int tstarts,
+                  const int *gate = nullptr) {
+  // gate: the temporal-gauge form's unitarity flag; this launch is the exact
+  // fallback and computes nothing when the flag says the gauge form ran
+  if (gate && *gate == 0)
+    return;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const size_t blk = (size_t)blockIdx.y * gridDim.x + blockIdx.x;
   const int ne = (rmax - rmin + 1) * (tmax - tmin + 1);
@@ -214,8 +219,13 @@ __global__ void __launch_bounds__(256)
   const int nu = local % 3, colblock = local / 3;
   const int colblocks = jb.blocks / 3;
   const int ne = (jb.rmax - jb.rmin + 1) * (jb.tmax - jb.tmin + 1);
-  if (wilson_threads(jb.cols, jb.rows, wilson_lanes(Store::NC, sizeof(CT))) > (int)blockDim.x)
-    return; // a lattice whose shape needs more threads than the launch has
+  if (wilson_threads(jb.cols, jb.rows, wilson_lanes(Store::NC, sizeof(CT))) > (int)blockDim.x) {
+    // a lattice whose shape needs more threads than the launch has: its table
+    // would be wrong, so the batch reports an error instead of a result
+    if (threadIdx.x == 0 && jb.status)
+      *jb.status = 1;
+    return;
+  }
   wilson_block<Store, CT, false>(jb.g, jb.U, jb.U, jb.rmin, jb.rmax, jb.tmin, jb.tmax, jb.cols,
                                  jb.rows, colblock, nu,
                                  jb.partials + ((size_t)nu * colblocks + colblock) * ne,
@@ -411,6 +421,33 @@ int launch_wilson_mode(const Geom &g, const Fields4 &U, const Fields4 &U2, int r
 }
 
 template <class Store, class CT>
+int launch_wilson_exact_gated(const Geom &g, const Fields4 &U, int rmin, int rmax, int tmin,
+                              int tmax, bool adjoint, const int *gate, double *partials,
+                              int *blocks, cudaStream_t s) {
+  const int nr = rmax - rmin + 1, nt = tmax - tmin + 1;
+  WilsonPlan p = wilson_plan(g, nr, nt, Store::NC, (int)sizeof(CT), 3);
+  if (!p.fits || nr * nt > kWilsonMaxEntries)
+    return plan_error("wilson_kernel: time extent or (R,T) range too large for "
+                      "one block's shared memory");
+  int rc;
+  if (adjoint) {
+    rc = allow_large_smem(wilson_kernel<Store, CT, true, false>, p.smem);
+    if (rc)
+      return rc;
+    wilson_kernel<Store, CT, true, false><<<dim3(p.blocks / 3, 3), p.threads, p.smem, s>>>(
+        g, U, U, rmin, rmax, tmin, tmax, p.cols_per_block, p.rows, partials, g.L[3], gate);
+  } else {
+    rc = allow_large_smem(wilson_kernel<Store, CT, false, false>, p.smem);
+    if (rc)
+      return rc;
+    wilson_kernel<Store, CT, false, false><<<dim3(p.blocks / 3, 3), p.threads, p.smem, s>>>(
+        g, U, U, rmin, rmax, tmin, tmax, p.cols_per_block, p.rows, partials, g.L[3], gate);
+  }
+  *blocks = p.blocks;
+  return launch_check("wilson_kernel");
+}
+
+template <class Store, class CT>
 int launch_wilson(const Geom &g, const Fields4 &U, int rmin, int rmax,
                   int tmin, int tmax, double *partials, double *out_dev,
                   cudaStream_t s, bool adjoint, const Fields4 *second, int tstarts) {
@@ -547,7 +584,10 @@ int launch_reduce_batch(const RJob *jobs, int njobs, int entries, cudaStream_t s
   template int launch_wilson_plan<STORE, CT>(const Geom &, const Fields4 &,   \
                                              int, int, int, int,              \
                                              const WilsonPlan &, double *,    \
-                                             double *, cudaStream_t);
+                                             double *, cudaStream_t);         \
+  template int launch_wilson_exact_gated<STORE, CT>(                          \
+      const Geom &, const Fields4 &, int, int, int, int, bool, const int *,   \
+      double *, int *, cudaStream_t);
 
 GC_INSTANTIATE_W(StoreF64SU3, double)
 GC_INSTANTIATE_W(StoreF64SU2, double)

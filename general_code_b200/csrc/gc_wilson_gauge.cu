@@ -25,8 +25,12 @@
 // The identity needs unitary temporal links. The lines kernel measures the
 // largest unitarity defect max |U_t U_t^dag - 1| of the lattice's temporal
 // links and raises a flag above the form's tolerance (FP64: 1e-14, a few
-// roundings; mixed: 1e-6, FP32 rounding of the 12-real links is 2.6e-7);
-// the host then runs the exact recursion instead. With defect d per link a
+// roundings; mixed: 1e-6, FP32 rounding of the 12-real links is 2.6e-7).
+// Both W kernels are launched and read the flag on the device: the exact
+// product (gc_wilson.cu) computes when it is raised, this form when it is
+// not, and the reduction sums the partials of the one that ran; no host
+// synchronisation, so the sequence can be captured in a graph. With defect
+// d per link a
 // loop differs from the reference's product of links by at most about
 // 2 T d (the two time lines), well inside the parity tolerances at these d.
 //
@@ -158,7 +162,10 @@ template <class Store, class CT, bool ADJ>
 __global__ void __launch_bounds__(256)
     wilson_gauge_kernel(const __grid_constant__ Geom g, const __grid_constant__ Fields4 UA,
                         const __grid_constant__ Fields4 UB, int rmin, int rmax, int tmin,
-                        int tmax, int cols, int rows, double *partials) {
+                        int tmax, int cols, int rows, double *partials, const int *flag) {
+  // the exact product runs instead when a temporal link failed the check
+  if (flag && *flag != 0)
+    return;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   constexpr int LANES = wilson_lanes(Store::NC, sizeof(CT));
   using LL = LaneLoad<Store, CT, LANES>;
@@ -242,6 +249,31 @@ __global__ void __launch_bounds__(256)
   }
 }
 
+// The fixed-order tree over blocks (as reduce_partials_kernel in
+// gc_wilson.cu) over the partials of whichever method ran.
+__global__ void __launch_bounds__(256)
+    reduce_select_kernel(const double *partials, int blocks_exact, int blocks_gauge,
+                         const int *flag, int nr, int nt, double scale, double *out) {
+  __shared__ double sh[256];
+  const int e = blockIdx.x;
+  const int nblocks = *flag ? blocks_exact : blocks_gauge;
+  const int nentries = nr * nt;
+  double s = 0.0;
+  for (int b = threadIdx.x; b < nblocks; b += blockDim.x)
+    s += partials[(size_t)b * nentries + e];
+  sh[threadIdx.x] = s;
+  __syncthreads();
+  for (int w = blockDim.x / 2; w > 0; w >>= 1) {
+    if (threadIdx.x < w)
+      sh[threadIdx.x] += sh[threadIdx.x + w];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    const int ir = e / nt, it = e % nt;
+    out[it * nr + ir] = sh[0] * scale;
+  }
+}
+
 int largest_divisor_upto_g(int n, int cap) {
   for (int d = cap < n ? cap : n; d > 1; d--)
     if (n % d == 0)
@@ -254,13 +286,13 @@ int largest_divisor_upto_g(int n, int cap) {
 // Block shape: every start slice of a column has a thread (rows = Lt up to
 // 64; beyond, the largest divisor of Lt up to 64 with Lt/rows slices each),
 // and about 128 threads per block.
-WilsonPlan wilson_gauge_plan(const Geom &g, int nt, int nc, int ct_bytes) {
+WilsonPlan wilson_gauge_plan(const Geom &g, int nt, int nc, int ct_bytes, int units_req) {
   WilsonPlan p{};
   const int Lt = g.L[3];
   const int ncomp = (nc == 3) ? 18 : 4;
   const int lanes = wilson_lanes(nc, ct_bytes);
   p.rows = largest_divisor_upto_g(Lt, 64);
-  const int units = std::max(1, 128 / p.rows);
+  const int units = units_req > 0 ? units_req : std::max(1, 128 / p.rows);
   p.cols_per_block = units * lanes;
   p.threads = wilson_threads(p.cols_per_block, p.rows, lanes);
   p.blocks = ((g.Vs + p.cols_per_block - 1) / p.cols_per_block) * 3;
@@ -301,34 +333,106 @@ int launch_wilson_gauge_prep(const Geom &g, const Fields4 &U, void *GA, void *GB
 }
 
 template <class Store, class CT>
-int launch_wilson_gauge(const Geom &g, const Fields4 &UA, const Fields4 &UB, int rmin,
-                        int rmax, int tmin, int tmax, bool adjoint, double *partials,
-                        double *out_dev, cudaStream_t s) {
+int launch_wilson_gauge_kernel(const Geom &g, const Fields4 &UA, const Fields4 &UB, int rmin,
+                               int rmax, int tmin, int tmax, bool adjoint, const int *flag,
+                               double *partials, int *blocks, cudaStream_t s, int units = 0) {
   const int nr = rmax - rmin + 1, nt = tmax - tmin + 1;
   if (tmax > g.L[3] / 2)
     return plan_error("wilson_gauge_kernel: time_max above Lt/2");
-  const WilsonPlan p = wilson_gauge_plan(g, nt, Store::NC, (int)sizeof(CT));
+  const WilsonPlan p = wilson_gauge_plan(g, nt, Store::NC, (int)sizeof(CT), units);
+  cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+  cudaStreamIsCapturing(s, &cap);
+  const bool capturing = cap != cudaStreamCaptureStatusNone;
   if (!p.fits || nr * nt > kWilsonMaxEntries)
     return plan_error("wilson_gauge_kernel: block shape does not fit");
   int rc;
   if (adjoint) {
-    rc = allow_large_smem(wilson_gauge_kernel<Store, CT, true>, p.smem);
+    rc = allow_large_smem(wilson_gauge_kernel<Store, CT, true>, p.smem, capturing);
     if (rc)
       return rc;
     wilson_gauge_kernel<Store, CT, true><<<dim3(p.blocks / 3, 3), p.threads, p.smem, s>>>(
-        g, UA, UB, rmin, rmax, tmin, tmax, p.cols_per_block, p.rows, partials);
+        g, UA, UB, rmin, rmax, tmin, tmax, p.cols_per_block, p.rows, partials, flag);
   } else {
-    rc = allow_large_smem(wilson_gauge_kernel<Store, CT, false>, p.smem);
+    rc = allow_large_smem(wilson_gauge_kernel<Store, CT, false>, p.smem, capturing);
     if (rc)
       return rc;
     wilson_gauge_kernel<Store, CT, false><<<dim3(p.blocks / 3, 3), p.threads, p.smem, s>>>(
-        g, UA, UB, rmin, rmax, tmin, tmax, p.cols_per_block, p.rows, partials);
+        g, UA, UB, rmin, rmax, tmin, tmax, p.cols_per_block, p.rows, partials, flag);
   }
-  rc = launch_check("wilson_gauge_kernel");
+  *blocks = p.blocks;
+  return launch_check("wilson_gauge_kernel");
+}
+
+template <class Store, class CT>
+int launch_wilson_gauge(const Geom &g, const Fields4 &UA, const Fields4 &UB, int rmin,
+                        int rmax, int tmin, int tmax, bool adjoint, double *partials,
+                        double *out_dev, cudaStream_t s) {
+  int blocks = 0;
+  const int rc = launch_wilson_gauge_kernel<Store, CT>(g, UA, UB, rmin, rmax, tmin, tmax,
+                                                       adjoint, nullptr, partials, &blocks, s);
   if (rc)
     return rc;
-  return launch_reduce_wilson(partials, p.blocks, nr, nt, wilson_scale(g.V, Store::NC, adjoint),
-                              out_dev, s);
+  return launch_reduce_wilson(partials, blocks, rmax - rmin + 1, tmax - tmin + 1,
+                              wilson_scale(g.V, Store::NC, adjoint), out_dev, s);
+}
+
+template <class Store, class CT>
+int launch_wilson_auto(const Geom &g, const Fields4 &U, const Fields4 &UA, const Fields4 &UB,
+                       int rmin, int rmax, int tmin, int tmax, bool adjoint, const int *flag,
+                       double *partials, double *out_dev, cudaStream_t s, int units) {
+  int b_exact = 0, b_gauge = 0;
+  int rc = launch_wilson_exact_gated<Store, CT>(g, U, rmin, rmax, tmin, tmax, adjoint, flag,
+                                                partials, &b_exact, s);
+  if (rc)
+    return rc;
+  rc = launch_wilson_gauge_kernel<Store, CT>(g, UA, UB, rmin, rmax, tmin, tmax, adjoint, flag,
+                                             partials, &b_gauge, s, units);
+  if (rc)
+    return rc;
+  const int nr = rmax - rmin + 1, nt = tmax - tmin + 1;
+  reduce_select_kernel<<<nr * nt, 256, 0, s>>>(partials, b_exact, b_gauge, flag, nr, nt,
+                                               wilson_scale(g.V, Store::NC, adjoint), out_dev);
+  return launch_check("reduce_select_kernel");
+}
+
+size_t wilson_auto_partials_count(const Geom &g, int nr, int nt, int nc, int units) {
+  const WilsonPlan a = wilson_gauge_plan(g, nt, nc, 4, units),
+                   b = wilson_gauge_plan(g, nt, nc, 8, units);
+  return std::max<size_t>(wilson_partials_count(g, nr, nt, nc),
+                          (size_t)std::max(a.blocks, b.blocks) * nr * nt);
+}
+
+// Times one launch of the gauge W kernel of a lattice with `units` column
+// units per block (the autotuner's candidate), from prepared transformed
+// links; partials must hold wilson_auto_partials_count(.., units) doubles.
+template <class Store, class CT>
+int time_wilson_gauge(const Geom &g, const Fields4 &UA, const Fields4 &UB, int rmin, int rmax,
+                      int tmin, int tmax, int units, double *partials, cudaStream_t s,
+                      float *ms) {
+  const WilsonPlan p = wilson_gauge_plan(g, tmax - tmin + 1, Store::NC, (int)sizeof(CT), units);
+  if (!p.fits)
+    return GC_ERR_ARG;
+  int blocks = 0;
+  int rc = launch_wilson_gauge_kernel<Store, CT>(g, UA, UB, rmin, rmax, tmin, tmax, false,
+                                                 nullptr, partials, &blocks, s, units);
+  cudaEvent_t e0, e1;
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  float best = 1e30f;
+  for (int rep = 0; rep < 3 && rc == GC_OK; rep++) {
+    cudaEventRecord(e0, s);
+    rc = launch_wilson_gauge_kernel<Store, CT>(g, UA, UB, rmin, rmax, tmin, tmax, false,
+                                               nullptr, partials, &blocks, s, units);
+    cudaEventRecord(e1, s);
+    cudaEventSynchronize(e1);
+    float t = 0;
+    cudaEventElapsedTime(&t, e0, e1);
+    best = std::min(best, t);
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  *ms = best;
+  return rc;
 }
 
 #define GC_INSTANTIATE_WG(STORE, CT)                                                        \
@@ -337,7 +441,14 @@ int launch_wilson_gauge(const Geom &g, const Fields4 &UA, const Fields4 &UB, int
                                                    int *, cudaStream_t);                    \
   template int launch_wilson_gauge<STORE, CT>(const Geom &, const Fields4 &, const Fields4 &, \
                                               int, int, int, int, bool, double *, double *,  \
-                                              cudaStream_t);
+                                              cudaStream_t);                                 \
+  template int launch_wilson_auto<STORE, CT>(const Geom &, const Fields4 &, const Fields4 &,  \
+                                             const Fields4 &, int, int, int, int, bool,       \
+                                             const int *, double *, double *, cudaStream_t,   \
+                                             int);                                            \
+  template int time_wilson_gauge<STORE, CT>(const Geom &, const Fields4 &, const Fields4 &,   \
+                                            int, int, int, int, int, double *, cudaStream_t,  \
+                                            float *);
 
 GC_INSTANTIATE_WG(StoreF64SU3, double)
 GC_INSTANTIATE_WG(StoreF64SU2, double)
