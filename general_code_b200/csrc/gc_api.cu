@@ -1483,7 +1483,8 @@ long long gc_job_device_bytes(const int dims[4], int nc, int precision,
   g.Vs = dims[0] * dims[1] * dims[2];
   const int nr = std::max(1, rmax), nt = std::max(1, tmax);
   const long long partials =
-      (long long)wilson_partials_count(g, std::min(nr, std::max(1, 1024 / nt)), nt, nc) * 8;
+      (long long)wilson_auto_partials_count(g, std::min(nr, std::max(1, 1024 / nt)), nt, nc) *
+      8;
   const long long hfield =
       ((long long)inter_link_bytes(nc, precision) * V + 255) / 256 * 256;
   return 8 * field + 15 * hfield + staging + partials + 64LL * 1024;

@@ -683,7 +683,9 @@ int gc_batch_create(const gc_job *jobs, int njobs, int precision, gc_batch **out
     j.nr = w ? j.desc.r_max - j.desc.r_min + 1 : 0;
     j.nt = w ? j.desc.time_max - j.desc.time_min + 1 : 0;
     j.hyp_bytes = align256(inter_link_bytes(j.desc.nc, precision) * (size_t)j.g.V);
-    total += 12 * j.field_bytes + (j.desc.hyp_steps > 0 ? 15 * j.hyp_bytes : 0);
+    // the HYP decorated-link scratch also holds the gauge-form W's lines and
+    // transformed links, so a job that measures W has it without HYP steps
+    total += 12 * j.field_bytes + (j.desc.hyp_steps > 0 || w ? 15 * j.hyp_bytes : 0);
     staging = std::max(staging, (size_t)(j.desc.nc == 3 ? 18 : 4) * 8 * 4 * (size_t)j.g.V);
     outs += (size_t)j.nr * j.nt;
     if (w)
@@ -704,7 +706,7 @@ int gc_batch_create(const gc_job *jobs, int njobs, int precision, gc_batch **out
       j.setA[d] = base + (4 + d) * j.field_bytes;
       j.setB[d] = base + (8 + d) * j.field_bytes;
     }
-    const int nh = j.desc.hyp_steps > 0 ? 15 : 0;
+    const int nh = j.desc.hyp_steps > 0 || j.nr > 0 ? 15 : 0;
     for (int f = 0; f < 15; f++)
       j.hyp[f] = nh ? base + 12 * j.field_bytes + f * j.hyp_bytes : nullptr;
     off += 12 * j.field_bytes + nh * j.hyp_bytes;
@@ -740,7 +742,7 @@ int gc_batch_create(const gc_job *jobs, int njobs, int precision, gc_batch **out
     // the temporal-gauge W: its lines and transformed links go into the HYP
     // decorated-link scratch (a job without HYP steps has none)
     const size_t lb = wilson_gauge_line_bytes(j.g, j.desc.nc);
-    j.gauge = ok && j.nr > 0 && j.desc.hyp_steps > 0 &&
+    j.gauge = ok && j.nr > 0 &&
               wilson_gauge_applies(j.g, j.desc.time_max, j.nt, j.desc.nc, ct_bytes) &&
               2 * lb + 6 * j.field_bytes <= 15 * j.hyp_bytes;
     if (j.gauge) {
