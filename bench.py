@@ -527,6 +527,34 @@ def bench_observables(steps: int):
                                                     "slabs run one after another on one GPU")}
 
 
+def bench_dropin():
+    """The apps/smearing job as the reference's app runs it (HYP, APE x20, the
+    W table, SU(3) 24^4 FP64; smearing.cpp:228-301), through the C++ drop-in
+    overloads (every call uploads and downloads the whole configuration) and
+    through the reference's templates on the host cores: both timed by
+    oracle/_ref/dropin_check --time, the reference compiled with the drop-in
+    header."""
+    exe = ROOT / "oracle" / "_ref" / "dropin_check"
+    if not exe.exists():
+        return {"unavailable": "oracle/_ref/dropin_check not built (needs the reference sources)"}
+    env = dict(os.environ, OMP_NUM_THREADS=str(os.cpu_count() or 1))
+    p = subprocess.run([str(exe), "--time", "3", "24", "24", "20", "12", "12"],
+                       capture_output=True, text=True, timeout=900, env=env)
+    if p.returncode != 0:
+        return {"error": (p.stdout + p.stderr)[-500:], "rc": p.returncode}
+    d = json.loads(p.stdout.strip().splitlines()[-1])
+    V = 24 ** 4
+    gpu = sum(d["dropin_s"].values())
+    ref = sum(d["reference_s"].values())
+    copy_bytes = 2 * d["config_bytes"] * d["calls"]
+    return {"workload": "SU(3) 24^4 FP64, HYP + APE x20 + W R,T<=12, the app's call sequence",
+            "dropin_s": d["dropin_s"], "reference_s": d["reference_s"],
+            "dropin_sites_per_s": V / gpu, "reference_sites_per_s": V / ref,
+            "speedup": ref / gpu, "host_device_bytes": copy_bytes,
+            "calls": d["calls"], "w_max_rel_diff": d["w_max_rel_diff"],
+            "reference_threads": os.cpu_count()}
+
+
 def run_tslab(args, wl, rank, world, dist):
     """One lattice (the workload's) split into time slabs over the ranks:
     strong scaling. Each step smears and measures from the rank's resident raw
@@ -879,9 +907,9 @@ def main():
     ap.add_argument("--form", choices=["both", "fp64", "mixed"], default="both")
     ap.add_argument("--workload", choices=sorted(WORKLOADS), default=DEFAULT_WORKLOAD)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--sections", default="su2,batch,serving,observables",
-                    help="extra single-GPU measurements: su2, batch, serving, observables "
-                         "(comma list, or none)")
+    ap.add_argument("--sections", default="su2,batch,serving,observables,dropin",
+                    help="extra single-GPU measurements: su2, batch, serving, observables, "
+                         "dropin (comma list, or none)")
     ap.add_argument("--serving-seconds", type=float, default=10.0)
     ap.add_argument("--decomp", choices=["replicas", "tslab"], default="replicas",
                     help="replicas: one configuration per rank (weak scaling); tslab: one "
@@ -966,6 +994,8 @@ def main():
         line["serving"] = bench_serving(args.serving_seconds)
     if world == 1 and "observables" in sections:
         line["observables"] = bench_observables(min(args.steps, 5))
+    if world == 1 and "dropin" in sections:
+        line["dropin"] = bench_dropin()
     if world == 1 and not args.no_cpu_baseline:
         v, info = cpu_sample(wl, args.workload, host, steps=3)
         line["cpu_baseline"] = {"value": v, "unit": "sites/s", "cores": info["cores"],

@@ -17,7 +17,8 @@
 // when the drop-in reports that no GPU is present (it throws; the reference
 // templates never throw, so this also shows that the drop-in was called).
 //
-// Usage: dropin_check <nc 2|3> <L> <T> <ape_steps> <r_max> <t_max>
+// Usage: dropin_check [--time] <nc 2|3> <L> <T> <ape_steps> <r_max> <t_max>
+// (--time: the app's HYP + APE + W job timed through both, see time_app)
 #include "data.h"
 #include "indexing.h"
 #include "matrix.h"
@@ -28,8 +29,10 @@
 
 #include "gc_dropin.hpp"
 
+#include <chrono>
 #include <cmath>
 #include <cstdio>
+#include <string>
 #include <cstdlib>
 #include <type_traits>
 #include <unistd.h>
@@ -262,15 +265,99 @@ int run(const std::array<int, 4> &dims, int ape_steps, int rmax, int tmax) {
   return ok ? 0 : 1;
 }
 
+// Timing mode: the job of apps/smearing/smearing.cpp:228-301 as the app runs
+// it (HYP once, APE ape_steps times, then the W table), on the same seeded
+// configuration, once through the drop-in overloads (unqualified calls: each
+// uploads the whole configuration, runs on the GPU and downloads the result,
+// as gc_dropin.hpp does for every call) and once through the reference
+// templates named explicitly (CPU). Wall-clock seconds of each, one line.
+template <class MT>
+int time_app(const std::array<int, 4> &dims, int ape_steps, int rmax, int tmax) {
+  const int ds = MT::data_size;
+  Data::LatticeData<DP, MT> a(dims), b(dims);
+  std::vector<double> host((size_t)4 * dims[0] * dims[1] * dims[2] * dims[3] * ds);
+  if (gc_generate_host(dims.data(), ds == 4 ? 2 : 3, ds == 4 ? 0.3 : 0.25,
+                       20261203, 0, 1, host.data()) != GC_OK) {
+    std::printf("generator failed: %s\n", gc_last_error(nullptr));
+    return 1;
+  }
+  std::vector<double> buf(ds);
+  for (size_t i = 0; i < a.array.size(); i++) {
+    for (int k = 0; k < ds; k++)
+      buf[k] = host[i * ds + k];
+    a.array[i] = MT(buf);
+    b.array[i] = MT(buf);
+  }
+  using clk = std::chrono::steady_clock;
+  std::map<std::tuple<int, int>, double> wa, wb;
+  double t_hyp = 0, t_ape = 0, t_w = 0;
+  try {
+    plaket(a); // first call: CUDA context and library set-up, not timed
+    auto t0 = clk::now();
+    smearing_HYP(a, 1, 0.75, 0.6);
+    auto t1 = clk::now();
+    for (int i = 0; i < ape_steps; i++)
+      smearing_APE(a, 0.5);
+    auto t2 = clk::now();
+    wa = wilson_loop(a, 1, rmax, 1, tmax);
+    auto t3 = clk::now();
+    t_hyp = std::chrono::duration<double>(t1 - t0).count();
+    t_ape = std::chrono::duration<double>(t2 - t1).count();
+    t_w = std::chrono::duration<double>(t3 - t2).count();
+  } catch (const std::exception &e) {
+    std::printf("drop-in raised: %s\n", e.what());
+    return 3;
+  }
+  auto r0 = clk::now();
+  ::smearing_HYP<DP, MT>(b, 1, 0.75, 0.6);
+  auto r1 = clk::now();
+  for (int i = 0; i < ape_steps; i++)
+    ::smearing_APE<DP, MT>(b, 0.5);
+  auto r2 = clk::now();
+  wb = ::wilson_loop<DP, MT>(b, 1, rmax, 1, tmax);
+  auto r3 = clk::now();
+  bool ok = wa.size() == wb.size();
+  double dw = 0;
+  for (const auto &kv : wb) {
+    const double e = std::fabs(wa[kv.first] - kv.second);
+    dw = std::fmax(dw, e / std::fabs(kv.second));
+    ok = ok && e <= 1e-12 * std::fabs(kv.second) + 1e-14;
+  }
+  const double bytes = (double)a.array.size() * ds * 8;
+  std::printf("{\"dropin_s\": {\"hyp\": %.6f, \"ape_total\": %.6f, \"wilson\": %.6f}, "
+              "\"reference_s\": {\"hyp\": %.6f, \"ape_total\": %.6f, \"wilson\": %.6f}, "
+              "\"config_bytes\": %.0f, \"calls\": %d, \"w_max_rel_diff\": %.3e, "
+              "\"ok\": %s}\n",
+              t_hyp, t_ape, t_w, std::chrono::duration<double>(r1 - r0).count(),
+              std::chrono::duration<double>(r2 - r1).count(),
+              std::chrono::duration<double>(r3 - r2).count(), bytes, ape_steps + 2, dw,
+              ok ? "true" : "false");
+  return ok ? 0 : 1;
+}
+
 } // namespace
 
 int main(int argc, char **argv) {
+  bool timing = argc > 1 && std::string(argv[1]) == "--time";
+  if (timing) {
+    argv++;
+    argc--;
+  }
   if (argc < 7) {
-    std::printf("usage: %s nc L T ape_steps r_max t_max\n", argv[0]);
+    std::printf("usage: %s [--time] nc L T ape_steps r_max t_max\n", argv[0]);
     return 2;
   }
   const int nc = std::atoi(argv[1]), L = std::atoi(argv[2]), T = std::atoi(argv[3]);
   const int n_ape = std::atoi(argv[4]), rmax = std::atoi(argv[5]), tmax = std::atoi(argv[6]);
+  if (timing) {
+    std::array<int, 4> dims = {L, L, L, T};
+    x_size = y_size = z_size = L;
+    t_size = T;
+    size1 = L * L;
+    size2 = L * L * L;
+    return nc == 2 ? time_app<su2>(dims, n_ape, rmax, tmax)
+                   : time_app<su3>(dims, n_ape, rmax, tmax);
+  }
   std::array<int, 4> dims = {L, L, L, T};
   x_size = y_size = z_size = L;
   t_size = T;
