@@ -158,7 +158,12 @@ __global__ void __launch_bounds__(128)
 
 // Shared memory of one block: per-thread loop sums red[nt][threads] (FP64),
 // then the space lines of cut A and of cut B, one slot per (t, column unit).
-template <class Store, class CT, bool ADJ>
+// PAIR: a thread owns two consecutive start slices t0 = 2 row, 2 row + 1 (of
+// the same cut: the cut slice h is even), and one shared-memory load of a top
+// space line S(t) serves both starts' loops ending on t (T = t - t0 and
+// t - t0 - 1): nt + 1 loads for 2 nt loops. Otherwise a thread owns the
+// slices row + k rows and loads one line per loop.
+template <class Store, class CT, bool ADJ, bool PAIR>
 __global__ void __launch_bounds__(256)
     wilson_gauge_kernel(const __grid_constant__ Geom g, const __grid_constant__ Fields4 UA,
                         const __grid_constant__ Fields4 UB, int rmin, int rmax, int tmin,
@@ -205,7 +210,7 @@ __global__ void __launch_bounds__(256)
       const int l1 = s1 + ((xn1 + R - 1) % Ln - xn1) * stn;
 #pragma unroll 1
       for (int k = 0; k < kt; k++) {
-        const int t = row + k * rows;
+        const int t = PAIR ? 2 * row + k : row + k * rows;
         const int i = t * units + u;
         const M la = LL::load(UA.f[nu], V, l0 + t * g.Vs, l1 + t * g.Vs);
         CS::store(sa, nslots, i, (R == 1) ? la : mul(CS::load(sa, nslots, i), la));
@@ -214,7 +219,30 @@ __global__ void __launch_bounds__(256)
       }
     }
     __syncthreads();
-    if (R >= rmin) {
+    if (R >= rmin && PAIR) {
+      const int t0 = 2 * row;
+      const unsigned char *set = (t0 < h) ? sa : sb;
+      const M a0 = active ? CS::load(set, nslots, t0 * units + u) : unit(M());
+      const M a1 = active ? CS::load(set, nslots, (t0 + 1) * units + u) : unit(M());
+      int tt = t0 + tmin;
+      tt = (tt >= Lt) ? tt - Lt : tt;
+      double pending = 0.0;
+#pragma unroll 1
+      for (int j = 0; j <= nt; j++) {
+        double v0 = 0.0, v1 = 0.0;
+        if (active) {
+          const M b = CS::load(set, nslots, tt * units + u);
+          if (j >= 1)
+            v1 = loop_value<ADJ>(a1, b, lane1); // start t0 + 1, T = tmin + j - 1
+          if (j < nt)
+            v0 = loop_value<ADJ>(a0, b, lane1); // start t0, T = tmin + j
+        }
+        if (j >= 1)
+          red[(size_t)(j - 1) * nthreads + tid] = pending + v1;
+        pending = v0;
+        tt = (tt + 1 == Lt) ? 0 : tt + 1;
+      }
+    } else if (R >= rmin) {
 #pragma unroll 1
       for (int k = 0; k < kt; k++) {
         const int t0 = row + k * rows;
@@ -232,6 +260,8 @@ __global__ void __launch_bounds__(256)
           tt = (tt + 1 == Lt) ? 0 : tt + 1;
         }
       }
+    }
+    if (R >= rmin) {
       __syncthreads();
       // fixed-order sum over the block's threads: warp w takes T = w, w +
       // nwarps, ...; each lane sums a strided subset, then a warp tree
@@ -291,8 +321,11 @@ WilsonPlan wilson_gauge_plan(const Geom &g, int nt, int nc, int ct_bytes, int un
   const int Lt = g.L[3];
   const int ncomp = (nc == 3) ? 18 : 4;
   const int lanes = wilson_lanes(nc, ct_bytes);
-  p.rows = largest_divisor_upto_g(Lt, 64);
-  const int units = units_req > 0 ? units_req : std::max(1, 128 / p.rows);
+  // paired start slices when the cut slice Lt/2 is even
+  p.pair = Lt % 4 == 0 && Lt / 2 <= 64;
+  p.rows = p.pair ? Lt / 2 : largest_divisor_upto_g(Lt, 64);
+  const int units =
+      units_req > 0 ? units_req : std::max(1, (p.pair ? 64 : 128) / p.rows);
   p.cols_per_block = units * lanes;
   p.threads = wilson_threads(p.cols_per_block, p.rows, lanes);
   p.blocks = ((g.Vs + p.cols_per_block - 1) / p.cols_per_block) * 3;
@@ -345,20 +378,23 @@ int launch_wilson_gauge_kernel(const Geom &g, const Fields4 &UA, const Fields4 &
   const bool capturing = cap != cudaStreamCaptureStatusNone;
   if (!p.fits || nr * nt > kWilsonMaxEntries)
     return plan_error("wilson_gauge_kernel: block shape does not fit");
+  auto go = [&](auto kernel) {
+    int r = allow_large_smem(kernel, p.smem, capturing);
+    if (r)
+      return r;
+    kernel<<<dim3(p.blocks / 3, 3), p.threads, p.smem, s>>>(
+        g, UA, UB, rmin, rmax, tmin, tmax, p.cols_per_block, p.rows, partials, flag);
+    return GC_OK;
+  };
   int rc;
-  if (adjoint) {
-    rc = allow_large_smem(wilson_gauge_kernel<Store, CT, true>, p.smem, capturing);
-    if (rc)
-      return rc;
-    wilson_gauge_kernel<Store, CT, true><<<dim3(p.blocks / 3, 3), p.threads, p.smem, s>>>(
-        g, UA, UB, rmin, rmax, tmin, tmax, p.cols_per_block, p.rows, partials, flag);
-  } else {
-    rc = allow_large_smem(wilson_gauge_kernel<Store, CT, false>, p.smem, capturing);
-    if (rc)
-      return rc;
-    wilson_gauge_kernel<Store, CT, false><<<dim3(p.blocks / 3, 3), p.threads, p.smem, s>>>(
-        g, UA, UB, rmin, rmax, tmin, tmax, p.cols_per_block, p.rows, partials, flag);
-  }
+  if (adjoint)
+    rc = p.pair ? go(wilson_gauge_kernel<Store, CT, true, true>)
+                : go(wilson_gauge_kernel<Store, CT, true, false>);
+  else
+    rc = p.pair ? go(wilson_gauge_kernel<Store, CT, false, true>)
+                : go(wilson_gauge_kernel<Store, CT, false, false>);
+  if (rc)
+    return rc;
   *blocks = p.blocks;
   return launch_check("wilson_gauge_kernel");
 }
