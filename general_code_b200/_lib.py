@@ -116,6 +116,7 @@ SIGNATURES.update({
     "gc_batch_download": (_c_int, [_p, _c_int, _pdbl, _c_int]),
     "gc_batch_info": (_c_int, [_p, ctypes.POINTER(ctypes.c_longlong), _pint, _pint]),
     "gc_batch_job_shape": (_c_int, [_p, _c_int, _pint, _pint]),
+    "gc_batch_autotune_report": (_c_int, [_p, ctypes.c_char_p, _c_int]),
 })
 
 FREE_BYTES_FN = ctypes.CFUNCTYPE(ctypes.c_longlong, ctypes.c_void_p)

@@ -111,6 +111,12 @@ class Batch:
                                         ctypes.byref(l)))
         return {"device_bytes": b.value, "graph_nodes": n.value, "launches_per_run": l.value}
 
+    def autotune_report(self) -> str:
+        """The candidate block shapes the autotuner timed, with their times."""
+        buf = ctypes.create_string_buffer(1 << 16)
+        self._check(lib().gc_batch_autotune_report(self._h, buf, len(buf)))
+        return buf.value.decode()
+
     def shape(self, job: int) -> Tuple[int, int]:
         r, c = ctypes.c_int(), ctypes.c_int()
         self._check(lib().gc_batch_job_shape(self._h, job, ctypes.byref(r), ctypes.byref(c)))

@@ -151,6 +151,7 @@ struct gc_batch {
   cudaGraphExec_t exec = nullptr;
   int graph_nodes = 0;
   long long device_bytes = 0;
+  std::string tune_report; // gc_batch_autotune's measurements
   std::string err;
   std::mutex mu;
 };
@@ -565,6 +566,11 @@ int tune_job(gc_batch *b, JobState &j, double *scratch, cudaStream_t s, int *row
       }
       if (rc)
         return rc;
+      char line[192];
+      std::snprintf(line, sizeof line, "SU(%d) %dx%dx%dx%d R<=%d T<=%d exact-W rows=%d cols=%d "
+                    "%.4f ms\n", j.desc.nc, j.g.L[0], j.g.L[1], j.g.L[2], j.g.L[3],
+                    j.desc.r_max, j.desc.time_max, rows, cols, ms);
+      b->tune_report += line;
       if (ms < best) {
         best = ms;
         br = rows;
@@ -874,6 +880,7 @@ int gc_batch_autotune(gc_batch *b) {
   cudaError_t e = cudaMalloc(&scratch, std::max<size_t>(need, 1) * sizeof(double));
   if (e != cudaSuccess)
     return cfail(b, "cudaMalloc(autotune scratch)", e);
+  b->tune_report.clear();
   // one tuning per distinct (Lt, nc, nr, nt, Vs)
   std::map<std::tuple<int, int, int, int, int>, std::pair<int, int>> cache;
   std::map<std::tuple<int, int, int, int, int>, int> gcache;
@@ -900,6 +907,10 @@ int gc_batch_autotune(gc_batch *b) {
       int bu = 0;
       const WilsonPlan dp = wilson_gauge_plan(j.g, j.nt, j.desc.nc,
                                               b->prec == GC_PREC_FP64 ? 8 : 4);
+      char cls[96];
+      std::snprintf(cls, sizeof cls, "SU(%d) %dx%dx%dx%d R<=%d T<=%d", j.desc.nc, j.g.L[0],
+                    j.g.L[1], j.g.L[2], j.g.L[3], j.desc.r_max, j.desc.time_max);
+      std::string lines;
       for (int units = 1; units * dp.rows <= 256; units *= 2) {
         float ms = 0;
         rc = GC_DISPATCH_NC(j.desc.nc, b->prec, time_wilson_gauge, j.g, j.UA, j.UB,
@@ -912,6 +923,10 @@ int gc_batch_autotune(gc_batch *b) {
         }
         if (rc)
           break;
+        char line[192];
+        std::snprintf(line, sizeof line, "%s gauge-W rows=%d units=%d %.4f ms\n", cls, dp.rows,
+                      units, ms);
+        lines += line;
         if (ms < best) {
           best = ms;
           bu = units;
@@ -919,6 +934,10 @@ int gc_batch_autotune(gc_batch *b) {
       }
       if (rc)
         break;
+      b->tune_report += lines;
+      char line[192];
+      std::snprintf(line, sizeof line, "%s gauge-W chosen units=%d\n", cls, bu);
+      b->tune_report += line;
       j.gunits = bu;
       gcache[key] = bu;
       continue;
@@ -1072,6 +1091,15 @@ int gc_batch_info(const gc_batch *b, long long *device_bytes, int *graph_nodes,
       n += (L.kind == Launch::HYP) ? 3 : (L.kind == Launch::WAUTO) ? 5 : 1;
     *launches = n;
   }
+  return GC_OK;
+}
+
+int gc_batch_autotune_report(const gc_batch *b, char *buf, int len) {
+  if (!b || !buf || len <= 0)
+    return record_error(GC_ERR_ARG, "gc_batch_autotune_report: bad argument");
+  const size_t n = std::min(b->tune_report.size(), (size_t)len - 1);
+  std::memcpy(buf, b->tune_report.data(), n);
+  buf[n] = 0;
   return GC_OK;
 }
 

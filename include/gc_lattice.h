@@ -432,6 +432,10 @@ int gc_batch_info(const gc_batch *b, long long *device_bytes, int *graph_nodes,
                   int *launches);
 /* The W block shape (threads per column, columns per block) used for job j. */
 int gc_batch_job_shape(const gc_batch *b, int job, int *rows, int *cols);
+/* What gc_batch_autotune measured: one line per candidate block shape timed
+ * ("<job class> <kernel> <shape> <ms>"), the chosen ones marked; copied into
+ * buf (at most len bytes, NUL-terminated). No counterpart in the reference. */
+int gc_batch_autotune_report(const gc_batch *b, char *buf, int len);
 
 /* ---------------------------------------------------------------- serving
  * A request loop: each request is one configuration (a gc_job and its host
