@@ -255,11 +255,42 @@ def cpu_sample(wl, workload, host_links, steps, warmup=0):
                        "phase_seconds": mean}
 
 
+def batch_serial(jobs, form, first_index):
+    """The batch's jobs one after another through the single-lattice API on
+    one stream (input resident, restored by a device copy; HYP, APE, the W
+    table read back): the sum of the jobs' CUDA-event times, and their W
+    tables."""
+    import torch
+    from general_code_b200 import Lattice, generate_config
+    s = torch.cuda.Stream()
+    total, tables = 0.0, []
+    for k, j in enumerate(jobs):
+        links = generate_config(j.dims, j.nc, 0.3 if j.nc == 2 else 0.25, SEED, first_index + k)
+        with Lattice(j.dims, j.nc, form) as pristine, Lattice(j.dims, j.nc, form) as lat:
+            for x in (pristine, lat):
+                x.set_stream(s.cuda_stream)
+            pristine.upload(links)
+            w = None
+            for rep in range(2):  # the first run sets up the handle
+                lat.copy_from(pristine)
+                e0, e1 = (torch.cuda.Event(enable_timing=True) for _ in range(2))
+                e0.record(s)
+                lat.hyp(*j.hyp_alpha, j.hyp_steps)
+                lat.ape(j.ape_alpha, j.ape_steps)
+                w = lat.wilson_loop(j.r_min, j.r_max, j.t_min, j.t_max)
+                e1.record(s)
+                s.synchronize()
+            total += e0.elapsed_time(e1)
+            tables.append(w)
+    return total, tables
+
+
 def bench_batch(steps: int):
     """64 configurations of uneven sizes ({8^4, 12^4, 16^4, 16^3x32, 24^4,
     24^3x48}, SU(2)/SU(3) 50/50, APE 5..30, R,T up to L_s/2) as one batch:
     autotuned W shapes, one CUDA graph launch per run. Times `steps` graph
-    launches with CUDA events after the capture run."""
+    launches with CUDA events after the capture run, and the same jobs one
+    after another through the single-lattice API (batch_serial)."""
     import torch
     from general_code_b200.batch import Batch, uneven_jobs
     out = {}
@@ -281,10 +312,19 @@ def bench_batch(steps: int):
                 s.synchronize()
                 ms.append(e0.elapsed_time(e1))
             info = b.info()
-        out[form] = {"sites_per_s": sites / (sum(ms) / len(ms) * 1e-3),
-                     "ms_per_batch": sum(ms) / len(ms), "graph_nodes": info["graph_nodes"],
+            w_batch = [b.wilson(k) for k in range(len(jobs))]
+            report = b.autotune_report()
+        serial_ms, w_serial = batch_serial(jobs, form, 1000)
+        worst = max(float(np.max(np.abs(a - c) / np.abs(c))) for a, c in zip(w_batch, w_serial))
+        batch_ms = sum(ms) / len(ms)
+        out[form] = {"sites_per_s": sites / (batch_ms * 1e-3),
+                     "ms_per_batch": batch_ms, "graph_nodes": info["graph_nodes"],
                      "kernel_launches_per_batch": info["launches_per_run"],
-                     "device_bytes": info["device_bytes"]}
+                     "device_bytes": info["device_bytes"],
+                     "serial_ms": serial_ms, "batch_over_serial": batch_ms / serial_ms,
+                     "serial_sites_per_s": sites / (serial_ms * 1e-3),
+                     "max_rel_diff_W_vs_serial": worst,
+                     "autotune_report": report.splitlines()}
     return {"workload": "64 uneven configurations, one CUDA graph per run", "jobs": 64,
             "sites": sites, "total_ape_steps": sum(j.ape_steps for j in jobs),
             "value": out["mixed"]["sites_per_s"], "unit": "sites/s", "forms": out}
