@@ -790,12 +790,12 @@ static int wilson_impl(gc_lattice *h, int rmin, int rmax, int tmin, int tmax,
     return rc;
   double *chunk_out = h->dev_out + (size_t)nr * nt;
   // The temporal-gauge form (gc_wilson_gauge.cu) for one configuration's
-  // on-axis or adjoint loops over the whole lattice with T <= Lt/2; it runs
-  // only after the device has checked that the temporal links are unitary to
-  // the form's tolerance, and the exact recursion otherwise.
+  // on-axis or adjoint loops with T <= Lt/2 (the t-slab entry, whose slabs'
+  // loops partition the lattice's, keeps the exact product); it runs only
+  // where the device finds the temporal links unitary to the form's
+  // tolerance, and the exact recursion otherwise.
   const int ct_bytes = h->prec == GC_PREC_FP64 ? 8 : 4;
-  bool gauge = h->wilson_method == GC_WILSON_AUTO && !second &&
-               (tstarts <= 0 || tstarts == h->g.L[3]) &&
+  bool gauge = h->wilson_method == GC_WILSON_AUTO && !second && tstarts <= 0 &&
                wilson_gauge_applies(h->g, tmax, nt, h->nc, ct_bytes);
   Fields4 UA{}, UB{};
   if (gauge) {

@@ -13,9 +13,6 @@
 // the mixed form); the SU(N) projection always runs in FP64.
 #include "gc_internal.cuh"
 #include "gc_kernels.h"
-#include "gc_pair.cuh"
-
-#include <type_traits>
 
 namespace gc {
 
@@ -111,61 +108,11 @@ __device__ __forceinline__ Nbr neighbours(const Geom &g, int site,
 
 constexpr int kSmearBlock = 128;
 
-// One (site, mu) of an APE step of the mixed SU(3) form: the staples of the
-// two planes (mu, nu1) and (mu, nu2) are computed together as lane-packed
-// matrices (lane 0 = nu1, lane 1 = nu2), so every product, scale and sum of
-// the staples is one packed FP32x2 instruction for both planes; the lanes are
-// added to (1 - alpha) U at the end, then projected as in the other forms.
-// The same products as the reference (smearing.h:134-149) per plane; the
-// factor alpha/4 is applied to each staple as it is added (the reference
-// scales the first product of each staple).
-__device__ __forceinline__ void ape_site_mixed_su3(const Geom &g, const Fields4 &in,
-                                                   const Fields4 &out, double alpha,
-                                                   int site, int mu) {
-  int x[4];
-  site_coords(g, site, x);
-  const size_t V = g.V;
-  const int nu1 = (mu == 0) ? 1 : 0, nu2 = (mu == 2) ? 1 : 2;
-  const Nbr n1 = neighbours(g, site, x, mu, nu1), n2 = neighbours(g, site, x, mu, nu2);
-  const float4 *fmu = reinterpret_cast<const float4 *>(in.f[mu]);
-  const float4 *fa = reinterpret_cast<const float4 *>(in.f[nu1]);
-  const float4 *fb = reinterpret_cast<const float4 *>(in.f[nu2]);
-  const float c = float(alpha / 4);
-  SU3<float> S = scale(StoreF32SU3::load<float>(in.f[mu], V, site), float(1 - alpha));
-  // S += c (lane 0 + lane 1) of a packed staple pair
-  auto fold = [&](const SU3<f2> &T) {
-#pragma unroll
-    for (int i = 0; i < 3; i++)
-#pragma unroll
-      for (int j = 0; j < 3; j++) {
-        S.e[i][j].re = fmaf(c, T.e[i][j].re.v.y, fmaf(c, T.e[i][j].re.v.x, S.e[i][j].re));
-        S.e[i][j].im = fmaf(c, T.e[i][j].im.v.y, fmaf(c, T.e[i][j].im.v.x, S.e[i][j].im));
-      }
-  };
-  // upper staples Fnu(x) Fmu(x+nu) Fnu(x+mu)^dag
-  {
-    const SU3<f2> a = mul(load_pair_f32su3(fa + site, fb + site, V),
-                          load_pair_f32su3(fmu + n1.pnu, fmu + n2.pnu, V));
-    fold(mul_ad(a, load_pair_f32su3(fa + n1.pmu, fb + n2.pmu, V)));
-  }
-  // lower staples Fnu(x-nu)^dag Fmu(x-nu) Fnu(x-nu+mu)
-  {
-    const SU3<f2> a = mul_da(load_pair_f32su3(fa + n1.mnu, fb + n2.mnu, V),
-                             load_pair_f32su3(fmu + n1.mnu, fmu + n2.mnu, V));
-    fold(mul(a, load_pair_f32su3(fa + n1.mnu_pmu, fb + n2.mnu_pmu, V)));
-  }
-  proj_store<StoreF32SU3, float, true>(out.f[mu], V, site, S);
-}
-
 // One (site, mu) of an APE step (smearing.h:121-155).
 template <class Store, class CT>
 __device__ __forceinline__ void ape_site(const Geom &g, const Fields4 &in,
                                          const Fields4 &out, double alpha,
                                          int site, int mu) {
-  if constexpr (std::is_same<Store, StoreF32SU3>::value) {
-    ape_site_mixed_su3(g, in, out, alpha, site, mu);
-    return;
-  }
   using M = typename Store::template M<CT>;
   int x[4];
   site_coords(g, site, x);
@@ -213,50 +160,6 @@ __device__ __forceinline__ int l1_spatial(int mu, int nu) {
 // Level-1 field holding Vbar_{t; a, b} (a, b spatial): staple dir 3 - a - b.
 __device__ __forceinline__ int l1_temporal(int a, int b) { return 6 + (3 - a - b); }
 
-// Level 2 of the mixed SU(3) form: the staples of the two planes (mu, rho1),
-// (mu, rho2) as lane-packed matrices (lane 0 = rho1, lane 1 = rho2), the
-// level-1 links in their 18-real FP32 fields; otherwise as hyp_l2_site.
-__device__ __forceinline__ void hyp_l2_site_mixed_su3(const Geom &g, const Fields4 &U,
-                                                      const HypL1 &l1, const HypL2 &out,
-                                                      double alpha2, int site, int f) {
-  int x[4];
-  site_coords(g, site, x);
-  const size_t V = g.V;
-  const bool temporal = f < 3;
-  const int nu = temporal ? f : f - 3;
-  const int mu = temporal ? 3 : nu;
-  const int r1 = (nu == 0) ? 1 : 0, r2 = (nu == 2) ? 1 : 2;
-  const float2 *fmu1 = reinterpret_cast<const float2 *>(
-      temporal ? l1.f[l1_temporal(nu, r1)] : l1.f[l1_spatial(nu, r1)]);
-  const float2 *fmu2 = reinterpret_cast<const float2 *>(
-      temporal ? l1.f[l1_temporal(nu, r2)] : l1.f[l1_spatial(nu, r2)]);
-  const float2 *fnu1 = reinterpret_cast<const float2 *>(l1.f[l1_spatial(r1, nu)]);
-  const float2 *fnu2 = reinterpret_cast<const float2 *>(l1.f[l1_spatial(r2, nu)]);
-  const Nbr n1 = neighbours(g, site, x, mu, r1), n2 = neighbours(g, site, x, mu, r2);
-  const float c = float(alpha2 / 4);
-  SU3<float> S = scale(StoreF32SU3::load<float>(U.f[mu], V, site), float(1 - alpha2));
-  auto fold = [&](const SU3<f2> &T) {
-#pragma unroll
-    for (int i = 0; i < 3; i++)
-#pragma unroll
-      for (int j = 0; j < 3; j++) {
-        S.e[i][j].re = fmaf(c, T.e[i][j].re.v.y, fmaf(c, T.e[i][j].re.v.x, S.e[i][j].re));
-        S.e[i][j].im = fmaf(c, T.e[i][j].im.v.y, fmaf(c, T.e[i][j].im.v.x, S.e[i][j].im));
-      }
-  };
-  {
-    const SU3<f2> a = mul(load_pair_f32full(fnu1 + site, fnu2 + site, V),
-                          load_pair_f32full(fmu1 + n1.pnu, fmu2 + n2.pnu, V));
-    fold(mul_ad(a, load_pair_f32full(fnu1 + n1.pmu, fnu2 + n2.pmu, V)));
-  }
-  {
-    const SU3<f2> a = mul_da(load_pair_f32full(fnu1 + n1.mnu, fnu2 + n2.mnu, V),
-                             load_pair_f32full(fmu1 + n1.mnu, fmu2 + n2.mnu, V));
-    fold(mul(a, load_pair_f32full(fnu1 + n1.mnu_pmu, fnu2 + n2.mnu_pmu, V)));
-  }
-  proj_store<StoreF32SU3Full, float>(out.f[f], V, site, S);
-}
-
 // Level-2 decorated links. Field index f:
 //   0..2 : Vtilde_{t;nu}, nu = f       (smearing.h:433-450)
 //   3..5 : Vtilde_{nu;t}, nu = f - 3   (smearing.h:455-466)
@@ -264,10 +167,6 @@ template <class Store, class CT>
 __device__ __forceinline__ void hyp_l2_site(const Geom &g, const Fields4 &U,
                                             const HypL1 &l1, const HypL2 &out,
                                             double alpha2, int site, int f) {
-  if constexpr (std::is_same<Store, StoreF32SU3>::value) {
-    hyp_l2_site_mixed_su3(g, U, l1, out, alpha2, site, f);
-    return;
-  }
   using M = typename Store::template M<CT>;
   int x[4];
   site_coords(g, site, x);

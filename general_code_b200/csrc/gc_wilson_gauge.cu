@@ -324,8 +324,10 @@ WilsonPlan wilson_gauge_plan(const Geom &g, int nt, int nc, int ct_bytes, int un
   // paired start slices when the cut slice Lt/2 is even
   p.pair = Lt % 4 == 0 && Lt / 2 <= 64;
   p.rows = p.pair ? Lt / 2 : largest_divisor_upto_g(Lt, 64);
-  const int units =
-      units_req > 0 ? units_req : std::max(1, (p.pair ? 64 : 128) / p.rows);
+  // (about 128 threads: at SU(3) 32^4 the paired kernel took 5.5, 4.6, 3.8,
+  // 3.1, 3.1 ms mixed with 1, 2, 4, 8, 16 column units of 16 threads; wider
+  // blocks coalesce the extension's link loads)
+  const int units = units_req > 0 ? units_req : std::max(1, 128 / p.rows);
   p.cols_per_block = units * lanes;
   p.threads = wilson_threads(p.cols_per_block, p.rows, lanes);
   p.blocks = ((g.Vs + p.cols_per_block - 1) / p.cols_per_block) * 3;

@@ -220,7 +220,8 @@ int gc_wilson_gevp_adjoint_onaxis(gc_lattice *h1, gc_lattice *h2, int r_min, int
  * (a0,a1) then (a2,a3); mixed SU(3) = 3 planes of V float4, (u00,u01),
  * (u02,u10), (u11,u12); mixed SU(2) = 1 plane of V float4) and a device
  * buffer out_dev of (time_max-time_min+1)*(r_max-r_min+1) doubles, filled as
- * gc_wilson_onaxis fills `out`. The work is queued on cuda_stream (a
+ * gc_wilson_onaxis fills `out` with the exact product of links
+ * (GC_WILSON_EXACT). The work is queued on cuda_stream (a
  * cudaStream_t as void*, NULL = default stream) and the call returns without
  * waiting. Working memory is a fixed 16 MiB array in the library's static
  * device memory. The CUDA runtime loads the library's device module lazily,

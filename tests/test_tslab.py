@@ -235,6 +235,8 @@ def test_wilson_tslab_full_is_wilson_loop(nc):
     links = generate_config(dims, nc, 0.3 if nc == 2 else 0.25, 20261203, 6)
     for form in ("fp64", "mixed"):
         with Lattice(dims, nc, form) as lat:
+            # the t-slab entry computes the exact product of links
+            lat.set_wilson_method("exact")
             lat.upload(links)
             lat.ape(0.5, 2)
             w = lat.wilson_loop(1, 3, 1, 4)
@@ -268,6 +270,7 @@ def test_emulated_slabs_match_one_lattice(nc, dims, slabs, t_max, form):
     links = generate_config(dims, nc, 0.3 if nc == 2 else 0.25, 20261203, 8)
     hyp, ape = (1.0, 0.75, 0.6), 3
     with Lattice(dims, nc, form) as lat:
+        lat.set_wilson_method("exact")  # the slabs' W is the exact product
         lat.upload(links)
         lat.hyp(*hyp, 1)
         lat.ape(0.5, ape)
@@ -304,6 +307,7 @@ def test_tslab_job_reuses_its_lattices(form):
     nc, dims = 3, (6, 6, 6, 10)
     links = generate_config(dims, nc, 0.25, 20261203, 12)
     with Lattice(dims, nc, form) as lat:
+        lat.set_wilson_method("exact")  # the slabs' W is the exact product
         lat.upload(links)
         lat.hyp(1.0, 0.75, 0.6, 1)
         lat.ape(0.5, 3)

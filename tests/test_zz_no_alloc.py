@@ -70,6 +70,9 @@ def test_noalloc_matches_handle_entry_point_twice(nc, dims, precision, rng):
     V = int(np.prod(dims))
     links = generate_config(dims, nc, 0.3 if nc == 2 else 0.25, 20261203, 5)
     with Lattice(dims, nc, precision) as lat:
+        # the no-allocation entry point computes the exact product of links,
+        # which is what the handle entry point computes with this method
+        lat.set_wilson_method("exact")
         lat.upload(links)
         expect = lat.wilson_loop(*rng)
     fields = device_fields(links, nc, precision, V)
