@@ -92,7 +92,7 @@ struct WilsonPlan {
   int blocks;         // ceil(Vs / cols_per_block) * 3
   size_t smem;        // dynamic shared memory bytes
   bool fits;          // false when even one column exceeds the budget
-  bool pair = false;  // temporal-gauge form: two start slices per thread
+  int starts = 1;     // temporal-gauge form: consecutive start slices per thread
 };
 // Doubles of a W block's per-warp accumulators in shared memory, rounded up
 // to an even count so the 16-byte arrays placed after them stay aligned.

@@ -43,8 +43,9 @@
 //   wilson_gauge_kernel     block = `cols` columns (s, nu) over all t: the
 //                           transformed space lines of both cuts in shared
 //                           memory, extended by one link per R; a thread per
-//                           (column unit, start slice) adds the traces of its
-//                           loops for every T into a per-thread slot; a
+//                           (column unit, 1, 2 or 4 start slices) adds the
+//                           traces of its loops for every T into a per-thread
+//                           slot; a
 //                           fixed-order sum over the block's threads gives
 //                           one partial per (block, R, T), and the fixed-order
 //                           tree over blocks of gc_wilson.cu finishes.
@@ -158,12 +159,13 @@ __global__ void __launch_bounds__(128)
 
 // Shared memory of one block: per-thread loop sums red[nt][threads] (FP64),
 // then the space lines of cut A and of cut B, one slot per (t, column unit).
-// PAIR: a thread owns two consecutive start slices t0 = 2 row, 2 row + 1 (of
-// the same cut: the cut slice h is even), and one shared-memory load of a top
-// space line S(t) serves both starts' loops ending on t (T = t - t0 and
-// t - t0 - 1): nt + 1 loads for 2 nt loops. Otherwise a thread owns the
-// slices row + k rows and loads one line per loop.
-template <class Store, class CT, bool ADJ, bool PAIR>
+// KS > 1: a thread owns KS consecutive start slices t0 = KS row + m, m < KS
+// (all of one cut: KS divides the cut slice h), and one shared-memory load of
+// a top space line S(t) serves the loops of all of them that end on t
+// (T = t - t0 - m): nt + KS - 1 loads for KS nt loops, the sums of the last
+// KS values of T kept in registers. KS = 1: a thread owns the slices
+// row + k rows and loads one line per loop.
+template <class Store, class CT, bool ADJ, int KS>
 __global__ void __launch_bounds__(256)
     wilson_gauge_kernel(const __grid_constant__ Geom g, const __grid_constant__ Fields4 UA,
                         const __grid_constant__ Fields4 UB, int rmin, int rmax, int tmin,
@@ -210,7 +212,7 @@ __global__ void __launch_bounds__(256)
       const int l1 = s1 + ((xn1 + R - 1) % Ln - xn1) * stn;
 #pragma unroll 1
       for (int k = 0; k < kt; k++) {
-        const int t = PAIR ? 2 * row + k : row + k * rows;
+        const int t = KS > 1 ? KS * row + k : row + k * rows;
         const int i = t * units + u;
         const M la = LL::load(UA.f[nu], V, l0 + t * g.Vs, l1 + t * g.Vs);
         CS::store(sa, nslots, i, (R == 1) ? la : mul(CS::load(sa, nslots, i), la));
@@ -219,27 +221,34 @@ __global__ void __launch_bounds__(256)
       }
     }
     __syncthreads();
-    if (R >= rmin && PAIR) {
-      const int t0 = 2 * row;
+    if (R >= rmin && KS > 1) {
+      const int t0 = KS * row;
       const unsigned char *set = (t0 < h) ? sa : sb;
-      const M a0 = active ? CS::load(set, nslots, t0 * units + u) : unit(M());
-      const M a1 = active ? CS::load(set, nslots, (t0 + 1) * units + u) : unit(M());
+      M a[KS];
+#pragma unroll
+      for (int m = 0; m < KS; m++)
+        a[m] = active ? CS::load(set, nslots, (t0 + m) * units + u) : unit(M());
       int tt = t0 + tmin;
       tt = (tt >= Lt) ? tt - Lt : tt;
-      double pending = 0.0;
+      double acc[KS]; // acc[m]: the sum for T index j - m
+#pragma unroll
+      for (int m = 0; m < KS; m++)
+        acc[m] = 0.0;
 #pragma unroll 1
-      for (int j = 0; j <= nt; j++) {
-        double v0 = 0.0, v1 = 0.0;
+      for (int j = 0; j < nt + KS - 1; j++) {
         if (active) {
           const M b = CS::load(set, nslots, tt * units + u);
-          if (j >= 1)
-            v1 = loop_value<ADJ>(a1, b, lane1); // start t0 + 1, T = tmin + j - 1
-          if (j < nt)
-            v0 = loop_value<ADJ>(a0, b, lane1); // start t0, T = tmin + j
+#pragma unroll
+          for (int m = 0; m < KS; m++)
+            if (j - m >= 0 && j - m < nt) // start t0 + m, T = tmin + j - m
+              acc[m] += loop_value<ADJ>(a[m], b, lane1);
         }
-        if (j >= 1)
-          red[(size_t)(j - 1) * nthreads + tid] = pending + v1;
-        pending = v0;
+        if (j - (KS - 1) >= 0) // T index j - KS + 1 has all KS starts
+          red[(size_t)(j - (KS - 1)) * nthreads + tid] = acc[KS - 1];
+#pragma unroll
+        for (int m = KS - 1; m > 0; m--)
+          acc[m] = acc[m - 1];
+        acc[0] = 0.0;
         tt = (tt + 1 == Lt) ? 0 : tt + 1;
       }
     } else if (R >= rmin) {
@@ -321,9 +330,14 @@ WilsonPlan wilson_gauge_plan(const Geom &g, int nt, int nc, int ct_bytes, int un
   const int Lt = g.L[3];
   const int ncomp = (nc == 3) ? 18 : 4;
   const int lanes = wilson_lanes(nc, ct_bytes);
-  // paired start slices when the cut slice Lt/2 is even
-  p.pair = Lt % 4 == 0 && Lt / 2 <= 64;
-  p.rows = p.pair ? Lt / 2 : largest_divisor_upto_g(Lt, 64);
+  // consecutive start slices per thread (a divisor of the cut slice h = Lt/2,
+  // so that a thread's starts share a cut): 2 for SU(3) (its registers hold
+  // two lane-packed matrices), 4 for SU(2) (quaternions are small)
+  p.starts = 1;
+  for (int ks : {nc == 2 ? 4 : 2, 2})
+    if (p.starts == 1 && Lt % (2 * ks) == 0 && Lt / ks <= 64)
+      p.starts = ks;
+  p.rows = p.starts > 1 ? Lt / p.starts : largest_divisor_upto_g(Lt, 64);
   // (about 128 threads: at SU(3) 32^4 the paired kernel took 5.5, 4.6, 3.8,
   // 3.1, 3.1 ms mixed with 1, 2, 4, 8, 16 column units of 16 threads; wider
   // blocks coalesce the extension's link loads)
@@ -389,12 +403,16 @@ int launch_wilson_gauge_kernel(const Geom &g, const Fields4 &UA, const Fields4 &
     return GC_OK;
   };
   int rc;
+  // (four starts per thread only for SU(2), as the plan chooses)
+  constexpr int K4 = Store::NC == 2 ? 4 : 2;
   if (adjoint)
-    rc = p.pair ? go(wilson_gauge_kernel<Store, CT, true, true>)
-                : go(wilson_gauge_kernel<Store, CT, true, false>);
+    rc = p.starts == 4   ? go(wilson_gauge_kernel<Store, CT, true, K4>)
+         : p.starts == 2 ? go(wilson_gauge_kernel<Store, CT, true, 2>)
+                         : go(wilson_gauge_kernel<Store, CT, true, 1>);
   else
-    rc = p.pair ? go(wilson_gauge_kernel<Store, CT, false, true>)
-                : go(wilson_gauge_kernel<Store, CT, false, false>);
+    rc = p.starts == 4   ? go(wilson_gauge_kernel<Store, CT, false, K4>)
+         : p.starts == 2 ? go(wilson_gauge_kernel<Store, CT, false, 2>)
+                         : go(wilson_gauge_kernel<Store, CT, false, 1>);
   if (rc)
     return rc;
   *blocks = p.blocks;
