@@ -157,6 +157,79 @@ __global__ void __launch_bounds__(128)
              GS::template load<double>(GB, V, sn)));
 }
 
+// The loop value from Tr[a b^dag] as loop_value (gc_wcol.cuh) computes it,
+// with the sum split into one fused chain per row and the three rows added at
+// the end: three independent chains instead of one of 18 dependent FMAs,
+// which the trace loop below (a few warps per scheduler, shared-memory
+// operands) needs to keep the FMA pipe fed.
+template <bool ADJ, class T>
+__device__ __forceinline__ double gauge_trace(const SU3<T> &a, const SU3<T> &b, bool) {
+  T re[3], im[3];
+#pragma unroll
+  for (int i = 0; i < 3; i++) {
+    re[i] = a.e[i][0].re * b.e[i][0].re;
+    re[i] = GC_FMA(a.e[i][0].im, b.e[i][0].im, re[i]);
+    if (ADJ) {
+      im[i] = a.e[i][0].im * b.e[i][0].re;
+      im[i] = GC_FMA(-a.e[i][0].re, b.e[i][0].im, im[i]);
+    }
+#pragma unroll
+    for (int j = 1; j < 3; j++) {
+      re[i] = GC_FMA(a.e[i][j].re, b.e[i][j].re, re[i]);
+      re[i] = GC_FMA(a.e[i][j].im, b.e[i][j].im, re[i]);
+      if (ADJ) {
+        im[i] = GC_FMA(a.e[i][j].im, b.e[i][j].re, im[i]);
+        im[i] = GC_FMA(-a.e[i][j].re, b.e[i][j].im, im[i]);
+      }
+    }
+  }
+  const double r = double((re[0] + re[1]) + re[2]);
+  if (!ADJ)
+    return r;
+  const double m = double((im[0] + im[1]) + im[2]);
+  return fma(r, r, fma(m, m, -1.0));
+}
+template <bool ADJ>
+__device__ __forceinline__ double gauge_trace(const SU3<f2> &a, const SU3<f2> &b, bool lane1) {
+  f2 re[3], im[3];
+#pragma unroll
+  for (int i = 0; i < 3; i++) {
+    re[i] = a.e[i][0].re * b.e[i][0].re;
+    re[i] = fma(a.e[i][0].im, b.e[i][0].im, re[i]);
+    if (ADJ) {
+      im[i] = a.e[i][0].im * b.e[i][0].re;
+      im[i] = fma(-a.e[i][0].re, b.e[i][0].im, im[i]);
+    }
+#pragma unroll
+    for (int j = 1; j < 3; j++) {
+      re[i] = fma(a.e[i][j].re, b.e[i][j].re, re[i]);
+      re[i] = fma(a.e[i][j].im, b.e[i][j].im, re[i]);
+      if (ADJ) {
+        im[i] = fma(a.e[i][j].im, b.e[i][j].re, im[i]);
+        im[i] = fma(-a.e[i][j].re, b.e[i][j].im, im[i]);
+      }
+    }
+  }
+  const float2 r = make_float2((re[0].v.x + re[1].v.x) + re[2].v.x,
+                               (re[0].v.y + re[1].v.y) + re[2].v.y);
+  if (!ADJ) {
+    const double v0 = double(r.x);
+    return lane1 ? v0 + double(r.y) : v0;
+  }
+  const float2 m = make_float2((im[0].v.x + im[1].v.x) + im[2].v.x,
+                               (im[0].v.y + im[1].v.y) + im[2].v.y);
+  const double r0 = double(r.x), i0 = double(m.x);
+  const double v0 = fma(r0, r0, fma(i0, i0, -1.0));
+  if (!lane1)
+    return v0;
+  const double r1 = double(r.y), i1 = double(m.y);
+  return v0 + fma(r1, r1, fma(i1, i1, -1.0));
+}
+template <bool ADJ, class T>
+__device__ __forceinline__ double gauge_trace(const SU2<T> &a, const SU2<T> &b, bool lane1) {
+  return loop_value<ADJ>(a, b, lane1);
+}
+
 // Shared memory of one block: per-thread loop sums red[nt][threads] (FP64),
 // then the space lines of cut A and of cut B, one slot per (t, column unit).
 // KS > 1: a thread owns KS consecutive start slices t0 = KS row + m, m < KS
@@ -214,10 +287,16 @@ __global__ void __launch_bounds__(256)
       for (int k = 0; k < kt; k++) {
         const int t = KS > 1 ? KS * row + k : row + k * rows;
         const int i = t * units + u;
+        // both cuts' links are loaded before either product needs them
         const M la = LL::load(UA.f[nu], V, l0 + t * g.Vs, l1 + t * g.Vs);
-        CS::store(sa, nslots, i, (R == 1) ? la : mul(CS::load(sa, nslots, i), la));
         const M lb = LL::load(UB.f[nu], V, l0 + t * g.Vs, l1 + t * g.Vs);
-        CS::store(sb, nslots, i, (R == 1) ? lb : mul(CS::load(sb, nslots, i), lb));
+        if (R == 1) {
+          CS::store(sa, nslots, i, la);
+          CS::store(sb, nslots, i, lb);
+        } else {
+          CS::store(sa, nslots, i, mul(CS::load(sa, nslots, i), la));
+          CS::store(sb, nslots, i, mul(CS::load(sb, nslots, i), lb));
+        }
       }
     }
     __syncthreads();
@@ -234,14 +313,17 @@ __global__ void __launch_bounds__(256)
 #pragma unroll
       for (int m = 0; m < KS; m++)
         acc[m] = 0.0;
+      // the next top line is loaded while the current one's traces run
+      M b = active ? CS::load(set, nslots, tt * units + u) : unit(M());
 #pragma unroll 1
       for (int j = 0; j < nt + KS - 1; j++) {
+        tt = (tt + 1 == Lt) ? 0 : tt + 1;
+        const M bn = (active && j + 1 < nt + KS - 1) ? CS::load(set, nslots, tt * units + u) : b;
         if (active) {
-          const M b = CS::load(set, nslots, tt * units + u);
 #pragma unroll
           for (int m = 0; m < KS; m++)
             if (j - m >= 0 && j - m < nt) // start t0 + m, T = tmin + j - m
-              acc[m] += loop_value<ADJ>(a[m], b, lane1);
+              acc[m] += gauge_trace<ADJ>(a[m], b, lane1);
         }
         if (j - (KS - 1) >= 0) // T index j - KS + 1 has all KS starts
           red[(size_t)(j - (KS - 1)) * nthreads + tid] = acc[KS - 1];
@@ -249,7 +331,7 @@ __global__ void __launch_bounds__(256)
         for (int m = KS - 1; m > 0; m--)
           acc[m] = acc[m - 1];
         acc[0] = 0.0;
-        tt = (tt + 1 == Lt) ? 0 : tt + 1;
+        b = bn;
       }
     } else if (R >= rmin) {
 #pragma unroll 1
@@ -263,7 +345,7 @@ __global__ void __launch_bounds__(256)
 #pragma unroll 1
         for (int T = 0; T < nt; T++) {
           const double v =
-              active ? loop_value<ADJ>(a, CS::load(set, nslots, tt * units + u), lane1) : 0.0;
+              active ? gauge_trace<ADJ>(a, CS::load(set, nslots, tt * units + u), lane1) : 0.0;
           double *r = red + (size_t)T * nthreads + tid;
           *r = (k == 0) ? v : *r + v;
           tt = (tt + 1 == Lt) ? 0 : tt + 1;
