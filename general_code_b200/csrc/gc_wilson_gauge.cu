@@ -313,12 +313,9 @@ __global__ void __launch_bounds__(256)
 #pragma unroll
       for (int m = 0; m < KS; m++)
         acc[m] = 0.0;
-      // the next top line is loaded while the current one's traces run
-      M b = active ? CS::load(set, nslots, tt * units + u) : unit(M());
-#pragma unroll 1
-      for (int j = 0; j < nt + KS - 1; j++) {
-        tt = (tt + 1 == Lt) ? 0 : tt + 1;
-        const M bn = (active && j + 1 < nt + KS - 1) ? CS::load(set, nslots, tt * units + u) : b;
+      // One step of the sweep: the loops of all starts that end on top line
+      // b (index j), then the completed sum of T index j - KS + 1.
+      auto step = [&](int j, const M &b) {
         if (active) {
 #pragma unroll
           for (int m = 0; m < KS; m++)
@@ -331,7 +328,26 @@ __global__ void __launch_bounds__(256)
         for (int m = KS - 1; m > 0; m--)
           acc[m] = acc[m - 1];
         acc[0] = 0.0;
-        b = bn;
+      };
+      // two top lines in flight (b0, b1 alternate): the next line's load is
+      // issued before the current line's traces (a slot past the last step
+      // is still a slot of the column: its load is in bounds and unused;
+      // inactive threads use no line)
+      const int nsteps = nt + KS - 1;
+      M b0, b1;
+      if (active)
+        b0 = CS::load(set, nslots, tt * units + u);
+#pragma unroll 1
+      for (int j = 0; j < nsteps; j += 2) {
+        tt = (tt + 1 == Lt) ? 0 : tt + 1;
+        if (active)
+          b1 = CS::load(set, nslots, tt * units + u);
+        step(j, b0);
+        tt = (tt + 1 == Lt) ? 0 : tt + 1;
+        if (active)
+          b0 = CS::load(set, nslots, tt * units + u);
+        if (j + 1 < nsteps)
+          step(j + 1, b1);
       }
     } else if (R >= rmin) {
 #pragma unroll 1
