@@ -14,6 +14,8 @@
 #include "gc_internal.cuh"
 #include "gc_kernels.h"
 
+#include <type_traits>
+
 namespace gc {
 
 namespace {
@@ -108,11 +110,150 @@ __device__ __forceinline__ Nbr neighbours(const Geom &g, int site,
 
 constexpr int kSmearBlock = 128;
 
+// ---------------------------------------------------- mixed SU(3) staples
+// The mixed form stores two rows of an SU(3) link and rebuilds the third as
+// conj(row0 x row1); a product of such links is again in SU(3), so a staple
+// needs only its first two rows computed, and its third row is rebuilt the
+// same way. Rows 0 and 1 of a product take 2/3 of its multiply-adds, and the
+// left factor of a product needs no rebuilt row.
+// rows 0 and 1 of a stored link (row 2 not set)
+__device__ __forceinline__ SU3<float> load_rows01(const void *f, size_t V, int site) {
+  const float4 *p = reinterpret_cast<const float4 *>(f) + site;
+  const float4 a = __ldg(p), b = __ldg(p + V), c = __ldg(p + 2 * V);
+  SU3<float> u;
+  u.e[0][0] = {a.x, a.y};
+  u.e[0][1] = {a.z, a.w};
+  u.e[0][2] = {b.x, b.y};
+  u.e[1][0] = {b.z, b.w};
+  u.e[1][1] = {c.x, c.y};
+  u.e[1][2] = {c.z, c.w};
+  return u;
+}
+// row 2 = conj(row0 x row1), as StoreF32SU3::load rebuilds it
+__device__ __forceinline__ void rebuild_row2(SU3<float> &u) {
+#pragma unroll
+  for (int j = 0; j < 3; j++) {
+    const int a1 = (j + 1) % 3, b1 = (j + 2) % 3;
+    cx<float> t = csub(cmul(u.e[0][a1], u.e[1][b1]), cmul(u.e[0][b1], u.e[1][a1]));
+    u.e[2][j] = {t.re, -t.im};
+  }
+}
+// rows 0 and 1 of A B (A: rows 0, 1; B: all rows)
+__device__ __forceinline__ SU3<float> mul01(const SU3<float> &A, const SU3<float> &B) {
+  SU3<float> C;
+#pragma unroll
+  for (int i = 0; i < 2; i++)
+#pragma unroll
+    for (int j = 0; j < 3; j++) {
+      float re = A.e[i][0].re * B.e[0][j].re;
+      float im = A.e[i][0].re * B.e[0][j].im;
+      re = fmaf(-A.e[i][0].im, B.e[0][j].im, re);
+      im = fmaf(A.e[i][0].im, B.e[0][j].re, im);
+#pragma unroll
+      for (int k = 1; k < 3; k++) {
+        re = fmaf(A.e[i][k].re, B.e[k][j].re, re);
+        re = fmaf(-A.e[i][k].im, B.e[k][j].im, re);
+        im = fmaf(A.e[i][k].re, B.e[k][j].im, im);
+        im = fmaf(A.e[i][k].im, B.e[k][j].re, im);
+      }
+      C.e[i][j] = {re, im};
+    }
+  return C;
+}
+// rows 0 and 1 of A B^dag (A: rows 0, 1; B: all rows)
+__device__ __forceinline__ SU3<float> mul_ad01(const SU3<float> &A, const SU3<float> &B) {
+  SU3<float> C;
+#pragma unroll
+  for (int i = 0; i < 2; i++)
+#pragma unroll
+    for (int j = 0; j < 3; j++) {
+      float re = A.e[i][0].re * B.e[j][0].re;
+      float im = A.e[i][0].im * B.e[j][0].re;
+      re = fmaf(A.e[i][0].im, B.e[j][0].im, re);
+      im = fmaf(-A.e[i][0].re, B.e[j][0].im, im);
+#pragma unroll
+      for (int k = 1; k < 3; k++) {
+        re = fmaf(A.e[i][k].re, B.e[j][k].re, re);
+        re = fmaf(A.e[i][k].im, B.e[j][k].im, re);
+        im = fmaf(A.e[i][k].im, B.e[j][k].re, im);
+        im = fmaf(-A.e[i][k].re, B.e[j][k].im, im);
+      }
+      C.e[i][j] = {re, im};
+    }
+  return C;
+}
+// rows 0 and 1 of A^dag B (A, B: all rows)
+__device__ __forceinline__ SU3<float> mul_da01(const SU3<float> &A, const SU3<float> &B) {
+  SU3<float> C;
+#pragma unroll
+  for (int i = 0; i < 2; i++)
+#pragma unroll
+    for (int j = 0; j < 3; j++) {
+      float re = A.e[0][i].re * B.e[0][j].re;
+      float im = A.e[0][i].re * B.e[0][j].im;
+      re = fmaf(A.e[0][i].im, B.e[0][j].im, re);
+      im = fmaf(-A.e[0][i].im, B.e[0][j].re, im);
+#pragma unroll
+      for (int k = 1; k < 3; k++) {
+        re = fmaf(A.e[k][i].re, B.e[k][j].re, re);
+        re = fmaf(A.e[k][i].im, B.e[k][j].im, re);
+        im = fmaf(A.e[k][i].re, B.e[k][j].im, im);
+        im = fmaf(-A.e[k][i].im, B.e[k][j].re, im);
+      }
+      C.e[i][j] = {re, im};
+    }
+  return C;
+}
+// S += c T, T's row 2 rebuilt from its rows 0 and 1
+__device__ __forceinline__ void add_staple01(SU3<float> &S, SU3<float> T, float c) {
+  rebuild_row2(T);
+#pragma unroll
+  for (int i = 0; i < 3; i++)
+#pragma unroll
+    for (int j = 0; j < 3; j++) {
+      S.e[i][j].re = fmaf(c, T.e[i][j].re, S.e[i][j].re);
+      S.e[i][j].im = fmaf(c, T.e[i][j].im, S.e[i][j].im);
+    }
+}
+
+// One (site, mu) of an APE step of the mixed SU(3) form: the reference's
+// staples (smearing.h:134-149), each computed in its first two rows; alpha/4
+// is applied as each staple is added (the reference scales its first
+// product).
+__device__ __forceinline__ void ape_site_mixed_su3(const Geom &g, const Fields4 &in,
+                                                   const Fields4 &out, double alpha,
+                                                   int site, int mu) {
+  int x[4];
+  site_coords(g, site, x);
+  const size_t V = g.V;
+  const float c = float(alpha / 4);
+  SU3<float> S = scale(StoreF32SU3::load<float>(in.f[mu], V, site), float(1 - alpha));
+#pragma unroll 1
+  for (int nu = 0; nu < 3; nu++) {
+    if (nu == mu)
+      continue;
+    const Nbr n = neighbours(g, site, x, mu, nu);
+    // upper staple Fnu(x) Fmu(x+nu) Fnu(x+mu)^dag
+    SU3<float> a = mul01(load_rows01(in.f[nu], V, site),
+                         StoreF32SU3::load<float>(in.f[mu], V, n.pnu));
+    add_staple01(S, mul_ad01(a, StoreF32SU3::load<float>(in.f[nu], V, n.pmu)), c);
+    // lower staple Fnu(x-nu)^dag Fmu(x-nu) Fnu(x-nu+mu)
+    a = mul_da01(StoreF32SU3::load<float>(in.f[nu], V, n.mnu),
+                 StoreF32SU3::load<float>(in.f[mu], V, n.mnu));
+    add_staple01(S, mul01(a, StoreF32SU3::load<float>(in.f[nu], V, n.mnu_pmu)), c);
+  }
+  proj_store<StoreF32SU3, float, true>(out.f[mu], V, site, S);
+}
+
 // One (site, mu) of an APE step (smearing.h:121-155).
 template <class Store, class CT>
 __device__ __forceinline__ void ape_site(const Geom &g, const Fields4 &in,
                                          const Fields4 &out, double alpha,
                                          int site, int mu) {
+  if constexpr (std::is_same<Store, StoreF32SU3>::value) {
+    ape_site_mixed_su3(g, in, out, alpha, site, mu);
+    return;
+  }
   using M = typename Store::template M<CT>;
   int x[4];
   site_coords(g, site, x);
