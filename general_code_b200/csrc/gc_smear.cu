@@ -282,6 +282,25 @@ template <class Store, class CT>
 __device__ __forceinline__ void hyp_l1_site(const Geom &g, const Fields4 &U,
                                             const HypL1 &out, double alpha3,
                                             int site, int f) {
+  if constexpr (std::is_same<Store, StoreF32SU3>::value) {
+    // the mixed form's staples of stored (SU(3)) links, in two rows as in
+    // ape_site_mixed_su3
+    int x[4];
+    site_coords(g, site, x);
+    const size_t V = g.V;
+    const int mu = kL1Mu[f], eta = kL1Eta[f];
+    SU3<float> S = scale(StoreF32SU3::load<float>(U.f[mu], V, site), float(1 - alpha3));
+    const Nbr n = neighbours(g, site, x, mu, eta);
+    const float c = float(alpha3 / 2);
+    SU3<float> a = mul01(load_rows01(U.f[eta], V, site),
+                         StoreF32SU3::load<float>(U.f[mu], V, n.pnu));
+    add_staple01(S, mul_ad01(a, StoreF32SU3::load<float>(U.f[eta], V, n.pmu)), c);
+    a = mul_da01(StoreF32SU3::load<float>(U.f[eta], V, n.mnu),
+                 StoreF32SU3::load<float>(U.f[mu], V, n.mnu));
+    add_staple01(S, mul01(a, StoreF32SU3::load<float>(U.f[eta], V, n.mnu_pmu)), c);
+    proj_store<StoreF32SU3Full, float>(out.f[f], V, site, S);
+    return;
+  }
   using M = typename Store::template M<CT>;
   int x[4];
   site_coords(g, site, x);
