@@ -282,7 +282,9 @@ int build_schedule(gc_batch *b) {
           a.out.f[d] = alt[i].f[d];
         a.alpha = j.desc.ape_alpha;
         a.block_start = blocks;
-        blocks += 3 * ((j.g.V + kBlock - 1) / kBlock);
+        // (one thread per site and link for SU(3), per site for SU(2): see
+        // ape_items in gc_smear.cu)
+        blocks += (nc == 2 ? 1 : 3) * ((j.g.V + kBlock - 1) / kBlock);
         t.push_back(a);
         for (int d = 0; d < 3; d++)
           std::swap(cur[i].f[d], alt[i].f[d]);
