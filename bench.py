@@ -90,20 +90,28 @@ def link_bytes(nc, form):
     return 32 if form == "fp64" else 16
 
 
-def algorithmic(wl, form):
-    """Algorithmic bytes and FP flops per site for each kernel family."""
+def algorithmic(wl, form, w_method="exact"):
+    """Algorithmic bytes and FP flops per site for each kernel family. W's
+    flops are those of the method that ran: the exact product (two products
+    and a dot per (x, nu, R, T)) or the temporal-gauge form (per site: the
+    gauge lines of two cuts, the six transformed links, per (nu, R) one
+    product per cut for the space lines, per (nu, R, T) one dot)."""
     nc = wl["nc"]
     b = link_bytes(nc, form)
     mm = 198 if nc == 3 else 28          # one matrix product
+    dot = 36 if nc == 3 else 8           # Re Tr(A B^dag)
     proj = 3000 if nc == 3 else 11       # one projection
     nr = wl["r"][1] - wl["r"][0] + 1
     nt = wl["t"][1] - wl["t"][0] + 1
+    if w_method == "gauge":
+        w_flops = 2 * mm + 3 * 2 * 2 * mm + 3 * (2 * wl["r"][1] * mm + nr * nt * dot)
+    else:
+        w_flops = 3 * nr * nt * (2 * mm + dot)
     return {
         "ape": {"bytes": 6 * b, "flops": 3 * (8 * mm + proj)},
         "hyp": {"bytes": 5 * b, "flops": 96 * mm + 16 * proj},
-        # the fused W kernel needs the 4 link fields once (space and time
-        # lines stay on chip); two products + a dot per (x, nu, R, T)
-        "wilson": {"bytes": 4 * b, "flops": 3 * nr * nt * (2 * mm + (36 if nc == 3 else 8))},
+        # W needs the 4 link fields once (the lines stay on chip)
+        "wilson": {"bytes": 4 * b, "flops": w_flops, "method": w_method},
     }
 
 
@@ -831,12 +839,13 @@ class Runner:
         w_pipe = e2e_pipelined(steps, rec_pipe)
         self.barrier()
         assert np.array_equal(w, w_pipe), "device and pipelined end-to-end runs disagree"
+        w_method = work.wilson_method_used()  # (after the timed runs: it synchronises)
         pristine.close()
         work.close()
         work2.close()
         from general_code_b200 import launches_per_job
         per_job = launches_per_job(nc, wl["ape"])
-        return {"w": w,
+        return {"w": w, "w_method": w_method,
                 "total_ms": self.max_over_ranks(sum(r[0] for r in rec)),
                 "total_e2e_ms": self.max_over_ranks(sum(rec_pipe)),
                 "total_serial_ms": self.max_over_ranks(sum(rec_e2e)),
@@ -852,7 +861,7 @@ class Runner:
 def summarize(wl, name, form, r, steps, world, peak, peak_kind, fp_peak, traffic):
     """Throughput, phase times and per-kernel-family rooflines of one form."""
     V = int(np.prod(wl["dims"]))
-    alg = algorithmic(wl, form)
+    alg = algorithmic(wl, form, r["w_method"])
     per_launch = {"hyp": r["hyp_ms"], "ape": r["ape_ms"] / wl["ape"], "wilson": r["w_ms"]}
     totals = {"hyp": r["hyp_ms"], "ape": r["ape_ms"], "wilson": r["w_ms"]}
     pipe = "fp64" if form == "fp64" else "fp32"
@@ -867,6 +876,8 @@ def summarize(wl, name, form, r, steps, world, peak, peak_kind, fp_peak, traffic
                       "traffic_per_launch": (tr["dram_bytes_per_site"] * V if tr else None),
                       "fp_flops_per_launch": alg[k]["flops"] * V, "fp_tflops": tf,
                       "fp_pipe": pipe, "fp_frac": tf / fp_peak[pipe]}
+        if k == "wilson":
+            kernels[k]["method"] = alg[k]["method"]
     dom = max(totals, key=totals.get)
     kd = kernels[dom]
     return {

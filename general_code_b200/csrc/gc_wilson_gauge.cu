@@ -230,6 +230,30 @@ __device__ __forceinline__ double gauge_trace(const SU2<T> &a, const SU2<T> &b, 
   return loop_value<ADJ>(a, b, lane1);
 }
 
+// First spatial site of a column block. When the block's columns tile the x
+// extent, consecutive blocks step along nu (for nu = y, z), so that the
+// blocks running at the same time extend their space lines with the same
+// transformed links (they hit L2 instead of each reading HBM); otherwise the
+// blocks take consecutive runs of sites.
+__device__ __forceinline__ int column_base(const Geom &g, int cb, int cols, int nu) {
+  if (nu == 0 || g.L[0] % cols != 0)
+    return cb * cols;
+  const int nxc = g.L[0] / cols;
+  int xc, y, z;
+  if (nu == 1) {
+    y = cb % g.L[1];
+    const int rest = cb / g.L[1];
+    xc = rest % nxc;
+    z = rest / nxc;
+  } else {
+    z = cb % g.L[2];
+    const int rest = cb / g.L[2];
+    xc = rest % nxc;
+    y = rest / nxc;
+  }
+  return xc * cols + g.L[0] * (y + g.L[1] * z);
+}
+
 // Shared memory of one block: per-thread loop sums red[nt][threads] (FP64),
 // then the space lines of cut A and of cut B, one slot per (t, column unit).
 // KS > 1: a thread owns KS consecutive start slices t0 = KS row + m, m < KS
@@ -265,8 +289,8 @@ __global__ void __launch_bounds__(256)
   const int warp = tid >> 5, lane = tid & 31, nwarps = nthreads >> 5;
   const int u = tid % units;
   const int row = tid / units;
-  const int colblock = blockIdx.x, nu = blockIdx.y;
-  const int s0 = colblock * cols + LANES * u;
+  const int nu = blockIdx.y;
+  const int s0 = column_base(g, blockIdx.x, cols, nu) + LANES * u;
   const bool active = (row < rows) && (s0 < g.Vs);
   const bool lane1 = LANES == 2 && active && (LANES * u + 1 < cols) && (s0 + 1 < g.Vs);
   const int s1 = lane1 ? s0 + 1 : s0;
