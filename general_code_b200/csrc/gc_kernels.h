@@ -150,7 +150,8 @@ int launch_wilson(const Geom &g, const Fields4 &U, int rmin, int rmax,
 // configuration's loops over the whole lattice with T <= Lt/2 when the block
 // shape fits; exact to rounding when the temporal links are unitary.
 // units: column units (threads per time row) per block; 0 = about 128 threads.
-WilsonPlan wilson_gauge_plan(const Geom &g, int nt, int nc, int ct_bytes, int units = 0);
+WilsonPlan wilson_gauge_plan(const Geom &g, int nt, int nc, int ct_bytes, int units = 0,
+                             bool adjoint = false);
 bool wilson_gauge_applies(const Geom &g, int tmax, int nt, int nc, int ct_bytes);
 // Largest unitarity defect max |U U^dag - 1| of a temporal link for which the
 // form is used (FP64: ct_bytes 8; mixed: 4).

@@ -55,6 +55,7 @@
 #include "gc_wcol.cuh"
 
 #include <algorithm>
+#include <type_traits>
 
 namespace gc {
 
@@ -162,8 +163,15 @@ __global__ void __launch_bounds__(128)
 // the end: three independent chains instead of one of 18 dependent FMAs,
 // which the trace loop below (a few warps per scheduler, shared-memory
 // operands) needs to keep the FMA pipe fed.
+// Per-thread sums of the loop values: FP32 for the fundamental loops of the
+// mixed form (a thread adds at most a few loops; every loop value is an FP32
+// dot product), FP64 otherwise; the block and the grid sum them in FP64.
+template <bool ADJ, class CT>
+using GAcc = typename std::conditional<!ADJ && std::is_same<CT, float>::value, float,
+                                       double>::type;
+
 template <bool ADJ, class T>
-__device__ __forceinline__ double gauge_trace(const SU3<T> &a, const SU3<T> &b, bool) {
+__device__ __forceinline__ GAcc<ADJ, T> gauge_trace(const SU3<T> &a, const SU3<T> &b, bool) {
   T re[3], im[3];
 #pragma unroll
   for (int i = 0; i < 3; i++) {
@@ -183,14 +191,15 @@ __device__ __forceinline__ double gauge_trace(const SU3<T> &a, const SU3<T> &b, 
       }
     }
   }
-  const double r = double((re[0] + re[1]) + re[2]);
   if (!ADJ)
-    return r;
+    return (re[0] + re[1]) + re[2];
+  const double r = double((re[0] + re[1]) + re[2]);
   const double m = double((im[0] + im[1]) + im[2]);
   return fma(r, r, fma(m, m, -1.0));
 }
 template <bool ADJ>
-__device__ __forceinline__ double gauge_trace(const SU3<f2> &a, const SU3<f2> &b, bool lane1) {
+__device__ __forceinline__ GAcc<ADJ, float> gauge_trace(const SU3<f2> &a, const SU3<f2> &b,
+                                                        bool lane1) {
   f2 re[3], im[3];
 #pragma unroll
   for (int i = 0; i < 3; i++) {
@@ -212,10 +221,8 @@ __device__ __forceinline__ double gauge_trace(const SU3<f2> &a, const SU3<f2> &b
   }
   const float2 r = make_float2((re[0].v.x + re[1].v.x) + re[2].v.x,
                                (re[0].v.y + re[1].v.y) + re[2].v.y);
-  if (!ADJ) {
-    const double v0 = double(r.x);
-    return lane1 ? v0 + double(r.y) : v0;
-  }
+  if (!ADJ)
+    return lane1 ? r.x + r.y : r.x;
   const float2 m = make_float2((im[0].v.x + im[1].v.x) + im[2].v.x,
                                (im[0].v.y + im[1].v.y) + im[2].v.y);
   const double r0 = double(r.x), i0 = double(m.x);
@@ -226,7 +233,10 @@ __device__ __forceinline__ double gauge_trace(const SU3<f2> &a, const SU3<f2> &b
   return v0 + fma(r1, r1, fma(i1, i1, -1.0));
 }
 template <bool ADJ, class T>
-__device__ __forceinline__ double gauge_trace(const SU2<T> &a, const SU2<T> &b, bool lane1) {
+__device__ __forceinline__ GAcc<ADJ, T> gauge_trace(const SU2<T> &a, const SU2<T> &b,
+                                                    bool lane1) {
+  if (!ADJ)
+    return dot4(a.a0, b.a0, a.a1, b.a1, a.a2, b.a2, a.a3, b.a3);
   return loop_value<ADJ>(a, b, lane1);
 }
 
@@ -254,7 +264,7 @@ __device__ __forceinline__ int column_base(const Geom &g, int cb, int cols, int 
   return xc * cols + g.L[0] * (y + g.L[1] * z);
 }
 
-// Shared memory of one block: per-thread loop sums red[nt][threads] (FP64),
+// Shared memory of one block: per-thread loop sums red[nt][threads] (GAcc),
 // then the space lines of cut A and of cut B, one slot per (t, column unit).
 // KS > 1: a thread owns KS consecutive start slices t0 = KS row + m, m < KS
 // (all of one cut: KS divides the cut slice h), and one shared-memory load of
@@ -281,8 +291,9 @@ __global__ void __launch_bounds__(256)
   const int cs = wilson_col_stride(cols, LANES);
   const int units = cs / LANES;
   const int nslots = Lt * units;
-  double *red = reinterpret_cast<double *>(smem_raw); // [nt][nthreads]
-  unsigned char *sa = reinterpret_cast<unsigned char *>(red + (size_t)nt * nthreads);
+  using Acc = GAcc<ADJ, CT>;
+  Acc *red = reinterpret_cast<Acc *>(smem_raw); // [nt][nthreads]
+  unsigned char *sa = smem_raw + ((sizeof(Acc) * nt * nthreads + 15) & ~(size_t)15);
   unsigned char *sb = sa + (size_t)CS::kBytes * nslots;
 
   const int tid = threadIdx.x;
@@ -333,10 +344,10 @@ __global__ void __launch_bounds__(256)
         a[m] = active ? CS::load(set, nslots, (t0 + m) * units + u) : unit(M());
       int tt = t0 + tmin;
       tt = (tt >= Lt) ? tt - Lt : tt;
-      double acc[KS]; // acc[m]: the sum for T index j - m
+      Acc acc[KS]; // acc[m]: the sum for T index j - m
 #pragma unroll
       for (int m = 0; m < KS; m++)
-        acc[m] = 0.0;
+        acc[m] = Acc(0);
       // One step of the sweep: the loops of all starts that end on top line
       // b (index j), then the completed sum of T index j - KS + 1.
       auto step = [&](int j, const M &b) {
@@ -351,7 +362,7 @@ __global__ void __launch_bounds__(256)
 #pragma unroll
         for (int m = KS - 1; m > 0; m--)
           acc[m] = acc[m - 1];
-        acc[0] = 0.0;
+        acc[0] = Acc(0);
       };
       // two top lines in flight (b0, b1 alternate): the next line's load is
       // issued before the current line's traces (a slot past the last step
@@ -384,9 +395,9 @@ __global__ void __launch_bounds__(256)
         tt = (tt >= Lt) ? tt - Lt : tt;
 #pragma unroll 1
         for (int T = 0; T < nt; T++) {
-          const double v =
-              active ? gauge_trace<ADJ>(a, CS::load(set, nslots, tt * units + u), lane1) : 0.0;
-          double *r = red + (size_t)T * nthreads + tid;
+          const Acc v =
+              active ? gauge_trace<ADJ>(a, CS::load(set, nslots, tt * units + u), lane1) : Acc(0);
+          Acc *r = red + (size_t)T * nthreads + tid;
           *r = (k == 0) ? v : *r + v;
           tt = (tt + 1 == Lt) ? 0 : tt + 1;
         }
@@ -400,7 +411,7 @@ __global__ void __launch_bounds__(256)
       for (int T = warp; T < nt; T += nwarps) {
         double v = 0.0;
         for (int i = lane; i < nthreads; i += 32)
-          v += red[(size_t)T * nthreads + i];
+          v += double(red[(size_t)T * nthreads + i]);
         v = warp_sum(v);
         if (lane == 0)
           part[(R - rmin) * nt + T] = v;
@@ -447,7 +458,8 @@ int largest_divisor_upto_g(int n, int cap) {
 // Block shape: every start slice of a column has a thread (rows = Lt up to
 // 64; beyond, the largest divisor of Lt up to 64 with Lt/rows slices each),
 // and about 128 threads per block.
-WilsonPlan wilson_gauge_plan(const Geom &g, int nt, int nc, int ct_bytes, int units_req) {
+WilsonPlan wilson_gauge_plan(const Geom &g, int nt, int nc, int ct_bytes, int units_req,
+                             bool adjoint) {
   WilsonPlan p{};
   const int Lt = g.L[3];
   const int ncomp = (nc == 3) ? 18 : 4;
@@ -469,7 +481,9 @@ WilsonPlan wilson_gauge_plan(const Geom &g, int nt, int nc, int ct_bytes, int un
   p.blocks = ((g.Vs + p.cols_per_block - 1) / p.cols_per_block) * 3;
   const size_t sets = 2 * (size_t)ncomp * Lt * wilson_col_stride(p.cols_per_block, lanes) *
                       ct_bytes;
-  p.smem = (size_t)nt * p.threads * sizeof(double) + sets;
+  // (the per-thread sums: GAcc, FP32 for the mixed form's fundamental loops)
+  const size_t acc = (!adjoint && ct_bytes == 4) ? 4 : 8;
+  p.smem = ((size_t)nt * p.threads * acc + 15) / 16 * 16 + sets;
   p.fits = p.threads <= 256 && p.smem <= 200 * 1024;
   return p;
 }
@@ -477,7 +491,7 @@ WilsonPlan wilson_gauge_plan(const Geom &g, int nt, int nc, int ct_bytes, int un
 bool wilson_gauge_applies(const Geom &g, int tmax, int nt, int nc, int ct_bytes) {
   if (tmax > g.L[3] / 2 || g.L[3] < 2)
     return false;
-  return wilson_gauge_plan(g, nt, nc, ct_bytes).fits;
+  return wilson_gauge_plan(g, nt, nc, ct_bytes, 0, true).fits;
 }
 
 double wilson_gauge_tolerance(int ct_bytes) { return ct_bytes == 8 ? 1e-14 : 1e-6; }
@@ -510,7 +524,7 @@ int launch_wilson_gauge_kernel(const Geom &g, const Fields4 &UA, const Fields4 &
   const int nr = rmax - rmin + 1, nt = tmax - tmin + 1;
   if (tmax > g.L[3] / 2)
     return plan_error("wilson_gauge_kernel: time_max above Lt/2");
-  const WilsonPlan p = wilson_gauge_plan(g, nt, Store::NC, (int)sizeof(CT), units);
+  const WilsonPlan p = wilson_gauge_plan(g, nt, Store::NC, (int)sizeof(CT), units, adjoint);
   cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
   cudaStreamIsCapturing(s, &cap);
   const bool capturing = cap != cudaStreamCaptureStatusNone;
@@ -587,7 +601,8 @@ template <class Store, class CT>
 int time_wilson_gauge(const Geom &g, const Fields4 &UA, const Fields4 &UB, int rmin, int rmax,
                       int tmin, int tmax, int units, double *partials, cudaStream_t s,
                       float *ms) {
-  const WilsonPlan p = wilson_gauge_plan(g, tmax - tmin + 1, Store::NC, (int)sizeof(CT), units);
+  const WilsonPlan p =
+      wilson_gauge_plan(g, tmax - tmin + 1, Store::NC, (int)sizeof(CT), units, false);
   if (!p.fits)
     return GC_ERR_ARG;
   int blocks = 0;
