@@ -844,7 +844,7 @@ class Runner:
         work.close()
         work2.close()
         from general_code_b200 import launches_per_job
-        per_job = launches_per_job(nc, wl["ape"])
+        per_job = launches_per_job(nc, wl["ape"], w_method=w_method or "exact")
         return {"w": w, "w_method": w_method,
                 "total_ms": self.max_over_ranks(sum(r[0] for r in rec)),
                 "total_e2e_ms": self.max_over_ranks(sum(rec_pipe)),

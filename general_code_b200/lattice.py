@@ -58,17 +58,19 @@ def generate_config(dims: Sequence[int], nc: int, eps: float, seed: int,
 
 
 # Kernels one call launches: gc_hyp per step, gc_ape per step, and
-# gc_wilson_onaxis (the W kernel and its fixed-order reduction) for the
-# ranges the benchmark uses.
+# gc_wilson_onaxis for the ranges the benchmark uses: the exact W kernel and
+# its fixed-order reduction, or, where the temporal-gauge form applies, the
+# gauge lines, the transformed links, both gated W kernels and the reduction.
 HYP_LAUNCHES_PER_STEP = 3
 APE_LAUNCHES_PER_STEP = 1
-WILSON_LAUNCHES = 2
+WILSON_LAUNCHES = {"exact": 2, "gauge": 5}
 
 
-def launches_per_job(nc: int, ape_steps: int, hyp_steps: int = 1) -> int:
+def launches_per_job(nc: int, ape_steps: int, hyp_steps: int = 1,
+                     w_method: str = "gauge") -> int:
     """Our kernel launches in one smear-and-measure job (HYP, APE, W)."""
     return (hyp_steps * HYP_LAUNCHES_PER_STEP + ape_steps * APE_LAUNCHES_PER_STEP
-            + WILSON_LAUNCHES)
+            + WILSON_LAUNCHES[w_method])
 
 
 def fma_peak(precision: str = "mixed") -> float:
