@@ -81,7 +81,7 @@ SU2<double> haar_su2(NormalStream &ns) {
   double a[4];
   for (int k = 0; k < 4; k++)
     a[k] = ns.next();
-  return proj(SU2<double>{a[0], a[1], a[2], a[3]});
+  return proj_div(SU2<double>{a[0], a[1], a[2], a[3]});
 }
 
 void store_link(double *out, long long l, const SU3<double> &U) {
@@ -175,10 +175,10 @@ int generate_host(const int dims[4], int nc, double eps, unsigned seed,
       double n = std::sqrt(a1 * a1 + a2 * a2 + a3 * a3);
       double th = eps * n;
       double sn = (n > 0) ? std::sin(th) / n : 0.0;
-      SU2<double> U = proj(SU2<double>{std::cos(th), sn * a1, sn * a2, sn * a3});
+      SU2<double> U = proj_div(SU2<double>{std::cos(th), sn * a1, sn * a2, sn * a3});
       if (gauge) {
         const int site = (int)(l >> 2), mu = (int)(l & 3);
-        U = proj(mul_ad(mul(g[site], U), g[neighbour(dims, site, mu)]));
+        U = proj_div(mul_ad(mul(g[site], U), g[neighbour(dims, site, mu)]));
       }
       store_link(out, l, U);
     });

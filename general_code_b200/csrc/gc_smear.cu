@@ -85,6 +85,15 @@ __device__ __forceinline__ void proj_store(void *out, size_t V, int site,
     }
     const MF f = ns_until(a, 2e-5f, 5, &n);
     Store::template store<double>(out, V, site, ns_step(convert(f, (MD *)nullptr)));
+  } else if constexpr (Store::NC == 2 && Store::kBytes == 16) {
+    // FP32-stored SU(2): a / |a| with |a|^2 and 1/|a| in FP64 (one
+    // reciprocal square root instead of a square root and four divisions),
+    // each element rounded to FP32 on its own. (1/|a| in FP32 scales all four
+    // elements by the same rounding error; over R + T links of a loop that
+    // grew W's error against FP64 from 3e-9 to 2e-7 at SU(2) 48^4.)
+    const SU2<double> a = convert(S, (SU2<double> *)nullptr);
+    const double r = rsqrt(dot4(a.a0, a.a0, a.a1, a.a1, a.a2, a.a2, a.a3, a.a3));
+    Store::template store<double>(out, V, site, SU2<double>{a.a0 * r, a.a1 * r, a.a2 * r, a.a3 * r});
   } else {
     MD d = convert(S, (MD *)nullptr);
     Store::template store<double>(out, V, site, proj(d, ProjTol<Store>::value));
@@ -424,11 +433,19 @@ __device__ __forceinline__ void ape_site_su2(const Geom &g, const Fields4 &in,
 // SU(3), one thread for all three for SU(2).
 template <class Store> constexpr int ape_items() { return Store::NC == 2 ? 1 : 3; }
 
+// Resident blocks of 128 threads per SM that an APE kernel is compiled for:
+// 6 (80 registers) for the FP32 SU(2) site kernel, whose time is the links'
+// load latency (measured at 48^4: 0.163 ms per step against 0.174 ms at 4
+// blocks and 0.166 ms at 8, where it spills); 4 otherwise.
+template <class Store, class CT> constexpr int ape_min_blocks() {
+  return (Store::NC == 2 && sizeof(CT) == 4) ? 6 : 4;
+}
+
 // ---------------------------------------------------------- single lattice
 // The field / direction index varies fastest over blocks, so all fields of
 // a block of sites are computed back to back while their inputs are in L2.
 template <class Store, class CT>
-__global__ void __launch_bounds__(128, 4)
+__global__ void __launch_bounds__(128, ape_min_blocks<Store, CT>())
     ape_kernel(Geom g, const __grid_constant__ Fields4 in,
                const __grid_constant__ Fields4 out, double alpha) {
   if constexpr (Store::NC == 2) {
@@ -494,7 +511,7 @@ __device__ __forceinline__ int hyp_start2(const HypJob &j) { return j.start2; }
 __device__ __forceinline__ int hyp_start3(const HypJob &j) { return j.start3; }
 
 template <class Store, class CT>
-__global__ void __launch_bounds__(128, 4)
+__global__ void __launch_bounds__(128, ape_min_blocks<Store, CT>())
     ape_batch_kernel(const ApeJob *__restrict__ jobs, int njobs) {
   const int j = find_job<ApeJob, ape_start>(jobs, njobs, blockIdx.x);
   const ApeJob &jb = jobs[j];
