@@ -434,11 +434,12 @@ __device__ __forceinline__ void ape_site_su2(const Geom &g, const Fields4 &in,
 template <class Store> constexpr int ape_items() { return Store::NC == 2 ? 1 : 3; }
 
 // Resident blocks of 128 threads per SM that an APE kernel is compiled for:
-// 6 (80 registers) for the FP32 SU(2) site kernel, whose time is the links'
-// load latency (measured at 48^4: 0.163 ms per step against 0.174 ms at 4
-// blocks and 0.166 ms at 8, where it spills); 4 otherwise.
+// 6 (80 registers) in FP32, 4 in FP64. The FP32 kernels wait on the links'
+// loads at 4 blocks: SU(2) site kernel at 48^4 0.174 -> 0.163 ms per step
+// (0.166 at 8 blocks, where it spills), SU(3) at 32^4 0.248 -> 0.238 ms
+// (0.244 at 5 blocks). The FP64 kernels need their 128 registers.
 template <class Store, class CT> constexpr int ape_min_blocks() {
-  return (Store::NC == 2 && sizeof(CT) == 4) ? 6 : 4;
+  return sizeof(CT) == 4 ? 6 : 4;
 }
 
 // ---------------------------------------------------------- single lattice
