@@ -32,6 +32,9 @@ GC_LAYOUT_ROWMAJOR = 0
 GC_WILSON_AUTO = 0
 GC_WILSON_EXACT = 1
 GC_WILSON_GAUGE = 2
+GC_HYP_AUTO = 0
+GC_HYP_LEVELS = 1
+GC_HYP_SLICES = 2
 GC_LAYOUT_EIGEN_COLMAJOR = 1
 
 ERROR_NAMES = {
@@ -65,6 +68,7 @@ SIGNATURES = {
     "gc_wilson_onaxis": (_c_int, [_p, _c_int, _c_int, _c_int, _c_int, _pdbl]),
     "gc_wilson_adjoint_onaxis": (_c_int, [_p, _c_int, _c_int, _c_int, _c_int, _pdbl]),
     "gc_set_wilson_method": (_c_int, [_p, _c_int]),
+    "gc_set_hyp_method": (_c_int, [_p, _c_int]),
     "gc_wilson_method_used": (_c_int, [_p, _pint]),
     "gc_plaquette": (_c_int, [_p, _pdbl]),
     "gc_plaquette_space": (_c_int, [_p, _pdbl]),

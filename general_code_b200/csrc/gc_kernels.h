@@ -40,6 +40,12 @@ template <class Store, class CT>
 int launch_hyp(const Geom &g, const Fields4 &U, const HypL1 &l1,
                const HypL2 &l2, void *out_t, double a1, double a2, double a3,
                cudaStream_t s);
+// HYP as a pipeline over time slices (Lt >= 3): Lt + 3 launches, the
+// decorated links in rings of 3 slices inside l1/l2's fields; the same links
+// as launch_hyp bit for bit.
+template <class Store, class CT>
+int launch_hyp_slices(const Geom &g, const Fields4 &U, const HypL1 &l1, const HypL2 &l2,
+                      void *out_t, double a1, double a2, double a3, cudaStream_t s);
 
 struct HypJob {
   Geom g;

@@ -23,17 +23,26 @@ namespace {
 // S += ((c * (Fnu(x) Fmu(x+nu))) Fnu(x+mu)^dag)                  upper staple
 //    + ((c * (Fnu(x-nu)^dag Fmu(x-nu))) Fnu(x-nu+mu))             lower staple
 // exactly in the operation order of smearing.h:134-149 / :305-318 / :343-356.
+// The storage indices of Fnu's and Fmu's links are given separately (they
+// differ when the two fields are kept in different slice rings).
+template <class Store, class CT, class M>
+__device__ __forceinline__ void add_staples2(M &S, const void *fmu, const void *fnu, size_t V,
+                                             int nu_x, int mu_pnu, int nu_pmu, int nu_mnu,
+                                             int mu_mnu, int nu_mnu_pmu, CT c) {
+  M a = mul(Store::template load<CT>(fnu, V, nu_x),
+            Store::template load<CT>(fmu, V, mu_pnu));
+  S = add(S, mul_ad(scale(a, c), Store::template load<CT>(fnu, V, nu_pmu)));
+  M b = mul_da(Store::template load<CT>(fnu, V, nu_mnu),
+               Store::template load<CT>(fmu, V, mu_mnu));
+  S = add(S, mul(scale(b, c), Store::template load<CT>(fnu, V, nu_mnu_pmu)));
+}
+
 template <class Store, class CT, class M>
 __device__ __forceinline__ void add_staples(M &S, const void *fmu,
                                             const void *fnu, size_t V, int x,
                                             int x_pnu, int x_pmu, int x_mnu,
                                             int x_mnu_pmu, CT c) {
-  M a = mul(Store::template load<CT>(fnu, V, x),
-            Store::template load<CT>(fmu, V, x_pnu));
-  S = add(S, mul_ad(scale(a, c), Store::template load<CT>(fnu, V, x_pmu)));
-  M b = mul_da(Store::template load<CT>(fnu, V, x_mnu),
-               Store::template load<CT>(fmu, V, x_mnu));
-  S = add(S, mul(scale(b, c), Store::template load<CT>(fnu, V, x_mnu_pmu)));
+  add_staples2<Store, CT>(S, fmu, fnu, V, x, x_pnu, x_pmu, x_mnu, x_mnu, x_mnu_pmu, c);
 }
 
 // Projection tolerance of the FP64 iteration: an update below it ends the
@@ -287,10 +296,24 @@ __device__ __forceinline__ void ape_site(const Geom &g, const Fields4 &in,
 __constant__ int kL1Mu[9] = {0, 0, 1, 1, 2, 2, 3, 3, 3};
 __constant__ int kL1Eta[9] = {2, 1, 2, 0, 1, 0, 0, 1, 2};
 
+// Where a site's decorated links are kept. The whole-lattice kernels keep a
+// field per decoration over all V sites (index = site, plane stride V); the
+// slice pipeline keeps them in rings of slices (plane stride VR = 3 Vs):
+// index = site + o0 for the site's own slice and site' + o1 for a site' on the
+// slice above, in the fields that the next level reads on two slices (level-1
+// spatial, level-2 spatial: three ring slots), and site + q0 in the fields
+// read on one slice (level-1 and level-2 temporal: two ring slots).
+struct DecAddr {
+  size_t VR;
+  int o0, o1, q0;
+};
+__device__ __forceinline__ DecAddr whole_lattice(const Geom &g) { return {(size_t)g.V, 0, 0, 0}; }
+
 template <class Store, class CT>
 __device__ __forceinline__ void hyp_l1_site(const Geom &g, const Fields4 &U,
                                             const HypL1 &out, double alpha3,
-                                            int site, int f) {
+                                            int site, int f, const DecAddr &d) {
+  const int oi = site + (f < 6 ? d.o0 : d.q0); // storage index of the result
   if constexpr (std::is_same<Store, StoreF32SU3>::value) {
     // the mixed form's staples of stored (SU(3)) links, in two rows as in
     // ape_site_mixed_su3
@@ -307,7 +330,7 @@ __device__ __forceinline__ void hyp_l1_site(const Geom &g, const Fields4 &U,
     a = mul_da01(StoreF32SU3::load<float>(U.f[eta], V, n.mnu),
                  StoreF32SU3::load<float>(U.f[mu], V, n.mnu));
     add_staple01(S, mul01(a, StoreF32SU3::load<float>(U.f[eta], V, n.mnu_pmu)), c);
-    proj_store<StoreF32SU3Full, float>(out.f[f], V, site, S);
+    proj_store<StoreF32SU3Full, float>(out.f[f], d.VR, oi, S);
     return;
   }
   using M = typename Store::template M<CT>;
@@ -319,7 +342,7 @@ __device__ __forceinline__ void hyp_l1_site(const Geom &g, const Fields4 &U,
   Nbr n = neighbours(g, site, x, mu, eta);
   add_staples<Store, CT>(S, U.f[mu], U.f[eta], V, site, n.pnu, n.pmu, n.mnu,
                          n.mnu_pmu, CT(alpha3 / 2));
-  proj_store<typename InterStore<Store>::type, CT>(out.f[f], V, site, S);
+  proj_store<typename InterStore<Store>::type, CT>(out.f[f], d.VR, oi, S);
 }
 
 // Level-1 field holding Vbar_{mu; nu, t} for spatial mu != nu.
@@ -332,11 +355,16 @@ __device__ __forceinline__ int l1_temporal(int a, int b) { return 6 + (3 - a - b
 // Level-2 decorated links. Field index f:
 //   0..2 : Vtilde_{t;nu}, nu = f       (smearing.h:433-450)
 //   3..5 : Vtilde_{nu;t}, nu = f - 3   (smearing.h:455-466)
+// Vtilde_{t;nu} reads level-1 temporal links on the site's slice and level-1
+// spatial links on it and on the slice above; Vtilde_{nu;t} reads level-1
+// spatial links of the site's slice only.
 template <class Store, class CT>
 __device__ __forceinline__ void hyp_l2_site(const Geom &g, const Fields4 &U,
                                             const HypL1 &l1, const HypL2 &out,
-                                            double alpha2, int site, int f) {
+                                            double alpha2, int site, int f,
+                                            const DecAddr &d) {
   using M = typename Store::template M<CT>;
+  using I = typename InterStore<Store>::type;
   int x[4];
   site_coords(g, site, x);
   const size_t V = g.V;
@@ -345,6 +373,10 @@ __device__ __forceinline__ void hyp_l2_site(const Geom &g, const Fields4 &U,
   const int mu = temporal ? 3 : nu;
   M S = scale(Store::template load<CT>(U.f[mu], V, site), CT(1 - alpha2));
   const CT c = CT(alpha2 / 4);
+  // offsets of the level-1 fields' links: Fmu's on this slice, Fnu's on this
+  // slice and (x + mu, x - nu + mu) on the slice above when mu = t
+  const int om = temporal ? d.q0 : d.o0;
+  const int on1 = temporal ? d.o1 : d.o0;
 #pragma unroll 1
   for (int rho = 0; rho < 3; rho++) {
     if (rho == nu)
@@ -353,17 +385,19 @@ __device__ __forceinline__ void hyp_l2_site(const Geom &g, const Fields4 &U,
                                : l1.f[l1_spatial(nu, rho)];
     const void *fnu = l1.f[l1_spatial(rho, nu)];
     Nbr n = neighbours(g, site, x, mu, rho);
-    add_staples<typename InterStore<Store>::type, CT>(S, fmu, fnu, V, site, n.pnu, n.pmu,
-                                                      n.mnu, n.mnu_pmu, c);
+    add_staples2<I, CT>(S, fmu, fnu, d.VR, site + d.o0, n.pnu + om, n.pmu + on1,
+                        n.mnu + d.o0, n.mnu + om, n.mnu_pmu + on1, c);
   }
-  proj_store<typename InterStore<Store>::type, CT>(out.f[f], V, site, S);
+  proj_store<I, CT>(out.f[f], d.VR, site + (temporal ? d.q0 : d.o0), S);
 }
 
-// Level 3: the new temporal link (smearing.h:484-503).
+// Level 3: the new temporal link (smearing.h:484-503). Reads the level-2
+// temporal links on the site's slice and the level-2 spatial links on it and
+// on the slice above.
 template <class Store, class CT>
 __device__ __forceinline__ void hyp_l3_site(const Geom &g, const void *Ut,
                                             const HypL2 &l2, void *out_t,
-                                            double alpha1, int site) {
+                                            double alpha1, int site, const DecAddr &d) {
   using M = typename Store::template M<CT>;
   int x[4];
   site_coords(g, site, x);
@@ -373,8 +407,9 @@ __device__ __forceinline__ void hyp_l3_site(const Geom &g, const void *Ut,
 #pragma unroll 1
   for (int nu = 0; nu < 3; nu++) {
     Nbr n = neighbours(g, site, x, 3, nu);
-    add_staples<typename InterStore<Store>::type, CT>(S, l2.f[nu], l2.f[3 + nu], V, site,
-                                                      n.pnu, n.pmu, n.mnu, n.mnu_pmu, c);
+    add_staples2<typename InterStore<Store>::type, CT>(
+        S, l2.f[nu], l2.f[3 + nu], d.VR, site + d.o0, n.pnu + d.q0, n.pmu + d.o1,
+        n.mnu + d.o0, n.mnu + d.q0, n.mnu_pmu + d.o1, c);
   }
   proj_store<Store, CT>(out_t, V, site, S);
 }
@@ -468,7 +503,7 @@ __global__ void __launch_bounds__(128, 4)
   const int f = blockIdx.x % 9;
   const int site = (blockIdx.x / 9) * blockDim.x + threadIdx.x;
   if (site < g.V)
-    hyp_l1_site<Store, CT>(g, U, out, alpha3, site, f);
+    hyp_l1_site<Store, CT>(g, U, out, alpha3, site, f, whole_lattice(g));
 }
 
 template <class Store, class CT>
@@ -479,7 +514,7 @@ __global__ void __launch_bounds__(128, 4)
   const int f = blockIdx.x % 6;
   const int site = (blockIdx.x / 6) * blockDim.x + threadIdx.x;
   if (site < g.V)
-    hyp_l2_site<Store, CT>(g, U, l1, out, alpha2, site, f);
+    hyp_l2_site<Store, CT>(g, U, l1, out, alpha2, site, f, whole_lattice(g));
 }
 
 template <class Store, class CT>
@@ -488,7 +523,61 @@ __global__ void __launch_bounds__(128)
                       void *out_t, double alpha1) {
   const int site = blockIdx.x * blockDim.x + threadIdx.x;
   if (site < g.V)
-    hyp_l3_site<Store, CT>(g, Ut, l2, out_t, alpha1, site);
+    hyp_l3_site<Store, CT>(g, Ut, l2, out_t, alpha1, site, whole_lattice(g));
+}
+
+// ------------------------------------------------------ HYP slice pipeline
+// HYP as a pipeline over time slices, with the decorated links in rings of
+// slices instead of whole-lattice fields, so that they stay in L2 between the
+// level that writes them and the levels that read them. What a slice needs
+// lies on it and on the slice above: level 3 of slice k reads level-2
+// temporal links of k and level-2 spatial links of k and k + 1; level-2
+// temporal of k reads level-1 temporal of k and level-1 spatial of k, k + 1;
+// level-2 spatial and level-1 spatial read their own slice; level 1 reads
+// the links of its slice and the one above. Launch m computes
+//   part 0: level-1 spatial of slice m       part 1: level-1 temporal of m-1
+//   part 2: level-2 spatial of slice m - 1   part 3: level-2 temporal of m-2
+//   part 4: level 3 of slice m - 3
+// for m = 0 .. Lt + 2, each part whose slice is in range. Slices are counted
+// without wrapping: slice Lt is slice 0 computed again, for level 3 of slice
+// Lt - 1. A spatial level's ring slot is j mod 3 and a temporal level's
+// j mod 2: a slot is rewritten three (two) launches after it was written,
+// after its last reader, and no part reads what another part of the same
+// launch writes. Each site is computed by the same site functions as in the
+// level kernels, so the links are the same bit for bit.
+struct HypStage {
+  int start[6]; // first block of part p (start[5] = blocks of the launch)
+  int slice[5]; // slice of part p (unwrapped, 0 .. Lt), -1 if absent
+};
+
+template <class Store, class CT>
+__global__ void __launch_bounds__(128, 4)
+    hyp_slices_kernel(Geom g, const __grid_constant__ Fields4 U,
+                      const __grid_constant__ HypL1 l1, const __grid_constant__ HypL2 l2,
+                      void *out_t, double a1, double a2, double a3,
+                      const __grid_constant__ HypStage st) {
+  const int b = blockIdx.x;
+  const int p = b < st.start[1] ? 0 : b < st.start[2] ? 1 : b < st.start[3] ? 2
+              : b < st.start[4] ? 3 : 4;
+  const int nf = p == 0 ? 6 : p == 4 ? 1 : 3;
+  const int local = b - st.start[p];
+  const int fl = local % nf;
+  const int s = (local / nf) * blockDim.x + threadIdx.x;
+  if (s >= g.Vs)
+    return;
+  const int Lt = g.L[3], Vs = g.Vs;
+  const int j = st.slice[p];
+  const int t = j == Lt ? 0 : j;
+  const int t1 = t + 1 == Lt ? 0 : t + 1;
+  const int site = s + t * Vs;
+  const DecAddr d{3 * (size_t)Vs, (j % 3 - t) * Vs, ((j + 1) % 3 - t1) * Vs, (j % 2 - t) * Vs};
+  switch (p) {
+  case 0: hyp_l1_site<Store, CT>(g, U, l1, a3, site, fl, d); break;
+  case 1: hyp_l1_site<Store, CT>(g, U, l1, a3, site, 6 + fl, d); break;
+  case 2: hyp_l2_site<Store, CT>(g, U, l1, l2, a2, site, 3 + fl, d); break;
+  case 3: hyp_l2_site<Store, CT>(g, U, l1, l2, a2, site, fl, d); break;
+  default: hyp_l3_site<Store, CT>(g, U.f[3], l2, out_t, a1, site, d); break;
+  }
 }
 
 // ---------------------------------------------------------- many lattices
@@ -537,7 +626,7 @@ __global__ void __launch_bounds__(128, 4)
   const int local = blockIdx.x - jb.start1;
   const int site = (local / 9) * blockDim.x + threadIdx.x;
   if (site < jb.g.V)
-    hyp_l1_site<Store, CT>(jb.g, jb.U, jb.l1, jb.a3, site, local % 9);
+    hyp_l1_site<Store, CT>(jb.g, jb.U, jb.l1, jb.a3, site, local % 9, whole_lattice(jb.g));
 }
 
 template <class Store, class CT>
@@ -548,7 +637,8 @@ __global__ void __launch_bounds__(128, 4)
   const int local = blockIdx.x - jb.start2;
   const int site = (local / 6) * blockDim.x + threadIdx.x;
   if (site < jb.g.V)
-    hyp_l2_site<Store, CT>(jb.g, jb.U, jb.l1, jb.l2, jb.a2, site, local % 6);
+    hyp_l2_site<Store, CT>(jb.g, jb.U, jb.l1, jb.l2, jb.a2, site, local % 6,
+                           whole_lattice(jb.g));
 }
 
 template <class Store, class CT>
@@ -558,7 +648,7 @@ __global__ void __launch_bounds__(128)
   const HypJob &jb = jobs[j];
   const int site = (blockIdx.x - jb.start3) * blockDim.x + threadIdx.x;
   if (site < jb.g.V)
-    hyp_l3_site<Store, CT>(jb.g, jb.U.f[3], jb.l2, jb.out_t, jb.a1, site);
+    hyp_l3_site<Store, CT>(jb.g, jb.U.f[3], jb.l2, jb.out_t, jb.a1, site, whole_lattice(jb.g));
 }
 
 // Two-dimensional APE step of two single-direction fields, links along axes
@@ -627,6 +717,38 @@ int launch_hyp(const Geom &g, const Fields4 &U, const HypL1 &l1,
   return launch_check("hyp_level3_kernel");
 }
 
+// Lattices with Lt >= 3 (the rings' 3 Vs sites per field fit in the
+// whole-lattice fields' V).
+template <class Store, class CT>
+int launch_hyp_slices(const Geom &g, const Fields4 &U, const HypL1 &l1, const HypL2 &l2,
+                      void *out_t, double a1, double a2, double a3, cudaStream_t s) {
+  const int Lt = g.L[3];
+  if (Lt < 3)
+    return plan_error("hyp_slices_kernel: needs Lt >= 3");
+  const int nbs = (g.Vs + kSmearBlock - 1) / kSmearBlock;
+  static constexpr int kFields[5] = {6, 3, 3, 3, 1};
+  for (int m = 0; m <= Lt + 2; m++) {
+    HypStage st;
+    const int slice[5] = {m <= Lt ? m : -1, m >= 1 && m <= Lt ? m - 1 : -1,
+                          m >= 1 && m <= Lt + 1 ? m - 1 : -1,
+                          m >= 2 && m <= Lt + 1 ? m - 2 : -1, m >= 3 ? m - 3 : -1};
+    int blocks = 0;
+    for (int p = 0; p < 5; p++) {
+      st.start[p] = blocks;
+      st.slice[p] = slice[p];
+      if (slice[p] >= 0)
+        blocks += kFields[p] * nbs;
+    }
+    st.start[5] = blocks;
+    hyp_slices_kernel<Store, CT><<<blocks, kSmearBlock, 0, s>>>(g, U, l1, l2, out_t, a1, a2,
+                                                                 a3, st);
+    const int rc = launch_check("hyp_slices_kernel");
+    if (rc)
+      return rc;
+  }
+  return GC_OK;
+}
+
 template <class Store, class CT>
 int launch_ape_batch(const ApeJob *jobs, int njobs, int blocks, cudaStream_t s) {
   if (njobs <= 0 || blocks <= 0)
@@ -671,6 +793,10 @@ int launch_ape_plane(const Geom &g, const void *f1, const void *f2, void *o1, vo
   template int launch_hyp<STORE, CT>(const Geom &, const Fields4 &,           \
                                      const HypL1 &, const HypL2 &, void *,    \
                                      double, double, double, cudaStream_t);   \
+  template int launch_hyp_slices<STORE, CT>(const Geom &, const Fields4 &,    \
+                                            const HypL1 &, const HypL2 &,      \
+                                            void *, double, double, double,    \
+                                            cudaStream_t);                     \
   template int launch_ape_batch<STORE, CT>(const ApeJob *, int, int,          \
                                            cudaStream_t);                     \
   template int launch_hyp_batch<STORE, CT>(const HypJob *, int, const int *,  \

@@ -221,6 +221,15 @@ class Lattice:
         self._check(lib().gc_hyp(self._h, float(alpha1), float(alpha2), float(alpha3),
                                  int(steps)))
 
+    def set_hyp_method(self, method: str) -> None:
+        """"auto" (the library's choice: the level kernels), "levels" (one
+        launch per decoration level) or "slices" (a pipeline over time slices
+        with the decorated links in rings of three slices; Lt >= 3). The links
+        are the same bit for bit."""
+        m = {"auto": _lib.GC_HYP_AUTO, "levels": _lib.GC_HYP_LEVELS,
+             "slices": _lib.GC_HYP_SLICES}[method]
+        self._check(lib().gc_set_hyp_method(self._h, m))
+
     def wilson_loop(self, r_min: int, r_max: int, time_min: int, time_max: int) -> np.ndarray:
         """W table, shape (time_max-time_min+1, r_max-r_min+1): [T-t_min, R-r_min]."""
         out = np.empty((time_max - time_min + 1, r_max - r_min + 1), dtype=np.float64)

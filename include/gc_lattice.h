@@ -54,6 +54,13 @@ extern "C" {
 #define GC_WILSON_EXACT 1  /* always the exact product of links               */
 #define GC_WILSON_GAUGE 2  /* (reported by gc_wilson_method_used)             */
 
+/* Methods of HYP smearing (gc_set_hyp_method). */
+#define GC_HYP_AUTO 0    /* the library's choice (the level kernels)          */
+#define GC_HYP_LEVELS 1  /* one launch per decoration level, whole-lattice    */
+                         /* decorated-link fields                             */
+#define GC_HYP_SLICES 2  /* a pipeline over time slices, decorated links in   */
+                         /* rings of three slices (Lt >= 3)                   */
+
 #define GC_LAYOUT_ROWMAJOR 0
 #define GC_LAYOUT_EIGEN_COLMAJOR 1
 
@@ -158,6 +165,13 @@ int gc_ape(gc_lattice *h, double alpha, int steps);
  * called steps times. */
 int gc_hyp(gc_lattice *h, double alpha1, double alpha2, double alpha3,
            int steps);
+
+/* Selects how gc_hyp runs on this handle: GC_HYP_AUTO (default), GC_HYP_LEVELS
+ * or GC_HYP_SLICES (GC_ERR_ARG if Lt < 3). Both give the same links bit for
+ * bit; the slice pipeline keeps the decorated links of three time slices at a
+ * time instead of fifteen whole-lattice fields (less DRAM traffic, more time:
+ * Lt + 3 launches). No counterpart in the reference. */
+int gc_set_hyp_method(gc_lattice *h, int method);
 
 /* On-axis Wilson loops averaged over sites and the three spatial directions,
  * for R in [r_min, r_max] (space) and T in [time_min, time_max] (time).
