@@ -271,7 +271,7 @@ def batch_serial(jobs, form, first_index):
     import torch
     from general_code_b200 import Lattice, generate_config
     s = torch.cuda.Stream()
-    total, tables = 0.0, []
+    total, tables, per_job = 0.0, [], []
     for k, j in enumerate(jobs):
         links = generate_config(j.dims, j.nc, 0.3 if j.nc == 2 else 0.25, SEED, first_index + k)
         with Lattice(j.dims, j.nc, form) as pristine, Lattice(j.dims, j.nc, form) as lat:
@@ -289,8 +289,9 @@ def batch_serial(jobs, form, first_index):
                 e1.record(s)
                 s.synchronize()
             total += e0.elapsed_time(e1)
+            per_job.append(e0.elapsed_time(e1))
             tables.append(w)
-    return total, tables
+    return total, tables, per_job
 
 
 def bench_batch(steps: int):
@@ -322,7 +323,13 @@ def bench_batch(steps: int):
             info = b.info()
             w_batch = [b.wilson(k) for k in range(len(jobs))]
             report = b.autotune_report()
-        serial_ms, w_serial = batch_serial(jobs, form, 1000)
+        serial_ms, w_serial, per_job = batch_serial(jobs, form, 1000)
+        # where the serial time goes: per lattice shape (jobs, ms)
+        by_shape = {}
+        for j, t in zip(jobs, per_job):
+            key = f"SU({j.nc}) " + "x".join(map(str, j.dims))
+            n, ms_ = by_shape.get(key, (0, 0.0))
+            by_shape[key] = (n + 1, ms_ + t)
         worst = max(float(np.max(np.abs(a - c) / np.abs(c))) for a, c in zip(w_batch, w_serial))
         batch_ms = sum(ms) / len(ms)
         out[form] = {"sites_per_s": sites / (batch_ms * 1e-3),
@@ -332,6 +339,8 @@ def bench_batch(steps: int):
                      "serial_ms": serial_ms, "batch_over_serial": batch_ms / serial_ms,
                      "serial_sites_per_s": sites / (serial_ms * 1e-3),
                      "max_rel_diff_W_vs_serial": worst,
+                     "serial_ms_by_shape": {k: {"jobs": n, "ms": round(t, 3)}
+                                            for k, (n, t) in sorted(by_shape.items())},
                      "autotune_report": report.splitlines()}
     return {"workload": "64 uneven configurations, one CUDA graph per run", "jobs": 64,
             "sites": sites, "total_ape_steps": sum(j.ape_steps for j in jobs),
