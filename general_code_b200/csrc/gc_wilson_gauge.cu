@@ -95,6 +95,26 @@ __device__ __forceinline__ double unitarity_defect(const SU2<double> &u) {
   return fabs(dot4(u.a0, u.a0, u.a1, u.a1, u.a2, u.a2, u.a3, u.a3) - 1.0);
 }
 
+// The temporal link the gauge lines are built from. FP64 links are unitary to
+// rounding. An FP32 link's last projection step leaves its singular values
+// 1 - O(d^2) (d the defect before that step, up to 2e-5), a shrink of up to a
+// few 1e-10 with one sign; through G^dag G != 1 it entered every transformed
+// link, and W's error against FP64 grew linearly in R and T (3.4e-8 at 24^4,
+// R,T = 12, against 4.3e-9 for the exact product). One FP64 Newton-Schulz
+// step (SU(2): a / |a|) makes the link unitary to FP64 rounding; it moves
+// the link by that shrink only, well inside the FP32 rounding of the stored
+// link.
+template <class Store>
+__device__ __forceinline__ typename Store::template M<double> gauge_time_link(
+    const typename Store::template M<double> &u) {
+  if constexpr (Store::kBytes == 48 || Store::kBytes == 72)
+    return ns_step(u);
+  else if constexpr (Store::kBytes == 16)
+    return proj(u);
+  else
+    return u;
+}
+
 template <class Store>
 __global__ void __launch_bounds__(128)
     gauge_lines_kernel(const __grid_constant__ Geom g, const void *Ut, void *GA, void *GB,
@@ -115,7 +135,7 @@ __global__ void __launch_bounds__(128)
     const MD u = Store::template load<double>(Ut, V, s + t * g.Vs);
     dmax = fmax(dmax, unitarity_defect(u));
     if (t + 1 < Lt)
-      G = mul(G, u);
+      G = mul(G, gauge_time_link<Store>(u));
   }
   // cut B: G_B(s,h) = 1, forward through Lt-1 and around to h-1
   G = unit(MD());
@@ -124,7 +144,7 @@ __global__ void __launch_bounds__(128)
   for (int k = 0; k < Lt; k++) {
     GS::template store<double>(GB, V, s + t * g.Vs, G);
     if (k + 1 < Lt)
-      G = mul(G, Store::template load<double>(Ut, V, s + t * g.Vs));
+      G = mul(G, gauge_time_link<Store>(Store::template load<double>(Ut, V, s + t * g.Vs)));
     t = (t + 1 == Lt) ? 0 : t + 1;
   }
   if (!(dmax <= tol)) // (a NaN link counts as not unitary)

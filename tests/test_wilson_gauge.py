@@ -114,3 +114,29 @@ def test_long_time_range_takes_the_exact_product():
         assert lat.wilson_method_used() == "gauge"
         lat.wilson_loop(1, 2, 1, 5)
         assert lat.wilson_method_used() == "exact"
+
+
+@pytest.mark.parametrize("nc,dims,n_ape,rt", [
+    (3, (24, 24, 24, 24), 20, 12),
+    (3, (8, 8, 8, 16), 3, 8),
+    (2, (16, 16, 16, 16), 10, 8),
+])
+def test_mixed_gauge_form_keeps_the_exact_products_accuracy(nc, dims, n_ape, rt):
+    """The mixed form's temporal links leave their last projection step with
+    singular values a few 1e-10 below one; the gauge lines are built from the
+    links made unitary in FP64, so the gauge form's W error against FP64 stays
+    at the exact product's (measured 2-6e-9; with the stored links it grew
+    linearly in R and T to 3.4e-8 at 24^4)."""
+    links = generate_config(dims, nc, 0.25 if nc == 3 else 0.3, 20261203, 0)
+    res = {}
+    for form in ("fp64", "mixed"):
+        with Lattice(dims, nc, form) as lat:
+            lat.upload(links)
+            lat.hyp(1.0, 0.75, 0.6, 1)
+            lat.ape(0.5, n_ape)
+            res[form] = _both(lat, (1, rt, 1, rt))
+    ref = res["fp64"]["exact"]
+    assert res["mixed"]["auto_used"] == "gauge"
+    err = {m: float(np.max(np.abs(res["mixed"][m] - ref) / np.abs(ref))) for m in ("auto", "exact")}
+    assert err["auto"] <= 1e-8, err
+    assert err["auto"] <= 2 * err["exact"] + 2e-9, err
