@@ -9,8 +9,13 @@
 //                 alpha3/2)  — thread per (site, field)
 //        level 2: 6 fields   Vtilde_{t;nu}, Vtilde_{nu;t}  (alpha2/4)
 //        level 3: U_t'       (alpha1/6), written to a second temporal buffer.
+//      or, as an option, one kernel per time slice that runs the three
+//      levels of three consecutive slices (hyp_slices_kernel), with the
+//      decorated links in rings of slices that stay in L2.
 // The staple sums use the compute type CT (FP64 for the plain form, FP32 for
-// the mixed form); the SU(N) projection always runs in FP64.
+// the mixed form). The projection: FP64 SU(3) runs the reference's
+// Newton-Schulz iteration in FP64; mixed SU(3) runs FP32 steps and a last
+// FP64 step (proj_store); SU(2) normalises with |a|^2 and 1/|a| in FP64.
 #include "gc_internal.cuh"
 #include "gc_kernels.h"
 
