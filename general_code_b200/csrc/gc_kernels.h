@@ -99,6 +99,7 @@ struct WilsonPlan {
   size_t smem;        // dynamic shared memory bytes
   bool fits;          // false when even one column exceeds the budget
   int starts = 1;     // temporal-gauge form: consecutive start slices per thread
+  bool one_column = false; // temporal-gauge form: one column per thread, lines in registers
 };
 // Doubles of a W block's per-warp accumulators in shared memory, rounded up
 // to an even count so the 16-byte arrays placed after them stay aligned.

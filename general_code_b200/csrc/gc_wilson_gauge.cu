@@ -52,6 +52,7 @@
 #include "gc_internal.cuh"
 #include "gc_kernels.h"
 #include "gc_pair.cuh"
+#include "gc_rows01.cuh"
 #include "gc_wcol.cuh"
 
 #include <algorithm>
@@ -441,6 +442,174 @@ __global__ void __launch_bounds__(256)
   }
 }
 
+// Shared-memory record of an FP32 SU(3) space line for the one-column kernel
+// below: rows 0 and 1 (row 2 = conj(row0 x row1) is rebuilt where a trace
+// needs it), 48 bytes moved as three 16-byte vectors at immediate offsets, in
+// the element order of the stored links (StoreF32SU3). Consecutive threads
+// hold consecutive records (a 12-word stride), so each quarter-warp phase of a
+// 16-byte access covers the 32 banks once.
+struct Rows01Set {
+  static constexpr int kBytes = 48;
+  __device__ __forceinline__ static void store(unsigned char *set, int i, const SU3<float> &m) {
+    float4 *p = reinterpret_cast<float4 *>(set + (size_t)kBytes * i);
+    p[0] = make_float4(m.e[0][0].re, m.e[0][0].im, m.e[0][1].re, m.e[0][1].im);
+    p[1] = make_float4(m.e[0][2].re, m.e[0][2].im, m.e[1][0].re, m.e[1][0].im);
+    p[2] = make_float4(m.e[1][1].re, m.e[1][1].im, m.e[1][2].re, m.e[1][2].im);
+  }
+  // rows 0 and 1 (row 2 not set)
+  __device__ __forceinline__ static SU3<float> load(const unsigned char *set, int i) {
+    const float4 *p = reinterpret_cast<const float4 *>(set + (size_t)kBytes * i);
+    const float4 a = p[0], b = p[1], c = p[2];
+    SU3<float> m;
+    m.e[0][0] = {a.x, a.y};
+    m.e[0][1] = {a.z, a.w};
+    m.e[0][2] = {b.x, b.y};
+    m.e[1][0] = {b.z, b.w};
+    m.e[1][1] = {c.x, c.y};
+    m.e[1][2] = {c.z, c.w};
+    return m;
+  }
+};
+
+// The fundamental loops of the mixed SU(3) form with one column per thread
+// and KS consecutive start slices t0 = KS row + m (all of one cut: KS divides
+// the cut slice h) whose space lines stay in registers from one R to the
+// next. The trace sweep reads each top line once for the KS starts, as in
+// wilson_gauge_kernel, but the lines are not lane-packed, so KS = 4 starts
+// fit in the registers: twice the loops per shared-memory byte of the
+// two-column, two-start form. Each R the thread extends its own starts' lines
+// in registers (and stores them for the other threads' sweeps) and the other
+// cut's lines of the same slices in shared memory. Lines are products of
+// SU(3) links, so they are computed and kept in shared memory as rows 0 and 1
+// (48 bytes a line instead of 72; 72 instead of 108 multiply-adds a product),
+// and row 2 is rebuilt where a trace needs it. Compiled for 16 warps per SM
+// (128 registers, a few spilled): at SU(3) 32^4 that ran 2.45 ms against 2.98
+// ms at 175 registers (8 warps) and 3.01 ms for the two-column kernel.
+// Partials, block sums and the per-thread FP32 loop sums as
+// wilson_gauge_kernel.
+template <int KS>
+__global__ void __launch_bounds__(256, 2)
+    wilson_gauge_reg_kernel(const __grid_constant__ Geom g, const __grid_constant__ Fields4 UA,
+                            const __grid_constant__ Fields4 UB, int rmin, int rmax, int tmin,
+                            int tmax, int cols, int rows, double *partials, const int *flag) {
+  if (flag && *flag != 0)
+    return;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int Lt = g.L[3], h = Lt / 2;
+  const int nt = tmax - tmin + 1;
+  const int nthreads = blockDim.x;
+  const int nslots = Lt * cols;
+  float *red = reinterpret_cast<float *>(smem_raw); // [nt][nthreads]
+  unsigned char *sa = smem_raw + ((sizeof(float) * nt * nthreads + 15) & ~(size_t)15);
+  unsigned char *sb = sa + (size_t)Rows01Set::kBytes * nslots;
+
+  const int tid = threadIdx.x;
+  const int warp = tid >> 5, lane = tid & 31, nwarps = nthreads >> 5;
+  const int u = tid % cols;
+  const int row = tid / cols;
+  const int nu = blockIdx.y;
+  const int s0 = column_base(g, blockIdx.x, cols, nu) + u;
+  const bool active = (row < rows) && (s0 < g.Vs);
+  const int t0 = KS * row;
+  // the cut of this thread's starts, and the other one
+  const bool cut_a = t0 < h;
+  unsigned char *own = cut_a ? sa : sb;
+  unsigned char *other = cut_a ? sb : sa;
+  const void *f_own = cut_a ? UA.f[nu] : UB.f[nu];
+  const void *f_other = cut_a ? UB.f[nu] : UA.f[nu];
+  const int Ln = sel4(g.L, nu), stn = sel4(g.stride, nu);
+  const int xn = (s0 / stn) % Ln;
+  const size_t V = g.V;
+  const int ne = (rmax - rmin + 1) * nt;
+  double *part = partials + ((size_t)blockIdx.y * gridDim.x + blockIdx.x) * ne;
+
+  SU3<float> a[KS];
+#pragma unroll 1
+  for (int R = 1; R <= rmax; R++) {
+    // extend both cuts' lines of slices t0 .. t0 + KS - 1 by the link at
+    // x + (R-1) nu
+    if (active) {
+      const int l = s0 + ((xn + R - 1) % Ln - xn) * stn;
+#pragma unroll
+      for (int m = 0; m < KS; m++) {
+        const int t = t0 + m;
+        const int i = t * cols + u;
+        const SU3<float> lo = StoreF32SU3::load<float>(f_own, V, l + t * g.Vs);
+        const SU3<float> lx = StoreF32SU3::load<float>(f_other, V, l + t * g.Vs);
+        if (R == 1) {
+          a[m] = lo;
+          Rows01Set::store(other, i, lx);
+        } else {
+          // rows 0 and 1 of the products; the own line's row 2 rebuilt for
+          // its traces
+          a[m] = mul01(a[m], lo);
+          rebuild_row2(a[m]);
+          Rows01Set::store(other, i, mul01(Rows01Set::load(other, i), lx));
+        }
+        Rows01Set::store(own, i, a[m]);
+      }
+    }
+    __syncthreads();
+    if (R >= rmin) {
+      int tt = t0 + tmin;
+      tt = (tt >= Lt) ? tt - Lt : tt;
+      float acc[KS]; // acc[m]: the sum for T index j - m
+#pragma unroll
+      for (int m = 0; m < KS; m++)
+        acc[m] = 0.f;
+      // the loops of all starts that end on top line b (index j), then the
+      // completed sum of T index j - KS + 1
+      auto step = [&](int j, const SU3<float> &b) {
+        if (active) {
+#pragma unroll
+          for (int m = 0; m < KS; m++)
+            if (j - m >= 0 && j - m < nt) // start t0 + m, T = tmin + j - m
+              acc[m] += gauge_trace<false>(a[m], b, false);
+        }
+        if (j - (KS - 1) >= 0)
+          red[(size_t)(j - (KS - 1)) * nthreads + tid] = acc[KS - 1];
+#pragma unroll
+        for (int m = KS - 1; m > 0; m--)
+          acc[m] = acc[m - 1];
+        acc[0] = 0.f;
+      };
+      // two top lines in flight (b0, b1 alternate); a slot one past the last
+      // step is still a slot of the column (in bounds, unused)
+      const int nsteps = nt + KS - 1;
+      SU3<float> b0, b1;
+      if (active)
+        b0 = Rows01Set::load(own, tt * cols + u);
+#pragma unroll 1
+      for (int j = 0; j < nsteps; j += 2) {
+        tt = (tt + 1 == Lt) ? 0 : tt + 1;
+        if (active)
+          b1 = Rows01Set::load(own, tt * cols + u);
+        rebuild_row2(b0);
+        step(j, b0);
+        tt = (tt + 1 == Lt) ? 0 : tt + 1;
+        if (active)
+          b0 = Rows01Set::load(own, tt * cols + u);
+        if (j + 1 < nsteps) {
+          rebuild_row2(b1);
+          step(j + 1, b1);
+        }
+      }
+      __syncthreads();
+      // fixed-order sum over the block's threads (as wilson_gauge_kernel)
+#pragma unroll 1
+      for (int T = warp; T < nt; T += nwarps) {
+        double v = 0.0;
+        for (int i = lane; i < nthreads; i += 32)
+          v += double(red[(size_t)T * nthreads + i]);
+        v = warp_sum(v);
+        if (lane == 0)
+          part[(R - rmin) * nt + T] = v;
+      }
+    }
+    __syncthreads();
+  }
+}
+
 // The fixed-order tree over blocks (as reduce_partials_kernel in
 // gc_wilson.cu) over the partials of whichever method ran.
 __global__ void __launch_bounds__(256)
@@ -466,6 +635,12 @@ __global__ void __launch_bounds__(256)
   }
 }
 
+// The one-column kernel runs the fundamental loops of the mixed SU(3) form
+// when four consecutive start slices share a cut (8 divides Lt).
+bool gauge_reg_applies(int Lt, int nc, int ct_bytes, bool adjoint) {
+  return nc == 3 && ct_bytes == 4 && !adjoint && Lt % 8 == 0 && Lt / 4 <= 64;
+}
+
 int largest_divisor_upto_g(int n, int cap) {
   for (int d = cap < n ? cap : n; d > 1; d--)
     if (n % d == 0)
@@ -483,6 +658,27 @@ WilsonPlan wilson_gauge_plan(const Geom &g, int nt, int nc, int ct_bytes, int un
   WilsonPlan p{};
   const int Lt = g.L[3];
   const int ncomp = (nc == 3) ? 18 : 4;
+  if (gauge_reg_applies(Lt, nc, ct_bytes, adjoint)) {
+    // the one-column kernel: four starts per thread, columns of Lt/4 threads,
+    // by default the largest power of two of columns with at most 128 threads
+    // per block (SU(3) mixed, R,T <= L/2: 2.45 ms at 32^4 with 16 columns,
+    // 0.59 ms at 24^4 with 16, 1.11 ms at 24^3 x 48 with 8; 2-15% slower
+    // with twice or half the columns, 10-50% with a quarter)
+    p.one_column = true;
+    p.starts = 4;
+    p.rows = Lt / 4;
+    int units = units_req;
+    if (units <= 0)
+      for (units = 1; 2 * units * p.rows <= 128;)
+        units *= 2;
+    p.cols_per_block = units;
+    p.threads = wilson_threads(units, p.rows, 1);
+    p.blocks = ((g.Vs + units - 1) / units) * 3;
+    p.smem = ((size_t)nt * p.threads * sizeof(float) + 15) / 16 * 16 +
+             2 * (size_t)Rows01Set::kBytes * Lt * units;
+    p.fits = p.threads <= 256 && p.smem <= 200 * 1024;
+    return p;
+  }
   const int lanes = wilson_lanes(nc, ct_bytes);
   // consecutive start slices per thread (a divisor of the cut slice h = Lt/2,
   // so that a thread's starts share a cut): 2 for SU(3) (its registers hold
@@ -559,8 +755,20 @@ int launch_wilson_gauge_kernel(const Geom &g, const Fields4 &UA, const Fields4 &
     return GC_OK;
   };
   int rc;
-  // (four starts per thread only for SU(2), as the plan chooses)
+  // (four starts per thread for SU(2), and in the one-column kernel for the
+  // mixed SU(3) form's fundamental loops, as the plan chooses)
   constexpr int K4 = Store::NC == 2 ? 4 : 2;
+  if constexpr (std::is_same<Store, StoreF32SU3>::value) {
+    if (p.one_column) {
+      int r = allow_large_smem(wilson_gauge_reg_kernel<4>, p.smem, capturing);
+      if (r)
+        return r;
+      wilson_gauge_reg_kernel<4><<<dim3(p.blocks / 3, 3), p.threads, p.smem, s>>>(
+          g, UA, UB, rmin, rmax, tmin, tmax, p.cols_per_block, p.rows, partials, flag);
+      *blocks = p.blocks;
+      return launch_check("wilson_gauge_reg_kernel");
+    }
+  }
   if (adjoint)
     rc = p.starts == 4   ? go(wilson_gauge_kernel<Store, CT, true, K4>)
          : p.starts == 2 ? go(wilson_gauge_kernel<Store, CT, true, 2>)
@@ -608,10 +816,11 @@ int launch_wilson_auto(const Geom &g, const Fields4 &U, const Fields4 &UA, const
 }
 
 size_t wilson_auto_partials_count(const Geom &g, int nr, int nt, int nc, int units) {
-  const WilsonPlan a = wilson_gauge_plan(g, nt, nc, 4, units),
-                   b = wilson_gauge_plan(g, nt, nc, 8, units);
-  return std::max<size_t>(wilson_partials_count(g, nr, nt, nc),
-                          (size_t)std::max(a.blocks, b.blocks) * nr * nt);
+  int blocks = 0;
+  for (int ct : {4, 8})
+    for (bool adj : {false, true})
+      blocks = std::max(blocks, wilson_gauge_plan(g, nt, nc, ct, units, adj).blocks);
+  return std::max<size_t>(wilson_partials_count(g, nr, nt, nc), (size_t)blocks * nr * nt);
 }
 
 // Times one launch of the gauge W kernel of a lattice with `units` column

@@ -60,6 +60,11 @@ def test_both_methods_match_reference_fixture(name, meta):
     (2, (4, 3, 5, 40), 0.3, 2, (1, 2, 3, 20)),
     (3, (12, 12, 12, 12), 0.25, 4, (1, 6, 1, 6)),
     (2, (6, 6, 6, 96), 0.3, 1, (1, 3, 1, 12)),     # two start slices per thread
+    # mixed SU(3) with 8 | Lt runs the one-column kernel (four starts per
+    # thread): blocks of 32 columns over runs of sites, the last block part
+    # full, R and T ranges not starting at 1
+    (3, (5, 6, 7, 16), 0.25, 2, (2, 4, 3, 8)),
+    (3, (3, 3, 3, 64), 0.25, 1, (1, 2, 1, 32)),    # 16 threads per column
 ])
 def test_gauge_form_matches_oracle_seeded(port, nc, dims, eps, n_ape, rng):
     links = generate_config(dims, nc, eps, 20261203, 11)
