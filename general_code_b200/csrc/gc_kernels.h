@@ -99,7 +99,10 @@ struct WilsonPlan {
   size_t smem;        // dynamic shared memory bytes
   bool fits;          // false when even one column exceeds the budget
   int starts = 1;     // temporal-gauge form: consecutive start slices per thread
-  bool one_column = false; // temporal-gauge form: one column per thread, lines in registers
+  // temporal-gauge form: 0 wilson_gauge_kernel; one column per thread with
+  // the lines of its starts in registers: 1 wilson_gauge_reg_kernel (mixed
+  // SU(3)), 2 wilson_gauge_q_kernel (SU(2))
+  int kernel = 0;
 };
 // Doubles of a W block's per-warp accumulators in shared memory, rounded up
 // to an even count so the 16-byte arrays placed after them stay aligned.

@@ -48,7 +48,11 @@
 //                           slot; a
 //                           fixed-order sum over the block's threads gives
 //                           one partial per (block, R, T), and the fixed-order
-//                           tree over blocks of gc_wilson.cu finishes.
+//                           tree over blocks of gc_wilson.cu finishes
+//   wilson_gauge_reg_kernel the mixed SU(3) fundamental loops (8 | Lt), and
+//   wilson_gauge_q_kernel   the SU(2) fundamental loops (8 | Lt): one column
+//                           per thread, the space lines of its 4 start slices
+//                           kept in registers
 #include "gc_internal.cuh"
 #include "gc_kernels.h"
 #include "gc_pair.cuh"
@@ -610,6 +614,166 @@ __global__ void __launch_bounds__(256, 2)
   }
 }
 
+// Shared-memory records of SU(2) space lines (quaternions) for the SU(2)
+// one-column kernel: FP32 one 16-byte vector per slot; FP64 two planes of
+// 16-byte (a0, a1) and (a2, a3) pairs. A quarter-warp phase of 8 consecutive
+// slots reads 128 contiguous bytes of a plane: conflict-free when the block's
+// columns are a multiple of 8.
+template <class T> struct QuatSet;
+template <> struct QuatSet<float> {
+  static constexpr int kBytes = 16;
+  __device__ __forceinline__ static void store(unsigned char *set, int, int i,
+                                               const SU2<float> &q) {
+    reinterpret_cast<float4 *>(set)[i] = make_float4(q.a0, q.a1, q.a2, q.a3);
+  }
+  __device__ __forceinline__ static SU2<float> load(const unsigned char *set, int, int i) {
+    const float4 v = reinterpret_cast<const float4 *>(set)[i];
+    return {v.x, v.y, v.z, v.w};
+  }
+};
+template <> struct QuatSet<double> {
+  static constexpr int kBytes = 32;
+  __device__ __forceinline__ static void store(unsigned char *set, int nslots, int i,
+                                               const SU2<double> &q) {
+    double2 *p = reinterpret_cast<double2 *>(set);
+    p[i] = make_double2(q.a0, q.a1);
+    p[nslots + i] = make_double2(q.a2, q.a3);
+  }
+  __device__ __forceinline__ static SU2<double> load(const unsigned char *set, int nslots,
+                                                     int i) {
+    const double2 *p = reinterpret_cast<const double2 *>(set);
+    const double2 a = p[i], b = p[nslots + i];
+    return {a.x, a.y, b.x, b.y};
+  }
+};
+
+// The fundamental SU(2) loops with one column per thread and KS consecutive
+// start slices of one cut whose space lines stay in registers (as wilson_gauge_reg_kernel for SU(3)). A quaternion loop is a
+// 4-term dot product, so in the two-column kernel a step of the trace sweep
+// spent more instructions on its shared-memory loads, bounds checks, rolling
+// sums and index updates than on the loops themselves (0.87 instructions per
+// cycle per scheduler, issue-bound). Here the sweep runs over T: each step
+// loads one line into a register window and adds the KS loops of that T,
+// with no checks and no moves. Per-thread sums in the compute type (FP32 for
+// the mixed form), block and grid sums in FP64.
+template <class Store, class CT, int KS>
+__global__ void __launch_bounds__(256)
+    wilson_gauge_q_kernel(const __grid_constant__ Geom g, const __grid_constant__ Fields4 UA,
+                          const __grid_constant__ Fields4 UB, int rmin, int rmax, int tmin,
+                          int tmax, int cols, int rows, double *partials, const int *flag) {
+  if (flag && *flag != 0)
+    return;
+  using Q = SU2<CT>;
+  using QS = QuatSet<CT>;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int Lt = g.L[3], h = Lt / 2;
+  const int nt = tmax - tmin + 1;
+  const int nthreads = blockDim.x;
+  const int nslots = Lt * cols;
+  CT *red = reinterpret_cast<CT *>(smem_raw); // [nt][nthreads]
+  unsigned char *sa = smem_raw + ((sizeof(CT) * nt * nthreads + 15) & ~(size_t)15);
+  unsigned char *sb = sa + (size_t)QS::kBytes * nslots;
+
+  const int tid = threadIdx.x;
+  const int warp = tid >> 5, lane = tid & 31, nwarps = nthreads >> 5;
+  const int u = tid % cols;
+  const int row = tid / cols;
+  const int nu = blockIdx.y;
+  const int s0 = column_base(g, blockIdx.x, cols, nu) + u;
+  const bool active = (row < rows) && (s0 < g.Vs);
+  const int t0 = KS * row;
+  const bool cut_a = t0 < h;
+  unsigned char *own = cut_a ? sa : sb;
+  unsigned char *other = cut_a ? sb : sa;
+  const void *f_own = cut_a ? UA.f[nu] : UB.f[nu];
+  const void *f_other = cut_a ? UB.f[nu] : UA.f[nu];
+  const int Ln = sel4(g.L, nu), stn = sel4(g.stride, nu);
+  const int xn = (s0 / stn) % Ln;
+  const size_t V = g.V;
+  const int ne = (rmax - rmin + 1) * nt;
+  double *part = partials + ((size_t)blockIdx.y * gridDim.x + blockIdx.x) * ne;
+
+  Q a[KS];
+#pragma unroll 1
+  for (int R = 1; R <= rmax; R++) {
+    if (active) {
+      const int l = s0 + ((xn + R - 1) % Ln - xn) * stn;
+#pragma unroll
+      for (int m = 0; m < KS; m++) {
+        const int t = t0 + m;
+        const int i = t * cols + u;
+        const Q lo = Store::template load<CT>(f_own, V, l + t * g.Vs);
+        const Q lx = Store::template load<CT>(f_other, V, l + t * g.Vs);
+        if (R == 1) {
+          a[m] = lo;
+          QS::store(other, nslots, i, lx);
+        } else {
+          a[m] = mul(a[m], lo);
+          QS::store(other, nslots, i, mul(QS::load(other, nslots, i), lx));
+        }
+        QS::store(own, nslots, i, a[m]);
+      }
+    }
+    __syncthreads();
+    if (R >= rmin) {
+      // T-major sweep: the thread's sum for T index q is its KS loops of
+      // starts t0 + m ending on the lines of relative index p = q + m
+      // (slice t0 + tmin + p). A window of W = KS + 1 lines in registers
+      // holds relative index p in w[p % W]; step q (unrolled by W, so every
+      // slot index is a constant) loads the line p = q + KS that step q + 1
+      // needs and adds the KS dot products of step q. Inactive threads load
+      // nothing (zero lines) and write zero sums.
+      constexpr int W = KS + 1;
+      if (!active) {
+#pragma unroll
+        for (int m = 0; m < KS; m++)
+          a[m] = Q{CT(0), CT(0), CT(0), CT(0)};
+      }
+      Q w[W];
+      int tp = t0 + tmin; // slice of the next line to load
+      tp = (tp >= Lt) ? tp - Lt : tp;
+#pragma unroll
+      for (int m = 0; m < KS; m++) {
+        w[m] = active ? QS::load(own, nslots, tp * cols + u) : a[0];
+        tp = (tp + 1 == Lt) ? 0 : tp + 1;
+      }
+#pragma unroll 1
+      for (int q0 = 0; q0 < nt; q0 += W) {
+#pragma unroll
+        for (int r = 0; r < W; r++) {
+          if (q0 + r < nt) {
+            w[(r + KS) % W] = active ? QS::load(own, nslots, tp * cols + u) : a[0];
+            tp = (tp + 1 == Lt) ? 0 : tp + 1;
+            CT d[KS];
+#pragma unroll
+            for (int m = 0; m < KS; m++) {
+              const Q &b = w[(r + m) % W];
+              d[m] = dot4(a[m].a0, b.a0, a[m].a1, b.a1, a[m].a2, b.a2, a[m].a3, b.a3);
+            }
+#pragma unroll
+            for (int k = 1; k < KS; k *= 2)
+#pragma unroll
+              for (int m = 0; m + k < KS; m += 2 * k)
+                d[m] += d[m + k];
+            red[(size_t)(q0 + r) * nthreads + tid] = d[0];
+          }
+        }
+      }
+      __syncthreads();
+#pragma unroll 1
+      for (int T = warp; T < nt; T += nwarps) {
+        double v = 0.0;
+        for (int i = lane; i < nthreads; i += 32)
+          v += double(red[(size_t)T * nthreads + i]);
+        v = warp_sum(v);
+        if (lane == 0)
+          part[(R - rmin) * nt + T] = v;
+      }
+    }
+    __syncthreads();
+  }
+}
+
 // The fixed-order tree over blocks (as reduce_partials_kernel in
 // gc_wilson.cu) over the partials of whichever method ran.
 __global__ void __launch_bounds__(256)
@@ -641,6 +805,18 @@ bool gauge_reg_applies(int Lt, int nc, int ct_bytes, bool adjoint) {
   return nc == 3 && ct_bytes == 4 && !adjoint && Lt % 8 == 0 && Lt / 4 <= 64;
 }
 
+// Start slices per thread of the SU(2) one-column kernel. Four in both
+// forms: at SU(2) 48^4 mixed, R,T <= 24, eight starts (122 registers, 15
+// warps per SM) took 5.68 ms against 5.15 ms for four (70 registers), which
+// keep twice the threads per column resident.
+constexpr int gauge_q_starts(int) { return 4; }
+// The SU(2) one-column kernel runs the fundamental loops when a thread's
+// consecutive start slices share a cut (2 x starts divides Lt).
+bool gauge_q_applies(int Lt, int nc, int ct_bytes, bool adjoint) {
+  const int ks = gauge_q_starts(ct_bytes);
+  return nc == 2 && !adjoint && Lt % (2 * ks) == 0 && Lt / ks <= 64;
+}
+
 int largest_divisor_upto_g(int n, int cap) {
   for (int d = cap < n ? cap : n; d > 1; d--)
     if (n % d == 0)
@@ -664,7 +840,7 @@ WilsonPlan wilson_gauge_plan(const Geom &g, int nt, int nc, int ct_bytes, int un
     // per block (SU(3) mixed, R,T <= L/2: 2.45 ms at 32^4 with 16 columns,
     // 0.59 ms at 24^4 with 16, 1.11 ms at 24^3 x 48 with 8; 2-15% slower
     // with twice or half the columns, 10-50% with a quarter)
-    p.one_column = true;
+    p.kernel = 1;
     p.starts = 4;
     p.rows = Lt / 4;
     int units = units_req;
@@ -676,6 +852,26 @@ WilsonPlan wilson_gauge_plan(const Geom &g, int nt, int nc, int ct_bytes, int un
     p.blocks = ((g.Vs + units - 1) / units) * 3;
     p.smem = ((size_t)nt * p.threads * sizeof(float) + 15) / 16 * 16 +
              2 * (size_t)Rows01Set::kBytes * Lt * units;
+    p.fits = p.threads <= 256 && p.smem <= 200 * 1024;
+    return p;
+  }
+  if (gauge_q_applies(Lt, nc, ct_bytes, adjoint)) {
+    // the SU(2) one-column kernel: four starts per thread, columns of Lt / 4
+    // threads, by default the largest power of two (at least 8) of columns
+    // with at most 192 threads per block (48^4 mixed: 5.15 ms with 16
+    // columns of 12 threads, 5.47 ms with 8)
+    p.kernel = 2;
+    p.starts = gauge_q_starts(ct_bytes);
+    p.rows = Lt / p.starts;
+    int units = units_req;
+    if (units <= 0)
+      for (units = 8; 2 * units * p.rows <= 192;)
+        units *= 2;
+    p.cols_per_block = units;
+    p.threads = wilson_threads(units, p.rows, 1);
+    p.blocks = ((g.Vs + units - 1) / units) * 3;
+    p.smem = ((size_t)nt * p.threads * ct_bytes + 15) / 16 * 16 +
+             2 * (size_t)(ct_bytes == 4 ? 16 : 32) * Lt * units;
     p.fits = p.threads <= 256 && p.smem <= 200 * 1024;
     return p;
   }
@@ -758,8 +954,20 @@ int launch_wilson_gauge_kernel(const Geom &g, const Fields4 &UA, const Fields4 &
   // (four starts per thread for SU(2), and in the one-column kernel for the
   // mixed SU(3) form's fundamental loops, as the plan chooses)
   constexpr int K4 = Store::NC == 2 ? 4 : 2;
+  if constexpr (Store::NC == 2) {
+    if (p.kernel == 2) {
+      constexpr int KS = gauge_q_starts((int)sizeof(CT));
+      int r = allow_large_smem(wilson_gauge_q_kernel<Store, CT, KS>, p.smem, capturing);
+      if (r)
+        return r;
+      wilson_gauge_q_kernel<Store, CT, KS><<<dim3(p.blocks / 3, 3), p.threads, p.smem, s>>>(
+          g, UA, UB, rmin, rmax, tmin, tmax, p.cols_per_block, p.rows, partials, flag);
+      *blocks = p.blocks;
+      return launch_check("wilson_gauge_q_kernel");
+    }
+  }
   if constexpr (std::is_same<Store, StoreF32SU3>::value) {
-    if (p.one_column) {
+    if (p.kernel == 1) {
       int r = allow_large_smem(wilson_gauge_reg_kernel<4>, p.smem, capturing);
       if (r)
         return r;

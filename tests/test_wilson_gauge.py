@@ -65,6 +65,11 @@ def test_both_methods_match_reference_fixture(name, meta):
     # full, R and T ranges not starting at 1
     (3, (5, 6, 7, 16), 0.25, 2, (2, 4, 3, 8)),
     (3, (3, 3, 3, 64), 0.25, 1, (1, 2, 1, 32)),    # 16 threads per column
+    # SU(2) with 8 | Lt runs its one-column kernel (four starts per thread,
+    # the T sweep in steps of five): fewer T values than one step, and a T
+    # range that is not a multiple of five
+    (2, (4, 5, 3, 32), 0.3, 2, (2, 3, 4, 7)),
+    (2, (6, 5, 7, 48), 0.3, 1, (1, 3, 3, 24)),
 ])
 def test_gauge_form_matches_oracle_seeded(port, nc, dims, eps, n_ape, rng):
     links = generate_config(dims, nc, eps, 20261203, 11)
