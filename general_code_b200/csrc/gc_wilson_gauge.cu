@@ -35,8 +35,9 @@
 // 2 T d (the two time lines), well inside the parity tolerances at these d.
 //
 // Kernels:
-//   gauge_lines_kernel      thread per spatial site: G_A(s,t), G_B(s,t) for
-//                           all t (FP64, stored as FP64 fields), the defect
+//   gauge_lines_kernel      thread per (spatial site, cut): G_A(s,t) and the
+//                           defect, or G_B(s,t), for all t (FP64, stored as
+//                           FP64 fields)
 //   gauge_transform_kernel  thread per (site, spatial nu): U'_nu for both
 //                           cuts, computed in FP64, stored in the lattice's
 //                           link format
@@ -131,19 +132,24 @@ __global__ void __launch_bounds__(128)
     return;
   const size_t V = g.V;
   const int Lt = g.L[3];
-  double dmax = 0.0;
-  // cut A: G_A(s,0) = 1, G_A(s,t+1) = G_A(s,t) U_t(s,t)
-  MD G = unit(MD());
+  if (blockIdx.y == 0) {
+    // cut A: G_A(s,0) = 1, G_A(s,t+1) = G_A(s,t) U_t(s,t); the defect check
+    double dmax = 0.0;
+    MD G = unit(MD());
 #pragma unroll 1
-  for (int t = 0; t < Lt; t++) {
-    GS::template store<double>(GA, V, s + t * g.Vs, G);
-    const MD u = Store::template load<double>(Ut, V, s + t * g.Vs);
-    dmax = fmax(dmax, unitarity_defect(u));
-    if (t + 1 < Lt)
-      G = mul(G, gauge_time_link<Store>(u));
+    for (int t = 0; t < Lt; t++) {
+      GS::template store<double>(GA, V, s + t * g.Vs, G);
+      const MD u = Store::template load<double>(Ut, V, s + t * g.Vs);
+      dmax = fmax(dmax, unitarity_defect(u));
+      if (t + 1 < Lt)
+        G = mul(G, gauge_time_link<Store>(u));
+    }
+    if (!(dmax <= tol)) // (a NaN link counts as not unitary)
+      *flag = 1;
+    return;
   }
   // cut B: G_B(s,h) = 1, forward through Lt-1 and around to h-1
-  G = unit(MD());
+  MD G = unit(MD());
   int t = h;
 #pragma unroll 1
   for (int k = 0; k < Lt; k++) {
@@ -152,8 +158,6 @@ __global__ void __launch_bounds__(128)
       G = mul(G, gauge_time_link<Store>(Store::template load<double>(Ut, V, s + t * g.Vs)));
     t = (t + 1 == Lt) ? 0 : t + 1;
   }
-  if (!(dmax <= tol)) // (a NaN link counts as not unitary)
-    *flag = 1;
 }
 
 // U'_nu(x) = G(x) U_nu(x) G(x + nu)^dag for both cuts; thread per (site, nu).
@@ -919,7 +923,9 @@ int launch_wilson_gauge_prep(const Geom &g, const Fields4 &U, void *GA, void *GB
   cudaError_t e = cudaMemsetAsync(flag, 0, sizeof(int), s);
   if (e != cudaSuccess)
     return launch_check("gauge flag reset");
-  gauge_lines_kernel<Store><<<(g.Vs + 127) / 128, 128, 0, s>>>(
+  // (the two cuts' lines in separate blocks: blockIdx.y = 0 for cut A and
+  // the defect check, 1 for cut B)
+  gauge_lines_kernel<Store><<<dim3((g.Vs + 127) / 128, 2), 128, 0, s>>>(
       g, U.f[3], GA, GB, g.L[3] / 2, wilson_gauge_tolerance((int)sizeof(CT)), flag);
   int rc = launch_check("gauge_lines_kernel");
   if (rc)
