@@ -816,9 +816,10 @@ bool gauge_reg_applies(int Lt, int nc, int ct_bytes, bool adjoint) {
 constexpr int gauge_q_starts(int) { return 4; }
 // The SU(2) one-column kernel runs the fundamental loops when a thread's
 // consecutive start slices share a cut (2 x starts divides Lt).
+// (at most 32 threads per column, so that a block of 8 columns fits)
 bool gauge_q_applies(int Lt, int nc, int ct_bytes, bool adjoint) {
   const int ks = gauge_q_starts(ct_bytes);
-  return nc == 2 && !adjoint && Lt % (2 * ks) == 0 && Lt / ks <= 64;
+  return nc == 2 && !adjoint && Lt % (2 * ks) == 0 && Lt / ks <= 32;
 }
 
 int largest_divisor_upto_g(int n, int cap) {
@@ -907,7 +908,9 @@ WilsonPlan wilson_gauge_plan(const Geom &g, int nt, int nc, int ct_bytes, int un
 bool wilson_gauge_applies(const Geom &g, int tmax, int nt, int nc, int ct_bytes) {
   if (tmax > g.L[3] / 2 || g.L[3] < 2)
     return false;
-  return wilson_gauge_plan(g, nt, nc, ct_bytes, 0, true).fits;
+  // (the fundamental and the adjoint loops may take different kernels)
+  return wilson_gauge_plan(g, nt, nc, ct_bytes, 0, true).fits &&
+         wilson_gauge_plan(g, nt, nc, ct_bytes, 0, false).fits;
 }
 
 double wilson_gauge_tolerance(int ct_bytes) { return ct_bytes == 8 ? 1e-14 : 1e-6; }

@@ -70,6 +70,10 @@ def test_both_methods_match_reference_fixture(name, meta):
     # range that is not a multiple of five
     (2, (4, 5, 3, 32), 0.3, 2, (2, 3, 4, 7)),
     (2, (6, 5, 7, 48), 0.3, 1, (1, 3, 3, 24)),
+    # long time extents: SU(2) beyond the one-column kernel's 32 threads per
+    # column (the two-column kernel), SU(3) at 32 threads per column
+    (2, (2, 3, 2, 192), 0.3, 1, (1, 1, 20, 24)),
+    (3, (2, 2, 2, 128), 0.25, 1, (1, 2, 1, 4)),
 ])
 def test_gauge_form_matches_oracle_seeded(port, nc, dims, eps, n_ape, rng):
     links = generate_config(dims, nc, eps, 20261203, 11)
