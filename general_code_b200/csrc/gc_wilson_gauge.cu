@@ -652,14 +652,15 @@ template <> struct QuatSet<double> {
 };
 
 // The fundamental SU(2) loops with one column per thread and KS consecutive
-// start slices of one cut whose space lines stay in registers (as wilson_gauge_reg_kernel for SU(3)). A quaternion loop is a
-// 4-term dot product, so in the two-column kernel a step of the trace sweep
-// spent more instructions on its shared-memory loads, bounds checks, rolling
-// sums and index updates than on the loops themselves (0.87 instructions per
-// cycle per scheduler, issue-bound). Here the sweep runs over T: each step
-// loads one line into a register window and adds the KS loops of that T,
-// with no checks and no moves. Per-thread sums in the compute type (FP32 for
-// the mixed form), block and grid sums in FP64.
+// start slices of one cut whose space lines stay in registers (as
+// wilson_gauge_reg_kernel for SU(3)). A quaternion loop is a 4-term dot
+// product, so in the two-column kernel a step of the trace sweep spent more
+// instructions on its shared-memory loads, bounds checks, rolling sums and
+// index updates than on the loops themselves (0.87 instructions per cycle per
+// scheduler, issue-bound). Here the sweep runs over T: each step loads one
+// line into a register window and adds the KS loops of that T, with no checks
+// and no moves. Per-thread sums in the compute type (FP32 for the mixed
+// form), block and grid sums in FP64.
 template <class Store, class CT, int KS>
 __global__ void __launch_bounds__(256)
     wilson_gauge_q_kernel(const __grid_constant__ Geom g, const __grid_constant__ Fields4 UA,
