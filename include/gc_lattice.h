@@ -183,7 +183,8 @@ int gc_set_hyp_method(gc_lattice *h, int method);
  * (checked on the device for every call: defect max |U U^dag - 1| at most
  * 1e-14 in FP64, 1e-6 in the mixed form), the same loops in the temporal
  * gauge (one trace per loop instead of two matrix products); see
- * gc_set_wilson_method.
+ * gc_set_wilson_method. A block keeps one column's lines of all Lt slices in
+ * shared memory: GC_ERR_ARG when they do not fit (SU(3): Lt > 246).
  * Replaces: wilson_loop(conf, r_min, r_max, time_min, time_max)
  * (wilson_loops.h:1047-1074) and the legacy vector overload
  * (basic_observables.h:108-111). */
