@@ -620,6 +620,7 @@ def run_tslab(args, wl, rank, world, dist):
     events on the current stream, max over ranks. The mixed form."""
     import torch
     from general_code_b200 import generate_config, link_size
+    from general_code_b200.lattice import HYP_LAUNCHES_PER_STEP, WILSON_LAUNCHES
     from general_code_b200.tslab import TSlabJob
 
     nc, dims = wl["nc"], wl["dims"]
@@ -670,6 +671,7 @@ def run_tslab(args, wl, rank, world, dist):
         barrier()
         slab = job.plan.bounds[rank][1]
         runs = job.plan.upload_runs(rank)
+        w_method = job.meas.wilson_method_used() or "exact"
     h2d = sum(k for _, _, k in runs) * 4 * (V // dims[3]) * link_size(nc) * 8
     assert np.array_equal(w, w_e2e), "resident and end-to-end runs disagree"
     ms, ms_e2e = max_over_ranks(ms), max_over_ranks(ms_e2e)
@@ -686,9 +688,11 @@ def run_tslab(args, wl, rank, world, dist):
                        "parallelism": f"tslab x{world}"},
             "e2e": {"value": V * args.steps / (ms_e2e * 1e-3), "unit": "sites/s",
                     "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": int(w.nbytes)},
-            # per step: HYP 3 + APE n + W 2 kernels; e2e adds a layout conversion
-            # per uploaded run of slices
-            "gpu_launches": args.steps * (2 * (3 + wl["ape"] + 2) + len(runs)),
+            # per step: HYP 3 + APE n + W kernels (of the method the slab took);
+            # e2e adds a layout conversion per uploaded run of slices
+            "gpu_launches": args.steps * (2 * (HYP_LAUNCHES_PER_STEP + wl["ape"]
+                                               + WILSON_LAUNCHES[w_method]) + len(runs)),
+            "w_method": w_method,
             "roofline": None,
             "note": "the headline run (--decomp replicas) carries the roofline and CPU baseline"}),
             flush=True)

@@ -797,13 +797,14 @@ static int wilson_impl(gc_lattice *h, int rmin, int rmax, int tmin, int tmax,
     return rc;
   double *chunk_out = h->dev_out + (size_t)nr * nt;
   // The temporal-gauge form (gc_wilson_gauge.cu) for one configuration's
-  // on-axis or adjoint loops with T <= Lt/2 (the t-slab entry, whose slabs'
-  // loops partition the lattice's, keeps the exact product); it runs only
-  // where the device finds the temporal links unitary to the form's
-  // tolerance, and the exact recursion otherwise.
+  // on-axis or adjoint loops with T <= Lt/2, or, for the t-slab entry's start
+  // slices [0, t_starts), with T <= Lt - t_starts (one cut at slice 0: no
+  // counted loop passes the slab lattice's last slice); it runs only where
+  // the device finds the temporal links unitary to the form's tolerance, and
+  // the exact recursion otherwise.
   const int ct_bytes = h->prec == GC_PREC_FP64 ? 8 : 4;
-  bool gauge = h->wilson_method == GC_WILSON_AUTO && !second && tstarts <= 0 &&
-               wilson_gauge_applies(h->g, tmax, nt, h->nc, ct_bytes);
+  bool gauge = h->wilson_method == GC_WILSON_AUTO && !second &&
+               wilson_gauge_applies(h->g, tmax, nt, h->nc, ct_bytes, tstarts);
   Fields4 UA{}, UB{};
   if (gauge) {
     rc = gauge_prepare(h, &UA, &UB, &gauge);
@@ -822,7 +823,7 @@ static int wilson_impl(gc_lattice *h, int rmin, int rmax, int tmin, int tmax,
     const int ncr = r1 - r0 + 1;
     if (gauge)
       rc = GC_DISPATCH(h, launch_wilson_auto, h->g, h->cur, UA, UB, r0, r1, tmin, tmax,
-                       adjoint, h->flag_dev, h->partials, chunk_out, h->stream);
+                       adjoint, h->flag_dev, h->partials, chunk_out, h->stream, 0, tstarts);
     else
       rc = GC_DISPATCH(h, launch_wilson, h->g, h->cur, r0, r1, tmin, tmax,
                        h->partials, chunk_out, h->stream, adjoint, u2, tstarts);

@@ -162,7 +162,10 @@ int launch_wilson(const Geom &g, const Fields4 &U, int rmin, int rmax,
 // units: column units (threads per time row) per block; 0 = about 128 threads.
 WilsonPlan wilson_gauge_plan(const Geom &g, int nt, int nc, int ct_bytes, int units = 0,
                              bool adjoint = false);
-bool wilson_gauge_applies(const Geom &g, int tmax, int nt, int nc, int ct_bytes);
+// tstarts in (0, Lt): the start slices [0, tstarts) of a time slab, in one
+// cut (time_max <= Lt - tstarts); otherwise every start slice (T <= Lt/2).
+bool wilson_gauge_applies(const Geom &g, int tmax, int nt, int nc, int ct_bytes,
+                          int tstarts = 0);
 // Largest unitarity defect max |U U^dag - 1| of a temporal link for which the
 // form is used (FP64: ct_bytes 8; mixed: 4).
 double wilson_gauge_tolerance(int ct_bytes);
@@ -187,22 +190,27 @@ int launch_wilson_gauge(const Geom &g, const Fields4 &UA, const Fields4 &UB, int
 // round; the fixed-order reduction then sums the partials of the method that
 // ran. No host synchronisation (usable inside stream capture once each
 // kernel's shared-memory attribute has been set by an earlier launch).
-// partials: wilson_auto_partials_count doubles.
+// partials: wilson_auto_partials_count doubles. tstarts in (0, Lt): the
+// loops of the start slices [0, tstarts) only (a time slab's lattice of its
+// own slices and the ones above them), in one cut at slice 0; the caller
+// guarantees time_max <= Lt - tstarts (no loop passes the lattice's end).
 template <class Store, class CT>
 int launch_wilson_auto(const Geom &g, const Fields4 &U, const Fields4 &UA, const Fields4 &UB,
                        int rmin, int rmax, int tmin, int tmax, bool adjoint, const int *flag,
-                       double *partials, double *out_dev, cudaStream_t s, int units = 0);
+                       double *partials, double *out_dev, cudaStream_t s, int units = 0,
+                       int tstarts = 0);
 size_t wilson_auto_partials_count(const Geom &g, int nr, int nt, int nc, int units = 0);
 template <class Store, class CT>
 int time_wilson_gauge(const Geom &g, const Fields4 &UA, const Fields4 &UB, int rmin, int rmax,
                       int tmin, int tmax, int units, double *partials, cudaStream_t s,
                       float *ms);
 // The exact W kernel, gated on *gate != 0, without the reduction; *blocks
-// receives the number of blocks (rows of partials).
+// receives the number of blocks (rows of partials). tstarts as for
+// launch_wilson_auto (0: every start slice).
 template <class Store, class CT>
 int launch_wilson_exact_gated(const Geom &g, const Fields4 &U, int rmin, int rmax, int tmin,
                               int tmax, bool adjoint, const int *gate, double *partials,
-                              int *blocks, cudaStream_t s);
+                              int *blocks, cudaStream_t s, int tstarts = 0);
 
 // An explicit block shape (rows must divide Lt, at most 256 threads).
 WilsonPlan wilson_plan_shape(const Geom &g, int nr, int nt, int nc, int ct_bytes, int rows,

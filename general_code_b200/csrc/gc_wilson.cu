@@ -423,8 +423,10 @@ int launch_wilson_mode(const Geom &g, const Fields4 &U, const Fields4 &U2, int r
 template <class Store, class CT>
 int launch_wilson_exact_gated(const Geom &g, const Fields4 &U, int rmin, int rmax, int tmin,
                               int tmax, bool adjoint, const int *gate, double *partials,
-                              int *blocks, cudaStream_t s) {
+                              int *blocks, cudaStream_t s, int tstarts) {
   const int nr = rmax - rmin + 1, nt = tmax - tmin + 1;
+  if (tstarts <= 0 || tstarts > g.L[3])
+    tstarts = g.L[3];
   WilsonPlan p = wilson_plan(g, nr, nt, Store::NC, (int)sizeof(CT), 3);
   if (!p.fits || nr * nt > kWilsonMaxEntries)
     return plan_error("wilson_kernel: time extent or (R,T) range too large for "
@@ -435,13 +437,13 @@ int launch_wilson_exact_gated(const Geom &g, const Fields4 &U, int rmin, int rma
     if (rc)
       return rc;
     wilson_kernel<Store, CT, true, false><<<dim3(p.blocks / 3, 3), p.threads, p.smem, s>>>(
-        g, U, U, rmin, rmax, tmin, tmax, p.cols_per_block, p.rows, partials, g.L[3], gate);
+        g, U, U, rmin, rmax, tmin, tmax, p.cols_per_block, p.rows, partials, tstarts, gate);
   } else {
     rc = allow_large_smem(wilson_kernel<Store, CT, false, false>, p.smem);
     if (rc)
       return rc;
     wilson_kernel<Store, CT, false, false><<<dim3(p.blocks / 3, 3), p.threads, p.smem, s>>>(
-        g, U, U, rmin, rmax, tmin, tmax, p.cols_per_block, p.rows, partials, g.L[3], gate);
+        g, U, U, rmin, rmax, tmin, tmax, p.cols_per_block, p.rows, partials, tstarts, gate);
   }
   *blocks = p.blocks;
   return launch_check("wilson_kernel");
@@ -587,7 +589,7 @@ int launch_reduce_batch(const RJob *jobs, int njobs, int entries, cudaStream_t s
                                              double *, cudaStream_t);         \
   template int launch_wilson_exact_gated<STORE, CT>(                          \
       const Geom &, const Fields4 &, int, int, int, int, bool, const int *,   \
-      double *, int *, cudaStream_t);
+      double *, int *, cudaStream_t, int);
 
 GC_INSTANTIATE_W(StoreF64SU3, double)
 GC_INSTANTIATE_W(StoreF64SU2, double)

@@ -305,7 +305,7 @@ template <class Store, class CT, bool ADJ, int KS>
 __global__ void __launch_bounds__(256)
     wilson_gauge_kernel(const __grid_constant__ Geom g, const __grid_constant__ Fields4 UA,
                         const __grid_constant__ Fields4 UB, int rmin, int rmax, int tmin,
-                        int tmax, int cols, int rows, double *partials, const int *flag) {
+                        int tmax, int cols, int rows, double *partials, const int *flag, int split, int tstarts) {
   // the exact product runs instead when a temporal link failed the check
   if (flag && *flag != 0)
     return;
@@ -314,7 +314,7 @@ __global__ void __launch_bounds__(256)
   using LL = LaneLoad<Store, CT, LANES>;
   using M = typename LL::M;
   using CS = ColSet<M>;
-  const int Lt = g.L[3], h = Lt / 2;
+  const int Lt = g.L[3], h = split; // the first slice of cut B
   const int nt = tmax - tmin + 1;
   const int nthreads = blockDim.x;
   const int cs = wilson_col_stride(cols, LANES);
@@ -383,7 +383,7 @@ __global__ void __launch_bounds__(256)
         if (active) {
 #pragma unroll
           for (int m = 0; m < KS; m++)
-            if (j - m >= 0 && j - m < nt) // start t0 + m, T = tmin + j - m
+            if (j - m >= 0 && j - m < nt && t0 + m < tstarts) // start t0 + m, T = tmin + j - m
               acc[m] += gauge_trace<ADJ>(a[m], b, lane1);
         }
         if (j - (KS - 1) >= 0) // T index j - KS + 1 has all KS starts
@@ -425,7 +425,7 @@ __global__ void __launch_bounds__(256)
 #pragma unroll 1
         for (int T = 0; T < nt; T++) {
           const Acc v =
-              active ? gauge_trace<ADJ>(a, CS::load(set, nslots, tt * units + u), lane1) : Acc(0);
+              (active && t0 < tstarts) ? gauge_trace<ADJ>(a, CS::load(set, nslots, tt * units + u), lane1) : Acc(0);
           Acc *r = red + (size_t)T * nthreads + tid;
           *r = (k == 0) ? v : *r + v;
           tt = (tt + 1 == Lt) ? 0 : tt + 1;
@@ -499,11 +499,11 @@ template <int KS>
 __global__ void __launch_bounds__(256, 2)
     wilson_gauge_reg_kernel(const __grid_constant__ Geom g, const __grid_constant__ Fields4 UA,
                             const __grid_constant__ Fields4 UB, int rmin, int rmax, int tmin,
-                            int tmax, int cols, int rows, double *partials, const int *flag) {
+                            int tmax, int cols, int rows, double *partials, const int *flag, int split, int tstarts) {
   if (flag && *flag != 0)
     return;
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  const int Lt = g.L[3], h = Lt / 2;
+  const int Lt = g.L[3], h = split; // the first slice of cut B
   const int nt = tmax - tmin + 1;
   const int nthreads = blockDim.x;
   const int nslots = Lt * cols;
@@ -571,7 +571,7 @@ __global__ void __launch_bounds__(256, 2)
         if (active) {
 #pragma unroll
           for (int m = 0; m < KS; m++)
-            if (j - m >= 0 && j - m < nt) // start t0 + m, T = tmin + j - m
+            if (j - m >= 0 && j - m < nt && t0 + m < tstarts) // start t0 + m, T = tmin + j - m
               acc[m] += gauge_trace<false>(a[m], b, false);
         }
         if (j - (KS - 1) >= 0)
@@ -665,13 +665,13 @@ template <class Store, class CT, int KS>
 __global__ void __launch_bounds__(256)
     wilson_gauge_q_kernel(const __grid_constant__ Geom g, const __grid_constant__ Fields4 UA,
                           const __grid_constant__ Fields4 UB, int rmin, int rmax, int tmin,
-                          int tmax, int cols, int rows, double *partials, const int *flag) {
+                          int tmax, int cols, int rows, double *partials, const int *flag, int split, int tstarts) {
   if (flag && *flag != 0)
     return;
   using Q = SU2<CT>;
   using QS = QuatSet<CT>;
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  const int Lt = g.L[3], h = Lt / 2;
+  const int Lt = g.L[3], h = split; // the first slice of cut B
   const int nt = tmax - tmin + 1;
   const int nthreads = blockDim.x;
   const int nslots = Lt * cols;
@@ -753,7 +753,7 @@ __global__ void __launch_bounds__(256)
 #pragma unroll
             for (int m = 0; m < KS; m++) {
               const Q &b = w[(r + m) % W];
-              d[m] = dot4(a[m].a0, b.a0, a[m].a1, b.a1, a[m].a2, b.a2, a[m].a3, b.a3);
+              d[m] = t0 + m < tstarts ? dot4(a[m].a0, b.a0, a[m].a1, b.a1, a[m].a2, b.a2, a[m].a3, b.a3) : CT(0);
             }
 #pragma unroll
             for (int k = 1; k < KS; k *= 2)
@@ -906,8 +906,10 @@ WilsonPlan wilson_gauge_plan(const Geom &g, int nt, int nc, int ct_bytes, int un
   return p;
 }
 
-bool wilson_gauge_applies(const Geom &g, int tmax, int nt, int nc, int ct_bytes) {
-  if (tmax > g.L[3] / 2 || g.L[3] < 2)
+bool wilson_gauge_applies(const Geom &g, int tmax, int nt, int nc, int ct_bytes, int tstarts) {
+  const int Lt = g.L[3];
+  const bool slab = tstarts > 0 && tstarts < Lt;
+  if (Lt < 2 || tmax > (slab ? Lt - tstarts : Lt / 2))
     return false;
   // (the fundamental and the adjoint loops may take different kernels)
   return wilson_gauge_plan(g, nt, nc, ct_bytes, 0, true).fits &&
@@ -942,10 +944,19 @@ int launch_wilson_gauge_prep(const Geom &g, const Fields4 &U, void *GA, void *GB
 template <class Store, class CT>
 int launch_wilson_gauge_kernel(const Geom &g, const Fields4 &UA, const Fields4 &UB, int rmin,
                                int rmax, int tmin, int tmax, bool adjoint, const int *flag,
-                               double *partials, int *blocks, cudaStream_t s, int units = 0) {
+                               double *partials, int *blocks, cudaStream_t s, int units = 0,
+                               int tstarts = 0) {
   const int nr = rmax - rmin + 1, nt = tmax - tmin + 1;
-  if (tmax > g.L[3] / 2)
-    return plan_error("wilson_gauge_kernel: time_max above Lt/2");
+  // every start slice in two cuts (A at slice 0, B at Lt/2), or the start
+  // slices [0, tstarts) of a time slab in cut A alone
+  const int Lt = g.L[3];
+  const bool slab = tstarts > 0 && tstarts < Lt;
+  const int split = slab ? Lt : Lt / 2;
+  if (!slab)
+    tstarts = Lt;
+  if (tmax > (slab ? Lt - tstarts : Lt / 2))
+    return plan_error(slab ? "wilson_gauge_kernel: time_max above Lt - t_starts"
+                           : "wilson_gauge_kernel: time_max above Lt/2");
   const WilsonPlan p = wilson_gauge_plan(g, nt, Store::NC, (int)sizeof(CT), units, adjoint);
   cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
   cudaStreamIsCapturing(s, &cap);
@@ -957,7 +968,8 @@ int launch_wilson_gauge_kernel(const Geom &g, const Fields4 &UA, const Fields4 &
     if (r)
       return r;
     kernel<<<dim3(p.blocks / 3, 3), p.threads, p.smem, s>>>(
-        g, UA, UB, rmin, rmax, tmin, tmax, p.cols_per_block, p.rows, partials, flag);
+        g, UA, UB, rmin, rmax, tmin, tmax, p.cols_per_block, p.rows, partials, flag, split,
+        tstarts);
     return GC_OK;
   };
   int rc;
@@ -971,7 +983,8 @@ int launch_wilson_gauge_kernel(const Geom &g, const Fields4 &UA, const Fields4 &
       if (r)
         return r;
       wilson_gauge_q_kernel<Store, CT, KS><<<dim3(p.blocks / 3, 3), p.threads, p.smem, s>>>(
-          g, UA, UB, rmin, rmax, tmin, tmax, p.cols_per_block, p.rows, partials, flag);
+          g, UA, UB, rmin, rmax, tmin, tmax, p.cols_per_block, p.rows, partials, flag, split,
+        tstarts);
       *blocks = p.blocks;
       return launch_check("wilson_gauge_q_kernel");
     }
@@ -982,7 +995,8 @@ int launch_wilson_gauge_kernel(const Geom &g, const Fields4 &UA, const Fields4 &
       if (r)
         return r;
       wilson_gauge_reg_kernel<4><<<dim3(p.blocks / 3, 3), p.threads, p.smem, s>>>(
-          g, UA, UB, rmin, rmax, tmin, tmax, p.cols_per_block, p.rows, partials, flag);
+          g, UA, UB, rmin, rmax, tmin, tmax, p.cols_per_block, p.rows, partials, flag, split,
+        tstarts);
       *blocks = p.blocks;
       return launch_check("wilson_gauge_reg_kernel");
     }
@@ -1017,19 +1031,24 @@ int launch_wilson_gauge(const Geom &g, const Fields4 &UA, const Fields4 &UB, int
 template <class Store, class CT>
 int launch_wilson_auto(const Geom &g, const Fields4 &U, const Fields4 &UA, const Fields4 &UB,
                        int rmin, int rmax, int tmin, int tmax, bool adjoint, const int *flag,
-                       double *partials, double *out_dev, cudaStream_t s, int units) {
+                       double *partials, double *out_dev, cudaStream_t s, int units,
+                       int tstarts) {
+  if (tstarts <= 0 || tstarts > g.L[3])
+    tstarts = g.L[3];
   int b_exact = 0, b_gauge = 0;
   int rc = launch_wilson_exact_gated<Store, CT>(g, U, rmin, rmax, tmin, tmax, adjoint, flag,
-                                                partials, &b_exact, s);
+                                                partials, &b_exact, s, tstarts);
   if (rc)
     return rc;
   rc = launch_wilson_gauge_kernel<Store, CT>(g, UA, UB, rmin, rmax, tmin, tmax, adjoint, flag,
-                                             partials, &b_gauge, s, units);
+                                             partials, &b_gauge, s, units, tstarts);
   if (rc)
     return rc;
   const int nr = rmax - rmin + 1, nt = tmax - tmin + 1;
-  reduce_select_kernel<<<nr * nt, 256, 0, s>>>(partials, b_exact, b_gauge, flag, nr, nt,
-                                               wilson_scale(g.V, Store::NC, adjoint), out_dev);
+  // average over the loops counted: every site, or the tstarts slices
+  reduce_select_kernel<<<nr * nt, 256, 0, s>>>(
+      partials, b_exact, b_gauge, flag, nr, nt,
+      wilson_scale((long long)g.Vs * tstarts, Store::NC, adjoint), out_dev);
   return launch_check("reduce_select_kernel");
 }
 
@@ -1085,7 +1104,7 @@ int time_wilson_gauge(const Geom &g, const Fields4 &UA, const Fields4 &UB, int r
   template int launch_wilson_auto<STORE, CT>(const Geom &, const Fields4 &, const Fields4 &,  \
                                              const Fields4 &, int, int, int, int, bool,       \
                                              const int *, double *, double *, cudaStream_t,   \
-                                             int);                                            \
+                                             int, int);                                       \
   template int time_wilson_gauge<STORE, CT>(const Geom &, const Fields4 &, const Fields4 &,   \
                                             int, int, int, int, int, double *, cudaStream_t,  \
                                             float *);

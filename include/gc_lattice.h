@@ -149,7 +149,10 @@ int gc_copy_slices(gc_lattice *dst, int dst_t0, gc_lattice *src, int src_t0, int
  * halo of a t-slab, at least time_max slices deep so no loop wraps. The
  * global average over slabs is sum_slab W_slab * t_starts / Lt. Same output
  * layout as gc_wilson_onaxis. With t_starts = Lt it is gc_wilson_onaxis
- * (wilson_loops.h:1047-1074). */
+ * (wilson_loops.h:1047-1074). Methods as gc_wilson_onaxis: for
+ * time_max <= Lt - t_starts (no counted loop passes slice Lt - 1) the
+ * temporal gauge with one cut at slice 0 where the device finds the temporal
+ * links unitary, else the exact product. */
 int gc_wilson_onaxis_tslab(gc_lattice *h, int t_starts, int r_min, int r_max, int time_min,
                            int time_max, int adjoint, double *out);
 

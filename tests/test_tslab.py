@@ -235,7 +235,8 @@ def test_wilson_tslab_full_is_wilson_loop(nc):
     links = generate_config(dims, nc, 0.3 if nc == 2 else 0.25, 20261203, 6)
     for form in ("fp64", "mixed"):
         with Lattice(dims, nc, form) as lat:
-            # the t-slab entry computes the exact product of links
+            # the exact product of links on both entries (the temporal-gauge
+            # form of the t-slab entry: the next test)
             lat.set_wilson_method("exact")
             lat.upload(links)
             lat.ape(0.5, 2)
@@ -249,10 +250,42 @@ def test_wilson_tslab_full_is_wilson_loop(nc):
             total = np.zeros_like(w)
             for a, k in [(0, 3), (3, 2), (5, 3)]:
                 with Lattice(dims, nc, form) as moved:
+                    moved.set_wilson_method("exact")
                     moved.upload(_global_rows(links, dims, nc, a, dims[3]))
                     moved.ape(0.5, 2)
                     total += moved.wilson_loop_tslab(k, 1, 3, 1, 4) * k
             np.testing.assert_allclose(total / dims[3], w, rtol=1e-12, atol=1e-15)
+
+
+# A slab's W in the temporal gauge against the exact product of the whole
+# lattice: FP64 to rounding, mixed within the mixed form's tolerance.
+_SLAB_RTOL = {"fp64": 1e-12, "mixed": 1e-6}
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("nc", [2, 3])
+@pytest.mark.parametrize("form", ["fp64", "mixed"])
+def test_wilson_tslab_partition_in_the_temporal_gauge(nc, form):
+    """The t-slab entry's loops of the start slices [0, t_starts), in the
+    temporal gauge with one cut at slice 0 (no counted loop passes the
+    lattice's last slice): a partition of the start slices of translated
+    lattices adds up to the whole lattice's table."""
+    from general_code_b200 import Lattice
+    dims = (6, 6, 6, 8)
+    links = generate_config(dims, nc, 0.3 if nc == 2 else 0.25, 20261203, 6)
+    with Lattice(dims, nc, form) as lat:
+        lat.upload(links)
+        lat.ape(0.5, 2)
+        w = lat.wilson_loop(1, 3, 1, 4)
+        assert lat.wilson_method_used() == "gauge"
+    total = np.zeros_like(w)
+    for a, k in [(0, 3), (3, 2), (5, 3)]:
+        with Lattice(dims, nc, form) as moved:
+            moved.upload(_global_rows(links, dims, nc, a, dims[3]))
+            moved.ape(0.5, 2)
+            total += moved.wilson_loop_tslab(k, 1, 3, 1, 4) * k
+            assert moved.wilson_method_used() == "gauge"
+    np.testing.assert_allclose(total / dims[3], w, rtol=_SLAB_RTOL[form], atol=1e-15)
 
 
 @pytest.mark.gpu
@@ -277,7 +310,9 @@ def test_emulated_slabs_match_one_lattice(nc, dims, slabs, t_max, form):
         ref = lat.wilson_loop(1, 3, 1, t_max)
     w = emulate(links, dims, nc, slabs, precision=form, hyp=hyp, hyp_steps=1, ape_alpha=0.5,
                 ape_steps=ape, r_min=1, r_max=3, time_min=1, time_max=t_max)
-    np.testing.assert_allclose(w, ref, rtol=1e-12, atol=1e-15)
+    # (the slabs take the temporal-gauge form: the exact product's table to
+    # FP64 rounding, within the mixed form's 1e-6 of it in FP32)
+    np.testing.assert_allclose(w, ref, rtol=_SLAB_RTOL[form], atol=1e-15)
 
 
 @pytest.mark.gpu
@@ -321,4 +356,4 @@ def test_tslab_job_reuses_its_lattices(form):
         b = job.run()
         c = job.run(links)
     assert np.array_equal(a, b) and np.array_equal(a, c)
-    np.testing.assert_allclose(a, ref, rtol=1e-12, atol=1e-15)
+    np.testing.assert_allclose(a, ref, rtol=_SLAB_RTOL[form], atol=1e-15)
