@@ -301,7 +301,7 @@ __device__ __forceinline__ int column_base(const Geom &g, int cb, int cols, int 
 // (T = t - t0 - m): nt + KS - 1 loads for KS nt loops, the sums of the last
 // KS values of T kept in registers. KS = 1: a thread owns the slices
 // row + k rows and loads one line per loop.
-template <class Store, class CT, bool ADJ, int KS>
+template <class Store, class CT, bool ADJ, int KS, bool SLAB>
 __global__ void __launch_bounds__(256)
     wilson_gauge_kernel(const __grid_constant__ Geom g, const __grid_constant__ Fields4 UA,
                         const __grid_constant__ Fields4 UB, int rmin, int rmax, int tmin,
@@ -383,7 +383,7 @@ __global__ void __launch_bounds__(256)
         if (active) {
 #pragma unroll
           for (int m = 0; m < KS; m++)
-            if (j - m >= 0 && j - m < nt && t0 + m < tstarts) // start t0 + m, T = tmin + j - m
+            if (j - m >= 0 && j - m < nt && (!SLAB || t0 + m < tstarts)) // T = tmin + j - m
               acc[m] += gauge_trace<ADJ>(a[m], b, lane1);
         }
         if (j - (KS - 1) >= 0) // T index j - KS + 1 has all KS starts
@@ -425,7 +425,7 @@ __global__ void __launch_bounds__(256)
 #pragma unroll 1
         for (int T = 0; T < nt; T++) {
           const Acc v =
-              (active && t0 < tstarts) ? gauge_trace<ADJ>(a, CS::load(set, nslots, tt * units + u), lane1) : Acc(0);
+              (active && (!SLAB || t0 < tstarts)) ? gauge_trace<ADJ>(a, CS::load(set, nslots, tt * units + u), lane1) : Acc(0);
           Acc *r = red + (size_t)T * nthreads + tid;
           *r = (k == 0) ? v : *r + v;
           tt = (tt + 1 == Lt) ? 0 : tt + 1;
@@ -495,7 +495,7 @@ struct Rows01Set {
 // ms at 175 registers (8 warps) and 3.01 ms for the two-column kernel.
 // Partials, block sums and the per-thread FP32 loop sums as
 // wilson_gauge_kernel.
-template <int KS>
+template <int KS, bool SLAB>
 __global__ void __launch_bounds__(256, 2)
     wilson_gauge_reg_kernel(const __grid_constant__ Geom g, const __grid_constant__ Fields4 UA,
                             const __grid_constant__ Fields4 UB, int rmin, int rmax, int tmin,
@@ -571,7 +571,7 @@ __global__ void __launch_bounds__(256, 2)
         if (active) {
 #pragma unroll
           for (int m = 0; m < KS; m++)
-            if (j - m >= 0 && j - m < nt && t0 + m < tstarts) // start t0 + m, T = tmin + j - m
+            if (j - m >= 0 && j - m < nt && (!SLAB || t0 + m < tstarts)) // T = tmin + j - m
               acc[m] += gauge_trace<false>(a[m], b, false);
         }
         if (j - (KS - 1) >= 0)
@@ -661,7 +661,7 @@ template <> struct QuatSet<double> {
 // line into a register window and adds the KS loops of that T, with no checks
 // and no moves. Per-thread sums in the compute type (FP32 for the mixed
 // form), block and grid sums in FP64.
-template <class Store, class CT, int KS>
+template <class Store, class CT, int KS, bool SLAB>
 __global__ void __launch_bounds__(256)
     wilson_gauge_q_kernel(const __grid_constant__ Geom g, const __grid_constant__ Fields4 UA,
                           const __grid_constant__ Fields4 UB, int rmin, int rmax, int tmin,
@@ -753,7 +753,7 @@ __global__ void __launch_bounds__(256)
 #pragma unroll
             for (int m = 0; m < KS; m++) {
               const Q &b = w[(r + m) % W];
-              d[m] = t0 + m < tstarts ? dot4(a[m].a0, b.a0, a[m].a1, b.a1, a[m].a2, b.a2, a[m].a3, b.a3) : CT(0);
+              d[m] = (!SLAB || t0 + m < tstarts) ? dot4(a[m].a0, b.a0, a[m].a1, b.a1, a[m].a2, b.a2, a[m].a3, b.a3) : CT(0);
             }
 #pragma unroll
             for (int k = 1; k < KS; k *= 2)
@@ -979,36 +979,39 @@ int launch_wilson_gauge_kernel(const Geom &g, const Fields4 &UA, const Fields4 &
   if constexpr (Store::NC == 2) {
     if (p.kernel == 2) {
       constexpr int KS = gauge_q_starts((int)sizeof(CT));
-      int r = allow_large_smem(wilson_gauge_q_kernel<Store, CT, KS>, p.smem, capturing);
-      if (r)
-        return r;
-      wilson_gauge_q_kernel<Store, CT, KS><<<dim3(p.blocks / 3, 3), p.threads, p.smem, s>>>(
-          g, UA, UB, rmin, rmax, tmin, tmax, p.cols_per_block, p.rows, partials, flag, split,
-        tstarts);
+      rc = slab ? go(wilson_gauge_q_kernel<Store, CT, KS, true>)
+                : go(wilson_gauge_q_kernel<Store, CT, KS, false>);
+      if (rc)
+        return rc;
       *blocks = p.blocks;
       return launch_check("wilson_gauge_q_kernel");
     }
   }
   if constexpr (std::is_same<Store, StoreF32SU3>::value) {
     if (p.kernel == 1) {
-      int r = allow_large_smem(wilson_gauge_reg_kernel<4>, p.smem, capturing);
-      if (r)
-        return r;
-      wilson_gauge_reg_kernel<4><<<dim3(p.blocks / 3, 3), p.threads, p.smem, s>>>(
-          g, UA, UB, rmin, rmax, tmin, tmax, p.cols_per_block, p.rows, partials, flag, split,
-        tstarts);
+      rc = slab ? go(wilson_gauge_reg_kernel<4, true>) : go(wilson_gauge_reg_kernel<4, false>);
+      if (rc)
+        return rc;
       *blocks = p.blocks;
       return launch_check("wilson_gauge_reg_kernel");
     }
   }
+  // (the start-slice checks of a t-slab compiled in only where they are used)
+  auto go2 = [&](auto k_all, auto k_slab) { return slab ? go(k_slab) : go(k_all); };
   if (adjoint)
-    rc = p.starts == 4   ? go(wilson_gauge_kernel<Store, CT, true, K4>)
-         : p.starts == 2 ? go(wilson_gauge_kernel<Store, CT, true, 2>)
-                         : go(wilson_gauge_kernel<Store, CT, true, 1>);
+    rc = p.starts == 4   ? go2(wilson_gauge_kernel<Store, CT, true, K4, false>,
+                               wilson_gauge_kernel<Store, CT, true, K4, true>)
+         : p.starts == 2 ? go2(wilson_gauge_kernel<Store, CT, true, 2, false>,
+                               wilson_gauge_kernel<Store, CT, true, 2, true>)
+                         : go2(wilson_gauge_kernel<Store, CT, true, 1, false>,
+                               wilson_gauge_kernel<Store, CT, true, 1, true>);
   else
-    rc = p.starts == 4   ? go(wilson_gauge_kernel<Store, CT, false, K4>)
-         : p.starts == 2 ? go(wilson_gauge_kernel<Store, CT, false, 2>)
-                         : go(wilson_gauge_kernel<Store, CT, false, 1>);
+    rc = p.starts == 4   ? go2(wilson_gauge_kernel<Store, CT, false, K4, false>,
+                               wilson_gauge_kernel<Store, CT, false, K4, true>)
+         : p.starts == 2 ? go2(wilson_gauge_kernel<Store, CT, false, 2, false>,
+                               wilson_gauge_kernel<Store, CT, false, 2, true>)
+                         : go2(wilson_gauge_kernel<Store, CT, false, 1, false>,
+                               wilson_gauge_kernel<Store, CT, false, 1, true>);
   if (rc)
     return rc;
   *blocks = p.blocks;
