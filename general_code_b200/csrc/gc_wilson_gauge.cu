@@ -301,6 +301,10 @@ __device__ __forceinline__ int column_base(const Geom &g, int cb, int cols, int 
 // (T = t - t0 - m): nt + KS - 1 loads for KS nt loops, the sums of the last
 // KS values of T kept in registers. KS = 1: a thread owns the slices
 // row + k rows and loads one line per loop.
+// split = h is the first start slice of cut B: Lt/2, or Lt for a time slab,
+// whose counted starts [0, tstarts) all take cut A. SLAB (the same in the
+// one-column kernels below) compiles in the check that a start is counted;
+// the whole-lattice kernels count every start.
 template <class Store, class CT, bool ADJ, int KS, bool SLAB>
 __global__ void __launch_bounds__(256)
     wilson_gauge_kernel(const __grid_constant__ Geom g, const __grid_constant__ Fields4 UA,
